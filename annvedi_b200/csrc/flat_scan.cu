@@ -1,0 +1,365 @@
+// Exact FP32 brute-force scan with fused top-k: the B200 form of the reference's linear scan
+// (LinearIndex::query, competitors/linear/src/linear_index.cpp:90-121, distance kernel
+// competitors/linear/src/simd.h:32-115) in its exact semantics: the true top-k by
+// (squared L2 distance, id), or by (-inner product, id).
+//
+// Layout: base rows [n, dpad] FP32 in HBM, dpad = dim rounded up to 32 floats with zero padding
+// (zeros add nothing to either metric). Grid = (query tiles of BQ) x (row splits). Each CTA
+// streams its split's rows through a cp.async shared-memory pipeline in KC=32-float chunks,
+// keeps its BQ queries' chunks beside them, and computes a BQ x BR distance tile per thread
+// micro-tile (TQ queries x TR rows, direct sum of (x - q)^2). After each row tile, distances that
+// beat a query's current k-th best are appended to that query's shared-memory buffer, which one
+// warp sorts and truncates to k when it fills. Each CTA writes its split's top-k; a merge kernel
+// reduces the splits to the final top-k per query.
+//
+// Roofline: one pass over the base per query tile: N*dpad*4 bytes, 2*N*dpad FP32 instructions
+// per query (sub + fma for L2; 1 fma for IP). HBM-bound below ~11 queries per tile, FP32-bound
+// above.
+#include "common.cuh"
+#include "flat_scan.cuh"
+
+namespace annb {
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int sz = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// One warp sorts a query's shared-memory buffer (`*count` entries, at most cap) and keeps the
+// best k, updating the bar (tau, tau_id) once k entries are held.
+__device__ __forceinline__ void smem_compact(float* key, int* id, int* count, float* tau, int* tau_id, int cap, int k) {
+    const int kept = warp_compact_smem(key, id, *count, cap, k);
+    if ((threadIdx.x & 31) == 0) {
+        *count = kept;
+        if (kept == k) {
+            *tau = key[k - 1];
+            *tau_id = id[k - 1];
+        }
+    }
+    __syncwarp();
+}
+
+template <int BQ, int TQ, int TR, int STAGES, int METRIC>
+struct ScanCfg {
+    static constexpr int THREADS = 256;
+    static constexpr int WQ = BQ / TQ;
+    static constexpr int WR = THREADS / WQ;
+    static constexpr int BR = WR * TR;
+    static constexpr int KC = 32;
+    static constexpr int PITCH = KC + 4;  // floats; 16-byte pad keeps 128-bit row reads conflict-free
+    static constexpr size_t SX = (size_t)BR * PITCH;  // floats per stage
+    static constexpr size_t SQ = (size_t)BQ * PITCH;
+    static constexpr size_t PIPE = sizeof(float) * STAGES * (SX + SQ);
+    static size_t smem(int cap) { return PIPE + (size_t)BQ * cap * 8 + (size_t)BQ * 16; }
+    static_assert(WR >= 32, "a warp must share one query group so query reads broadcast");
+    static_assert(BQ % TQ == 0 && THREADS % WQ == 0, "bad tile");
+};
+
+template <int BQ, int TQ, int TR, int STAGES, int METRIC>
+__global__ void __launch_bounds__(256) flat_scan_kernel(FlatScanArgs a) {
+    using C = ScanCfg<BQ, TQ, TR, STAGES, METRIC>;
+    const int cap = a.cap;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* sX = reinterpret_cast<float*>(smem_raw);
+    float* sQ = sX + STAGES * C::SX;
+    float* sKey = sQ + STAGES * C::SQ;
+    int* sId = reinterpret_cast<int*>(sKey + BQ * cap);
+    int* sCnt = sId + BQ * cap;
+    float* sTau = reinterpret_cast<float*>(sCnt + BQ);
+    int* sTauId = reinterpret_cast<int*>(sTau + BQ);
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int tq = tid / C::WR;
+    const int tr = tid % C::WR;
+    const int q0 = blockIdx.x * BQ;
+    const int split = blockIdx.y;
+    const int64_t row_begin = (int64_t)split * a.rows_per_split;
+    int64_t row_end = row_begin + a.rows_per_split;
+    if (row_end > a.n) row_end = a.n;
+    const int k = a.k;
+
+    for (int i = tid; i < BQ; i += C::THREADS) {
+        sCnt[i] = 0;
+        sTau[i] = kInf;
+        sTauId[i] = kNoId;
+    }
+
+    const int nkc = a.dpad / C::KC;
+    const int64_t ntiles = row_end > row_begin ? ceil_div(row_end - row_begin, C::BR) : 0;
+    const int64_t nsteps = ntiles * nkc;
+
+    auto issue = [&](int64_t step) {
+        if (step < nsteps) {
+            const int buf = (int)(step % STAGES);
+            const int64_t t = step / nkc;
+            const int kc = (int)(step % nkc);
+            const int64_t r0 = row_begin + t * C::BR;
+            float* dx = sX + buf * C::SX;
+            // BR rows x 8 16-byte pieces
+#pragma unroll
+            for (int c = tid; c < C::BR * 8; c += C::THREADS) {
+                const int r = c >> 3, piece = c & 7;
+                const int64_t row = r0 + r;
+                const bool ok = row < row_end;
+                const float* src = a.base + (ok ? row : row_begin) * (int64_t)a.dpad + kc * C::KC + piece * 4;
+                cp_async16(dx + r * C::PITCH + piece * 4, src, ok);
+            }
+            float* dq = sQ + buf * C::SQ;
+            for (int c = tid; c < BQ * 8; c += C::THREADS) {
+                const int qq = c >> 3, piece = c & 7;
+                const bool ok = (q0 + qq) < a.nq;
+                const float* src = a.q + (int64_t)(ok ? q0 + qq : 0) * a.dpad + kc * C::KC + piece * 4;
+                cp_async16(dq + qq * C::PITCH + piece * 4, src, ok);
+            }
+        }
+        cp_async_commit();
+    };
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) issue(s);
+
+    float acc[TQ][TR];
+#pragma unroll
+    for (int j = 0; j < TQ; ++j)
+#pragma unroll
+        for (int i = 0; i < TR; ++i) acc[j][i] = 0.f;
+
+    for (int64_t step = 0; step < nsteps; ++step) {
+        cp_async_wait<STAGES - 2>();
+        __syncthreads();
+        issue(step + STAGES - 1);
+        const int buf = (int)(step % STAGES);
+        const float* xs = sX + buf * C::SX;
+        const float* qs = sQ + buf * C::SQ;
+#pragma unroll
+        for (int kk = 0; kk < C::KC; kk += 4) {
+            float4 xv[TR], qv[TQ];
+#pragma unroll
+            for (int i = 0; i < TR; ++i) xv[i] = *reinterpret_cast<const float4*>(xs + (tr + i * C::WR) * C::PITCH + kk);
+#pragma unroll
+            for (int j = 0; j < TQ; ++j) qv[j] = *reinterpret_cast<const float4*>(qs + (tq * TQ + j) * C::PITCH + kk);
+#pragma unroll
+            for (int j = 0; j < TQ; ++j)
+#pragma unroll
+                for (int i = 0; i < TR; ++i) {
+                    if (METRIC == ANN_METRIC_L2) {
+                        float d0 = xv[i].x - qv[j].x, d1 = xv[i].y - qv[j].y;
+                        float d2 = xv[i].z - qv[j].z, d3 = xv[i].w - qv[j].w;
+                        acc[j][i] = fmaf(d0, d0, acc[j][i]);
+                        acc[j][i] = fmaf(d1, d1, acc[j][i]);
+                        acc[j][i] = fmaf(d2, d2, acc[j][i]);
+                        acc[j][i] = fmaf(d3, d3, acc[j][i]);
+                    } else {
+                        acc[j][i] = fmaf(xv[i].x, qv[j].x, acc[j][i]);
+                        acc[j][i] = fmaf(xv[i].y, qv[j].y, acc[j][i]);
+                        acc[j][i] = fmaf(xv[i].z, qv[j].z, acc[j][i]);
+                        acc[j][i] = fmaf(xv[i].w, qv[j].w, acc[j][i]);
+                    }
+                }
+        }
+
+        if ((int)(step % nkc) == nkc - 1) {
+            // ---- epilogue for row tile t: offer distances to the per-query buffers ----
+            const int64_t r0 = row_begin + (step / nkc) * C::BR;
+            uint32_t pend = 0;
+#pragma unroll
+            for (int j = 0; j < TQ; ++j)
+#pragma unroll
+                for (int i = 0; i < TR; ++i) {
+                    const int64_t row = r0 + tr + i * C::WR;
+                    if (row < row_end && q0 + tq * TQ + j < a.nq) pend |= 1u << (j * TR + i);
+                }
+            while (true) {
+#pragma unroll
+                for (int j = 0; j < TQ; ++j) {
+                    const int ql = tq * TQ + j;
+#pragma unroll
+                    for (int i = 0; i < TR; ++i) {
+                        const uint32_t bit = 1u << (j * TR + i);
+                        if (pend & bit) {
+                            const int row = (int)(r0 + tr + i * C::WR);
+                            const float key = METRIC == ANN_METRIC_L2 ? acc[j][i] : -acc[j][i];
+                            if (pair_less(key, row, sTau[ql], sTauId[ql])) {
+                                const int slot = atomicAdd(&sCnt[ql], 1);
+                                if (slot < cap) {
+                                    sKey[ql * cap + slot] = key;
+                                    sId[ql * cap + slot] = row;
+                                    pend &= ~bit;
+                                }
+                            } else {
+                                pend &= ~bit;
+                            }
+                        }
+                    }
+                }
+                const int overflow = __syncthreads_or(pend != 0);
+                for (int ql = warp; ql < BQ; ql += C::THREADS / 32) {
+                    if (sCnt[ql] >= cap / 2)
+                        smem_compact(sKey + ql * cap, sId + ql * cap, &sCnt[ql], &sTau[ql], &sTauId[ql], cap, k);
+                }
+                __syncthreads();
+                if (!overflow) break;
+            }
+#pragma unroll
+            for (int j = 0; j < TQ; ++j)
+#pragma unroll
+                for (int i = 0; i < TR; ++i) acc[j][i] = 0.f;
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+
+    // ---- final: each query's split top-k, sorted, padded with (+inf, INT_MAX) ----
+    for (int ql = warp; ql < BQ; ql += C::THREADS / 32) {
+        const int qi = q0 + ql;
+        if (qi >= a.nq) continue;
+        smem_compact(sKey + ql * cap, sId + ql * cap, &sCnt[ql], &sTau[ql], &sTauId[ql], cap, k);
+        const int cnt = sCnt[ql];
+        float* ok = a.out_key + ((int64_t)qi * a.nsplit + split) * k;
+        int* oi = a.out_id + ((int64_t)qi * a.nsplit + split) * k;
+        for (int e = threadIdx.x & 31; e < k; e += 32) {
+            ok[e] = e < cnt ? sKey[ql * cap + e] : kInf;
+            oi[e] = e < cnt ? sId[ql * cap + e] : kNoId;
+        }
+    }
+}
+
+// Merge kernel: one CTA (8 warps) per query reduces nsplit sorted lists of kin pairs to the
+// final top-k. Each warp keeps a private top-k over a strided share of the lists; warp 0 then
+// merges the eight.
+__global__ void __launch_bounds__(256) merge_splits_kernel(MergeArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int cap = topk_cap(a.k);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float* sKey = reinterpret_cast<float*>(smem_raw);
+    int* sId = reinterpret_cast<int*>(sKey + 8 * cap);
+    const int qi = blockIdx.x;
+    const int k = a.k;
+    WarpTopK top;
+    top.init(sKey + warp * cap, sId + warp * cap, k);
+    const int64_t total = (int64_t)a.nsplit * a.kin;
+    const float* ik = a.in_key + (int64_t)qi * total;
+    const int* ii = a.in_id + (int64_t)qi * total;
+    for (int64_t base = (int64_t)warp * 32; base < total; base += 8 * 32) {
+        const int64_t e = base + lane;
+        float kv = kInf;
+        int iv = kNoId;
+        if (e < total) {
+            kv = ik[e];
+            iv = ii[e];
+        }
+        top.offer(kv, iv, e < total && iv != kNoId);
+    }
+    top.compact();
+    __syncthreads();
+    if (warp == 0) {
+        for (int w = 1; w < 8; ++w) {
+            for (int e0 = 0; e0 < k; e0 += 32) {
+                const int e = e0 + lane;
+                const bool ok = e < k;
+                const float kv = ok ? sKey[w * cap + e] : kInf;
+                const int iv = ok ? sId[w * cap + e] : kNoId;
+                top.offer(kv, iv, ok && iv != kNoId);
+            }
+        }
+        top.compact();
+        const int cnt = top.count;
+        for (int e = lane; e < k; e += 32) {
+            const bool ok = e < cnt;
+            const float kv = ok ? sKey[e] : kInf;
+            const int iv = ok ? sId[e] : kNoId;
+            if (a.out_ids) a.out_ids[(int64_t)qi * k + e] = ok ? (int64_t)iv : -1;
+            if (a.out_dists) a.out_dists[(int64_t)qi * k + e] = ok ? (a.negate ? -kv : kv) : (a.negate ? -kInf : kInf);
+        }
+    }
+}
+
+// Copies rows [n, dim] (row stride ld floats) into [n, dpad] with zero padding.
+__global__ void pad_rows_kernel(const float* __restrict__ src, int64_t n, int dim, int64_t ld, float* __restrict__ dst,
+                                int dpad) {
+    const int64_t total = n * dpad;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = e / dpad;
+        const int c = (int)(e % dpad);
+        dst[e] = c < dim ? src[r * ld + c] : 0.f;
+    }
+}
+
+int launch_pad_rows(const float* src, int64_t n, int dim, int64_t ld, float* dst, int dpad, cudaStream_t st) {
+    if (n == 0) return ANN_OK;
+    const int64_t total = n * dpad;
+    int blocks = (int)std::min<int64_t>(ceil_div(total, 256), kNumSMs * 16);
+    pad_rows_kernel<<<blocks, 256, 0, st>>>(src, n, dim, ld, dst, dpad);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host-side launch selection.
+// ---------------------------------------------------------------------------------------------
+template <int BQ, int TQ, int TR, int STAGES, int METRIC>
+static int launch_scan_t(FlatScanArgs a, int n_qtiles, cudaStream_t st) {
+    using C = ScanCfg<BQ, TQ, TR, STAGES, METRIC>;
+    auto kern = flat_scan_kernel<BQ, TQ, TR, STAGES, METRIC>;
+    const size_t smem = C::smem(a.cap);
+    ANN_CHECK_ARG(smem <= 227 * 1024, "flat scan: %zu bytes of shared memory for k=%d", smem, a.k);
+    ANN_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid(n_qtiles, a.nsplit);
+    kern<<<grid, C::THREADS, smem, st>>>(a);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+// Largest query tile whose per-query top-k buffers still fit in shared memory.
+int flat_scan_max_bq(int k) { return k <= 128 ? 32 : (k <= 256 ? 16 : 8); }
+
+int flat_scan_bq(int nq) {
+    if (nq <= 1) return 1;
+    if (nq <= 2) return 2;
+    if (nq <= 4) return 4;
+    if (nq <= 8) return 8;
+    if (nq <= 64) return 16;
+    return 32;
+}
+
+template <int METRIC>
+static int dispatch_bq(const FlatScanArgs& a, int bq, int n_qtiles, cudaStream_t st) {
+    switch (bq) {
+    case 1: return launch_scan_t<1, 1, 1, 2, METRIC>(a, n_qtiles, st);
+    case 2: return launch_scan_t<2, 2, 1, 2, METRIC>(a, n_qtiles, st);
+    case 4: return launch_scan_t<4, 4, 1, 2, METRIC>(a, n_qtiles, st);
+    case 8: return launch_scan_t<8, 8, 1, 2, METRIC>(a, n_qtiles, st);
+    case 16: return launch_scan_t<16, 8, 2, 3, METRIC>(a, n_qtiles, st);
+    default: return launch_scan_t<32, 8, 4, 3, METRIC>(a, n_qtiles, st);
+    }
+}
+
+int launch_flat_scan(const FlatScanArgs& a0, int bq, cudaStream_t st) {
+    ANN_CHECK_ARG(a0.k >= 1 && a0.k <= 512, "flat scan: k=%d outside [1, 512]", a0.k);
+    ANN_CHECK_ARG(a0.dpad % 32 == 0, "flat scan: padded dim %d not a multiple of 32", a0.dpad);
+    FlatScanArgs a = a0;
+    a.cap = topk_cap(a.k);
+    if (bq > flat_scan_max_bq(a.k)) bq = flat_scan_max_bq(a.k);
+    const int n_qtiles = (int)ceil_div(a.nq, bq);
+    if (a.metric == ANN_METRIC_L2) return dispatch_bq<ANN_METRIC_L2>(a, bq, n_qtiles, st);
+    return dispatch_bq<ANN_METRIC_IP>(a, bq, n_qtiles, st);
+}
+
+int launch_merge_splits(const MergeArgs& a, cudaStream_t st) {
+    ANN_CHECK_ARG(a.k >= 1 && a.k <= 512, "merge: k=%d outside [1, 512]", a.k);
+    if (a.nq == 0) return ANN_OK;
+    const size_t smem = (size_t)8 * topk_cap(a.k) * 8;
+    ANN_CUDA_TRY(cudaFuncSetAttribute(merge_splits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    merge_splits_kernel<<<a.nq, 256, smem, st>>>(a);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+}  // namespace annb

@@ -1,0 +1,41 @@
+// Launch interfaces of the exact FP32 scan (flat_scan.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace annb {
+
+struct FlatScanArgs {
+    const float* base;       // [n, dpad] FP32, zero-padded rows
+    int64_t n;
+    int dpad;                // multiple of 32
+    const float* q;          // [nq, dpad] FP32, zero-padded
+    int nq;
+    int metric;              // ANN_METRIC_L2 / ANN_METRIC_IP
+    int k;                   // 1..512
+    int64_t rows_per_split;
+    int nsplit;
+    float* out_key;          // [nq, nsplit, k] scratch
+    int* out_id;             // [nq, nsplit, k] scratch
+    int cap;                 // per-query buffer capacity (set by launch_flat_scan)
+};
+
+struct MergeArgs {
+    const float* in_key;     // [nq, nsplit, kin] sorted per split, (+inf, INT_MAX) padded
+    const int* in_id;
+    int nq;
+    int nsplit;
+    int kin;
+    int k;
+    int negate;              // 1: output -key (inner-product scores)
+    int64_t* out_ids;        // [nq, k], -1 where fewer than k exist
+    float* out_dists;        // [nq, k] or nullptr
+};
+
+int flat_scan_bq(int nq);
+int flat_scan_max_bq(int k);
+int launch_flat_scan(const FlatScanArgs& a, int bq, cudaStream_t st);
+int launch_merge_splits(const MergeArgs& a, cudaStream_t st);
+int launch_pad_rows(const float* src, int64_t n, int dim, int64_t ld, float* dst, int dpad, cudaStream_t st);
+
+}  // namespace annb

@@ -1,0 +1,143 @@
+// Host runtime pieces shared by the C ABI entry points: device guard, workspaces (device scratch
+// arena + pinned host staging) and a bump allocator over them.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+struct ann_workspace {
+    int device = 0;
+    char* dev = nullptr;
+    size_t dev_cap = 0;
+    char* host = nullptr;  // pinned
+    size_t host_cap = 0;
+    std::mutex mu;         // serialises growth; concurrent calls must still use separate workspaces
+};
+
+namespace annb {
+
+// Makes `device` current for the scope and restores the previous device afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != device) ok = cudaSetDevice(device) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// Grows the workspace's device arena to at least `bytes` (drains the device first, since the old
+// block may be in use by earlier asynchronous work).
+int ws_reserve_device(ann_workspace* ws, size_t bytes);
+int ws_reserve_host(ann_workspace* ws, size_t bytes);
+
+// Stage timer: records CUDA events around named stages of a call on its stream; totals are
+// accumulated lazily (collect() synchronises on the recorded events).
+struct StageProfiler {
+    static constexpr int kStages = 4;
+    bool enabled = false;
+    struct Rec {
+        cudaEvent_t ev[kStages + 1];
+        int nstage;
+    };
+    std::vector<Rec> pending;
+    std::vector<cudaEvent_t> pool;
+    double total_ms[kStages] = {0, 0, 0, 0};
+    int64_t launches = 0;
+    int64_t calls = 0;
+    std::mutex mu;
+
+    cudaEvent_t get_event() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    // begin(): returns a record index; mark(rec, stage) after each stage
+    int begin(cudaStream_t st) {
+        if (!enabled) return -1;
+        std::lock_guard<std::mutex> lk(mu);
+        Rec r{};
+        r.nstage = 0;
+        r.ev[0] = get_event();
+        cudaEventRecord(r.ev[0], st);
+        pending.push_back(r);
+        return (int)pending.size() - 1;
+    }
+    void mark(int rec, cudaStream_t st) {
+        if (rec < 0) return;
+        std::lock_guard<std::mutex> lk(mu);
+        Rec& r = pending[rec];
+        if (r.nstage >= kStages) return;
+        r.ev[++r.nstage] = get_event();
+        cudaEventRecord(r.ev[r.nstage], st);
+    }
+    void collect() {
+        std::lock_guard<std::mutex> lk(mu);
+        for (Rec& r : pending) {
+            for (int s = 0; s < r.nstage; ++s) {
+                cudaEventSynchronize(r.ev[s + 1]);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, r.ev[s], r.ev[s + 1]);
+                total_ms[s] += ms;
+            }
+            for (int s = 0; s <= r.nstage; ++s) pool.push_back(r.ev[s]);
+            calls += 1;
+        }
+        pending.clear();
+    }
+    void reset() {
+        collect();
+        std::lock_guard<std::mutex> lk(mu);
+        for (double& t : total_ms) t = 0;
+        launches = 0;
+        calls = 0;
+    }
+    ~StageProfiler() {
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
+        for (Rec& r : pending)
+            for (int s = 0; s <= r.nstage; ++s) cudaEventDestroy(r.ev[s]);
+    }
+};
+
+// Carves aligned sub-buffers out of a base pointer.
+struct Carver {
+    char* base;
+    size_t off = 0;
+    explicit Carver(void* b) : base(static_cast<char*>(b)) {}
+    template <typename T>
+    T* take(size_t count, size_t align = 256) {
+        off = (off + align - 1) / align * align;
+        T* p = reinterpret_cast<T*>(base + off);
+        off += count * sizeof(T);
+        return p;
+    }
+    // bytes needed for the same sequence of takes when base is null
+};
+
+// Size calculator mirroring Carver.
+struct Sizer {
+    size_t off = 0;
+    template <typename T>
+    void take(size_t count, size_t align = 256) {
+        off = (off + align - 1) / align * align;
+        off += count * sizeof(T);
+    }
+    size_t bytes() const { return off + 256; }
+};
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace annb
