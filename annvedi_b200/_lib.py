@@ -77,6 +77,19 @@ SIGNATURES = [
     ("ann_flat_total_distances", _i64, [_vp]),
     ("ann_flat_dim", _i32, [_vp]),
     ("ann_flat_size", _i64, [_vp]),
+    ("ann_ivf_create", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int]),
+    ("ann_ivf_destroy", ctypes.c_int, [_vp]),
+    ("ann_ivf_fit", ctypes.c_int, [_vp, _vp, _i64, _i32, _i64, _i32, _vp, _vp, _i32, _i32, _vp]),
+    ("ann_ivf_import", ctypes.c_int, [_vp, _i64, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("ann_ivf_export", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("ann_ivf_info", ctypes.c_int, [_vp, ctypes.POINTER(_i64)]),
+    ("ann_ivf_query", ctypes.c_int, [_vp, _vp, _vp, _i32, _i64, _i32, _i32, _i32, _i32, _i64, _i32, _i32, _i32,
+                                     _vp, _vp, _vp]),
+    ("ann_ivf_total_distances", _i64, [_vp]),
+    ("ann_ivf_reset_distances", ctypes.c_int, [_vp]),
+    ("ann_ivf_set_profiling", ctypes.c_int, [_vp, _i32]),
+    ("ann_ivf_profile", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    ("ann_ivf_reset_profile", ctypes.c_int, [_vp]),
 ]
 
 

@@ -1,0 +1,662 @@
+// C ABI of the IVF-SQ8 index: the B200 form of ivf_lsh_cpp.LSHIndex
+// (competitors/ivf_lsh/src/lsh_index_optimized.cpp:124-667) for n_tables = 1, n_bits = 0.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+#include "flat_scan.cuh"
+#include "ivf.cuh"
+#include "refmath.cuh"
+#include "runtime.cuh"
+
+using namespace annb;
+
+struct ann_ivf {
+    int device = 0;
+    int64_t n = 0;
+    int dim = 0, dpad = 0, dpad8 = 0, C = 0;
+    float* centroids = nullptr;   // [C, dpad]
+    float* original = nullptr;    // [n, dpad]
+    uint8_t* codes = nullptr;     // [n, dpad8]
+    float* scale = nullptr;       // [dpad]
+    float* offset = nullptr;      // [dpad]
+    int32_t* r2o = nullptr;       // [n]
+    int64_t* list_off = nullptr;  // [C + 1]
+    unsigned long long* d_ndist = nullptr;
+    std::vector<int64_t> h_list_off;
+    std::vector<int64_t> sizes_desc;  // list sizes, largest first (bounds for planning)
+    ann_workspace ws;
+    StageProfiler prof;  // 0: coarse ranking, 1: plan, 2: SQ8 pass (+ merge), 3: re-rank
+    int64_t query_count = 0;
+
+    IvfView view() const {
+        IvfView v;
+        v.n = n;
+        v.dim = dim;
+        v.dpad = dpad;
+        v.dpad8 = dpad8;
+        v.C = C;
+        v.centroids = centroids;
+        v.original = original;
+        v.codes = codes;
+        v.scale = scale;
+        v.offset = offset;
+        v.r2o = r2o;
+        v.list_off = list_off;
+        return v;
+    }
+};
+
+static void ivf_free_state(ann_ivf* h) {
+    for (void* p : {(void*)h->centroids, (void*)h->original, (void*)h->codes, (void*)h->scale, (void*)h->offset,
+                    (void*)h->r2o, (void*)h->list_off})
+        if (p) cudaFree(p);
+    h->centroids = nullptr;
+    h->original = nullptr;
+    h->codes = nullptr;
+    h->scale = h->offset = nullptr;
+    h->r2o = nullptr;
+    h->list_off = nullptr;
+    h->n = 0;
+}
+
+template <typename T>
+static int dmalloc(T** p, size_t count) {
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * std::max<size_t>(count, 1));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        set_error("cannot allocate %zu bytes of device memory (%s)", sizeof(T) * count, cudaGetErrorString(e));
+        return ANN_ERR_NOMEM;
+    }
+    return ANN_OK;
+}
+
+// Host-side list bookkeeping after the device list offsets are final.
+static int ivf_finish_lists(ann_ivf* h, cudaStream_t st) {
+    h->h_list_off.resize(h->C + 1);
+    ANN_CUDA_TRY(cudaMemcpyAsync(h->h_list_off.data(), h->list_off, sizeof(int64_t) * (h->C + 1),
+                                 cudaMemcpyDeviceToHost, st));
+    ANN_CUDA_TRY(cudaStreamSynchronize(st));
+    h->sizes_desc.resize(h->C);
+    for (int c = 0; c < h->C; ++c) h->sizes_desc[c] = h->h_list_off[c + 1] - h->h_list_off[c];
+    std::sort(h->sizes_desc.begin(), h->sizes_desc.end(), std::greater<int64_t>());
+    if (!h->d_ndist) {
+        int rc = dmalloc(&h->d_ndist, 1);
+        if (rc) return rc;
+        ANN_CUDA_TRY(cudaMemsetAsync(h->d_ndist, 0, sizeof(unsigned long long), st));
+    }
+    return ANN_OK;
+}
+
+// Nearest centroid of every row (exact FP32 scan, k = 1): assign[i] in [0, C).
+static int assign_rows(const float* x, int64_t n, int dpad, const float* cent, int C, int32_t* assign,
+                       ann_workspace* ws, cudaStream_t st) {
+    const int bq = 32;
+    const int nq_chunk = 1 << 20;
+    for (int64_t r0 = 0; r0 < n; r0 += nq_chunk) {
+        const int nq = (int)std::min<int64_t>(nq_chunk, n - r0);
+        Sizer sz;
+        sz.take<float>((size_t)nq);
+        sz.take<int>((size_t)nq);
+        sz.take<int64_t>((size_t)nq);
+        int rc = ws_reserve_device(ws, sz.bytes());
+        if (rc) return rc;
+        Carver cv(ws->dev);
+        float* sk = cv.take<float>((size_t)nq);
+        int* si = cv.take<int>((size_t)nq);
+        FlatScanArgs a{cent, C, dpad, x + r0 * dpad, nq, ANN_METRIC_L2, 1, (int64_t)C, 1, sk, si};
+        rc = launch_flat_scan(a, bq, st);
+        if (rc) return rc;
+        MergeArgs m{sk, si, nq, 1, 1, 1, 0, nullptr, nullptr};
+        m.out_id32 = assign + r0;
+        rc = launch_merge_splits(m, st);
+        if (rc) return rc;
+    }
+    return ANN_OK;
+}
+
+extern "C" {
+
+int ann_ivf_create(ann_ivf** out, int device) {
+    clear_error();
+    ANN_CHECK_ARG(out != nullptr, "ann_ivf_create: out is NULL");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_error("no CUDA device visible (%s)", e == cudaSuccess ? "0 devices" : cudaGetErrorString(e));
+        return ANN_ERR_CUDA;
+    }
+    ANN_CHECK_ARG(device >= 0 && device < ndev, "ann_ivf_create: device %d not in [0, %d)", device, ndev);
+    ann_ivf* h = new (std::nothrow) ann_ivf();
+    if (!h) {
+        set_error("ann_ivf_create: out of host memory");
+        return ANN_ERR_NOMEM;
+    }
+    h->device = device;
+    h->ws.device = device;
+    *out = h;
+    return ANN_OK;
+}
+
+int ann_ivf_destroy(ann_ivf* h) {
+    if (!h) return ANN_OK;
+    {
+        DeviceGuard g(h->device);
+        ivf_free_state(h);
+        if (h->d_ndist) cudaFree(h->d_ndist);
+        if (h->ws.dev) cudaFree(h->ws.dev);
+        if (h->ws.host) cudaFreeHost(h->ws.host);
+        h->ws.dev = nullptr;
+        h->ws.host = nullptr;
+    }
+    delete h;
+    return ANN_OK;
+}
+
+int ann_ivf_fit(ann_ivf* h, const float* data, int64_t n, int32_t dim, int64_t ld, int32_t n_clusters,
+                const float* centroids, const int32_t* assign, int32_t kmeans_iters, int32_t mem, void* stream) {
+    clear_error();
+    ANN_CHECK_ARG(h != nullptr, "ann_ivf_fit: null index");
+    ANN_CHECK_ARG(n >= 1 && dim >= 1 && data, "ann_ivf_fit: need a non-empty 2-D array");
+    ANN_CHECK_ARG(n < INT32_MAX, "ann_ivf_fit: n=%lld exceeds 32-bit ids", (long long)n);
+    ANN_CHECK_ARG(ld >= dim, "ann_ivf_fit: row stride < dim");
+    ANN_CHECK_ARG(n_clusters >= 1, "ann_ivf_fit: n_clusters=%d < 1", n_clusters);
+    ANN_CHECK_ARG(kmeans_iters >= 0, "ann_ivf_fit: kmeans_iters < 0");
+    DeviceGuard g(h->device);
+    cudaStream_t st = as_stream(stream);
+    const int C = (int)std::min<int64_t>(n_clusters, n);  // the reference clamps too (:137)
+    const int dpad = (int)ceil_div(dim, 32) * 32;
+    const int dpad8 = (int)ceil_div(dim, 32) * 32;
+    ANN_CUDA_TRY(cudaDeviceSynchronize());
+    ivf_free_state(h);
+    const cudaMemcpyKind kind = mem == ANN_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+
+    float* X = nullptr;  // [n, dpad] input rows
+    int32_t* a_raw = nullptr;
+    int32_t* a_sorted = nullptr;
+    int32_t* idx = nullptr;
+    int32_t* order = nullptr;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+    float* mn = nullptr;
+    float* mx = nullptr;
+    float* fallback = nullptr;
+    int rc = ANN_OK;
+#define FIT_TRY(x)          \
+    do {                    \
+        rc = (x);           \
+        if (rc) goto fail;  \
+    } while (0)
+#define FIT_CUDA(x)                                                                                      \
+    do {                                                                                                 \
+        cudaError_t _e = (x);                                                                            \
+        if (_e != cudaSuccess) {                                                                         \
+            set_error("CUDA error %s at %s:%d", cudaGetErrorString(_e), __FILE__, __LINE__);             \
+            rc = ANN_ERR_CUDA;                                                                           \
+            goto fail;                                                                                   \
+        }                                                                                                \
+    } while (0)
+    {
+        FIT_TRY(dmalloc(&X, (size_t)n * dpad));
+        FIT_TRY(dmalloc(&h->centroids, (size_t)C * dpad));
+        FIT_TRY(dmalloc(&a_raw, n));
+        FIT_TRY(dmalloc(&a_sorted, n));
+        FIT_TRY(dmalloc(&idx, n));
+        FIT_TRY(dmalloc(&order, n));
+        FIT_TRY(dmalloc(&h->list_off, C + 1));
+        FIT_CUDA(cudaMemsetAsync(X, 0, sizeof(float) * (size_t)n * dpad, st));
+        FIT_CUDA(cudaMemcpy2DAsync(X, sizeof(float) * dpad, data, sizeof(float) * ld, sizeof(float) * dim, n, kind, st));
+        FIT_CUDA(cudaMemsetAsync(h->centroids, 0, sizeof(float) * (size_t)C * dpad, st));
+        if (centroids) {
+            FIT_CUDA(cudaMemcpy2DAsync(h->centroids, sizeof(float) * dpad, centroids, sizeof(float) * dim,
+                                       sizeof(float) * dim, C, kind, st));
+        } else {
+            // deterministic initial centroids: rows floor(c * n / C)
+            for (int c = 0; c < C; ++c) {
+                const int64_t r = (int64_t)c * n / C;
+                FIT_CUDA(cudaMemcpyAsync(h->centroids + (size_t)c * dpad, X + (size_t)r * dpad, sizeof(float) * dpad,
+                                         cudaMemcpyDeviceToDevice, st));
+            }
+        }
+        // iota for the sort values
+        {
+            std::vector<int32_t> io((size_t)n);
+            for (int64_t i = 0; i < n; ++i) io[i] = (int32_t)i;
+            FIT_CUDA(cudaMemcpyAsync(idx, io.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+            FIT_CUDA(cudaStreamSynchronize(st));
+        }
+        FIT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, a_raw, a_sorted, idx, order, (int)n, 0, 32, st));
+        FIT_CUDA(cudaMalloc(&tmp, tmp_bytes));
+        FIT_TRY(dmalloc(&fallback, (size_t)C * dpad));
+        // reseed rows for empty lists: rows ((c * 37) % n) as the reference does (:611)
+        for (int c = 0; c < C; ++c) {
+            const int64_t r = ((int64_t)c * 37) % n;
+            FIT_CUDA(cudaMemcpyAsync(fallback + (size_t)c * dpad, X + (size_t)r * dpad, sizeof(float) * dpad,
+                                     cudaMemcpyDeviceToDevice, st));
+        }
+        const bool given_assign = assign != nullptr;
+        const int iters = (centroids || given_assign) ? 0 : kmeans_iters;
+        for (int it = 0; it < iters; ++it) {
+            FIT_TRY(assign_rows(X, n, dpad, h->centroids, C, a_raw, &h->ws, st));
+            FIT_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, a_raw, a_sorted, idx, order, (int)n, 0, 32, st));
+            FIT_TRY(launch_list_offsets(a_sorted, n, C, h->list_off, st));
+            FIT_TRY(launch_centroid_update(X, dpad, dim, order, h->list_off, C, h->centroids, dpad, fallback, st));
+        }
+        // the lists: given assignment, else nearest to the current centroids (the last k-means
+        // assignment when iterating, as the reference's lists come from its last assign step)
+        if (given_assign) {
+            FIT_CUDA(cudaMemcpyAsync(a_raw, assign, sizeof(int32_t) * n, kind, st));
+        } else if (iters == 0) {
+            FIT_TRY(assign_rows(X, n, dpad, h->centroids, C, a_raw, &h->ws, st));
+        }
+        FIT_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, a_raw, a_sorted, idx, order, (int)n, 0, 32, st));
+        FIT_TRY(launch_list_offsets(a_sorted, n, C, h->list_off, st));
+        // reorder rows, SQ8 train / encode over the reordered rows
+        FIT_TRY(dmalloc(&h->original, (size_t)n * dpad));
+        FIT_TRY(dmalloc(&h->codes, (size_t)n * dpad8));
+        FIT_TRY(dmalloc(&h->scale, dpad));
+        FIT_TRY(dmalloc(&h->offset, dpad));
+        FIT_TRY(dmalloc(&mn, dpad));
+        FIT_TRY(dmalloc(&mx, dpad));
+        FIT_TRY(launch_gather_rows(X, n, dpad, order, h->original, dpad, st));
+        FIT_TRY(launch_sq8_minmax(h->original, n, dim, dpad, mn, mx, st));
+        FIT_TRY(launch_sq8_params(mn, mx, dim, dpad, h->scale, h->offset, st));
+        FIT_TRY(launch_sq8_encode(h->original, n, dim, dpad, h->scale, h->offset, h->codes, dpad8, st));
+        h->r2o = order;
+        order = nullptr;
+        h->n = n;
+        h->dim = dim;
+        h->dpad = dpad;
+        h->dpad8 = dpad8;
+        h->C = C;
+        FIT_TRY(ivf_finish_lists(h, st));
+        FIT_CUDA(cudaStreamSynchronize(st));
+    }
+fail:
+    for (void* p : {(void*)X, (void*)a_raw, (void*)a_sorted, (void*)idx, (void*)order, tmp, (void*)mn, (void*)mx,
+                    (void*)fallback})
+        if (p) cudaFree(p);
+    if (rc) ivf_free_state(h);
+    return rc;
+#undef FIT_TRY
+#undef FIT_CUDA
+}
+
+int ann_ivf_import(ann_ivf* h, int64_t n, int32_t dim, int32_t n_clusters, const float* centroids,
+                   const float* original, const uint8_t* codes, const float* scale, const float* offset,
+                   const int32_t* r2o, const int64_t* list_offsets) {
+    clear_error();
+    ANN_CHECK_ARG(h != nullptr, "ann_ivf_import: null index");
+    ANN_CHECK_ARG(n >= 1 && dim >= 1 && n_clusters >= 1, "ann_ivf_import: empty state");
+    ANN_CHECK_ARG(centroids && original && codes && scale && offset && r2o && list_offsets,
+                  "ann_ivf_import: null array");
+    ANN_CHECK_ARG(list_offsets[0] == 0 && list_offsets[n_clusters] == n, "ann_ivf_import: list offsets do not span n");
+    for (int c = 0; c < n_clusters; ++c)
+        ANN_CHECK_ARG(list_offsets[c + 1] >= list_offsets[c], "ann_ivf_import: list offsets not sorted");
+    DeviceGuard g(h->device);
+    ANN_CUDA_TRY(cudaDeviceSynchronize());
+    ivf_free_state(h);
+    const int dpad = (int)ceil_div(dim, 32) * 32;
+    const int dpad8 = dpad;
+    int rc = ANN_OK;
+    if ((rc = dmalloc(&h->centroids, (size_t)n_clusters * dpad)) || (rc = dmalloc(&h->original, (size_t)n * dpad)) ||
+        (rc = dmalloc(&h->codes, (size_t)n * dpad8)) || (rc = dmalloc(&h->scale, dpad)) ||
+        (rc = dmalloc(&h->offset, dpad)) || (rc = dmalloc(&h->r2o, n)) || (rc = dmalloc(&h->list_off, n_clusters + 1))) {
+        ivf_free_state(h);
+        return rc;
+    }
+    cudaStream_t st = nullptr;
+    ANN_CUDA_TRY(cudaMemset(h->centroids, 0, sizeof(float) * (size_t)n_clusters * dpad));
+    ANN_CUDA_TRY(cudaMemset(h->original, 0, sizeof(float) * (size_t)n * dpad));
+    ANN_CUDA_TRY(cudaMemset(h->codes, 0, (size_t)n * dpad8));
+    ANN_CUDA_TRY(cudaMemset(h->scale, 0, sizeof(float) * dpad));
+    ANN_CUDA_TRY(cudaMemset(h->offset, 0, sizeof(float) * dpad));
+    ANN_CUDA_TRY(cudaMemcpy2D(h->centroids, sizeof(float) * dpad, centroids, sizeof(float) * dim, sizeof(float) * dim,
+                              n_clusters, cudaMemcpyHostToDevice));
+    ANN_CUDA_TRY(cudaMemcpy2D(h->original, sizeof(float) * dpad, original, sizeof(float) * dim, sizeof(float) * dim, n,
+                              cudaMemcpyHostToDevice));
+    ANN_CUDA_TRY(cudaMemcpy2D(h->codes, dpad8, codes, dim, dim, n, cudaMemcpyHostToDevice));
+    ANN_CUDA_TRY(cudaMemcpy(h->scale, scale, sizeof(float) * dim, cudaMemcpyHostToDevice));
+    ANN_CUDA_TRY(cudaMemcpy(h->offset, offset, sizeof(float) * dim, cudaMemcpyHostToDevice));
+    ANN_CUDA_TRY(cudaMemcpy(h->r2o, r2o, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+    ANN_CUDA_TRY(cudaMemcpy(h->list_off, list_offsets, sizeof(int64_t) * (n_clusters + 1), cudaMemcpyHostToDevice));
+    h->n = n;
+    h->dim = dim;
+    h->dpad = dpad;
+    h->dpad8 = dpad8;
+    h->C = n_clusters;
+    return ivf_finish_lists(h, st);
+}
+
+int ann_ivf_export(ann_ivf* h, float* centroids, float* original, uint8_t* codes, float* scale, float* offset,
+                   int32_t* r2o, int64_t* list_offsets) {
+    clear_error();
+    ANN_CHECK_ARG(h != nullptr, "ann_ivf_export: null index");
+    if (h->n == 0) {
+        set_error("index not fitted");
+        return ANN_ERR_STATE;
+    }
+    DeviceGuard g(h->device);
+    const int dim = h->dim;
+    if (centroids)
+        ANN_CUDA_TRY(cudaMemcpy2D(centroids, sizeof(float) * dim, h->centroids, sizeof(float) * h->dpad,
+                                  sizeof(float) * dim, h->C, cudaMemcpyDeviceToHost));
+    if (original)
+        ANN_CUDA_TRY(cudaMemcpy2D(original, sizeof(float) * dim, h->original, sizeof(float) * h->dpad,
+                                  sizeof(float) * dim, h->n, cudaMemcpyDeviceToHost));
+    if (codes) ANN_CUDA_TRY(cudaMemcpy2D(codes, dim, h->codes, h->dpad8, dim, h->n, cudaMemcpyDeviceToHost));
+    if (scale) ANN_CUDA_TRY(cudaMemcpy(scale, h->scale, sizeof(float) * dim, cudaMemcpyDeviceToHost));
+    if (offset) ANN_CUDA_TRY(cudaMemcpy(offset, h->offset, sizeof(float) * dim, cudaMemcpyDeviceToHost));
+    if (r2o) ANN_CUDA_TRY(cudaMemcpy(r2o, h->r2o, sizeof(int32_t) * h->n, cudaMemcpyDeviceToHost));
+    if (list_offsets)
+        ANN_CUDA_TRY(cudaMemcpy(list_offsets, h->list_off, sizeof(int64_t) * (h->C + 1), cudaMemcpyDeviceToHost));
+    return ANN_OK;
+}
+
+int ann_ivf_info(const ann_ivf* h, int64_t* out4) {
+    ANN_CHECK_ARG(h != nullptr && out4 != nullptr, "ann_ivf_info: null argument");
+    out4[0] = h->n;
+    out4[1] = h->dim;
+    out4[2] = h->C;
+    out4[3] = h->sizes_desc.empty() ? 0 : h->sizes_desc[0];
+    return ANN_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+struct IvfQueryCfg {
+    int k, npc, R, nsplit, num_threads, bqc, nsplit_c, ncp;
+    int64_t max_c, ub, rps_c;
+    bool ref, coarse_flat;
+};
+
+// Bytes of scratch one device-side query call of nq queries needs (mirrors the carving below).
+static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
+    Sizer sz;
+    sz.take<int32_t>((size_t)nq * c.npc);
+    sz.take<int64_t>((size_t)nq * c.npc);
+    sz.take<int64_t>((size_t)nq * (c.npc + 1));
+    sz.take<int32_t>((size_t)nq);
+    sz.take<int64_t>((size_t)nq);
+    if (c.coarse_flat) {
+        sz.take<float>((size_t)nq * c.nsplit_c * c.npc);
+        sz.take<int>((size_t)nq * c.nsplit_c * c.npc);
+    } else {
+        sz.take<float>((size_t)nq * h->C);
+        sz.take<float>((size_t)nq * c.npc);
+    }
+    sz.take<float>((size_t)nq * c.nsplit * c.R);
+    sz.take<int>((size_t)nq * c.nsplit * c.R);
+    sz.take<float>((size_t)nq * c.R);
+    sz.take<int>((size_t)nq * c.R);
+    if (c.ref) sz.take<float>((size_t)nq * c.ub * (c.ncp + 2));
+    return sz.off;
+}
+
+// All stages for nq device-resident padded queries; scratch carved from `base`.
+static int ivf_query_device(ann_ivf* h, const IvfQueryCfg& c, char* base, const float* qdev, int nq,
+                            int64_t* ids_dev, float* dists_dev, cudaStream_t st) {
+    Carver cv(base);
+    int32_t* probes = cv.take<int32_t>((size_t)nq * c.npc);
+    int64_t* seg_start = cv.take<int64_t>((size_t)nq * c.npc);
+    int64_t* seg_pref = cv.take<int64_t>((size_t)nq * (c.npc + 1));
+    int32_t* n_seg = cv.take<int32_t>((size_t)nq);
+    int64_t* n_cands = cv.take<int64_t>((size_t)nq);
+    float *ckey = nullptr, *Dc = nullptr, *pkey = nullptr;
+    int* cid = nullptr;
+    if (c.coarse_flat) {
+        ckey = cv.take<float>((size_t)nq * c.nsplit_c * c.npc);
+        cid = cv.take<int>((size_t)nq * c.nsplit_c * c.npc);
+    } else {
+        Dc = cv.take<float>((size_t)nq * h->C);
+        pkey = cv.take<float>((size_t)nq * c.npc);
+    }
+    float* keyS = cv.take<float>((size_t)nq * c.nsplit * c.R);
+    int* idS = cv.take<int>((size_t)nq * c.nsplit * c.R);
+    float* keyR = cv.take<float>((size_t)nq * c.R);
+    int* idR = cv.take<int>((size_t)nq * c.R);
+    float* DP = c.ref ? cv.take<float>((size_t)nq * c.ub * (c.ncp + 2)) : nullptr;
+
+    IvfQueryArgs a{};
+    a.ix = h->view();
+    a.plan.nq = nq;
+    a.plan.npc = c.npc;
+    a.plan.probes = probes;
+    a.plan.seg_start = seg_start;
+    a.plan.seg_pref = seg_pref;
+    a.plan.n_seg = n_seg;
+    a.plan.n_cands = n_cands;
+    a.q = qdev;
+    a.ldq = h->dpad;
+    a.k = c.k;
+    a.R = c.R;
+    a.max_cands = c.max_c;
+    a.nsplit = c.nsplit;
+    a.num_threads = c.num_threads;
+    a.ndist = h->d_ndist;
+    a.out_ids = ids_dev;
+    a.out_dists = dists_dev;
+
+    int rc;
+    const int prec = h->prof.begin(st);
+    // 1. coarse ranking
+    if (c.coarse_flat) {
+        FlatScanArgs fa{h->centroids, h->C, h->dpad, qdev, nq, ANN_METRIC_L2, c.npc, c.rps_c, c.nsplit_c, ckey, cid};
+        if ((rc = launch_flat_scan(fa, c.bqc, st))) return rc;
+        MergeArgs m{ckey, cid, nq, c.nsplit_c, c.npc, c.npc, 0, nullptr, nullptr};
+        m.out_id32 = probes;
+        if ((rc = launch_merge_splits(m, st))) return rc;
+    } else {
+        if ((rc = launch_ref_centroid_dists(a.ix, qdev, h->dpad, nq, Dc, st))) return rc;
+        if ((rc = launch_select_topk(Dc, h->C, nullptr, nq, c.npc, nullptr, pkey, probes, st))) return rc;
+    }
+    h->prof.mark(prec, st);
+    // 2. plan
+    if ((rc = launch_ivf_plan(a, st))) return rc;
+    h->prof.mark(prec, st);
+    // 3. SQ8 pass -> best R per query
+    if (!c.ref) {
+        a.keyR = keyS;
+        a.idR = idS;
+        if ((rc = launch_ivf_sq8_scan(a, st))) return rc;
+        if (c.nsplit > 1) {
+            MergeArgs m{keyS, idS, nq, c.nsplit, c.R, c.R, 0, nullptr, nullptr};
+            m.out_id32 = idR;
+            m.out_key32 = keyR;
+            if ((rc = launch_merge_splits(m, st))) return rc;
+        } else {
+            keyR = keyS;
+            idR = idS;
+        }
+    } else {
+        a.L = c.ub;
+        a.ncp = c.ncp;
+        a.D = DP;
+        a.V = DP + (size_t)nq * c.ub;
+        a.P = DP + (size_t)2 * nq * c.ub;
+        if ((rc = launch_ivf_ref_sq8(a, c.ub, st))) return rc;
+        if ((rc = launch_select_topk(a.V, c.ub, n_cands, nq, c.R, &a.plan, keyR, idR, st))) return rc;
+    }
+    h->prof.mark(prec, st);
+    // 4. FP32 re-rank and the final top-k
+    if ((rc = launch_ivf_rerank(a, keyR, idR, c.ref ? 1 : 0, st))) return rc;
+    h->prof.mark(prec, st);
+    return ANN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t nq, int64_t ldq, int32_t k,
+                  int32_t n_probes, int32_t n_probe_clusters, int32_t refine_r, int64_t max_candidates, int32_t mode,
+                  int32_t num_threads, int32_t mem, int64_t* out_ids, float* out_dists, void* stream) {
+    clear_error();
+    ANN_CHECK_ARG(h != nullptr, "ann_ivf_query: null index");
+    if (h->n == 0) {
+        set_error("index not fitted");
+        return ANN_ERR_STATE;
+    }
+    ANN_CHECK_ARG(nq >= 0 && k >= 1, "ann_ivf_query: nq=%d, k=%d", nq, k);
+    ANN_CHECK_ARG(ldq >= h->dim, "ann_ivf_query: query stride < dim");
+    ANN_CHECK_ARG(mode == ANN_MODE_EXACT || mode == ANN_MODE_REFERENCE, "ann_ivf_query: unknown mode %d", mode);
+    ANN_CHECK_ARG(nq == 0 || (queries && out_ids), "ann_ivf_query: null pointer");
+    ANN_CHECK_ARG(k <= 1024, "ann_ivf_query: k=%d > 1024", k);
+    if (n_probes != 0) {
+        set_error("ann_ivf_query: multiprobe LSH buckets (n_probes > 0) need n_bits > 0 tables, not built here");
+        return ANN_ERR_UNSUPPORTED;
+    }
+    if (nq == 0) return ANN_OK;
+    if (!ws) ws = &h->ws;
+    DeviceGuard g(h->device);
+    cudaStream_t st = as_stream(stream);
+
+    IvfQueryCfg c{};
+    c.ref = mode == ANN_MODE_REFERENCE;
+    c.k = k;
+    c.npc = std::max(1, std::min(n_probe_clusters, h->C));  // active_clusters (:332)
+    // R = max(k, refine_r > 0 ? refine_r : 4k) (:472-474); cap max(2000, 4 * target) (:357-358)
+    const int target = refine_r > 0 ? refine_r : 4 * k;
+    c.R = std::max(k, target);
+    c.max_c = max_candidates;
+    if (c.max_c < 0) c.max_c = std::max<int64_t>(2000, 4 * (int64_t)target);
+    if (c.max_c == 0) c.max_c = INT64_MAX;
+    c.num_threads = num_threads > 0 ? num_threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    if (c.ref) ANN_CHECK_ARG(c.R <= 8192, "reference mode: refine count %d > 8192", c.R);
+    if (!c.ref && c.R > 1024) {
+        set_error("ann_ivf_query: refine count %d > 1024 in exact mode", c.R);
+        return ANN_ERR_UNSUPPORTED;
+    }
+    // longest possible candidate stream: the npc largest lists up to the cap; every row when a
+    // query's lists could hold fewer than k points (the reference then scans all rows, :453-457)
+    // (a list is added while the stream is below the cap, so a capped stream ends below
+    // cap - 1 + the largest list)
+    int64_t ub = 0, smallest = 0;
+    for (int j = 0; j < c.npc; ++j) ub += h->sizes_desc[j];
+    if (c.max_c != INT64_MAX) ub = std::min(ub, c.max_c - 1 + h->sizes_desc[0]);
+    for (int j = 0; j < c.npc; ++j) smallest += h->sizes_desc[h->C - 1 - j];
+    if (smallest < k) ub = std::max(ub, h->n);
+    c.ub = std::max<int64_t>(ub, 1);
+    c.ncp = ref_num_checkpoints(h->dim);
+    c.coarse_flat = !c.ref && c.npc <= 512;
+    const int dpad = h->dpad;
+    const bool host = mem == ANN_MEM_HOST;
+
+    // queries per device call: bounded scratch in reference mode
+    int qc = nq;
+    if (c.ref) {
+        const size_t per_q = sizeof(float) * (size_t)c.ub * (c.ncp + 2) + 4096;
+        qc = (int)std::max<size_t>(1, std::min<size_t>(nq, ((size_t)2 << 30) / per_q));
+    }
+    c.nsplit = c.ref ? 1 : (int)std::max<int64_t>(1, std::min<int64_t>(64, ceil_div(2 * kNumSMs, qc)));
+    c.bqc = std::min(flat_scan_bq(qc), flat_scan_max_bq(c.npc));
+    {
+        const int n_qt = (int)ceil_div(qc, c.bqc);
+        c.nsplit_c = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(kNumSMs, n_qt), ceil_div(h->C, 512)));
+        c.rps_c = ceil_div(ceil_div(h->C, c.nsplit_c), 256) * 256;
+        c.nsplit_c = (int)ceil_div(h->C, c.rps_c);
+    }
+    Sizer head;
+    head.take<float>((size_t)nq * dpad);
+    if (host) {
+        head.take<int64_t>((size_t)nq * k);
+        head.take<float>((size_t)nq * k);
+    }
+    const size_t head_bytes = (head.off + 255) / 256 * 256;
+    int rc = ws_reserve_device(ws, head_bytes + ivf_scratch(h, c, qc) + 512);
+    if (rc) return rc;
+    Carver cv(ws->dev);
+    float* qdev = cv.take<float>((size_t)nq * dpad);
+    int64_t* ids_dev = out_ids;
+    float* dists_dev = out_dists;
+    if (host) {
+        ids_dev = cv.take<int64_t>((size_t)nq * k);
+        dists_dev = cv.take<float>((size_t)nq * k);
+    }
+    char* scratch = ws->dev + head_bytes;
+    if (host) {
+        rc = ws_reserve_host(ws, std::max(sizeof(float) * (size_t)nq * dpad, (sizeof(int64_t) + 4) * (size_t)nq * k));
+        if (rc) return rc;
+        float* hq = reinterpret_cast<float*>(ws->host);
+        for (int i = 0; i < nq; ++i) {
+            std::memcpy(hq + (size_t)i * dpad, queries + (size_t)i * ldq, sizeof(float) * h->dim);
+            if (dpad > h->dim) std::memset(hq + (size_t)i * dpad + h->dim, 0, sizeof(float) * (dpad - h->dim));
+        }
+        ANN_CUDA_TRY(cudaMemcpyAsync(qdev, hq, sizeof(float) * (size_t)nq * dpad, cudaMemcpyHostToDevice, st));
+    } else {
+        rc = launch_pad_rows(queries, nq, h->dim, ldq, qdev, dpad, st);
+        if (rc) return rc;
+    }
+    for (int q0 = 0; q0 < nq; q0 += qc) {
+        const int nc = std::min(qc, nq - q0);
+        rc = ivf_query_device(h, c, scratch, qdev + (size_t)q0 * dpad, nc, ids_dev + (size_t)q0 * k,
+                              dists_dev ? dists_dev + (size_t)q0 * k : nullptr, st);
+        if (rc) return rc;
+    }
+    h->query_count += nq;
+    if (host) {
+        int64_t* hid = reinterpret_cast<int64_t*>(ws->host);
+        float* hd = reinterpret_cast<float*>(ws->host + sizeof(int64_t) * (size_t)nq * k);
+        ANN_CUDA_TRY(cudaMemcpyAsync(hid, ids_dev, sizeof(int64_t) * (size_t)nq * k, cudaMemcpyDeviceToHost, st));
+        if (out_dists)
+            ANN_CUDA_TRY(cudaMemcpyAsync(hd, dists_dev, sizeof(float) * (size_t)nq * k, cudaMemcpyDeviceToHost, st));
+        ANN_CUDA_TRY(cudaStreamSynchronize(st));
+        std::memcpy(out_ids, hid, sizeof(int64_t) * (size_t)nq * k);
+        if (out_dists) std::memcpy(out_dists, hd, sizeof(float) * (size_t)nq * k);
+    }
+    return ANN_OK;
+}
+
+int64_t ann_ivf_total_distances(ann_ivf* h) {
+    if (!h || !h->d_ndist) return 0;
+    DeviceGuard g(h->device);
+    unsigned long long v = 0;
+    if (cudaMemcpy(&v, h->d_ndist, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return (int64_t)v;
+}
+
+int ann_ivf_reset_distances(ann_ivf* h) {
+    ANN_CHECK_ARG(h != nullptr, "null index");
+    if (!h->d_ndist) return ANN_OK;
+    DeviceGuard g(h->device);
+    ANN_CUDA_TRY(cudaMemset(h->d_ndist, 0, sizeof(unsigned long long)));
+    return ANN_OK;
+}
+
+int ann_ivf_set_profiling(ann_ivf* h, int32_t enable) {
+    ANN_CHECK_ARG(h != nullptr, "null index");
+    h->prof.enabled = enable != 0;
+    return ANN_OK;
+}
+
+int ann_ivf_profile(ann_ivf* h, double* out6) {
+    ANN_CHECK_ARG(h != nullptr && out6 != nullptr, "null argument");
+    DeviceGuard g(h->device);
+    h->prof.collect();
+    for (int i = 0; i < 4; ++i) out6[i] = h->prof.total_ms[i];
+    out6[4] = (double)h->prof.calls;
+    out6[5] = (double)h->query_count;
+    return ANN_OK;
+}
+
+int ann_ivf_reset_profile(ann_ivf* h) {
+    ANN_CHECK_ARG(h != nullptr, "null index");
+    DeviceGuard g(h->device);
+    h->prof.reset();
+    h->query_count = 0;
+    return ANN_OK;
+}
+
+}  // extern "C"

@@ -277,6 +277,8 @@ __global__ void __launch_bounds__(256) merge_splits_kernel(MergeArgs a) {
             const int iv = ok ? sId[e] : kNoId;
             if (a.out_ids) a.out_ids[(int64_t)qi * k + e] = ok ? (int64_t)iv : -1;
             if (a.out_dists) a.out_dists[(int64_t)qi * k + e] = ok ? (a.negate ? -kv : kv) : (a.negate ? -kInf : kInf);
+            if (a.out_id32) a.out_id32[(int64_t)qi * k + e] = ok ? iv : kNoId;
+            if (a.out_key32) a.out_key32[(int64_t)qi * k + e] = ok ? kv : kInf;
         }
     }
 }
@@ -353,7 +355,7 @@ int launch_flat_scan(const FlatScanArgs& a0, int bq, cudaStream_t st) {
 }
 
 int launch_merge_splits(const MergeArgs& a, cudaStream_t st) {
-    ANN_CHECK_ARG(a.k >= 1 && a.k <= 512, "merge: k=%d outside [1, 512]", a.k);
+    ANN_CHECK_ARG(a.k >= 1 && a.k <= 1024, "merge: k=%d outside [1, 1024]", a.k);
     if (a.nq == 0) return ANN_OK;
     const size_t smem = (size_t)8 * topk_cap(a.k) * 8;
     ANN_CUDA_TRY(cudaFuncSetAttribute(merge_splits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

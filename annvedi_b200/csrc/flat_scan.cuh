@@ -30,6 +30,8 @@ struct MergeArgs {
     int negate;              // 1: output -key (inner-product scores)
     int64_t* out_ids;        // [nq, k], -1 where fewer than k exist
     float* out_dists;        // [nq, k] or nullptr
+    int* out_id32 = nullptr;   // [nq, k] raw ids (INT_MAX where fewer than k exist), optional
+    float* out_key32 = nullptr; // [nq, k] raw keys (+inf where fewer), optional
 };
 
 int flat_scan_bq(int nq);

@@ -1,0 +1,220 @@
+"""IVF-SQ8 index on the GPU: the drop-in for ivf_lsh_cpp.LSHIndex with n_tables = 1, n_bits = 0.
+
+Surface of the reference (competitors/ivf_lsh/src/lsh_index_optimized.cpp:658-666):
+``fit(data, n_tables, n_bits, n_clusters=256)``, ``query(query, k, n_probes=0, n_probe_clusters=8,
+refine_r=-1) -> int64[k]``, ``total_distances_count()``, ``reset_distances_count()``,
+``get_profile_results()``, ``reset_profile_results()``.
+
+Two semantics (``mode``):
+
+* ``"reference"``: the reference's ranking bit for bit -- its coarse ranking arithmetic, candidate
+  cap, per-ThreadPool-chunk 64-entry early-abandon SQ8 pass (``num_threads`` = the reference host's
+  hardware concurrency, default this host's), FP32 re-rank and id mapping;
+* ``"exact"``: the same pipeline with full SQ8 distances (no early abandon) and, by default, no
+  candidate cap -- the batched GPU form used for throughput.
+
+Extras: ``search(queries, k, ...)`` (batched; numpy in -> numpy out, CUDA tensor in -> CUDA tensor
+out on the current stream), ``import_state`` / ``export_state`` (the reference's state layout, used
+for parity), and ``fit(..., centroids=, assign=)`` to build lists from a given coarse quantiser.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+
+
+class IVFIndex:
+    def __init__(self, device: int = 0, mode: str = "reference", num_threads: int | None = None):
+        self._lib = _lib.load()
+        if mode not in _lib.MODES:
+            raise ValueError(f"unknown mode {mode!r}")
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.ann_ivf_create(ctypes.byref(h), device))
+        self._h = h
+        self.device = device
+        self.mode = mode
+        self.num_threads = int(num_threads) if num_threads else (os.cpu_count() or 1)
+        self._n = 0
+        self._dim = 0
+        self._C = 0
+
+    # ---- build -----------------------------------------------------------------------------------
+    def fit(self, data, n_tables: int = 1, n_bits: int = 0, n_clusters: int = 256, kmeans_iters: int = 15,
+            centroids=None, assign=None) -> None:
+        if int(n_tables) != 1 or int(n_bits) != 0:
+            raise NotImplementedError("LSH bucket tables (n_tables > 1 or n_bits > 0) are not built on the GPU; "
+                                      "use n_tables=1, n_bits=0 (inverted lists)")
+        if _lib.is_torch(data):
+            x = _lib.as_f32_2d(data, "data")
+            mem = _lib.MEM_DEVICE if x.is_cuda else _lib.MEM_HOST
+            if not x.is_cuda:
+                x = x.numpy()
+            ld = x.stride(0) if mem == _lib.MEM_DEVICE else x.shape[1]
+        else:
+            a = np.asarray(data)
+            if a.ndim != 2:
+                raise RuntimeError("Input data must be 2D")
+            x = np.ascontiguousarray(a, np.float32)
+            mem, ld = _lib.MEM_HOST, x.shape[1]
+        n, d = x.shape
+        if n == 0 or d == 0:
+            raise RuntimeError("Input data must be a non-empty 2D array")
+        cen = asg = None
+        if centroids is not None:
+            cen = self._like(centroids, mem, np.float32, x)
+            if tuple(cen.shape) != (min(int(n_clusters), n), d):
+                raise RuntimeError("centroids must have shape [n_clusters, dim]")
+        if assign is not None:
+            asg = self._like(assign, mem, np.int32, x)
+            if asg.shape[0] != n:
+                raise RuntimeError("assign must have one entry per row")
+        st = _lib.stream_ptr(x) if mem == _lib.MEM_DEVICE else None
+        _lib.check(self._lib.ann_ivf_fit(self._h, _lib.ptr(x), n, d, ld, int(n_clusters), _lib.ptr(cen),
+                                         _lib.ptr(asg), int(kmeans_iters), mem, st))
+        self._n, self._dim = n, d
+        self._C = min(int(n_clusters), n)
+
+    @staticmethod
+    def _like(v, mem, dtype, x):
+        if mem == _lib.MEM_DEVICE:
+            import torch
+            t = v if _lib.is_torch(v) else torch.from_numpy(np.asarray(v))
+            return t.to(device=x.device, dtype=torch.float32 if dtype == np.float32 else torch.int32).contiguous()
+        return np.ascontiguousarray(v.cpu().numpy() if _lib.is_torch(v) else v, dtype)
+
+    def import_state(self, state: dict) -> None:
+        """Loads a state in the reference's layout (n_tables = 1, n_bits = 0): keys npts, dim,
+        n_clusters, centroids, original_data, quantized_data, scale, offset,
+        reordered_to_original, table_offsets (= list offsets)."""
+        if int(state.get("n_tables", 1)) != 1 or int(state.get("n_bits", 0)) != 0:
+            raise NotImplementedError("only inverted-list states (n_tables = 1, n_bits = 0) can be imported")
+        n, d, c = int(state["npts"]), int(state["dim"]), int(state["n_clusters"])
+        arrs = [np.ascontiguousarray(state[k], t) for k, t in (
+            ("centroids", np.float32), ("original_data", np.float32), ("quantized_data", np.uint8),
+            ("scale", np.float32), ("offset", np.float32), ("reordered_to_original", np.int32),
+            ("table_offsets", np.int64))]
+        _lib.check(self._lib.ann_ivf_import(self._h, n, d, c, *[_lib.ptr(a) for a in arrs]))
+        self._n, self._dim, self._C = n, d, c
+
+    def export_state(self) -> dict:
+        n, d, c = self._n, self._dim, self._C
+        out = {"npts": n, "dim": d, "n_clusters": c, "n_tables": 1, "n_bits": 0,
+               "centroids": np.empty((c, d), np.float32), "original_data": np.empty((n, d), np.float32),
+               "quantized_data": np.empty((n, d), np.uint8), "scale": np.empty(d, np.float32),
+               "offset": np.empty(d, np.float32), "reordered_to_original": np.empty(n, np.int32),
+               "table_offsets": np.empty(c + 1, np.int64)}
+        _lib.check(self._lib.ann_ivf_export(self._h, *[_lib.ptr(out[k]) for k in (
+            "centroids", "original_data", "quantized_data", "scale", "offset", "reordered_to_original",
+            "table_offsets")]))
+        out["mean"] = np.zeros(d, np.float32)
+        out["projections"] = np.zeros((0, d), np.float32)
+        out["table_ids"] = np.arange(n, dtype=np.int32)
+        return out
+
+    # ---- reference surface -----------------------------------------------------------------------
+    def query(self, query, k: int, n_probes: int = 0, n_probe_clusters: int = 8, refine_r: int = -1,
+              max_candidates: int | None = None) -> np.ndarray:
+        qa = np.asarray(query.cpu() if _lib.is_torch(query) else query, np.float32)
+        if qa.ndim != 1 or qa.shape[0] != self._dim:
+            raise RuntimeError("Query dimension mismatch")
+        ids, _ = self.search(qa.reshape(1, -1), k, n_probes=n_probes, n_probe_clusters=n_probe_clusters,
+                             refine_r=refine_r, max_candidates=max_candidates)
+        return ids[0]
+
+    def total_distances_count(self) -> int:
+        return int(self._lib.ann_ivf_total_distances(self._h))
+
+    def reset_distances_count(self) -> None:
+        _lib.check(self._lib.ann_ivf_reset_distances(self._h))
+
+    def set_profiling(self, enable: bool = True) -> None:
+        _lib.check(self._lib.ann_ivf_set_profiling(self._h, int(enable)))
+
+    def get_profile_results(self) -> dict:
+        """The reference's keys (lsh_index_optimized.cpp:535-548), from CUDA events: averages per
+        query of the batched stages (a batch's stage time divided by its queries)."""
+        out = (ctypes.c_double * 6)()
+        _lib.check(self._lib.ann_ivf_profile(self._h, out))
+        nq = int(out[5])
+        if nq == 0 or out[4] == 0:
+            return {"query_count": nq}
+        return {"avg_centroid_search_ms": out[0] / nq, "avg_signature_calc_ms": 0.0,
+                "avg_bucket_lookup_ms": out[1] / nq, "avg_distance_calc_ms": (out[2] + out[3]) / nq,
+                "avg_candidate_sort_ms": 0.0, "query_count": nq,
+                "stage_ms": {"coarse": out[0], "plan": out[1], "sq8": out[2], "rerank": out[3]},
+                "profiled_calls": int(out[4])}
+
+    def reset_profile_results(self) -> None:
+        _lib.check(self._lib.ann_ivf_reset_profile(self._h))
+
+    # ---- batched API -----------------------------------------------------------------------------
+    def search(self, queries, k: int, n_probes: int = 0, n_probe_clusters: int = 8, refine_r: int = -1,
+               max_candidates: int | None = None, mode: str | None = None, workspace=None, out_ids=None,
+               out_dists=None, stream=None, with_dists: bool = True):
+        """Top-k per query row: (ids int64 [nq, k], squared distances float32 [nq, k]).
+        max_candidates: None = the mode's default (reference: the reference's cap; exact: none),
+        -1 = the reference's cap, 0 = none, > 0 = that cap."""
+        if self._n == 0:
+            raise RuntimeError("index not fitted")
+        k = int(k)
+        if k < 1:
+            raise RuntimeError("k must be >= 1")
+        mode = mode or self.mode
+        if max_candidates is None:
+            max_candidates = -1 if mode == "reference" else 0
+        ws = workspace.handle if workspace is not None else None
+        args = (int(n_probes), int(n_probe_clusters), int(refine_r), int(max_candidates), _lib.MODES[mode],
+                int(self.num_threads))
+        if _lib.is_torch(queries) and queries.is_cuda:
+            import torch
+            x = _lib.as_f32_2d(queries, "queries")
+            if x.shape[1] != self._dim:
+                raise RuntimeError("Query dimension mismatch")
+            nq = x.shape[0]
+            if out_ids is None:
+                out_ids = torch.empty(nq, k, dtype=torch.int64, device=x.device)
+            if out_dists is None and with_dists:
+                out_dists = torch.empty(nq, k, dtype=torch.float32, device=x.device)
+            _lib.check(self._lib.ann_ivf_query(self._h, ws, _lib.ptr(x), nq, x.stride(0), k, *args, _lib.MEM_DEVICE,
+                                               _lib.ptr(out_ids), _lib.ptr(out_dists), _lib.stream_ptr(x, stream)))
+            return out_ids, out_dists
+        x = _lib.as_f32_2d(queries.numpy() if _lib.is_torch(queries) else queries, "queries")
+        if x.shape[1] != self._dim:
+            raise RuntimeError("Query dimension mismatch")
+        nq = x.shape[0]
+        ids = np.empty((nq, k), np.int64)
+        dists = np.empty((nq, k), np.float32) if with_dists else None
+        _lib.check(self._lib.ann_ivf_query(self._h, ws, _lib.ptr(x), nq, x.shape[1], k, *args, _lib.MEM_HOST,
+                                           _lib.ptr(ids), _lib.ptr(dists), None))
+        return ids, dists
+
+    @property
+    def ntotal(self) -> int:
+        return self._n
+
+    @property
+    def dim(self) -> int:
+        return self._dim
+
+    @property
+    def n_lists(self) -> int:
+        return self._C
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ann_ivf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# the reference's class name
+LSHIndex = IVFIndex

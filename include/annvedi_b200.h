@@ -12,7 +12,7 @@
  *
  * Workspaces: scratch device memory for queries lives in an ann_workspace. Calls that run
  * concurrently (on different streams) must use different workspaces; passing NULL uses the
- * index's own workspace. Workspaces grow on demand (stream-ordered allocation on `stream`).
+ * index's own workspace. A workspace grows on demand; growing drains the device first.
  */
 #ifndef ANNVEDI_B200_H
 #define ANNVEDI_B200_H
@@ -46,6 +46,7 @@ extern "C" {
 #define ANN_MEM_DEVICE 1
 
 typedef struct ann_flat ann_flat;
+typedef struct ann_ivf ann_ivf;
 typedef struct ann_workspace ann_workspace;
 
 /* Library version string ("annvedi_b200 <major>.<minor> sm_100a"). */
@@ -100,6 +101,63 @@ int ann_flat_reset_profile(ann_flat* h);
 int64_t ann_flat_total_distances(const ann_flat* h);
 int32_t ann_flat_dim(const ann_flat* h);
 int64_t ann_flat_size(const ann_flat* h);
+
+/* ---- IVF-SQ8 index ------------------------------------------------------------------------
+ * Replaces ivf_lsh_cpp.LSHIndex (competitors/ivf_lsh/src/lsh_index_optimized.cpp:124-667) with
+ * n_tables = 1, n_bits = 0: inverted lists of per-dimension SQ8 codes and an FP32 re-rank. */
+
+/* LSHIndex() (lsh_index_optimized.cpp:126). */
+int ann_ivf_create(ann_ivf** out, int device);
+int ann_ivf_destroy(ann_ivf* h);
+
+/* LSHIndex::fit (lsh_index_optimized.cpp:128-292) on the GPU: `n_clusters` lists (clamped to n).
+ * Centroids: `centroids` [n_clusters, dim] if not NULL, else `kmeans_iters` k-means iterations
+ * from deterministic seeds. Lists: `assign` [n] if not NULL, else the nearest centroid (the last
+ * k-means assignment when iterating). Rows are reordered list by list and SQ8-encoded with
+ * per-dimension scale/offset exactly as the reference computes them. `data`, `centroids` and
+ * `assign` live where `mem` says. */
+int ann_ivf_fit(ann_ivf* h, const float* data, int64_t n, int32_t dim, int64_t ld, int32_t n_clusters,
+                const float* centroids, const int32_t* assign, int32_t kmeans_iters, int32_t mem, void* stream);
+
+/* Imports an index state in the reference's layout (all host pointers, rows in list order):
+ * centroids [C, dim], original [n, dim] FP32, codes [n, dim] uint8, scale / offset [dim],
+ * r2o [n] list-order row -> original id, list_offsets [C + 1]. The parity path: the reference
+ * (through a state export) and this index then answer queries over the same lists. */
+int ann_ivf_import(ann_ivf* h, int64_t n, int32_t dim, int32_t n_clusters, const float* centroids,
+                   const float* original, const uint8_t* codes, const float* scale, const float* offset,
+                   const int32_t* r2o, const int64_t* list_offsets);
+
+/* Copies the state out to host arrays of the same shapes (NULL skips an array). */
+int ann_ivf_export(ann_ivf* h, float* centroids, float* original, uint8_t* codes, float* scale, float* offset,
+                   int32_t* r2o, int64_t* list_offsets);
+
+/* out4 = {n, dim, n_clusters, largest list}. */
+int ann_ivf_info(const ann_ivf* h, int64_t* out4);
+
+/* LSHIndex::query (lsh_index_optimized.cpp:304-516), batched over `nq` queries:
+ * lists ranked by centroid distance, the first `n_probe_clusters` probed whole, in order, until the
+ * candidate stream reaches `max_candidates` (-1: the reference's max(2000, 4 * refine target);
+ * 0: no cap); a query whose probed lists hold fewer than k points scans every row; SQ8 distances
+ * over the stream; the best R = max(k, refine_r > 0 ? refine_r : 4k) re-ranked with exact FP32
+ * distances; the best k returned as original ids (-1 padded) with their squared distances.
+ * ANN_MODE_REFERENCE reproduces the reference's own ranking, including the 64-entry early-abandon
+ * heap of each of `num_threads` ThreadPool chunks (<= 0: this host's hardware concurrency, as the
+ * reference sizes its pool); ANN_MODE_EXACT ranks by full SQ8 distances. `n_probes` (multiprobe
+ * LSH buckets) must be 0. Adds each query's candidate count to the distance counter (:459-460). */
+int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t nq, int64_t ldq, int32_t k,
+                  int32_t n_probes, int32_t n_probe_clusters, int32_t refine_r, int64_t max_candidates, int32_t mode,
+                  int32_t num_threads, int32_t mem, int64_t* out_ids, float* out_dists, void* stream);
+
+/* LSHIndex::total_distances_count / reset_distances_count (lsh_index_optimized.cpp:518-524). */
+int64_t ann_ivf_total_distances(ann_ivf* h);
+int ann_ivf_reset_distances(ann_ivf* h);
+
+/* LSHIndex::get_profile_results / reset_profile_results (lsh_index_optimized.cpp:526-548), timed
+ * with CUDA events on the query stream: out6 = {coarse ranking ms, plan ms, SQ8 pass ms,
+ * re-rank ms, profiled calls, queries}. Totals, not averages. */
+int ann_ivf_set_profiling(ann_ivf* h, int32_t enable);
+int ann_ivf_profile(ann_ivf* h, double* out6);
+int ann_ivf_reset_profile(ann_ivf* h);
 
 #ifdef __cplusplus
 }

@@ -195,7 +195,8 @@ def sq8_encode(x, scale, offset):
 
 
 def exact_topk_f64(data, queries, k, metric="l2", chunk=256):
-    """FP64 exact top-k (ids, distances) by brute force; ties broken by lower id."""
+    """FP64 exact top-k by brute force, ties broken by lower id: (ids, squared distances) for
+    "l2", (ids, inner products, best first) for "ip"."""
     data64 = np.asarray(data, np.float64)
     queries = np.atleast_2d(np.asarray(queries, np.float64))
     xn = np.einsum("ij,ij->i", data64, data64)
@@ -214,5 +215,6 @@ def exact_topk_f64(data, queries, k, metric="l2", chunk=256):
         pk = np.take_along_axis(key, part, 1)
         order = np.lexsort((part, pk), axis=1)
         ids[s:s + chunk] = np.take_along_axis(part, order, 1)
-        dist[s:s + chunk] = np.take_along_axis(pk, order, 1)
+        sk = np.take_along_axis(pk, order, 1)
+        dist[s:s + chunk] = -sk if metric == "ip" else sk
     return ids, dist

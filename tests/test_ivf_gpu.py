@@ -1,0 +1,212 @@
+"""GPU parity of the IVF-SQ8 index through the C ABI.
+
+* reference mode over an imported state returns the reference's ids and get_n_distances exactly
+  (golden fixtures made by the reference's own LSHIndex, and the oracle restatement);
+* the GPU build (given centroids and lists) produces the reference's state bit for bit
+  (reorder, per-dimension SQ8 scale/offset, codes);
+* exact mode returns the exact-selection result: ids may differ from the oracle only at ties
+  within 1e-5 relative, distances match FP64 within 1e-5 relative.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from annvedi_b200 import synth
+from oracle import ivf_state, refmod
+from tests.golden import make_golden as mg
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ivf_fx(golden_dir):
+    return np.load(os.path.join(golden_dir, "ivf_ref.npz"))
+
+
+def _ivf(mode="reference", threads=8):
+    from annvedi_b200.ivf import IVFIndex
+    return IVFIndex(device=0, mode=mode, num_threads=threads)
+
+
+def test_reference_mode_matches_golden(cuda, ivf_fx):
+    cases, _ = mg.ivf_cases()
+    for name, spec, cfgs in cases:
+        if spec["n_bits"]:
+            continue  # LSH bucket tables are not built on the GPU
+        w = mg.make_workload(spec["workload"])
+        st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
+        for ci, (k, n_probes, npc, rr, nt) in enumerate(cfgs):
+            ix = _ivf(threads=nt)
+            ix.import_state(st)
+            ids, d = ix.search(w.queries, k, n_probes, npc, rr)
+            np.testing.assert_array_equal(ids, ivf_fx[f"{name}/cfg{ci}/ids"], err_msg=f"{name} cfg{ci}")
+            assert ix.total_distances_count() == int(ivf_fx[f"{name}/cfg{ci}/ndist"])
+            # one query at a time through the drop-in surface gives the same ids
+            if ci == 0:
+                one = np.stack([ix.query(q, k, n_probes, npc, rr) for q in w.queries[:4]])
+                np.testing.assert_array_equal(one, ivf_fx[f"{name}/cfg{ci}/ids"][:4])
+
+
+def test_reference_mode_matches_reference_fit_state(cuda, ivf_fx):
+    st = {key.split("/")[-1]: ivf_fx[key] for key in ivf_fx.files if key.startswith("reffit/state/")}
+    n, d = st["original_data"].shape
+    st.update(npts=n, dim=d, n_clusters=st["centroids"].shape[0], n_tables=1, n_bits=0)
+    k, n_probes, npc, rr, nt = [int(v) for v in ivf_fx["reffit/params"]]
+    ix = _ivf(threads=nt)
+    ix.import_state(st)
+    ids, _ = ix.search(ivf_fx["reffit/queries"], k, n_probes, npc, rr)
+    np.testing.assert_array_equal(ids, ivf_fx["reffit/ids"])
+    assert ix.total_distances_count() == int(ivf_fx["reffit/ndist"])
+
+
+def test_reference_mode_matches_oracle_random_configs(cuda):
+    w = synth.zipf_mixture(20000, 96, 24, c=48, lo=20, hi=2500, seed=77)
+    st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
+    for k, npc, rr, nt, cap in ((100, 6, 300, 16, -1), (20, 12, -1, 5, -1), (50, 48, 500, 16, 0), (1, 3, 10, 2, -1)):
+        ix = _ivf(threads=nt)
+        ix.import_state(st)
+        ids, dd = ix.search(w.queries, k, 0, npc, rr, max_candidates=cap)
+        nd = 0
+        for i, q in enumerate(w.queries):
+            oi, od, nc = refmod.ivf_query(st, q, k, 0, npc, rr, num_threads=nt, lanes=16, max_cands=cap)
+            np.testing.assert_array_equal(ids[i], oi, err_msg=f"k={k} npc={npc} rr={rr} T={nt} q={i}")
+            np.testing.assert_array_equal(dd[i], od)
+            nd += nc
+        assert ix.total_distances_count() == nd
+
+
+def test_gpu_build_matches_reference_state(cuda):
+    from annvedi_b200.ivf import IVFIndex
+    w = synth.zipf_mixture(12000, 100, 8, c=40, lo=20, hi=2000, seed=31)
+    ix = IVFIndex(device=0)
+    ix.fit(w.base, 1, 0, 40, centroids=w.centres, assign=w.assign)
+    got = ix.export_state()
+    want = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
+    for key in ("original_data", "quantized_data", "scale", "offset", "reordered_to_original", "table_offsets"):
+        np.testing.assert_array_equal(got[key], want[key], err_msg=key)
+    # lists from the given centroids alone (nearest centroid) match the FP64 assignment
+    ix2 = IVFIndex(device=0)
+    ix2.fit(w.base, 1, 0, 40, centroids=w.centres)
+    st2 = ix2.export_state()
+    a64 = ivf_state.nearest_centroid(w.base, w.centres)
+    sizes = np.diff(st2["table_offsets"])
+    np.testing.assert_array_equal(sizes, np.bincount(a64, minlength=40))
+
+
+def test_gpu_kmeans_fit_is_consistent(cuda):
+    from annvedi_b200.ivf import IVFIndex
+    w = synth.zipf_mixture(30000, 64, 16, c=64, lo=20, hi=3000, seed=5)
+    ix = IVFIndex(device=0, mode="exact")
+    ix.fit(w.base, 1, 0, 64, kmeans_iters=10)
+    st = ix.export_state()
+    # every row once, in list order; codes are the SQ8 encoding of the reordered rows
+    assert sorted(st["reordered_to_original"].tolist()) == list(range(30000))
+    np.testing.assert_array_equal(st["original_data"], w.base[st["reordered_to_original"]])
+    sc, of = refmod.sq8_train(st["original_data"])
+    np.testing.assert_array_equal(sc, st["scale"])
+    np.testing.assert_array_equal(refmod.sq8_encode(st["original_data"], sc, of), st["quantized_data"])
+    # deterministic: a second fit gives the same state
+    ix2 = IVFIndex(device=0, mode="exact")
+    ix2.fit(w.base, 1, 0, 64, kmeans_iters=10)
+    np.testing.assert_array_equal(ix2.export_state()["centroids"], st["centroids"])
+    # and it searches well
+    ids, d = ix.search(w.queries, 10, 0, 16, 100)
+    gt, gd = refmod.exact_topk_f64(w.base, w.queries, 10)
+    assert np.mean([len(set(a) & set(b)) / 10 for a, b in zip(ids, gt)]) > 0.9
+
+
+def _exact_ivf_oracle(st, queries, k, npc, R):
+    """Exact-mode semantics in FP64: lists by centroid distance, full SQ8 distances of every
+    candidate, best R, FP64 re-rank, best k. Returns (ids, d) with d the FP64 squared distances."""
+    cen = st["centroids"].astype(np.float64)
+    off = st["table_offsets"]
+    codes = st["quantized_data"].astype(np.float64)
+    recon = codes * st["scale"].astype(np.float64)
+    orig = st["original_data"].astype(np.float64)
+    out_i, out_d = [], []
+    for q in queries.astype(np.float64):
+        cd = ((cen - q) ** 2).sum(1)
+        probes = np.lexsort((np.arange(len(cd)), cd))[:npc]
+        rows = np.concatenate([np.arange(off[c], off[c + 1]) for c in probes])
+        qs = q - st["offset"].astype(np.float64)
+        sd = ((recon[rows] - qs) ** 2).sum(1)
+        top = rows[np.lexsort((rows, sd))[:R]]
+        ed = ((orig[top] - q) ** 2).sum(1)
+        o = np.lexsort((top, ed))[:k]
+        out_i.append(st["reordered_to_original"][top[o]])
+        out_d.append(ed[o])
+    return np.array(out_i), np.array(out_d)
+
+
+@pytest.mark.parametrize("nq", [1, 7, 64, 300])
+def test_exact_mode_matches_fp64_pipeline(cuda, nq):
+    w = synth.zipf_mixture(40000, 128, nq, c=96, lo=20, hi=4000, seed=nq)
+    st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
+    ix = _ivf(mode="exact")
+    ix.import_state(st)
+    k, npc, R = 100, 12, 300
+    ids, d = ix.search(w.queries, k, 0, npc, R)
+    oi, od = _exact_ivf_oracle(st, w.queries, k, npc, R)
+    from tests.helpers import fp64_dists
+    got = fp64_dists(w.base, w.queries, ids)
+    np.testing.assert_allclose(d, got, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(np.sort(got, 1), od, rtol=1e-5, atol=1e-6)
+    agree = np.mean([len(set(a) & set(b)) / k for a, b in zip(ids, oi)])
+    assert agree > 0.995
+
+
+def test_exact_mode_device_tensors_and_counter(cuda):
+    import torch
+    w = synth.zipf_mixture(20000, 64, 50, c=32, lo=20, hi=2000, seed=3)
+    st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
+    ix = _ivf(mode="exact")
+    ix.import_state(st)
+    qd = torch.from_numpy(w.queries).cuda()
+    a, ad = ix.search(qd, 50, 0, 8, 200)
+    torch.cuda.synchronize()
+    b, bd = ix.search(w.queries, 50, 0, 8, 200)
+    np.testing.assert_array_equal(a.cpu().numpy(), b)
+    np.testing.assert_array_equal(ad.cpu().numpy(), bd)
+    # the counter adds the candidates scanned: the probed lists' sizes
+    off = st["table_offsets"]
+    sizes = np.diff(off)
+    cd = ((st["centroids"][None].astype(np.float64) - w.queries[:, None].astype(np.float64)) ** 2).sum(-1)
+    probes = np.argsort(cd, axis=1, kind="stable")[:, :8]
+    assert ix.total_distances_count() == 2 * int(sizes[probes].sum())
+    ix.reset_distances_count()
+    assert ix.total_distances_count() == 0
+
+
+def test_ivf_errors_and_facade(cuda):
+    from annvedi_b200 import _lib
+    from annvedi_b200.algorithm import Algorithm
+    from annvedi_b200.ivf import IVFIndex
+    w = synth.zipf_mixture(5000, 32, 6, c=16, lo=20, hi=800, seed=1)
+    ix = IVFIndex(device=0)
+    with pytest.raises(RuntimeError):
+        ix.query(w.queries[0], 5)
+    with pytest.raises(NotImplementedError):
+        ix.fit(w.base, 10, 8, 16)
+    ix.fit(w.base, 1, 0, 16, centroids=w.centres, assign=w.assign)
+    with pytest.raises(_lib.AnnUnsupported):
+        ix.query(w.queries[0], 5, n_probes=2)
+    with pytest.raises(RuntimeError):
+        ix.query(w.queries[0][:5], 5)
+    algo = Algorithm()
+    algo.fit(w.base, backend="ivf", n_tables=1, n_bits=0, n_clusters=16)
+    res = algo.query(w.queries[0], 5, n_probe_clusters=4, refine_r=50)
+    assert len(res) == 5 and res.dtype == np.int64
+    assert algo.get_n_distances() > 0
+    algo2 = Algorithm()
+    algo2.fit(w.base, backend="gpu_ivf_sq8", n_clusters=16)
+    assert len(algo2.query(w.queries[1], 10, n_probe_clusters=16)) == 10
+
+
+def test_reference_ivf_unit_test_shape(cuda):
+    """tests/test_lsh.py::test_ivf_lsh_fit_query of the reference (with inverted lists)."""
+    from annvedi_b200.algorithm import Algorithm
+    data = np.random.default_rng(0).random((50, 16), dtype=np.float32)
+    a = Algorithm()
+    a.fit(data, backend="ivf_lsh", n_tables=1, n_bits=0, n_clusters=4)
+    assert len(a.query(data[0], 5)) == 5
