@@ -33,7 +33,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "QPS at recall@100>=0.95 (1M x 384)"
+METRIC = "QPS at recall@100>=0.95 (1M x 384) vs plain FP32 scan, same B200; p50/p99 ms"
 K_NN = 100
 
 
@@ -160,17 +160,31 @@ def ground_truth(base, queries, k):
 
 def recall_evaluator(base, queries, ids, kth):
     """mean(pred_d[:k] <= true_d[k-1]) with FP64 distances (orthogonal-competition/evaluator.py:149-157)."""
+    hits = 0.0
+    for s in range(0, queries.shape[0], 1000):
+        ii = ids[s:s + 1000]
+        ok = ii >= 0
+        x = base[ii.clamp(min=0)].double()
+        d = ((x - queries[s:s + 1000].double()[:, None, :]) ** 2).sum(-1)
+        hits += float(((d <= kth[s:s + 1000, None] * (1 + 1e-9) + 1e-12) & ok).double().sum().item())
+    return hits / ids.numel()
+
+
+def _time_steps(fn, steps, stream):
     import torch
-    ok = ids >= 0
-    x = base[ids.clamp(min=0)].double()
-    d = ((x - queries.double()[:, None, :]) ** 2).sum(-1)
-    hit = (d <= kth[:, None] * (1 + 1e-9) + 1e-12) & ok
-    return float(hit.double().mean().item())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
 
 
 def run_ours(args, rank, world, local):
     import torch
     from annvedi_b200 import _lib
+    from annvedi_b200.ivf import IVFIndex
     from annvedi_b200.linear import LinearIndex
 
     dev = f"cuda:{local}"
@@ -179,82 +193,177 @@ def run_ours(args, rank, world, local):
     w = make_workload(rank, dev, n, d, q)
     base, queries = w.base.contiguous(), w.queries.contiguous()
     hbm_peak, bf16_peak, peak_kind = _peaks()
-
-    ix = LinearIndex(device=local, metric="l2", mode="exact")
-    ix.fit(base)
     stream = torch.cuda.current_stream()
-    out_ids = torch.empty(q, K_NN, dtype=torch.int64, device=dev)
-    out_d = torch.empty(q, K_NN, dtype=torch.float32, device=dev)
+    kth = ground_truth(base, queries, K_NN)
+
+    # ---- the plain FP32 exact scan (the denominator) ----
+    flat = LinearIndex(device=local, metric="l2", mode="exact")
+    flat.fit(base)
+    f_ids = torch.empty(q, K_NN, dtype=torch.int64, device=dev)
+    f_d = torch.empty(q, K_NN, dtype=torch.float32, device=dev)
+
+    def flat_step():
+        flat.search(queries, K_NN, mode="exact", out_ids=f_ids, out_dists=f_d)
+
+    flat_step()
+    torch.cuda.synchronize()
+    flat_recall = recall_evaluator(base, queries[:1000], f_ids[:1000], kth[:1000])
+    flat.reset_profile_results()
+    flat.set_profiling(True)
+    fsteps = max(2, min(args.steps, 3))
+    flat_ms = _time_steps(flat_step, fsteps, stream) / fsteps
+    flat.set_profiling(False)
+    fprof = flat.get_profile_results()
+    flat_qps = q / (flat_ms / 1e3)
+    fscan_ms = fprof["scan_ms"] / max(1, fprof["scan_launches"])
+    fp32_instr = 2.0 * n * d * q  # one sub + one fma per element pair
+    flat_line = {"qps": round(flat_qps, 1), "ms_per_batch": round(flat_ms, 3), "recall_at_100": round(flat_recall, 4),
+                 "kernel": "flat_scan_kernel", "fp32_instr_per_s": round(fp32_instr / (fscan_ms / 1e3), 1)}
+    del flat
+    torch.cuda.empty_cache()
+
+    # ---- IVF-SQ8: lists = the 2,048 L2-normalised generating centres ----
+    ivf = IVFIndex(device=local, mode="exact")
+    t0 = time.perf_counter()
+    ivf.fit(base, 1, 0, 2048, centroids=w.centres)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    o_ids = torch.empty(q, K_NN, dtype=torch.int64, device=dev)
+    o_d = torch.empty(q, K_NN, dtype=torch.float32, device=dev)
+    sweep = []
+    chosen = None
+    for npc in (8, 16, 32, 64, 128):
+        ivf.search(queries, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids, out_dists=o_d)
+        torch.cuda.synchronize()
+        rec = recall_evaluator(base, queries, o_ids, kth)
+        ms = _time_steps(lambda: ivf.search(queries, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids,
+                                            out_dists=o_d), 2, stream) / 2
+        sweep.append({"nprobe": npc, "recall_at_100": round(rec, 4), "qps": round(q / (ms / 1e3), 1)})
+        if chosen is None and rec >= 0.95:
+            chosen = (npc, rec)
+    if chosen is None:
+        chosen = (128, sweep[-1]["recall_at_100"])
+    npc, rec = chosen
 
     def step():
-        ix.search(queries, K_NN, mode="exact", out_ids=out_ids, out_dists=out_d)
+        ivf.search(queries, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids, out_dists=o_d)
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    kth = ground_truth(base, queries[:512], K_NN)
-    rec = recall_evaluator(base, queries[:512], out_ids[:512], kth)
-
     clocks = ClockSampler(local).start()
-    ix.reset_profile_results()
-    ix.set_profiling(True)
+    ivf.reset_profile_results()
+    ivf.reset_distances_count()
+    ivf.set_profiling(True)
     launches0 = _lib.kernel_launches()
     barrier(world)
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize()
+    ms = _time_steps(step, args.steps, stream)
     barrier(world)
     launches = _lib.kernel_launches() - launches0
-    ix.set_profiling(False)
-    prof = ix.get_profile_results()
+    ivf.set_profiling(False)
+    prof = ivf.get_profile_results()
+    cands = ivf.total_distances_count()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms, world)
     qps = world * q * args.steps / (ms_max / 1e3)
 
-    # end to end through the public API with host buffers
-    qh = queries.cpu().numpy()
-    qpin = torch.from_numpy(qh).pin_memory().numpy()
+    # ---- end to end through the public API with host buffers ----
+    qpin = torch.empty(q, d, dtype=torch.float32, pin_memory=True)
+    qpin.copy_(queries)
+    qh = qpin.numpy()
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        ids_h, _ = ix.search(qpin, K_NN, mode="exact", with_dists=False)
-    t1 = time.perf_counter()
-    e2e_s = max_over_ranks(t1 - t0, world)
+        ids_h, _ = ivf.search(qh, K_NN, 0, npc, args.refine, max_candidates=0, with_dists=False)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e_qps = world * q * args.steps / e2e_s
 
-    # roofline of the dominant kernel (the fused scan): per launch, the base once + queries
-    scan_ms = prof["scan_ms"] / max(1, prof["scan_launches"])
-    flops = 3.0 * n * d * q  # sub, mul, add per element pair
-    bytes_alg = 4.0 * n * d + 4.0 * q * d
-    fp32_peak = 148 * 128 * 2 * (clk["sm_mhz"] or 1965.0) * 1e6 / 1e12
+    # ---- batch-1 latency (one query per call) ----
+    lat_dev, lat_host = [], []
+    one_ids = torch.empty(1, K_NN, dtype=torch.int64, device=dev)
+    for i in range(args.latency_queries):
+        qi = queries[i:i + 1]
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ivf.search(qi, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=one_ids, with_dists=False)
+        b.record(stream)
+        b.synchronize()
+        lat_dev.append(a.elapsed_time(b))
+        t1 = time.perf_counter()
+        ivf.search(qh[i:i + 1], K_NN, 0, npc, args.refine, max_candidates=0, with_dists=False)
+        lat_host.append((time.perf_counter() - t1) * 1e3)
+
+    # ---- roofline of the dominant kernel: the SQ8 list scan ----
+    stage = prof.get("stage_ms", {})
+    calls = max(1, prof.get("profiled_calls", 1))
+    sq8_ms = stage.get("sq8", 0.0) / calls
+    bytes_per_launch = (cands / max(1, args.steps)) * d  # codes of every candidate of every query
+    achieved = bytes_per_launch / (sq8_ms / 1e3) / 1e9 if sq8_ms > 0 else 0.0
     line = {
         "metric": METRIC, "value": round(qps, 1), "unit": "queries/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded zipf mixture)",
-        "config": {"workload": "flat_exact_fp32 over 1M x 384 zipf mixture (IVF-SQ8 config data)",
-                   "form": "flat", "n": n, "dim": d, "batch": q, "k": K_NN, "metric": "l2",
-                   "l2": "inputs larger than L2 (1.5 GB base)", "parallelism": f"replicas x{world}"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (sq8 codes, fp32 re-rank)",
+        "data": "synthetic (seeded zipf mixture, 2,048 centres, sigma 0.3, L2-normalised)",
+        "config": {"workload": "ivf_sq8 1M x 384, 10k-query batches, k=100", "form": "ivf-sq8 exact selection",
+                   "n": n, "dim": d, "batch": q, "k": K_NN, "metric": "l2", "n_lists": 2048, "nprobe": npc,
+                   "refine_r": args.refine, "candidate_cap": "none",
+                   "l2": "inputs larger than L2 (1.5 GB rows + 384 MB codes)", "parallelism": f"replicas x{world}"},
         "recall_at_100": round(rec, 4),
+        "speedup_vs_plain_fp32_scan": round(qps / (flat_qps * world), 2),
+        "plain_fp32_scan": flat_line,
+        "nprobe_sweep": sweep,
+        "latency_ms_batch1": {"device_p50": round(float(np.percentile(lat_dev, 50)), 4),
+                              "device_p99": round(float(np.percentile(lat_dev, 99)), 4),
+                              "host_api_p50": round(float(np.percentile(lat_host, 50)), 4),
+                              "host_api_p99": round(float(np.percentile(lat_host, 99)), 4),
+                              "queries": args.latency_queries},
+        "build_s": round(build_s, 3),
+        "candidates_per_query": round(cands / max(1, args.steps) / q, 1),
         "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": q * d * 4,
                 "d2h_bytes_per_step": q * K_NN * 8},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "achieved": round(bytes_alg / (scan_ms / 1e3) / 1e9, 1), "peak": hbm_peak,
-                     "unit": "GB/s", "frac": round(bytes_alg / (scan_ms / 1e3) / 1e9 / hbm_peak, 4),
-                     "traffic": None, "peak_kind": peak_kind, "kernel": "flat_scan_kernel",
-                     "fp32_tflops": round(flops / (scan_ms / 1e3) / 1e12, 2), "fp32_peak_tflops": round(fp32_peak, 1),
-                     "fp32_frac": round(flops / (scan_ms / 1e3) / 1e12 / fp32_peak, 4),
-                     "scan_ms_per_launch": round(scan_ms, 3)},
+        "stage_ms_per_batch": {k2: round(v / calls, 4) for k2, v in stage.items()},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                     "frac": round(achieved / hbm_peak, 4), "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "ivf_sq8_scan_kernel", "bytes_per_launch": int(bytes_per_launch),
+                     "kernel_ms": round(sq8_ms, 4)},
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_linear(base, queries, args)
+        line["cpu_baseline"] = cpu_baseline_ivf(ivf, queries, npc, args)
     return line
+
+
+def _reference_ivf_from(ivf):
+    """The reference's own LSHIndex (oracle/_ref, built from its sources) loaded with this index's
+    state, its ThreadPool sized to every host core as the reference sizes it."""
+    from oracle import refmod
+    mod = refmod.load_ref("ref_ivf_shim")
+    st = ivf.export_state()
+    ix = mod.LSHIndex()
+    mod.import_state(ix, st, os.cpu_count() or 1)
+    return ix, st
+
+
+def cpu_baseline_ivf(ivf, queries, npc, args):
+    """Reference IVF query on the host cores over a bounded sample. refine_r is raised until the
+    reference's candidate cap (max(2000, 4 * refine_r)) no longer truncates the probed lists, so it
+    does the same search (and reaches the same recall) as the GPU form."""
+    ix, st = _reference_ivf_from(ivf)
+    qs = queries[: args.cpu_sample].cpu().numpy()
+    sizes = np.diff(st["table_offsets"])
+    rr = max(args.refine, int(np.ceil(np.sort(sizes)[::-1][:npc].sum() / 4)))
+    ix.query(qs[0], K_NN, 0, npc, rr)
+    t0 = time.perf_counter()
+    for qq in qs:
+        ix.query(qq, K_NN, 0, npc, rr)
+    dt = time.perf_counter() - t0
+    cores = os.cpu_count() or 1
+    return {"value": round(len(qs) / dt, 2), "unit": "queries/s", "cores": cores, "kind": "reference",
+            "sample": f"{len(qs)} queries one at a time (the harness's pattern), ivf_lsh_cpp LSHIndex over this "
+                      f"index's state, n_probe_clusters={npc}, refine_r={rr} (cap lifted), ThreadPool of {cores}"}
 
 
 def cpu_baseline_linear(base, queries, args):
@@ -279,51 +388,62 @@ def cpu_baseline_linear(base, queries, args):
 
 
 def run_reference(args, rank, world):
-    """The reference's own CPU implementation on this host's cores (the reference arm)."""
+    """The reference's own CPU implementation of the path on this host's cores (the reference arm):
+    ivf_lsh_cpp's LSHIndex query over the same lists, one query per call as the harness issues
+    them, its ThreadPool over every core."""
     if rank != 0:
         return None
     import torch
-    from concurrent.futures import ThreadPoolExecutor
-    from oracle import refmod
-    from annvedi_b200 import synth
-    w = synth.zipf_mixture(args.n, args.dim, args.batch, c=2048, sigma=0.3, seed=1234, backend="torch",
-                           device="cpu")
-    xb = w.base.numpy()
-    lin = refmod.load_ref("linear_ann_cpp")
-    ix = lin.LinearIndex()
-    ix.fit(xb)
-    cores = os.cpu_count() or 1
-    nsample = max(cores, 8)
-    qs = list(w.queries[:nsample].numpy())
-    for _ in range(min(args.warmup, 1)):
-        ix.query(qs[0], K_NN)
+    from annvedi_b200 import _lib
+    from annvedi_b200.ivf import IVFIndex
+    if torch.cuda.is_available():
+        w = make_workload(0, "cuda:0", args.n, args.dim, args.batch)
+        ivf = IVFIndex(device=0, mode="exact")
+        ivf.fit(w.base, 1, 0, 2048, centroids=w.centres)
+        queries = w.queries
+    else:
+        return {"impl": "reference", "unavailable": "the IVF state is built on the GPU; no device visible"}
+    del _lib
+    npc = args.ref_nprobe
+    ix, st = _reference_ivf_from(ivf)
+    sizes = np.diff(st["table_offsets"])
+    rr = max(args.refine, int(np.ceil(np.sort(sizes)[::-1][:npc].sum() / 4)))
+    qs = queries[: args.cpu_sample].cpu().numpy()
+    for i in range(min(args.warmup, 3)):
+        ix.query(qs[i % len(qs)], K_NN, 0, npc, rr)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        with ThreadPoolExecutor(cores) as ex:
-            list(ex.map(lambda qq: ix.query(qq, K_NN), qs))
+        for qq in qs:
+            ix.query(qq, K_NN, 0, npc, rr)
         times.append(time.perf_counter() - t0)
     total = sum(times)
-    qps = nsample * args.steps / total
-    del torch
+    qps = len(qs) * args.steps / total
+    cores = os.cpu_count() or 1
+    sample = (f"{len(qs)} queries per step one at a time, ivf_lsh_cpp LSHIndex (oracle/_ref) over the GPU index's "
+              f"state, n_probe_clusters={npc}, refine_r={rr} (cap lifted), ThreadPool of {cores}")
     return {"metric": METRIC, "value": round(qps, 2), "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded zipf mixture)",
-            "config": {"workload": "flat_exact_fp32 over 1M x 384 zipf mixture (IVF-SQ8 config data)",
-                       "form": "flat", "n": args.n, "dim": args.dim, "batch": nsample, "k": K_NN},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (sq8 codes, fp32 re-rank)",
+            "data": "synthetic (seeded zipf mixture, 2,048 centres, sigma 0.3, L2-normalised)",
+            "config": {"workload": "ivf_sq8 1M x 384, 10k-query batches, k=100", "form": "reference cpu",
+                       "n": args.n, "dim": args.dim, "batch": len(qs), "k": K_NN, "nprobe": npc, "refine_r": rr},
             "impl": "reference",
             "cpu_baseline": {"value": round(qps, 2), "unit": "queries/s", "cores": cores, "kind": "reference",
-                             "sample": f"{nsample} queries per step, linear_ann_cpp ({refmod.host_isa()} build)"},
+                             "sample": sample},
             "e2e": {"value": round(qps, 2), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--form", choices=["flat"], default="flat")
+    ap.add_argument("--refine", type=int, default=300)
+    ap.add_argument("--ref-nprobe", type=int, default=32)
+    ap.add_argument("--cpu-sample", type=int, default=64)
+    ap.add_argument("--latency-queries", type=int, default=200)
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--dim", type=int, default=384)
     ap.add_argument("--batch", type=int, default=10_000)
