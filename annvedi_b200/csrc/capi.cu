@@ -14,6 +14,7 @@
 #include "compat.cuh"
 #include "flat_scan.cuh"
 #include "runtime.cuh"
+#include "flat_internal.cuh"
 
 namespace annb {
 
@@ -80,17 +81,6 @@ int ws_reserve_host(ann_workspace* ws, size_t bytes) {
 
 using namespace annb;
 
-struct ann_flat {
-    int device = 0;
-    int64_t n = 0;
-    int dim = 0;
-    int dpad = 0;
-    int metric = ANN_METRIC_L2;
-    float* base = nullptr;  // [n, dpad]
-    std::atomic<int64_t> ndist{0};
-    ann_workspace ws;       // default workspace
-    StageProfiler prof;     // stage 0: scan kernel(s); stage 1: merge / selection
-};
 
 extern "C" {
 
@@ -198,8 +188,10 @@ int ann_flat_fit(ann_flat* h, const float* data, int64_t n, int32_t dim, int64_t
     return ANN_OK;
 }
 
+}  // extern "C"
+
 // Number of row splits for an exact scan of n rows by nq queries in tiles of bq.
-static int choose_nsplit(int64_t n, int nq, int bq, int64_t* rows_per_split) {
+int annb::flat_choose_nsplit(int64_t n, int nq, int bq, int64_t* rows_per_split) {
     const int n_qtiles = (int)ceil_div(nq, bq);
     const int ctas_per_sm = bq <= 8 ? 2 : 1;
     const int64_t target = (int64_t)kNumSMs * ctas_per_sm;
@@ -212,6 +204,8 @@ static int choose_nsplit(int64_t n, int nq, int bq, int64_t* rows_per_split) {
     *rows_per_split = rps;
     return (int)nsplit;
 }
+
+extern "C" {
 
 int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t nq, int64_t ldq, int32_t k,
                    int32_t mode, int32_t mem, int64_t* out_ids, float* out_dists, void* stream) {
@@ -252,7 +246,7 @@ int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t
     }
     if (mode == ANN_MODE_EXACT) {
         bq = std::min(flat_scan_bq(nq), flat_scan_max_bq(kk));
-        nsplit = choose_nsplit(h->n, nq, bq, &rps);
+        nsplit = flat_choose_nsplit(h->n, nq, bq, &rps);
         sz.take<float>((size_t)nq * nsplit * kk);
         sz.take<int>((size_t)nq * nsplit * kk);
     } else {

@@ -1,0 +1,23 @@
+// The flat index handle, shared by the C ABI translation units.
+#pragma once
+#include <atomic>
+
+#include "common.cuh"
+#include "runtime.cuh"
+
+struct ann_flat {
+    int device = 0;
+    int64_t n = 0;
+    int dim = 0;
+    int dpad = 0;
+    int metric = ANN_METRIC_L2;
+    float* base = nullptr;  // [n, dpad]
+    std::atomic<int64_t> ndist{0};
+    ann_workspace ws;       // default workspace
+    annb::StageProfiler prof;     // stage 0: scan kernel(s); stage 1: merge / selection
+};
+
+namespace annb {
+// Number of row splits (and rows per split) for an exact scan of n rows by nq queries in tiles of bq.
+int flat_choose_nsplit(int64_t n, int nq, int bq, int64_t* rows_per_split);
+}  // namespace annb

@@ -97,6 +97,18 @@ int ann_flat_set_profiling(ann_flat* h, int32_t enable);
 int ann_flat_profile(ann_flat* h, double* out4);
 int ann_flat_reset_profile(ann_flat* h);
 
+/* Exact-mode ann_flat_query for callers that cannot let a library allocate device memory (an
+ * application that owns every device allocation through its own pool, or a serving thread that must
+ * not call cudaMalloc/cudaFree because they can synchronise the device). No counterpart in the
+ * reference. Queries and outputs are device pointers on the index's device (ANN_MEM_DEVICE); the
+ * call runs asynchronously on `stream`. Its scratch is a fixed 16 MiB array compiled into the library
+ * (held on every device that loads it until exit); batches needing more scratch are rejected with
+ * ANN_ERR_INVALID. The first call on a device resolves the array's device address (make that call
+ * before any stream capture). All calls share the array: calls that overlap on the GPU race. Adds n
+ * per query to the distance counter, as ann_flat_query does. */
+int ann_flat_query_noalloc(ann_flat* h, const float* queries, int32_t nq, int64_t ldq, int32_t k,
+                           int64_t* out_ids, float* out_dists, void* stream);
+
 /* LinearIndex::total_distances_count (linear_index.cpp:123). */
 int64_t ann_flat_total_distances(const ann_flat* h);
 int32_t ann_flat_dim(const ann_flat* h);
