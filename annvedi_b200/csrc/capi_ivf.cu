@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -28,6 +29,7 @@ struct ann_ivf {
     int32_t* r2o = nullptr;       // [n]
     int64_t* list_off = nullptr;  // [C + 1]
     unsigned long long* d_ndist = nullptr;
+    int* d_err = nullptr;             // set by a kernel whose bounded wait gave up
     std::vector<int64_t> h_list_off;
     std::vector<int64_t> sizes_desc;  // list sizes, largest first (bounds for planning)
     ann_workspace ws;
@@ -91,6 +93,11 @@ static int ivf_finish_lists(ann_ivf* h, cudaStream_t st) {
         if (rc) return rc;
         ANN_CUDA_TRY(cudaMemsetAsync(h->d_ndist, 0, sizeof(unsigned long long), st));
     }
+    if (!h->d_err) {
+        int rc = dmalloc(&h->d_err, 1);
+        if (rc) return rc;
+        ANN_CUDA_TRY(cudaMemsetAsync(h->d_err, 0, sizeof(int), st));
+    }
     return ANN_OK;
 }
 
@@ -151,6 +158,7 @@ int ann_ivf_destroy(ann_ivf* h) {
         DeviceGuard g(h->device);
         ivf_free_state(h);
         if (h->d_ndist) cudaFree(h->d_ndist);
+        if (h->d_err) cudaFree(h->d_err);
         if (h->ws.dev) cudaFree(h->ws.dev);
         if (h->ws.host) cudaFreeHost(h->ws.host);
         h->ws.dev = nullptr;
@@ -173,7 +181,7 @@ int ann_ivf_fit(ann_ivf* h, const float* data, int64_t n, int32_t dim, int64_t l
     cudaStream_t st = as_stream(stream);
     const int C = (int)std::min<int64_t>(n_clusters, n);  // the reference clamps too (:137)
     const int dpad = (int)ceil_div(dim, 32) * 32;
-    const int dpad8 = (int)ceil_div(dim, 32) * 32;
+    const int dpad8 = (int)ceil_div(dim, 128) * 128;  // 16 threads x (multiple of 8) code bytes per row
     ANN_CUDA_TRY(cudaDeviceSynchronize());
     ivf_free_state(h);
     const cudaMemcpyKind kind = mem == ANN_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
@@ -304,7 +312,7 @@ int ann_ivf_import(ann_ivf* h, int64_t n, int32_t dim, int32_t n_clusters, const
     ANN_CUDA_TRY(cudaDeviceSynchronize());
     ivf_free_state(h);
     const int dpad = (int)ceil_div(dim, 32) * 32;
-    const int dpad8 = dpad;
+    const int dpad8 = (int)ceil_div(dim, 128) * 128;
     int rc = ANN_OK;
     if ((rc = dmalloc(&h->centroids, (size_t)n_clusters * dpad)) || (rc = dmalloc(&h->original, (size_t)n * dpad)) ||
         (rc = dmalloc(&h->codes, (size_t)n * dpad8)) || (rc = dmalloc(&h->scale, dpad)) ||
@@ -372,6 +380,13 @@ int ann_ivf_info(const ann_ivf* h, int64_t* out4) {
 }  // extern "C"
 
 namespace {
+
+// The exact-mode SQ8 pass runs the cp.async kernel; ANNB_IVF_SCAN=stream selects the bulk-copy stream
+// kernel instead (slower on list-sharing query batches, kept for comparison).
+const int g_use_stream = [] {
+    const char* v = getenv("ANNB_IVF_SCAN");
+    return (v && std::strcmp(v, "stream") == 0) ? 1 : 0;
+}();
 
 struct IvfQueryCfg {
     int k, npc, R, nsplit, num_threads, bqc, nsplit_c, ncp;
@@ -443,6 +458,8 @@ static int ivf_query_device(ann_ivf* h, const IvfQueryCfg& c, char* base, const 
     a.nsplit = c.nsplit;
     a.num_threads = c.num_threads;
     a.ndist = h->d_ndist;
+    a.err = h->d_err;
+    a.use_stream = g_use_stream;
     a.out_ids = ids_dev;
     a.out_dists = dists_dev;
 
@@ -612,6 +629,21 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
         ANN_CUDA_TRY(cudaStreamSynchronize(st));
         std::memcpy(out_ids, hid, sizeof(int64_t) * (size_t)nq * k);
         if (out_dists) std::memcpy(out_dists, hd, sizeof(float) * (size_t)nq * k);
+        return ann_ivf_device_status(h);
+    }
+    return ANN_OK;
+}
+
+int ann_ivf_device_status(ann_ivf* h) {
+    ANN_CHECK_ARG(h != nullptr, "null index");
+    if (!h->d_err) return ANN_OK;
+    DeviceGuard g(h->device);
+    int v = 0;
+    ANN_CUDA_TRY(cudaMemcpy(&v, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (v) {
+        ANN_CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(int)));
+        set_error("a device-side wait gave up after its time limit; the results of the affected queries are invalid");
+        return ANN_ERR_TIMEOUT;
     }
     return ANN_OK;
 }

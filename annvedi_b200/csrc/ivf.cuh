@@ -52,6 +52,8 @@ struct IvfQueryArgs {
     float* P;                  // reference mode [nq, ncp, L]
     float* V;                  // reference mode [nq, L]
     unsigned long long* ndist; // device counter of candidates scanned (get_n_distances)
+    int* err;                  // device flag: a bounded wait gave up
+    int use_stream;            // exact mode: use the bulk-copy stream kernel where it applies
     int64_t* out_ids;          // [nq, k]
     float* out_dists;          // [nq, k]
 };

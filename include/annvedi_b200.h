@@ -160,6 +160,12 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
                   int32_t n_probes, int32_t n_probe_clusters, int32_t refine_r, int64_t max_candidates, int32_t mode,
                   int32_t num_threads, int32_t mem, int64_t* out_ids, float* out_dists, void* stream);
 
+/* Reads and clears the index's device error flag: ANN_ERR_TIMEOUT if a kernel's bounded wait gave up
+ * since the last check (its queries' results are invalid), else ANN_OK. Synchronous; host-memory
+ * queries check it themselves. No counterpart in the reference (its waits are host condition
+ * variables, src/thread_pool.h:119-122). */
+int ann_ivf_device_status(ann_ivf* h);
+
 /* LSHIndex::total_distances_count / reset_distances_count (lsh_index_optimized.cpp:518-524). */
 int64_t ann_ivf_total_distances(ann_ivf* h);
 int ann_ivf_reset_distances(ann_ivf* h);
