@@ -57,6 +57,32 @@ int ws_reserve_device(ann_workspace* ws, size_t bytes) {
     return ANN_OK;
 }
 
+int ws_reserve_big(ann_workspace* ws, size_t bytes) {
+    std::lock_guard<std::mutex> lk(ws->mu);
+    if (ws->big_cap >= bytes) return ANN_OK;
+    size_t cap = std::max(bytes, ws->big_cap + ws->big_cap / 4);
+    if (ws->big) {
+        ANN_CUDA_TRY(cudaDeviceSynchronize());
+        ANN_CUDA_TRY(cudaFree(ws->big));
+        ws->big = nullptr;
+        ws->big_cap = 0;
+    }
+    cudaError_t e = cudaMalloc(&ws->big, cap);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        e = cudaMalloc(&ws->big, bytes);
+        cap = bytes;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ws->big = nullptr;
+        set_error("workspace: cannot allocate %zu bytes of device scratch (%s)", bytes, cudaGetErrorString(e));
+        return ANN_ERR_NOMEM;
+    }
+    ws->big_cap = cap;
+    return ANN_OK;
+}
+
 int ws_reserve_host(ann_workspace* ws, size_t bytes) {
     std::lock_guard<std::mutex> lk(ws->mu);
     if (ws->host_cap >= bytes) return ANN_OK;
@@ -104,9 +130,11 @@ static void ws_release(ann_workspace* ws) {
     DeviceGuard g(ws->device);
     if (ws->dev) cudaFree(ws->dev);
     if (ws->host) cudaFreeHost(ws->host);
+    if (ws->big) cudaFree(ws->big);
     ws->dev = nullptr;
     ws->host = nullptr;
-    ws->dev_cap = ws->host_cap = 0;
+    ws->big = nullptr;
+    ws->dev_cap = ws->host_cap = ws->big_cap = 0;
 }
 
 int ann_workspace_destroy(ann_workspace* ws) {

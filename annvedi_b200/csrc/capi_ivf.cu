@@ -12,6 +12,7 @@
 #include "common.cuh"
 #include "flat_scan.cuh"
 #include "ivf.cuh"
+#include "ivf_batched.cuh"
 #include "refmath.cuh"
 #include "runtime.cuh"
 
@@ -381,17 +382,23 @@ int ann_ivf_info(const ann_ivf* h, int64_t* out4) {
 
 namespace {
 
-// The exact-mode SQ8 pass runs the cp.async kernel; ANNB_IVF_SCAN=stream selects the bulk-copy stream
-// kernel instead (slower on list-sharing query batches, kept for comparison).
-const int g_use_stream = [] {
+// Exact-mode SQ8 pass: batches of at least kBatchedMinQueries queries run list-major (ivf_batched.cu),
+// smaller ones query by query (ivf.cu). ANNB_IVF_SCAN=cpasync or =stream forces a per-query kernel
+// (for comparisons).
+constexpr int kBatchedMinQueries = 32;
+enum { kScanBatched = 0, kScanCpAsync = 1, kScanStream = 2 };
+const int g_scan_kind = [] {
     const char* v = getenv("ANNB_IVF_SCAN");
-    return (v && std::strcmp(v, "stream") == 0) ? 1 : 0;
+    if (v && std::strcmp(v, "stream") == 0) return (int)kScanStream;
+    if (v && std::strcmp(v, "cpasync") == 0) return (int)kScanCpAsync;
+    return (int)kScanBatched;
 }();
 
 struct IvfQueryCfg {
     int k, npc, R, nsplit, num_threads, bqc, nsplit_c, ncp;
     int64_t max_c, ub, rps_c;
-    bool ref, coarse_flat;
+    bool ref, coarse_flat, batched;
+    size_t sort_tmp, scan_tmp, bscratch;
 };
 
 // Bytes of scratch one device-side query call of nq queries needs (mirrors the carving below).
@@ -414,12 +421,16 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
     sz.take<float>((size_t)nq * c.R);
     sz.take<int>((size_t)nq * c.R);
     if (c.ref) sz.take<float>((size_t)nq * c.ub * (c.ncp + 2));
+    if (c.batched) {
+        sz.take<float>((size_t)nq * h->dpad);
+        sz.take<char>(c.bscratch);
+    }
     return sz.off;
 }
 
 // All stages for nq device-resident padded queries; scratch carved from `base`.
-static int ivf_query_device(ann_ivf* h, const IvfQueryCfg& c, char* base, const float* qdev, int nq,
-                            int64_t* ids_dev, float* dists_dev, cudaStream_t st) {
+static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, char* base, const float* qdev,
+                            int nq, int64_t* ids_dev, float* dists_dev, cudaStream_t st) {
     Carver cv(base);
     int32_t* probes = cv.take<int32_t>((size_t)nq * c.npc);
     int64_t* seg_start = cv.take<int64_t>((size_t)nq * c.npc);
@@ -440,6 +451,8 @@ static int ivf_query_device(ann_ivf* h, const IvfQueryCfg& c, char* base, const 
     float* keyR = cv.take<float>((size_t)nq * c.R);
     int* idR = cv.take<int>((size_t)nq * c.R);
     float* DP = c.ref ? cv.take<float>((size_t)nq * c.ub * (c.ncp + 2)) : nullptr;
+    float* qs = c.batched ? cv.take<float>((size_t)nq * h->dpad) : nullptr;
+    void* bscratch = c.batched ? cv.take<char>(c.bscratch) : nullptr;
 
     IvfQueryArgs a{};
     a.ix = h->view();
@@ -459,7 +472,7 @@ static int ivf_query_device(ann_ivf* h, const IvfQueryCfg& c, char* base, const 
     a.num_threads = c.num_threads;
     a.ndist = h->d_ndist;
     a.err = h->d_err;
-    a.use_stream = g_use_stream;
+    a.use_stream = g_scan_kind == kScanStream;
     a.out_ids = ids_dev;
     a.out_dists = dists_dev;
 
@@ -481,7 +494,21 @@ static int ivf_query_device(ann_ivf* h, const IvfQueryCfg& c, char* base, const 
     if ((rc = launch_ivf_plan(a, st))) return rc;
     h->prof.mark(prec, st);
     // 3. SQ8 pass -> best R per query
-    if (!c.ref) {
+    bool done = false;
+    if (!c.ref && c.batched) {
+        IvfBatchArgs b{};
+        int64_t tot[3] = {0, 0, 0};
+        if ((rc = batched_prepare(a, bscratch, c.sort_tmp, c.scan_tmp, &b, tot, st))) return rc;
+        if (tot[2] == 0) {  // no query fell back to scanning every row
+            if ((rc = ws_reserve_big(ws, sizeof(float) * (size_t)std::max<int64_t>(tot[1], 1)))) return rc;
+            float* D = reinterpret_cast<float*>(ws->big);
+            if ((rc = launch_batched(b, qdev, qs, D, st))) return rc;
+            if ((rc = launch_select_topk(D, 0, n_cands, nq, c.R, &a.plan, keyR, idR, st, b.cand_off))) return rc;
+            done = true;
+        }
+    }
+    if (done) {
+    } else if (!c.ref) {
         a.keyR = keyS;
         a.idR = idS;
         if ((rc = launch_ivf_sq8_scan(a, st))) return rc;
@@ -565,6 +592,7 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     c.ub = std::max<int64_t>(ub, 1);
     c.ncp = ref_num_checkpoints(h->dim);
     c.coarse_flat = !c.ref && c.npc <= 512;
+    c.batched = !c.ref && g_scan_kind == kScanBatched && nq >= kBatchedMinQueries;
     const int dpad = h->dpad;
     const bool host = mem == ANN_MEM_HOST;
 
@@ -582,6 +610,7 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
         c.rps_c = ceil_div(ceil_div(h->C, c.nsplit_c), 256) * 256;
         c.nsplit_c = (int)ceil_div(h->C, c.rps_c);
     }
+    if (c.batched) c.bscratch = batched_scratch_bytes(qc, c.npc, h->C, &c.sort_tmp, &c.scan_tmp);
     Sizer head;
     head.take<float>((size_t)nq * dpad);
     if (host) {
@@ -615,7 +644,7 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     }
     for (int q0 = 0; q0 < nq; q0 += qc) {
         const int nc = std::min(qc, nq - q0);
-        rc = ivf_query_device(h, c, scratch, qdev + (size_t)q0 * dpad, nc, ids_dev + (size_t)q0 * k,
+        rc = ivf_query_device(h, ws, c, scratch, qdev + (size_t)q0 * dpad, nc, ids_dev + (size_t)q0 * k,
                               dists_dev ? dists_dev + (size_t)q0 * k : nullptr, st);
         if (rc) return rc;
     }

@@ -582,9 +582,11 @@ int launch_ivf_ref_sq8(const IvfQueryArgs& a, int64_t Lmax, cudaStream_t st) {
 }
 
 // ---- generic per-query top-k selection over a dense key array -----------------------------------
-// keys[q * ld + p] for p < lens[q] (or ld when lens is null); id = plan_row(q, p) when a plan is
+// keys[q * ld + p] (keys[offs[q] + p] when offs is given) for p < lens[q] (or ld when lens is null);
+// id = plan_row(q, p) when a plan is
 // given, else p. Keeps the best kout (key, id) pairs, sorted, padded with (+inf, INT_MAX).
 __global__ void __launch_bounds__(256) select_topk_kernel(const float* __restrict__ keys, int64_t ld,
+                                                          const int64_t* __restrict__ offs,
                                                           const int64_t* __restrict__ lens, int kout,
                                                           IvfPlan plan, int use_plan, float* out_key,
                                                           int* out_id) {
@@ -598,7 +600,7 @@ __global__ void __launch_bounds__(256) select_topk_kernel(const float* __restric
     const int64_t len = lens ? lens[q] : ld;
     WarpTopK top;
     top.init(sKey + warp * cap, sId + warp * cap, kout);
-    const float* kq = keys + (int64_t)q * ld;
+    const float* kq = keys + (offs ? offs[q] : (int64_t)q * ld);
     for (int64_t base = (int64_t)warp * 32; base < len; base += (int64_t)warps * 32) {
         const int64_t p = base + lane;
         const bool ok = p < len;
@@ -625,7 +627,7 @@ __global__ void __launch_bounds__(256) select_topk_kernel(const float* __restric
 }
 
 int launch_select_topk(const float* keys, int64_t ld, const int64_t* lens, int nq, int kout, const IvfPlan* plan,
-                       float* out_key, int* out_id, cudaStream_t st) {
+                       float* out_key, int* out_id, cudaStream_t st, const int64_t* offs) {
     if (nq == 0) return ANN_OK;
     ANN_CHECK_ARG(kout >= 1 && kout <= 8192, "select: k=%d outside [1, 8192]", kout);
     const size_t per_warp = (size_t)topk_cap(kout) * 8;
@@ -635,7 +637,7 @@ int launch_select_topk(const float* keys, int64_t ld, const int64_t* lens, int n
     ANN_CUDA_TRY(cudaFuncSetAttribute(select_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     IvfPlan p{};
     if (plan) p = *plan;
-    select_topk_kernel<<<nq, warps * 32, smem, st>>>(keys, ld, lens, kout, p, plan ? 1 : 0, out_key, out_id);
+    select_topk_kernel<<<nq, warps * 32, smem, st>>>(keys, ld, offs, lens, kout, p, plan ? 1 : 0, out_key, out_id);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

@@ -15,6 +15,8 @@ struct ann_workspace {
     size_t dev_cap = 0;
     char* host = nullptr;  // pinned
     size_t host_cap = 0;
+    char* big = nullptr;   // second device arena for large per-batch buffers sized after planning
+    size_t big_cap = 0;
     std::mutex mu;         // serialises growth; concurrent calls must still use separate workspaces
 };
 
@@ -38,6 +40,7 @@ struct DeviceGuard {
 // block may be in use by earlier asynchronous work).
 int ws_reserve_device(ann_workspace* ws, size_t bytes);
 int ws_reserve_host(ann_workspace* ws, size_t bytes);
+int ws_reserve_big(ann_workspace* ws, size_t bytes);
 
 // Stage timer: records CUDA events around named stages of a call on its stream; totals are
 // accumulated lazily (collect() synchronises on the recorded events).
