@@ -15,6 +15,8 @@
 #include "flat_scan.cuh"
 #include "runtime.cuh"
 #include "flat_internal.cuh"
+#include "ivf.cuh"
+#include "tc_gemm.cuh"
 
 namespace annb {
 
@@ -173,6 +175,9 @@ int ann_flat_destroy(ann_flat* h) {
     {
         DeviceGuard g(h->device);
         if (h->base) cudaFree(h->base);
+        if (h->base_bf16) cudaFree(h->base_bf16);
+        if (h->norms) cudaFree(h->norms);
+        if (h->d_err) cudaFree(h->d_err);
     }
     ws_release(&h->ws);
     delete h;
@@ -195,6 +200,14 @@ int ann_flat_fit(ann_flat* h, const float* data, int64_t n, int32_t dim, int64_t
         ANN_CUDA_TRY(cudaDeviceSynchronize());
         ANN_CUDA_TRY(cudaFree(h->base));
         h->base = nullptr;
+    }
+    if (h->base_bf16) {
+        ANN_CUDA_TRY(cudaFree(h->base_bf16));
+        h->base_bf16 = nullptr;
+    }
+    if (h->norms) {
+        ANN_CUDA_TRY(cudaFree(h->norms));
+        h->norms = nullptr;
     }
     const size_t bytes = sizeof(float) * (size_t)n * dpad;
     cudaError_t e = cudaMalloc(&h->base, bytes);
@@ -388,6 +401,178 @@ int ann_flat_reset_profile(ann_flat* h) {
     DeviceGuard g(h->device);
     h->prof.reset();
     return ANN_OK;
+}
+
+// BF16 copy of the base (and FP32 row norms) for the tensor-core scan, built once.
+static int flat_ensure_bf16(ann_flat* h, cudaStream_t st) {
+    if (h->base_bf16) return ANN_OK;
+    const int kpad = (int)ceil_div(h->dim, 64) * 64;
+    __nv_bfloat16* b = nullptr;
+    float* nr = nullptr;
+    int* err = nullptr;
+    cudaError_t e = cudaMalloc(&b, sizeof(__nv_bfloat16) * (size_t)h->n * kpad);
+    if (e == cudaSuccess) e = cudaMalloc(&nr, sizeof(float) * (size_t)h->n);
+    if (e == cudaSuccess && !h->d_err) e = cudaMalloc(&err, sizeof(int));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (b) cudaFree(b);
+        if (nr) cudaFree(nr);
+        if (err) cudaFree(err);
+        set_error("tensor-core scan: cannot allocate the BF16 copy of the base (%s)", cudaGetErrorString(e));
+        return ANN_ERR_NOMEM;
+    }
+    if (err) {
+        ANN_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
+        h->d_err = err;
+    }
+    int rc = launch_to_bf16(h->base, h->n, h->dim, h->dpad, b, kpad, nr, st);
+    if (rc) return rc;
+    ANN_CUDA_TRY(cudaStreamSynchronize(st));
+    h->base_bf16 = b;
+    h->norms = nr;
+    h->kpad = kpad;
+    return ANN_OK;
+}
+
+static int flat_check_err(ann_flat* h) {
+    int v = 0;
+    if (!h->d_err) return ANN_OK;
+    ANN_CUDA_TRY(cudaMemcpy(&v, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (v) {
+        ANN_CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(int)));
+        set_error("a device-side wait gave up after its time limit; the results are invalid");
+        return ANN_ERR_TIMEOUT;
+    }
+    return ANN_OK;
+}
+
+int ann_flat_scores_tc(ann_flat* h, const float* queries, int32_t nq, int64_t ldq, float* out_keys, void* stream) {
+    clear_error();
+    ANN_CHECK_ARG(h != nullptr && h->base != nullptr, "ann_flat_scores_tc: index not fitted");
+    ANN_CHECK_ARG(nq >= 0 && ldq >= h->dim && (nq == 0 || (queries && out_keys)), "ann_flat_scores_tc: bad arguments");
+    if (nq == 0) return ANN_OK;
+    DeviceGuard g(h->device);
+    cudaStream_t st = as_stream(stream);
+    int rc = flat_ensure_bf16(h, st);
+    if (rc) return rc;
+    Sizer sz;
+    sz.take<__nv_bfloat16>((size_t)nq * h->kpad);
+    rc = ws_reserve_device(&h->ws, sz.bytes());
+    if (rc) return rc;
+    Carver cv(h->ws.dev);
+    __nv_bfloat16* qb = cv.take<__nv_bfloat16>((size_t)nq * h->kpad);
+    if ((rc = launch_to_bf16(queries, nq, h->dim, ldq, qb, h->kpad, nullptr, st))) return rc;
+    TcGemmArgs a{nq, (int)h->n, h->kpad, nullptr, h->norms, h->metric, out_keys, h->n, h->d_err};
+    if ((rc = launch_tc_gemm(qb, h->base_bf16, a, st))) return rc;
+    ANN_CUDA_TRY(cudaStreamSynchronize(st));
+    return flat_check_err(h);
+}
+
+int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int32_t nq, int64_t ldq, int32_t k,
+                      int32_t refine_r, int32_t mem, int64_t* out_ids, float* out_dists, void* stream) {
+    clear_error();
+    ANN_CHECK_ARG(h != nullptr, "ann_flat_query_tc: null index");
+    if (h->base == nullptr || h->n == 0) {
+        set_error("index not fitted");
+        return ANN_ERR_STATE;
+    }
+    ANN_CHECK_ARG(nq >= 0 && k >= 1, "ann_flat_query_tc: nq=%d, k=%d", nq, k);
+    ANN_CHECK_ARG(ldq >= h->dim, "ann_flat_query_tc: query stride < dim");
+    ANN_CHECK_ARG(nq == 0 || (queries && out_ids), "ann_flat_query_tc: null pointer");
+    if (nq == 0) return ANN_OK;
+    const int kk = (int)std::min<int64_t>(k, h->n);
+    const int R = (int)std::min<int64_t>(std::max(kk, refine_r > 0 ? refine_r : 4 * kk), h->n);
+    ANN_CHECK_ARG(kk <= 1024 && R <= 8192, "ann_flat_query_tc: k=%d, refine %d too large", kk, R);
+    if (!ws) ws = &h->ws;
+    DeviceGuard g(h->device);
+    cudaStream_t st = as_stream(stream);
+    int rc = flat_ensure_bf16(h, st);
+    if (rc) return rc;
+    const int dpad = h->dpad, kpad = h->kpad;
+    const bool host = mem == ANN_MEM_HOST;
+    // key matrix chunk: queries per pass bounded by ~4 GB of FP32 keys
+    const size_t budget = (size_t)4 << 30;
+    int qc = (int)std::max<int64_t>(128, (int64_t)(budget / (sizeof(float) * (size_t)h->n)) / 128 * 128);
+    qc = std::min(qc, nq);
+    Sizer sz;
+    sz.take<float>((size_t)nq * dpad);
+    sz.take<__nv_bfloat16>((size_t)nq * kpad);
+    sz.take<float>((size_t)nq * R);
+    sz.take<int>((size_t)nq * R);
+    if (host) {
+        sz.take<int64_t>((size_t)nq * kk);
+        sz.take<float>((size_t)nq * kk);
+    }
+    if ((rc = ws_reserve_device(ws, sz.bytes()))) return rc;
+    if ((rc = ws_reserve_big(ws, sizeof(float) * (size_t)qc * h->n))) return rc;
+    Carver cv(ws->dev);
+    float* qdev = cv.take<float>((size_t)nq * dpad);
+    __nv_bfloat16* qb = cv.take<__nv_bfloat16>((size_t)nq * kpad);
+    float* keyR = cv.take<float>((size_t)nq * R);
+    int* idR = cv.take<int>((size_t)nq * R);
+    int64_t* ids_dev = out_ids;
+    float* dists_dev = out_dists;
+    if (host) {
+        ids_dev = cv.take<int64_t>((size_t)nq * kk);
+        dists_dev = cv.take<float>((size_t)nq * kk);
+        if ((rc = ws_reserve_host(ws, std::max(sizeof(float) * (size_t)nq * dpad, (sizeof(int64_t) + 4) * (size_t)nq * kk))))
+            return rc;
+        float* hq = reinterpret_cast<float*>(ws->host);
+        for (int i = 0; i < nq; ++i) {
+            std::memcpy(hq + (size_t)i * dpad, queries + (size_t)i * ldq, sizeof(float) * h->dim);
+            if (dpad > h->dim) std::memset(hq + (size_t)i * dpad + h->dim, 0, sizeof(float) * (dpad - h->dim));
+        }
+        ANN_CUDA_TRY(cudaMemcpyAsync(qdev, hq, sizeof(float) * (size_t)nq * dpad, cudaMemcpyHostToDevice, st));
+    } else {
+        if ((rc = launch_pad_rows(queries, nq, h->dim, ldq, qdev, dpad, st))) return rc;
+    }
+    if ((rc = launch_to_bf16(qdev, nq, h->dim, dpad, qb, kpad, nullptr, st))) return rc;
+    float* keys = reinterpret_cast<float*>(ws->big);
+    const int prec = h->prof.begin(st);
+    for (int q0 = 0; q0 < nq; q0 += qc) {
+        const int nc = std::min(qc, nq - q0);
+        TcGemmArgs a{nc, (int)h->n, kpad, nullptr, h->norms, h->metric, keys, h->n, h->d_err};
+        if ((rc = launch_tc_gemm(qb + (size_t)q0 * kpad, h->base_bf16, a, st))) return rc;
+        if ((rc = launch_select_topk(keys, h->n, nullptr, nc, R, nullptr, keyR + (size_t)q0 * R, idR + (size_t)q0 * R, st)))
+            return rc;
+    }
+    h->prof.mark(prec, st);
+    IvfQueryArgs ra{};
+    ra.ix.n = h->n;
+    ra.ix.dim = h->dim;
+    ra.ix.dpad = dpad;
+    ra.ix.original = h->base;
+    ra.ix.r2o = nullptr;
+    ra.plan.nq = nq;
+    ra.q = qdev;
+    ra.ldq = dpad;
+    ra.k = kk;
+    ra.R = R;
+    ra.metric = h->metric;
+    ra.out_ids = ids_dev;
+    ra.out_dists = dists_dev;
+    if ((rc = launch_ivf_rerank(ra, keyR, idR, 0, st))) return rc;
+    h->prof.mark(prec, st);
+    if (prec >= 0) h->prof.launches += 1;
+    h->ndist.fetch_add(h->n * (int64_t)nq);
+    if (host) {
+        int64_t* hid = reinterpret_cast<int64_t*>(ws->host);
+        float* hd = reinterpret_cast<float*>(ws->host + sizeof(int64_t) * (size_t)nq * kk);
+        ANN_CUDA_TRY(cudaMemcpyAsync(hid, ids_dev, sizeof(int64_t) * (size_t)nq * kk, cudaMemcpyDeviceToHost, st));
+        if (out_dists)
+            ANN_CUDA_TRY(cudaMemcpyAsync(hd, dists_dev, sizeof(float) * (size_t)nq * kk, cudaMemcpyDeviceToHost, st));
+        ANN_CUDA_TRY(cudaStreamSynchronize(st));
+        std::memcpy(out_ids, hid, sizeof(int64_t) * (size_t)nq * kk);
+        if (out_dists) std::memcpy(out_dists, hd, sizeof(float) * (size_t)nq * kk);
+        return flat_check_err(h);
+    }
+    return ANN_OK;
+}
+
+int ann_flat_device_status(ann_flat* h) {
+    ANN_CHECK_ARG(h != nullptr, "null index");
+    DeviceGuard g(h->device);
+    return flat_check_err(h);
 }
 
 int64_t ann_flat_total_distances(const ann_flat* h) { return h ? h->ndist.load() : 0; }

@@ -2,6 +2,8 @@
 #pragma once
 #include <atomic>
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 #include "runtime.cuh"
 
@@ -15,6 +17,10 @@ struct ann_flat {
     std::atomic<int64_t> ndist{0};
     ann_workspace ws;       // default workspace
     annb::StageProfiler prof;     // stage 0: scan kernel(s); stage 1: merge / selection
+    __nv_bfloat16* base_bf16 = nullptr;  // [n, kpad] BF16 copy for the tensor-core scan (built on first use)
+    float* norms = nullptr;              // [n] squared FP32 norms of the rows
+    int kpad = 0;                        // dim rounded up to 64
+    int* d_err = nullptr;                // device flag of bounded waits
 };
 
 namespace annb {

@@ -683,16 +683,23 @@ __global__ void __launch_bounds__(256) ivf_rerank_kernel(IvfQueryArgs a, const f
                 for (int d = lane * 4; d < dpad; d += 128) {
                     const float4 xv = *reinterpret_cast<const float4*>(x + d);
                     const float4 q4 = *reinterpret_cast<const float4*>(sQ + d);
-                    const float d0 = xv.x - q4.x, d1 = xv.y - q4.y, d2 = xv.z - q4.z, d3 = xv.w - q4.w;
-                    acc = fmaf(d0, d0, acc);
-                    acc = fmaf(d1, d1, acc);
-                    acc = fmaf(d2, d2, acc);
-                    acc = fmaf(d3, d3, acc);
+                    if (a.metric == ANN_METRIC_IP) {
+                        acc = fmaf(xv.x, q4.x, acc);
+                        acc = fmaf(xv.y, q4.y, acc);
+                        acc = fmaf(xv.z, q4.z, acc);
+                        acc = fmaf(xv.w, q4.w, acc);
+                    } else {
+                        const float d0 = xv.x - q4.x, d1 = xv.y - q4.y, d2 = xv.z - q4.z, d3 = xv.w - q4.w;
+                        acc = fmaf(d0, d0, acc);
+                        acc = fmaf(d1, d1, acc);
+                        acc = fmaf(d2, d2, acc);
+                        acc = fmaf(d3, d3, acc);
+                    }
                 }
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane == 0) sD[e] = row != kNoId ? acc : kInf;
+            if (lane == 0) sD[e] = row != kNoId ? (a.metric == ANN_METRIC_IP ? -acc : acc) : kInf;
         }
     }
     __syncthreads();
@@ -707,8 +714,10 @@ __global__ void __launch_bounds__(256) ivf_rerank_kernel(IvfQueryArgs a, const f
         top.compact();
         for (int e = lane; e < k; e += 32) {
             const bool ok = e < top.count;
-            a.out_ids[(int64_t)q * k + e] = ok ? (int64_t)a.ix.r2o[sId[e]] : -1;
-            if (a.out_dists) a.out_dists[(int64_t)q * k + e] = ok ? sKey[e] : kInf;
+            a.out_ids[(int64_t)q * k + e] = ok ? (int64_t)(a.ix.r2o ? a.ix.r2o[sId[e]] : sId[e]) : -1;
+            if (a.out_dists)
+                a.out_dists[(int64_t)q * k + e] =
+                    ok ? (a.metric == ANN_METRIC_IP ? -sKey[e] : sKey[e]) : (a.metric == ANN_METRIC_IP ? -kInf : kInf);
         }
     }
 }

@@ -141,6 +141,46 @@ class LinearIndex:
                                             _lib.MEM_HOST, _lib.ptr(ids), _lib.ptr(dists), None))
         return ids, dists
 
+    def search_tc(self, queries, k: int, refine_r: int = -1, workspace: Workspace | None = None, out_ids=None,
+                  out_dists=None, stream=None, with_dists: bool = True):
+        """Tensor-core form: BF16 tcgen05 scores for every row, the best R = max(k, refine_r > 0 ?
+        refine_r : 4k) per query re-ranked with exact FP32 distances (inner products for metric "ip")."""
+        if self._n == 0:
+            raise RuntimeError("index not fitted")
+        k = int(k)
+        if k < 1:
+            raise RuntimeError("k must be >= 1")
+        kk = min(k, self._n)
+        ws = workspace.handle if workspace is not None else None
+        if _lib.is_torch(queries) and queries.is_cuda:
+            import torch
+            x = _lib.as_f32_2d(queries, "queries")
+            nq = x.shape[0]
+            if out_ids is None:
+                out_ids = torch.empty(nq, kk, dtype=torch.int64, device=x.device)
+            if out_dists is None and with_dists:
+                out_dists = torch.empty(nq, kk, dtype=torch.float32, device=x.device)
+            _lib.check(self._lib.ann_flat_query_tc(self._h, ws, _lib.ptr(x), nq, x.stride(0), kk, int(refine_r),
+                                                   _lib.MEM_DEVICE, _lib.ptr(out_ids), _lib.ptr(out_dists),
+                                                   _lib.stream_ptr(x, stream)))
+            return out_ids, out_dists
+        x = _lib.as_f32_2d(queries.numpy() if _lib.is_torch(queries) else queries, "queries")
+        nq = x.shape[0]
+        ids = np.empty((nq, kk), np.int64)
+        dists = np.empty((nq, kk), np.float32) if with_dists else None
+        _lib.check(self._lib.ann_flat_query_tc(self._h, ws, _lib.ptr(x), nq, x.shape[1], kk, int(refine_r),
+                                               _lib.MEM_HOST, _lib.ptr(ids), _lib.ptr(dists), None))
+        return ids, dists
+
+    def scores_tc(self, queries):
+        """Diagnostic: the tensor-core key matrix [nq, N] (device tensor in, device tensor out)."""
+        import torch
+        x = _lib.as_f32_2d(queries, "queries")
+        out = torch.empty(x.shape[0], self._n, dtype=torch.float32, device=x.device)
+        _lib.check(self._lib.ann_flat_scores_tc(self._h, _lib.ptr(x), x.shape[0], x.stride(0), _lib.ptr(out),
+                                                _lib.stream_ptr(x)))
+        return out
+
     # ---- profiling (CUDA events on the query stream) ---------------------------------------
     def set_profiling(self, enable: bool = True) -> None:
         _lib.check(self._lib.ann_flat_set_profiling(self._h, int(enable)))

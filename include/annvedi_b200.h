@@ -97,6 +97,20 @@ int ann_flat_set_profiling(ann_flat* h, int32_t enable);
 int ann_flat_profile(ann_flat* h, double* out4);
 int ann_flat_reset_profile(ann_flat* h);
 
+/* Tensor-core form of ann_flat_query (no counterpart in the reference; the reference's only fast scan
+ * is its CPU loop): keys for every (query, row) from a BF16 tcgen05 GEMM with FP32 accumulation
+ * (|x|^2 - 2 x.q for L2, -x.q for inner product; the base is copied to BF16 once, on first use), the
+ * best R = max(k, refine_r > 0 ? refine_r : 4k) rows per query by that key, then their exact FP32
+ * distances (or inner products) re-ranked to the final k. Same outputs and counter as ann_flat_query. */
+int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int32_t nq, int64_t ldq, int32_t k,
+                      int32_t refine_r, int32_t mem, int64_t* out_ids, float* out_dists, void* stream);
+
+/* Diagnostic: the tensor-core key matrix out_keys[nq][n] (device pointers; synchronous). */
+int ann_flat_scores_tc(ann_flat* h, const float* queries, int32_t nq, int64_t ldq, float* out_keys, void* stream);
+
+/* Reads and clears the index's device error flag (ANN_ERR_TIMEOUT if a bounded device wait gave up). */
+int ann_flat_device_status(ann_flat* h);
+
 /* Exact-mode ann_flat_query for callers that cannot let a library allocate device memory (an
  * application that owns every device allocation through its own pool, or a serving thread that must
  * not call cudaMalloc/cudaFree because they can synchronise the device). No counterpart in the

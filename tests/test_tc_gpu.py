@@ -1,0 +1,70 @@
+"""The tensor-core (tcgen05, BF16 in / FP32 accumulate) scan through the C ABI.
+
+1. The raw key matrix equals a torch FP32 computation on the same BF16-rounded operands (the only
+   difference is summation order), including partial 128 x 256 tiles and padded dimensions.
+2. The full form (BF16 keys -> best R -> exact FP32 re-rank) returns exact FP32 distances for its ids,
+   and its ids match the FP64 exact top-k up to ties when the re-rank depth covers the BF16 error.
+"""
+import numpy as np
+import pytest
+
+from annvedi_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref_keys(base, queries, metric):
+    import torch
+    xb = base.to(torch.bfloat16).float()
+    qb = queries.to(torch.bfloat16).float()
+    dot = qb @ xb.T
+    if metric == "ip":
+        return -dot
+    return (base.float() ** 2).sum(1)[None, :] - 2.0 * dot
+
+
+@pytest.mark.parametrize("n,dim,nq", [(1000, 100, 200), (300, 64, 130), (5000, 384, 256), (4096, 768, 64)])
+@pytest.mark.parametrize("metric", ["l2", "ip"])
+def test_tc_key_matrix(cuda, n, dim, nq, metric):
+    import torch
+    from annvedi_b200.linear import LinearIndex
+    w = synth.flat_normal(n, dim, nq, seed=n + dim)
+    base = torch.from_numpy(w.base).cuda()
+    q = torch.from_numpy(w.queries).cuda()
+    ix = LinearIndex(device=0, metric=metric, mode="exact")
+    ix.fit(base)
+    keys = ix.scores_tc(q)
+    torch.cuda.synchronize()
+    ref = _ref_keys(base, q, metric)
+    err = (keys - ref).abs().max().item()
+    assert err < 2e-4, f"max |key - ref| = {err}"
+
+
+@pytest.mark.parametrize("metric", ["l2", "ip"])
+def test_tc_search_matches_exact(cuda, metric):
+    from oracle.refmod import exact_topk_f64
+    from tests.helpers import check_exact_topk
+    from annvedi_b200.linear import LinearIndex
+    w = synth.mixture(30000, 256, 64, c=64, sigma=0.35, seed=11, metric=metric)
+    ix = LinearIndex(device=0, metric=metric, mode="exact")
+    ix.fit(w.base)
+    ids, d = ix.search_tc(w.queries, 50, refine_r=1000)
+    check_exact_topk(w.base, w.queries, ids, d, 50, metric=metric)
+    # a shallow re-rank still finds nearly all of the exact top-k on this data
+    ids2, _ = ix.search_tc(w.queries, 50, refine_r=100)
+    gt, _ = exact_topk_f64(w.base, w.queries, 50, metric)
+    assert np.mean([len(set(a) & set(b)) / 50 for a, b in zip(ids2, gt)]) > 0.97
+    assert ix.total_distances_count() == 2 * 30000 * 64
+
+
+def test_tc_device_and_host_agree(cuda):
+    import torch
+    from annvedi_b200.linear import LinearIndex
+    w = synth.flat_normal(20000, 384, 40, seed=2)
+    ix = LinearIndex(device=0, mode="exact")
+    ix.fit(torch.from_numpy(w.base).cuda())
+    a, ad = ix.search_tc(torch.from_numpy(w.queries).cuda(), 20)
+    torch.cuda.synchronize()
+    b, bd = ix.search_tc(w.queries, 20)
+    np.testing.assert_array_equal(a.cpu().numpy(), b)
+    np.testing.assert_array_equal(ad.cpu().numpy(), bd)
