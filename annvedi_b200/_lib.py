@@ -78,6 +78,7 @@ SIGNATURES = [
     ("ann_flat_set_profiling", ctypes.c_int, [_vp, _i32]),
     ("ann_flat_profile", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     ("ann_flat_reset_profile", ctypes.c_int, [_vp]),
+    ("ann_flat_profile_stages", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     ("ann_flat_total_distances", _i64, [_vp]),
     ("ann_flat_dim", _i32, [_vp]),
     ("ann_flat_size", _i64, [_vp]),

@@ -17,6 +17,8 @@
 #include "flat_internal.cuh"
 #include "ivf.cuh"
 #include "tc_gemm.cuh"
+#include "tc_search.cuh"
+#include "radix_select.cuh"
 
 namespace annb {
 
@@ -176,7 +178,6 @@ int ann_flat_destroy(ann_flat* h) {
         DeviceGuard g(h->device);
         if (h->base) cudaFree(h->base);
         if (h->base_bf16) cudaFree(h->base_bf16);
-        if (h->norms) cudaFree(h->norms);
         if (h->d_err) cudaFree(h->d_err);
     }
     ws_release(&h->ws);
@@ -204,10 +205,6 @@ int ann_flat_fit(ann_flat* h, const float* data, int64_t n, int32_t dim, int64_t
     if (h->base_bf16) {
         ANN_CUDA_TRY(cudaFree(h->base_bf16));
         h->base_bf16 = nullptr;
-    }
-    if (h->norms) {
-        ANN_CUDA_TRY(cudaFree(h->norms));
-        h->norms = nullptr;
     }
     const size_t bytes = sizeof(float) * (size_t)n * dpad;
     cudaError_t e = cudaMalloc(&h->base, bytes);
@@ -396,6 +393,17 @@ int ann_flat_profile(ann_flat* h, double* out4) {
     return ANN_OK;
 }
 
+int ann_flat_profile_stages(ann_flat* h, double* out8) {
+    ANN_CHECK_ARG(h != nullptr && out8 != nullptr, "null argument");
+    DeviceGuard g(h->device);
+    h->prof.collect();
+    for (int i = 0; i < 5; ++i) out8[i] = h->prof.total_ms[i];
+    out8[5] = (double)h->prof.launches;
+    out8[6] = (double)h->prof.tc_launches;
+    out8[7] = (double)h->prof.calls;
+    return ANN_OK;
+}
+
 int ann_flat_reset_profile(ann_flat* h) {
     ANN_CHECK_ARG(h != nullptr, "null index");
     DeviceGuard g(h->device);
@@ -403,20 +411,18 @@ int ann_flat_reset_profile(ann_flat* h) {
     return ANN_OK;
 }
 
-// BF16 copy of the base (and FP32 row norms) for the tensor-core scan, built once.
+// BF16 operand form of the base for the tensor-core scan (key columns included, rows in the Weyl
+// order of tc_row_mult), built once.
 static int flat_ensure_bf16(ann_flat* h, cudaStream_t st) {
     if (h->base_bf16) return ANN_OK;
-    const int kpad = (int)ceil_div(h->dim, 64) * 64;
+    const int kpad = tc_kpad(h->dim, h->metric);
     __nv_bfloat16* b = nullptr;
-    float* nr = nullptr;
     int* err = nullptr;
     cudaError_t e = cudaMalloc(&b, sizeof(__nv_bfloat16) * (size_t)h->n * kpad);
-    if (e == cudaSuccess) e = cudaMalloc(&nr, sizeof(float) * (size_t)h->n);
     if (e == cudaSuccess && !h->d_err) e = cudaMalloc(&err, sizeof(int));
     if (e != cudaSuccess) {
         cudaGetLastError();
         if (b) cudaFree(b);
-        if (nr) cudaFree(nr);
         if (err) cudaFree(err);
         set_error("tensor-core scan: cannot allocate the BF16 copy of the base (%s)", cudaGetErrorString(e));
         return ANN_ERR_NOMEM;
@@ -425,11 +431,12 @@ static int flat_ensure_bf16(ann_flat* h, cudaStream_t st) {
         ANN_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
         h->d_err = err;
     }
-    int rc = launch_to_bf16(h->base, h->n, h->dim, h->dpad, b, kpad, nr, st);
+    const int64_t mult = tc_row_mult(h->n);
+    int rc = launch_tc_operand(h->base, h->n, h->dim, h->dpad, b, kpad, kTcBase, h->metric, mult, st);
     if (rc) return rc;
     ANN_CUDA_TRY(cudaStreamSynchronize(st));
     h->base_bf16 = b;
-    h->norms = nr;
+    h->row_mult = mult;
     h->kpad = kpad;
     return ANN_OK;
 }
@@ -457,13 +464,15 @@ int ann_flat_scores_tc(ann_flat* h, const float* queries, int32_t nq, int64_t ld
     if (rc) return rc;
     Sizer sz;
     sz.take<__nv_bfloat16>((size_t)nq * h->kpad);
-    rc = ws_reserve_device(&h->ws, sz.bytes());
-    if (rc) return rc;
+    if ((rc = ws_reserve_device(&h->ws, sz.bytes()))) return rc;
+    if ((rc = ws_reserve_big(&h->ws, sizeof(float) * (size_t)nq * h->n))) return rc;
     Carver cv(h->ws.dev);
     __nv_bfloat16* qb = cv.take<__nv_bfloat16>((size_t)nq * h->kpad);
-    if ((rc = launch_to_bf16(queries, nq, h->dim, ldq, qb, h->kpad, nullptr, st))) return rc;
-    TcGemmArgs a{nq, (int)h->n, h->kpad, nullptr, h->norms, h->metric, out_keys, h->n, h->d_err};
+    float* tmp = reinterpret_cast<float*>(h->ws.big);
+    if ((rc = launch_tc_operand(queries, nq, h->dim, ldq, qb, h->kpad, kTcQuery, h->metric, 0, st))) return rc;
+    TcGemmArgs a{nq, (int)h->n, h->kpad, nullptr, tmp, h->n, h->d_err};
     if ((rc = launch_tc_gemm(qb, h->base_bf16, a, st))) return rc;
+    if ((rc = launch_tc_unpermute(tmp, nq, h->n, h->row_mult, out_keys, st))) return rc;
     ANN_CUDA_TRY(cudaStreamSynchronize(st));
     return flat_check_err(h);
 }
@@ -490,10 +499,6 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
     if (rc) return rc;
     const int dpad = h->dpad, kpad = h->kpad;
     const bool host = mem == ANN_MEM_HOST;
-    // key matrix chunk: queries per pass bounded by ~4 GB of FP32 keys
-    const size_t budget = (size_t)4 << 30;
-    int qc = (int)std::max<int64_t>(128, (int64_t)(budget / (sizeof(float) * (size_t)h->n)) / 128 * 128);
-    qc = std::min(qc, nq);
     Sizer sz;
     sz.take<float>((size_t)nq * dpad);
     sz.take<__nv_bfloat16>((size_t)nq * kpad);
@@ -504,7 +509,6 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
         sz.take<float>((size_t)nq * kk);
     }
     if ((rc = ws_reserve_device(ws, sz.bytes()))) return rc;
-    if ((rc = ws_reserve_big(ws, sizeof(float) * (size_t)qc * h->n))) return rc;
     Carver cv(ws->dev);
     float* qdev = cv.take<float>((size_t)nq * dpad);
     __nv_bfloat16* qb = cv.take<__nv_bfloat16>((size_t)nq * kpad);
@@ -526,17 +530,166 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
     } else {
         if ((rc = launch_pad_rows(queries, nq, h->dim, ldq, qdev, dpad, st))) return rc;
     }
-    if ((rc = launch_to_bf16(qdev, nq, h->dim, dpad, qb, kpad, nullptr, st))) return rc;
-    float* keys = reinterpret_cast<float*>(ws->big);
-    const int prec = h->prof.begin(st);
+    if ((rc = launch_tc_operand(qdev, nq, h->dim, dpad, qb, kpad, kTcQuery, h->metric, 0, st))) return rc;
+    // Sampled bars: keys over a strided sample of S positions of the BF16 copy (an even sample of the
+    // base, by its row order) give each query two bars. The safe bar, its R-th best sampled key, is at
+    // or above its R-th best key over all rows (about n * R / S keys pass it). The fast bar, its rF-th
+    // best sampled key with rF ~ 3 R S / n, lets about 3 R keys pass. The full pass keeps the keys
+    // under the fast bar; a query with fewer than R survivors (the count is exact) is re-run under its
+    // safe bar, so every query ends with its best R keys among its survivors. Small bases, or a
+    // survivor overflow, use the full key matrix.
+    const int64_t n = h->n;
+    const int64_t full_tiles = n / 256;
+    const int64_t want_tiles = std::max<int64_t>(128, ceil_div(16 * (int64_t)R, 256));
+    const bool sampled = full_tiles >= 4 * want_tiles;
+    const int stride = sampled ? (int)(full_tiles / want_tiles) : 1;
+    const int64_t S = sampled ? (full_tiles / stride) * 256 : 0;
+    const int rF = sampled ? (int)std::min<int64_t>(R, std::max<int64_t>(1, ceil_div(3 * (int64_t)R * S, n))) : 0;
+    constexpr int kRerunBatch = 128;
+    // queries per chunk: ~2 GB of sampled keys, or ~4 GB of full key matrix
+    const int64_t qfull64 = std::max<int64_t>(128, ((int64_t)4 << 30) / (int64_t)(sizeof(float) * n) / 128 * 128);
+    const int qfull = (int)std::min<int64_t>(qfull64, 65535);
+    const int qmax = sampled ? (int)std::clamp<int64_t>(((int64_t)2 << 30) / (4 * S) / 128 * 128, 128, 8192) : qfull;
+    const int nchunks = (int)ceil_div(nq, qmax);
+    const int qc = (int)std::min<int64_t>(qmax, ceil_div(ceil_div(nq, nchunks), 128) * 128);
     for (int q0 = 0; q0 < nq; q0 += qc) {
         const int nc = std::min(qc, nq - q0);
-        TcGemmArgs a{nc, (int)h->n, kpad, nullptr, h->norms, h->metric, keys, h->n, h->d_err};
-        if ((rc = launch_tc_gemm(qb + (size_t)q0 * kpad, h->base_bf16, a, st))) return rc;
-        if ((rc = launch_select_topk(keys, h->n, nullptr, nc, R, nullptr, keyR + (size_t)q0 * R, idR + (size_t)q0 * R, st)))
-            return rc;
+        const __nv_bfloat16* qbc = qb + (size_t)q0 * kpad;
+        float* keyRc = keyR + (size_t)q0 * R;
+        int* idRc = idR + (size_t)q0 * R;
+        bool done = false;
+        if (sampled) {
+            const int nwarps = tc_filter_warps(nc, (int)n);
+            const int64_t main_total = ceil_div((int64_t)nc * rF * n, S);
+            const int64_t rerun_total = ceil_div((int64_t)std::min(nc, kRerunBatch) * R * n, S);
+            const int64_t wcap64 = 4 * ceil_div(std::max(main_total, rerun_total), nwarps) + 1024;
+            const int wcap = (int)std::min<int64_t>(wcap64, INT32_MAX / std::max(1, nwarps));
+            const size_t ent = (size_t)nwarps * wcap;
+            Sizer s2;
+            s2.take<float>((size_t)nc * S);            // sample keys
+            s2.take<float>(ent);                       // survivors: key, column, row
+            s2.take<int>(ent);
+            s2.take<int>(ent);
+            s2.take<float>(ent);                       // grouped: key, id
+            s2.take<int>(ent);
+            s2.take<int>((size_t)nwarps);              // warp counts
+            for (int i = 0; i < 3; ++i) s2.take<float>((size_t)nc);  // fast, safe, gathered bars
+            for (int i = 0; i < 3; ++i) s2.take<int>((size_t)nc);    // row counts, cursors, re-run list
+            s2.take<int64_t>((size_t)nc);              // stream offsets
+            s2.take<int>(4);                           // flags
+            s2.take<__nv_bfloat16>((size_t)kRerunBatch * kpad);
+            if ((rc = ws_reserve_big(ws, s2.bytes()))) return rc;
+            Carver cb(ws->big);
+            float* kA = cb.take<float>((size_t)nc * S);
+            float* fkey = cb.take<float>(ent);
+            int* fcol = cb.take<int>(ent);
+            int* frow = cb.take<int>(ent);
+            float* gkey = cb.take<float>(ent);
+            int* gid = cb.take<int>(ent);
+            int* wcnt = cb.take<int>((size_t)nwarps);
+            float* tauF = cb.take<float>((size_t)nc);
+            float* tauS = cb.take<float>((size_t)nc);
+            float* tau2 = cb.take<float>((size_t)nc);
+            int* rowcnt = cb.take<int>((size_t)nc);
+            int* cursor = cb.take<int>((size_t)nc);
+            int* list = cb.take<int>((size_t)nc);
+            int64_t* offs = cb.take<int64_t>((size_t)nc);
+            int* flags = cb.take<int>(4);
+            __nv_bfloat16* A2 = cb.take<__nv_bfloat16>((size_t)kRerunBatch * kpad);
+
+            const int prec = h->prof.begin(st, 2);  // stages 2: tensor-core passes, 3: selections
+            TcGemmArgs sa{nc, (int)S, kpad, nullptr, kA, S, h->d_err};
+            sa.b_tile_stride = stride;
+            sa.b_rows = n;
+            if ((rc = launch_tc_gemm(qbc, h->base_bf16, sa, st))) return rc;
+            if (sample_bars_smem((int)S) <= kSampleBarsMaxSmem) {
+                if ((rc = launch_sample_bars(kA, (int)S, nc, rF, R, tauF, tauS, st))) return rc;
+            } else {
+                RadixSelectArgs bar{};
+                bar.keys = kA;
+                bar.ld = S;
+                bar.R = rF;
+                bar.out_kth = tauF;
+                bar.R2 = R;
+                bar.out_kth2 = tauS;
+                bar.kth_upper = 1;
+                if ((rc = launch_radix_select(bar, nc, st))) return rc;
+            }
+            auto filter = [&](const __nv_bfloat16* A, int M, const float* tau) -> int {
+                TcGemmArgs fa{M, (int)n, kpad, nullptr, nullptr, n, h->d_err};
+                fa.tau = tau;
+                fa.fkey = fkey;
+                fa.fcol = fcol;
+                fa.frow = frow;
+                fa.wcount = wcnt;
+                fa.wcap = wcap;
+                int r = launch_tc_gemm(A, h->base_bf16, fa, st);
+                if (r) return r;
+                TcGroupArgs ga{fkey, fcol, frow, wcnt, tc_filter_warps(M, (int)n), wcap, M, n, h->row_mult,
+                               rowcnt, offs, cursor, gkey, gid, flags + 1};
+                return launch_tc_group(ga, st);
+            };
+            if ((rc = filter(qbc, nc, tauF))) return rc;
+            h->prof.mark(prec, st);
+            ANN_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int), st));
+            if ((rc = launch_tc_bar_check(rowcnt, nc, R, list, flags, st))) return rc;
+            int hf[2] = {0, 0};  // re-runs, largest warp count
+            ANN_CUDA_TRY(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
+            ANN_CUDA_TRY(cudaStreamSynchronize(st));
+            int ngemm = 2;
+            if (hf[1] <= wcap) {
+                RadixSelectArgs sv{};
+                sv.keys = gkey;
+                sv.ld = (int64_t)ent;
+                sv.offs = offs;
+                sv.lens32 = rowcnt;
+                sv.ids = gid;
+                sv.R = R;
+                sv.out_key = keyRc;
+                sv.out_id = idRc;
+                if ((rc = launch_radix_select(sv, nc, st))) return rc;
+                done = true;
+                for (int j0 = 0; j0 < hf[0] && done; j0 += kRerunBatch) {
+                    const int nb = std::min(kRerunBatch, hf[0] - j0);
+                    if ((rc = launch_tc_gather(qbc, kpad, list + j0, nb, tauS, A2, tau2, st))) return rc;
+                    if ((rc = filter(A2, nb, tau2))) return rc;
+                    ++ngemm;
+                    int hmax = 0;
+                    ANN_CUDA_TRY(cudaMemcpyAsync(&hmax, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+                    ANN_CUDA_TRY(cudaStreamSynchronize(st));
+                    if (hmax > wcap) {
+                        done = false;
+                        break;
+                    }
+                    RadixSelectArgs sv2 = sv;
+                    sv2.out_rows = list + j0;
+                    if ((rc = launch_radix_select(sv2, nb, st))) return rc;
+                }
+            }
+            h->prof.mark(prec, st);
+            if (prec >= 0) h->prof.tc_launches += ngemm;
+        }
+        for (int f0 = 0; !done && f0 < nc; f0 += qfull) {  // the full key matrix, qfull queries at a time
+            const int nf = std::min(qfull, nc - f0);
+            if ((rc = ws_reserve_big(ws, sizeof(float) * (size_t)nf * n))) return rc;
+            float* keys = reinterpret_cast<float*>(ws->big);
+            const int prec = h->prof.begin(st, 2);
+            TcGemmArgs a{nf, (int)n, kpad, nullptr, keys, n, h->d_err};
+            if ((rc = launch_tc_gemm(qbc + (size_t)f0 * kpad, h->base_bf16, a, st))) return rc;
+            h->prof.mark(prec, st);
+            RadixSelectArgs fs{};
+            fs.keys = keys;
+            fs.ld = n;
+            fs.R = R;
+            fs.out_key = keyRc + (size_t)f0 * R;
+            fs.out_id = idRc + (size_t)f0 * R;
+            if ((rc = launch_radix_select(fs, nf, st))) return rc;
+            if ((rc = launch_tc_map_ids(fs.out_id, (int64_t)nf * R, n, h->row_mult, st))) return rc;
+            h->prof.mark(prec, st);
+            if (prec >= 0) h->prof.tc_launches += 1;
+        }
     }
-    h->prof.mark(prec, st);
+    const int prec = h->prof.begin(st, 4);  // stage 4: re-rank
     IvfQueryArgs ra{};
     ra.ix.n = h->n;
     ra.ix.dim = h->dim;
@@ -553,7 +706,6 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
     ra.out_dists = dists_dev;
     if ((rc = launch_ivf_rerank(ra, keyR, idR, 0, st))) return rc;
     h->prof.mark(prec, st);
-    if (prec >= 0) h->prof.launches += 1;
     h->ndist.fetch_add(h->n * (int64_t)nq);
     if (host) {
         int64_t* hid = reinterpret_cast<int64_t*>(ws->host);

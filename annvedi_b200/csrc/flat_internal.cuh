@@ -17,9 +17,9 @@ struct ann_flat {
     std::atomic<int64_t> ndist{0};
     ann_workspace ws;       // default workspace
     annb::StageProfiler prof;     // stage 0: scan kernel(s); stage 1: merge / selection
-    __nv_bfloat16* base_bf16 = nullptr;  // [n, kpad] BF16 copy for the tensor-core scan (built on first use)
-    float* norms = nullptr;              // [n] squared FP32 norms of the rows
-    int kpad = 0;                        // dim rounded up to 64
+    __nv_bfloat16* base_bf16 = nullptr;  // [n, kpad] BF16 operand form for the tensor-core scan (built on first use)
+    int64_t row_mult = 1;                // position p of base_bf16 holds row (p * row_mult) mod n
+    int kpad = 0;                        // operand columns: dim plus the key columns, rounded up to 64
     int* d_err = nullptr;                // device flag of bounded waits
 };
 

@@ -33,22 +33,6 @@ __device__ __forceinline__ void cp_async16_ivf(void* smem, const void* gmem, boo
 __device__ __forceinline__ void cp_async_commit_ivf() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all_ivf() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// Position p of query q's candidate stream -> list-order row.
-__device__ __forceinline__ int64_t plan_row(const IvfPlan& p, int q, int64_t pos) {
-    const int ns = p.n_seg[q];
-    if (ns < 0) return pos;
-    const int64_t* pref = p.seg_pref + (int64_t)q * (p.npc + 1);
-    int lo = 0, hi = ns - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (pref[mid] <= pos)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return p.seg_start[(int64_t)q * p.npc + lo] + (pos - pref[lo]);
-}
-
 // ---- 2. plan ---------------------------------------------------------------------------------
 __global__ void ivf_plan_kernel(IvfQueryArgs a) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;

@@ -34,6 +34,22 @@ struct IvfPlan {
     int64_t* n_cands;          // [nq]
 };
 
+// Position p of query q's candidate stream -> list-order row.
+__device__ __forceinline__ int64_t plan_row(const IvfPlan& p, int q, int64_t pos) {
+    const int ns = p.n_seg[q];
+    if (ns < 0) return pos;
+    const int64_t* pref = p.seg_pref + (int64_t)q * (p.npc + 1);
+    int lo = 0, hi = ns - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pref[mid] <= pos)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return p.seg_start[(int64_t)q * p.npc + lo] + (pos - pref[lo]);
+}
+
 struct IvfQueryArgs {
     IvfView ix;
     IvfPlan plan;

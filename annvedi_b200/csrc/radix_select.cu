@@ -1,0 +1,339 @@
+// Per-query radix selection: the R smallest keys of a long stream, as an unsorted set, or just the
+// R-th smallest key (a bar).
+//
+// Used where only the set of the best R matters (the candidates an exact FP32 re-rank will sort) or
+// only a bar. One CTA per query: histogram passes over the order-preserving integer image of the float
+// keys (11, 11 and 10 bits) narrow down the R-th smallest key t; a final pass collects every key < t
+// and, in stream order, as many keys == t as fill the set to R. Each pass reads the query's keys once
+// (coalesced); histograms live in shared memory. A second rank R2 can be resolved in the same passes
+// (a second histogram follows its own prefix). With kth_upper set and no set wanted, two passes
+// suffice: the bar reported is the upper edge of the 22-bit bin that holds the R-th key, which is at or
+// above that key and within 2^-13 of it relative to the key.
+#include "common.cuh"
+#include "ivf.cuh"
+#include "radix_select.cuh"
+
+namespace annb {
+
+namespace {
+
+__device__ __forceinline__ uint32_t ord(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float unord(uint32_t t) {
+    const float f = __uint_as_float((t & 0x80000000u) ? (t & 0x7fffffffu) : ~t);
+    return isnan(f) ? kInf : f;
+}
+
+constexpr int kThreads = 512;
+constexpr int kBins = 2048;
+
+// The bin holding the rank-th smallest (0-based) element of the histogram, and the count of elements
+// in lower bins. Whole block.
+__device__ int find_bin(const int* hist, int rank, int* below, int* sScan) {
+    constexpr int per = kBins / kThreads;
+    int local = 0;
+#pragma unroll
+    for (int i = 0; i < per; ++i) local += hist[threadIdx.x * per + i];
+    sScan[threadIdx.x] = local;
+    __syncthreads();
+    for (int off = 1; off < kThreads; off <<= 1) {
+        const int v = threadIdx.x >= off ? sScan[threadIdx.x - off] : 0;
+        __syncthreads();
+        sScan[threadIdx.x] += v;
+        __syncthreads();
+    }
+    const int incl = sScan[threadIdx.x];
+    const int excl = incl - local;
+    __shared__ int sBin, sBelow;
+    if (rank >= excl && rank < incl) {
+        int c = excl;
+#pragma unroll
+        for (int i = 0; i < per; ++i) {
+            const int h = hist[threadIdx.x * per + i];
+            if (rank < c + h) {
+                sBin = threadIdx.x * per + i;
+                sBelow = c;
+                break;
+            }
+            c += h;
+        }
+    }
+    __syncthreads();
+    *below = sBelow;
+    const int bin = sBin;
+    __syncthreads();
+    return bin;
+}
+
+__global__ void __launch_bounds__(kThreads) radix_select_kernel(RadixSelectArgs a) {
+    __shared__ int hist[2][kBins];
+    __shared__ int sScan[kThreads];
+    __shared__ int sCount, sTies;
+    const int q = blockIdx.x;
+    const int64_t off = a.offs ? a.offs[q] : (int64_t)q * a.ld;
+    int64_t len = a.lens ? a.lens[q] : a.ld;
+    if (a.lens32) len = min((int64_t)a.lens32[q], a.ld);
+    const float* kq = a.keys + off;
+    const int R = a.R;
+    const int64_t orow = a.out_rows ? a.out_rows[q] : q;
+    float* ok = a.out_key ? a.out_key + orow * R : nullptr;
+    int* oi = a.out_id ? a.out_id + orow * R : nullptr;
+    const bool two = a.out_kth2 != nullptr;
+    const bool want_set = ok || oi;
+
+    auto id_of = [&](int64_t p) -> int {
+        if (a.ids) return a.ids[off + p];
+        if (a.use_plan) return (int)plan_row(a.plan, q, p);
+        return (int)p;
+    };
+
+    if (len <= R && (!two || len <= a.R2)) {  // everything is in the set; no bar below +inf
+        for (int64_t p = threadIdx.x; p < R && want_set; p += kThreads) {
+            const bool v = p < len;
+            if (ok) ok[p] = v ? kq[p] : kInf;
+            if (oi) oi[p] = v ? id_of(p) : kNoId;
+        }
+        if (threadIdx.x == 0) {
+            if (a.out_kth) a.out_kth[orow] = kInf;
+            if (two) a.out_kth2[orow] = kInf;
+        }
+        return;
+    }
+    const int npass = (a.kth_upper && !want_set) ? 2 : 3;
+    uint32_t prefix[2] = {0, 0}, mask = 0;
+    int rank[2] = {(int)min((int64_t)R, len) - 1, two ? (int)min((int64_t)a.R2, len) - 1 : 0};
+    int below_total = 0;
+    for (int pass = 0; pass < npass; ++pass) {
+        const int sh = pass == 0 ? 21 : (pass == 1 ? 10 : 0);
+        const uint32_t dmask = pass == 2 ? 0x3FFu : 0x7FFu;
+        for (int i = threadIdx.x; i < kBins; i += kThreads) {
+            hist[0][i] = 0;
+            hist[1][i] = 0;
+        }
+        __syncthreads();
+        for (int64_t p = threadIdx.x; p < len; p += kThreads) {
+            const uint32_t o = ord(kq[p]);
+            if ((o & mask) == prefix[0]) atomicAdd(&hist[0][(o >> sh) & dmask], 1);
+            if (two && (o & mask) == prefix[1]) atomicAdd(&hist[1][(o >> sh) & dmask], 1);
+        }
+        __syncthreads();
+        for (int j = 0; j < (two ? 2 : 1); ++j) {
+            int below = 0;
+            const int bin = find_bin(hist[j], rank[j], &below, sScan);
+            rank[j] -= below;
+            if (j == 0) below_total += below;
+            prefix[j] |= (uint32_t)bin << sh;
+        }
+        mask |= dmask << sh;
+    }
+    const uint32_t low = npass == 2 ? 0x3FFu : 0u;  // upper edge of the last bin
+    if (threadIdx.x == 0) {
+        if (a.out_kth) a.out_kth[orow] = len >= R ? unord(prefix[0] | low) : kInf;
+        if (two) a.out_kth2[orow] = len >= a.R2 ? unord(prefix[1] | low) : kInf;
+    }
+    if (!want_set) return;
+    // collect: all keys < t, then keys == t in stream order up to R (fewer than R keys: all, padded)
+    const uint32_t t = prefix[0];
+    const int need_ties = R - below_total;
+    if (threadIdx.x == 0) {
+        sCount = 0;
+        sTies = 0;
+    }
+    __syncthreads();
+    for (int64_t p = threadIdx.x; p < len; p += kThreads) {
+        const float kv = kq[p];
+        const uint32_t o = ord(kv);
+        int slot = -1;
+        if (o < t) {
+            slot = atomicAdd(&sCount, 1);
+        } else if (o == t) {
+            const int tie = atomicAdd(&sTies, 1);
+            if (tie < need_ties) slot = below_total + tie;
+        }
+        if (slot >= 0 && slot < R) {
+            if (ok) ok[slot] = kv;
+            if (oi) oi[slot] = id_of(p);
+        }
+    }
+    for (int64_t p = len + threadIdx.x; p < R; p += kThreads) {
+        if (ok) ok[p] = kInf;
+        if (oi) oi[p] = kNoId;
+    }
+}
+
+// ---- bars from a resident row of sampled keys ----------------------------------------------------
+// One CTA per query holds its S keys in shared memory. Level 1: 2048 linear bins over [min, max]; the
+// bins holding the r1-th and r2-th smallest keys are found; level 2 splits each of those bins into 2048
+// linear sub-bins. The bar is the largest key of the bins at or below the chosen (bin, sub-bin): the
+// binning is monotone in the key, so exactly the keys <= that bar are counted below it, at least r of
+// them (a bar at or above the r-th smallest key, within a sub-bin of it).
+constexpr int kBarThreads = 1024;
+
+__device__ __forceinline__ int lin_bin(float k, float lo, float scale) {
+    const float f = (k - lo) * scale;  // NaN (0 * inf) counts as bin 0
+    return !(f > 0.f) ? 0 : (f >= (float)(kBins - 1) ? kBins - 1 : (int)f);
+}
+
+// rank-th smallest (0-based) bin of a histogram over kBins, kBarThreads threads.
+__device__ int find_bin_bar(const int* hist, int rank, int* below, int* sScan) {
+    constexpr int per = kBins / kBarThreads;
+    int local = 0;
+#pragma unroll
+    for (int i = 0; i < per; ++i) local += hist[threadIdx.x * per + i];
+    sScan[threadIdx.x] = local;
+    __syncthreads();
+    for (int off = 1; off < kBarThreads; off <<= 1) {
+        const int v = threadIdx.x >= off ? sScan[threadIdx.x - off] : 0;
+        __syncthreads();
+        sScan[threadIdx.x] += v;
+        __syncthreads();
+    }
+    const int incl = sScan[threadIdx.x];
+    const int excl = incl - local;
+    __shared__ int sBin, sBelow;
+    if (rank >= excl && rank < incl) {
+        int c = excl;
+#pragma unroll
+        for (int i = 0; i < per; ++i) {
+            const int h = hist[threadIdx.x * per + i];
+            if (rank < c + h) {
+                sBin = threadIdx.x * per + i;
+                sBelow = c;
+                break;
+            }
+            c += h;
+        }
+    }
+    __syncthreads();
+    *below = sBelow;
+    const int bin = sBin;
+    __syncthreads();
+    return bin;
+}
+
+__device__ float block_reduce(float v, bool is_max, float* sRed) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = is_max ? fmaxf(v, w) : fminf(v, w);
+    }
+    if ((threadIdx.x & 31) == 0) sRed[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = sRed[threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float w = __shfl_xor_sync(0xffffffffu, v, o);
+            v = is_max ? fmaxf(v, w) : fminf(v, w);
+        }
+        if (threadIdx.x == 0) sRed[32] = v;
+    }
+    __syncthreads();
+    const float r = sRed[32];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kBarThreads) sample_bars_kernel(const float* __restrict__ keys, int S, int r1,
+                                                                  int r2, float* bar1, float* bar2) {
+    extern __shared__ __align__(16) float sK[];  // [S]
+    __shared__ int hist[2][kBins];
+    __shared__ uint32_t smax[2][kBins];          // ordered image of the largest key per level-2 bin
+    __shared__ int sScan[kBarThreads];
+    __shared__ float sRed[33];
+    const int q = blockIdx.x;
+    const float4* src = reinterpret_cast<const float4*>(keys + (int64_t)q * S);
+    float4* sK4 = reinterpret_cast<float4*>(sK);
+    const int S4 = S / 4;
+    float lo = kInf, hi = -kInf;
+    for (int i = threadIdx.x; i < S4; i += kBarThreads) {
+        const float4 v = src[i];
+        sK4[i] = v;
+        lo = fminf(lo, fminf(fminf(v.x, v.y), fminf(v.z, v.w)));
+        hi = fmaxf(hi, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+    }
+    for (int i = threadIdx.x; i < kBins; i += kBarThreads) {
+        hist[0][i] = 0;
+        hist[1][i] = 0;
+        smax[0][i] = 0;
+        smax[1][i] = 0;
+    }
+    lo = block_reduce(lo, false, sRed);  // (synchronises, so the stores above are visible)
+    hi = block_reduce(hi, true, sRed);
+    const int rank[2] = {min(r1, S) - 1, min(r2, S) - 1};
+    if (!(hi > lo) || !isfinite((float)kBins / (hi - lo))) {  // all keys equal, or a range too narrow to bin
+        if (threadIdx.x == 0) {
+            bar1[q] = hi;
+            bar2[q] = hi;
+        }
+        return;
+    }
+    const float scale1 = (float)kBins / (hi - lo);
+    for (int i = threadIdx.x; i < S4; i += kBarThreads) {
+        const float4 v = sK4[i];
+        atomicAdd(&hist[0][lin_bin(v.x, lo, scale1)], 1);
+        atomicAdd(&hist[0][lin_bin(v.y, lo, scale1)], 1);
+        atomicAdd(&hist[0][lin_bin(v.z, lo, scale1)], 1);
+        atomicAdd(&hist[0][lin_bin(v.w, lo, scale1)], 1);
+    }
+    __syncthreads();
+    int b[2], rr[2];
+    for (int j = 0; j < 2; ++j) {
+        int below = 0;
+        b[j] = find_bin_bar(hist[0], rank[j], &below, sScan);
+        rr[j] = rank[j] - below;
+    }
+    for (int i = threadIdx.x; i < kBins; i += kBarThreads) hist[0][i] = 0;
+    __syncthreads();
+    // level 2 inside each chosen bin, with the largest key of every sub-bin
+    const float w = (hi - lo) / (float)kBins;
+    const float lo2[2] = {lo + w * (float)b[0], lo + w * (float)b[1]};
+    const float scale2 = (float)kBins / w;
+    for (int i = threadIdx.x; i < S; i += kBarThreads) {
+        const float k = sK[i];
+        const int bk = lin_bin(k, lo, scale1);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            if (bk == b[j]) {
+                const int sb = lin_bin(k, lo2[j], scale2);
+                atomicAdd(&hist[j][sb], 1);
+                atomicMax(&smax[j][sb], ord(k));
+            }
+        }
+    }
+    __syncthreads();
+    for (int j = 0; j < 2; ++j) {
+        int below = 0;
+        const int sb = find_bin_bar(hist[j], rr[j], &below, sScan);
+        // keys of bins below b[j], and of sub-bins below sb, are all smaller than those of sub-bin sb
+        if (threadIdx.x == 0) (j ? bar2 : bar1)[q] = unord(smax[j][sb]);
+    }
+}
+
+}  // namespace
+
+size_t sample_bars_smem(int S) { return sizeof(float) * (size_t)S; }
+
+int launch_sample_bars(const float* keys, int S, int nq, int r1, int r2, float* bar1, float* bar2, cudaStream_t st) {
+    if (nq == 0) return ANN_OK;
+    ANN_CHECK_ARG(S > 0 && S % 4 == 0 && sample_bars_smem(S) <= kSampleBarsMaxSmem && r1 >= 1 && r2 >= 1,
+                  "sample bars: S=%d, ranks %d, %d", S, r1, r2);
+    const int smem = (int)sample_bars_smem(S);
+    ANN_CUDA_TRY(cudaFuncSetAttribute(sample_bars_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    sample_bars_kernel<<<nq, kBarThreads, smem, st>>>(keys, S, r1, r2, bar1, bar2);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int launch_radix_select(const RadixSelectArgs& a, int nq, cudaStream_t st) {
+    if (nq == 0) return ANN_OK;
+    ANN_CHECK_ARG(a.R >= 1 && (a.out_kth2 == nullptr || a.R2 >= 1), "radix select: R=%d, R2=%d", a.R, a.R2);
+    ANN_CHECK_ARG(a.keys != nullptr && a.ld >= 0, "radix select: no keys");
+    radix_select_kernel<<<nq, kThreads, 0, st>>>(a);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+}  // namespace annb

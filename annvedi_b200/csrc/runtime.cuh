@@ -42,19 +42,22 @@ int ws_reserve_device(ann_workspace* ws, size_t bytes);
 int ws_reserve_host(ann_workspace* ws, size_t bytes);
 int ws_reserve_big(ann_workspace* ws, size_t bytes);
 
-// Stage timer: records CUDA events around named stages of a call on its stream; totals are
-// accumulated lazily (collect() synchronises on the recorded events).
+// Stage timer: records CUDA events around consecutive stages of a call on its stream; totals are
+// accumulated lazily (collect() synchronises on the recorded events). A call's first stage index is
+// chosen at begin(), so different call kinds report into different slots of one table.
 struct StageProfiler {
-    static constexpr int kStages = 4;
+    static constexpr int kStages = 6;
     bool enabled = false;
     struct Rec {
         cudaEvent_t ev[kStages + 1];
+        int first;
         int nstage;
     };
     std::vector<Rec> pending;
     std::vector<cudaEvent_t> pool;
-    double total_ms[kStages] = {0, 0, 0, 0};
-    int64_t launches = 0;
+    double total_ms[kStages] = {0, 0, 0, 0, 0, 0};
+    int64_t launches = 0;     // exact-scan launches
+    int64_t tc_launches = 0;  // tensor-core GEMM launches
     int64_t calls = 0;
     std::mutex mu;
 
@@ -68,11 +71,12 @@ struct StageProfiler {
         cudaEventCreate(&e);
         return e;
     }
-    // begin(): returns a record index; mark(rec, stage) after each stage
-    int begin(cudaStream_t st) {
+    // begin(): returns a record index; mark(rec) closes the next stage, starting at first_stage
+    int begin(cudaStream_t st, int first_stage = 0) {
         if (!enabled) return -1;
         std::lock_guard<std::mutex> lk(mu);
         Rec r{};
+        r.first = first_stage;
         r.nstage = 0;
         r.ev[0] = get_event();
         cudaEventRecord(r.ev[0], st);
@@ -83,7 +87,7 @@ struct StageProfiler {
         if (rec < 0) return;
         std::lock_guard<std::mutex> lk(mu);
         Rec& r = pending[rec];
-        if (r.nstage >= kStages) return;
+        if (r.first + r.nstage >= kStages) return;
         r.ev[++r.nstage] = get_event();
         cudaEventRecord(r.ev[r.nstage], st);
     }
@@ -94,7 +98,7 @@ struct StageProfiler {
                 cudaEventSynchronize(r.ev[s + 1]);
                 float ms = 0.f;
                 cudaEventElapsedTime(&ms, r.ev[s], r.ev[s + 1]);
-                total_ms[s] += ms;
+                total_ms[r.first + s] += ms;
             }
             for (int s = 0; s <= r.nstage; ++s) pool.push_back(r.ev[s]);
             calls += 1;
@@ -106,6 +110,7 @@ struct StageProfiler {
         std::lock_guard<std::mutex> lk(mu);
         for (double& t : total_ms) t = 0;
         launches = 0;
+        tc_launches = 0;
         calls = 0;
     }
     ~StageProfiler() {

@@ -1,8 +1,9 @@
 // BF16 distance GEMM on the 5th-generation tensor cores (tcgen05 + TMA + TMEM) for sm_100a.
 //
-// keys[m][n] = f(sum_k A[m][k] * B[n][k]) with A = queries [M, K] and B = base rows [N, K], both BF16
-// row-major (K-major for the MMA), FP32 accumulation; f gives the ranking key: for squared L2,
-// |b_n|^2 - 2 a.b (+ |a_m|^2) from FP32 norms; for inner product, -a.b (smaller is better).
+// keys[m][n] = sum_k A[m][k] * B[n][k] with A = queries [M, K] and B = base rows [N, K], both BF16
+// row-major (K-major for the MMA), FP32 accumulation. The operands carry the key (tc_gemm.cuh): for
+// squared L2 three extra columns add |b|^2 split into BF16 pieces against a query side scaled by -2,
+// so the accumulator holds |b|^2 - 2 a.b and the epilogue does no arithmetic per key.
 //
 // Structure (one CTA per SM, persistent over 128 x 256 output tiles, query tiles fastest so a base
 // tile is fetched from HBM once and reused from L2 by the query tiles that follow it):
@@ -11,8 +12,11 @@
 //   warp 1    allocates 512 TMEM columns (two 128 x 256 FP32 accumulators) and, from one thread,
 //             issues tcgen05.mma (kind::f16, BF16 in, FP32 out, M = 128, N = 256, K = 16 per
 //             instruction, 4 per stage); tcgen05.commit frees each stage and publishes each tile;
-//   warps 2-5 epilogue: tcgen05.ld 32 columns at a time from the warp's 32 TMEM lanes, apply f,
-//             store the keys, release the accumulator.
+//   warps 2-9 epilogue, two warps per TMEM lane quarter (warp w reads lanes 32 * (w % 4)), each
+//             taking half of the 256 columns: tcgen05.ld 2 x 32 columns per wait, then either store
+//             the keys (transposed through shared memory into coalesced rows) or, in filter mode,
+//             one predicate test per key against the row's bar; survivors go to the warp's own
+//             region at slots from a warp prefix sum (no atomics, nothing waits on memory).
 // Every mbarrier wait is bounded (about 2 s); a timeout raises a device flag and the CTA winds down.
 #include <cuda.h>
 
@@ -91,8 +95,9 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
                  : "memory");
 }
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
+// tcgen05.ld of 32 consecutive columns of the warp's 32 lanes; the registers are valid only after
+// tmem_wait (which names them, so no use is scheduled before the wait).
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,"
         "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
@@ -101,12 +106,33 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
           "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
           "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_wait(uint32_t (&r)[32]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]),
+                   "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]),
+                   "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+                 :
+                 : "memory");
+}
+// Orders a second register set after the wait already issued for the first.
+__device__ __forceinline__ void tmem_after_wait(uint32_t (&r)[32]) {
+    asm volatile(""
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]),
+                   "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]),
+                   "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+                 :
+                 : "memory");
 }
 
-__global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 64 + 32 * kEpiWarps;
+
+__global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
                                                          const __grid_constant__ CUtensorMap tmB, TcGemmArgs a) {
     extern __shared__ unsigned char smem_raw[];
     // 1024-byte alignment for the swizzled tiles
@@ -119,6 +145,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
     uint64_t* tempty = tfull + 2;
     uint64_t* done = tempty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    float* sT = reinterpret_cast<float*>(smem + kStages * (kABytes + kBBytes) + 256);  // [8 warps][32][33]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = (int)ceil_div(a.M, kBM), nt = (int)ceil_div(a.N, kBN), kt = a.K / kBK;
@@ -131,7 +158,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
         }
         for (int b = 0; b < 2; ++b) {
             bar_init(&tfull[b], 1);
-            bar_init(&tempty[b], 128);
+            bar_init(&tempty[b], 32 * kEpiWarps);
         }
         bar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -159,7 +186,7 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
                     if (!(ok = bar_wait(&empty[s], ph ^ 1u, a.err))) break;
                     bar_expect(&full[s], kABytes + kBBytes);
                     tma_load_2d(sA + s * kABytes, &tmA, kb * kBK, m0, &full[s]);
-                    tma_load_2d(sB + s * kBBytes, &tmB, kb * kBK, n0, &full[s]);
+                    tma_load_2d(sB + s * kBBytes, &tmB, kb * kBK, n0 * a.b_tile_stride, &full[s]);
                 }
             }
         }
@@ -190,8 +217,13 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
             mma_commit(done);
             bar_wait(done, 0, nullptr);
         }
-    } else {  // epilogue warps 2..5: TMEM lanes 32 * (warp % 4) ...
+    } else {  // epilogue warps 2..9
         const int lane_base = 32 * (warp & 3);
+        const int ew = warp - 2;
+        const int col0 = 128 * (ew >> 2);  // this warp's half of the tile's columns
+        float* tw = sT + ew * 32 * 33;
+        const int64_t wbase = ((int64_t)blockIdx.x * kEpiWarps + ew) * a.wcap;
+        int wcount = 0;  // survivors met by this warp (uniform across the warp)
         int64_t acc = 0;
         for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x, ++acc) {
             const int b = (int)(acc & 1);
@@ -200,38 +232,73 @@ __global__ void __launch_bounds__(192, 1) tc_gemm_kernel(const __grid_constant__
             const int m0 = (int)(t % mt) * kBM, n0 = (int)(t / mt) * kBN;
             const int m = m0 + lane_base + lane;
             const float an = (a.normA && m < a.M) ? a.normA[m] : 0.f;
-            for (int c = 0; c < kBN / 32; ++c) {
-                float v[32];
-                tmem_ld32(tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kBN + c * 32), v);
-                const int nb = n0 + c * 32;
-                if (m < a.M) {
-                    float* orow = a.out + (int64_t)m * a.ldo;
+            // rows past M (TMA zero fill) get a bar no key passes
+            const float tau = (a.tau && m < a.M) ? a.tau[m] : -kInf;
+            const uint32_t tbase = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kBN + col0);
+#pragma unroll 1
+            for (int c = 0; c < 128; c += 64) {
+                uint32_t r0[32], r1[32];
+                tmem_ld32(tbase + (uint32_t)c, r0);
+                tmem_ld32(tbase + (uint32_t)(c + 32), r1);
+                tmem_wait(r0);
+                tmem_after_wait(r1);
 #pragma unroll
-                    for (int j = 0; j < 32; j += 4) {
-                        float4 o;
-                        float* op = &o.x;
+                for (int h = 0; h < 2; ++h) {
+                    float v[32];
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const int n = nb + j + u;
-                            const float dot = v[j + u];
-                            float key;
-                            if (a.metric == ANN_METRIC_L2)
-                                key = (n < a.N ? a.normB[n] : 0.f) - 2.f * dot + an;
-                            else
-                                key = -dot;
-                            op[u] = n < a.N ? key : kInf;
+                    for (int u = 0; u < 32; ++u) v[u] = __uint_as_float(h ? r1[u] : r0[u]) + an;
+                    const int nb = n0 + col0 + c + 32 * h;  // output column of v[0]
+                    if (nb + 32 > a.N) {  // ragged last tile: columns past N pass no bar (NaN) and are not stored
+#pragma unroll
+                        for (int u = 0; u < 32; ++u)
+                            if (nb + u >= a.N) v[u] = __int_as_float(0x7fffffff);
+                    }
+                    if (a.out) {
+                        // transpose through shared memory so each store covers 32 consecutive columns
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) tw[lane * 33 + u] = v[u];
+                        __syncwarp();
+                        for (int r = 0; r < 32; ++r) {
+                            const int mr = m0 + lane_base + r;
+                            if (mr < a.M && nb + lane < a.N) a.out[(int64_t)mr * a.ldo + nb + lane] = tw[r * 33 + lane];
                         }
-                        if (nb + j + 3 < a.N)
-                            *reinterpret_cast<float4*>(orow + nb + j) = o;
-                        else
-                            for (int u = 0; u < 4; ++u)
-                                if (nb + j + u < a.N) orow[nb + j + u] = op[u];
+                        __syncwarp();
+                    } else {
+                        uint32_t msk = 0;
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) msk |= (v[u] <= tau ? 1u : 0u) << u;
+                        if (__any_sync(0xffffffffu, msk != 0)) {
+                            const int cnt = __popc(msk);
+                            int incl = cnt;
+#pragma unroll
+                            for (int o = 1; o < 32; o <<= 1) {
+                                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                                if (lane >= o) incl += y;
+                            }
+                            int slot = wcount + incl - cnt;
+                            wcount += __shfl_sync(0xffffffffu, incl, 31);
+                            while (msk) {
+                                const int u = __ffs(msk) - 1;
+                                msk &= msk - 1;
+                                if (slot < a.wcap) {
+                                    float kv = 0.f;
+#pragma unroll
+                                    for (int z = 0; z < 32; ++z)
+                                        if (z == u) kv = v[z];
+                                    a.fkey[wbase + slot] = kv;
+                                    a.fcol[wbase + slot] = nb + u;
+                                    a.frow[wbase + slot] = m;
+                                }
+                                ++slot;
+                            }
+                        }
                     }
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             bar_arrive(&tempty[b]);
         }
+        if (a.wcount && lane == 0) a.wcount[(int64_t)blockIdx.x * kEpiWarps + ew] = wcount;
     }
     __syncthreads();
     if (warp == 1) {
@@ -278,50 +345,78 @@ int make_map(CUtensorMap* tm, const void* base, int64_t rows, int cols, int box_
 
 }  // namespace
 
-size_t tc_gemm_smem() { return (size_t)kStages * (kABytes + kBBytes) + 1024 + 256; }
+size_t tc_gemm_smem() { return (size_t)kStages * (kABytes + kBBytes) + 1024 + 256 + kEpiWarps * 32 * 33 * 4; }
+
+int tc_kpad(int dim, int metric) { return (int)ceil_div(dim + (metric == ANN_METRIC_L2 ? 3 : 0), kBK) * kBK; }
+
+static int tc_grid(int M, int N) { return (int)std::min<int64_t>(ceil_div(M, kBM) * ceil_div(N, kBN), kNumSMs); }
+int tc_filter_warps(int M, int N) { return tc_grid(M, N) * kEpiWarps; }
 
 int launch_tc_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, const TcGemmArgs& a, cudaStream_t st) {
     ANN_CHECK_ARG(a.K % kBK == 0 && a.K > 0, "tensor-core scan: K=%d not a positive multiple of %d", a.K, kBK);
     ANN_CHECK_ARG((reinterpret_cast<uintptr_t>(A) & 15) == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0,
                   "tensor-core scan: operands must be 16-byte aligned");
-    ANN_CHECK_ARG(a.metric == ANN_METRIC_IP || a.normB != nullptr, "tensor-core scan: L2 keys need base norms");
+    ANN_CHECK_ARG(a.out != nullptr || (a.tau && a.fkey && a.fcol && a.frow && a.wcount && a.wcap > 0),
+                  "tensor-core scan: neither an output matrix nor a filter");
+    ANN_CHECK_ARG(a.b_tile_stride >= 1, "tensor-core scan: bad sample stride");
     if (a.M == 0 || a.N == 0) return ANN_OK;
+    const int64_t b_rows = a.b_rows > 0 ? a.b_rows : a.N;
+    // the last sampled tile must start inside B
+    ANN_CHECK_ARG((ceil_div(a.N, kBN) - 1) * kBN * (int64_t)a.b_tile_stride < b_rows,
+                  "tensor-core scan: sample runs past the base");
     CUtensorMap tmA, tmB;
     int rc = make_map(&tmA, A, a.M, a.K, kBM);
     if (rc) return rc;
-    rc = make_map(&tmB, B, a.N, a.K, kBN);
+    rc = make_map(&tmB, B, b_rows, a.K, kBN);
     if (rc) return rc;
     const size_t smem = tc_gemm_smem();
     ANN_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int64_t tiles = ceil_div(a.M, kBM) * ceil_div(a.N, kBN);
-    const int grid = (int)std::min<int64_t>(tiles, kNumSMs);
-    tc_gemm_kernel<<<grid, 192, smem, st>>>(tmA, tmB, a);
+    tc_gemm_kernel<<<tc_grid(a.M, a.N), kThreads, smem, st>>>(tmA, tmB, a);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }
 
-// FP32 [rows, ld] (first `cols` columns) -> BF16 [rows, kpad] zero-padded, plus optional FP32 row norms
-// of the converted values' sources (exact squared norms of the FP32 rows).
-__global__ void to_bf16_kernel(const float* __restrict__ x, int64_t rows, int cols, int64_t ld, __nv_bfloat16* out,
-                               int kpad, float* norms) {
-    const int64_t r = blockIdx.x * (int64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
+// One warp per output row: the BF16 operand form (tc_gemm.cuh) of an FP32 row. The squared norm is the
+// FP32 sum of the row's FP32 squares; its three BF16 pieces are hi = bf16(s), mid = bf16(s - hi) and
+// lo = bf16(s - hi - mid), each difference exact in FP32.
+__global__ void tc_operand_kernel(const float* __restrict__ x, int64_t rows, int cols, int64_t ld, __nv_bfloat16* out,
+                                  int kpad, float scale, int base_l2, int query_l2, int64_t row_mult) {
+    const int64_t p = blockIdx.x * (int64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
-    if (r >= rows) return;
+    if (p >= rows) return;
+    const int64_t r = row_mult > 0 ? (int64_t)(((unsigned __int128)p * (uint64_t)row_mult) % (uint64_t)rows) : p;
     float s = 0.f;
     for (int c = lane; c < kpad; c += 32) {
         const float v = c < cols ? x[r * ld + c] : 0.f;
-        out[r * kpad + c] = __float2bfloat16_rn(v);
         s = fmaf(v, v, s);
+        float o = v * scale;
+        if (query_l2 && c >= cols && c < cols + 3) o = 1.f;
+        out[p * kpad + c] = __float2bfloat16_rn(o);
     }
+    if (!base_l2) return;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (norms && lane == 0) norms[r] = s;
+    if (lane == 0) {
+        const __nv_bfloat16 hi = __float2bfloat16_rn(s);
+        const float r1 = s - __bfloat162float(hi);
+        const __nv_bfloat16 mid = __float2bfloat16_rn(r1);
+        const float r2 = r1 - __bfloat162float(mid);
+        out[p * kpad + cols] = hi;
+        out[p * kpad + cols + 1] = mid;
+        out[p * kpad + cols + 2] = __float2bfloat16_rn(r2);
+    }
 }
 
-int launch_to_bf16(const float* x, int64_t rows, int cols, int64_t ld, __nv_bfloat16* out, int kpad, float* norms,
-                   cudaStream_t st) {
+int launch_tc_operand(const float* x, int64_t rows, int cols, int64_t ld, __nv_bfloat16* out, int kpad, int role,
+                      int metric, int64_t row_mult, cudaStream_t st) {
+    ANN_CHECK_ARG(kpad >= tc_kpad(cols, metric) && kpad % kBK == 0, "tensor-core operand: kpad %d too small", kpad);
+    ANN_CHECK_ARG(row_mult == 0 || role == kTcBase, "tensor-core operand: only the base is reordered");
     if (rows == 0) return ANN_OK;
-    to_bf16_kernel<<<(unsigned)ceil_div(rows, 8), 256, 0, st>>>(x, rows, cols, ld, out, kpad, norms);
+    const bool l2 = metric == ANN_METRIC_L2;
+    const float scale = role == kTcBase ? 1.f : (l2 ? -2.f : -1.f);
+    tc_operand_kernel<<<(unsigned)ceil_div(rows, 8), 256, 0, st>>>(x, rows, cols, ld, out, kpad, scale,
+                                                                    (l2 && role == kTcBase) ? 1 : 0,
+                                                                    (l2 && role == kTcQuery) ? 1 : 0, row_mult);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

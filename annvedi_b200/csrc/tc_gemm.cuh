@@ -6,19 +6,42 @@
 
 namespace annb {
 
+// The GEMM output is the ranking key itself: the operands carry it (launch_tc_operand).
+//   L2: base row [bf16(b), hi, mid, lo] with hi + mid + lo = |b|^2 (FP32, split into three BF16),
+//       query row [bf16(-2a), 1, 1, 1]  ->  sum = |b|^2 - 2 a.b
+//   IP: base row [bf16(b)], query row [bf16(-a)]  ->  sum = -a.b
+// Smaller keys are better in both metrics.
 struct TcGemmArgs {
     int M, N, K;           // A [M, K], B [N, K] BF16 row-major; K a multiple of 64
-    const float* normA;    // [M] squared norms of A rows (L2; optional)
-    const float* normB;    // [N] squared norms of B rows (L2)
-    int metric;            // ANN_METRIC_L2: |b|^2 - 2 a.b (+ |a|^2); ANN_METRIC_IP: -a.b
-    float* out;            // [M, ldo] keys (smaller is better)
+    const float* normA;    // [M] optional per-row addend (|a|^2 turns the L2 key into the squared distance)
+    float* out;            // [M, ldo] keys; null in filter mode
     int64_t ldo;
     int* err;              // device flag set if a bounded wait gives up
+    int b_tile_stride = 1; // B rows of output tile j start at row j * 256 * b_tile_stride (a strided sample)
+    int64_t b_rows = 0;    // rows of the B matrix when sampling (0: N)
+    // Filter mode (out == null): keys <= tau[m] are appended, as (key, column, row m), to the region of
+    // the epilogue warp that met them: warp w of the grid owns entries [w * wcap, (w + 1) * wcap) of
+    // fkey / fcol / frow, and wcount[w] receives its count (which may exceed wcap: the caller checks).
+    const float* tau = nullptr;
+    float* fkey = nullptr;
+    int* fcol = nullptr;
+    int* frow = nullptr;
+    int* wcount = nullptr;
+    int wcap = 0;
 };
 
+enum TcRole { kTcBase = 0, kTcQuery = 1 };
+
+// Columns of the BF16 operands for vectors of `dim` FP32 values: the key columns included, rounded up
+// to the 64-column k-block.
+int tc_kpad(int dim, int metric);
+// Epilogue warps of a filter launch over M x N keys (the size of the wcount array).
+int tc_filter_warps(int M, int N);
 size_t tc_gemm_smem();
 int launch_tc_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, const TcGemmArgs& a, cudaStream_t st);
-int launch_to_bf16(const float* x, int64_t rows, int cols, int64_t ld, __nv_bfloat16* out, int kpad, float* norms,
-                   cudaStream_t st);
+// FP32 [rows, ld] (first `cols` columns) -> the BF16 operand form of `role` for `metric`, [rows, kpad].
+// With row_mult > 0 (base only), output row p holds input row (p * row_mult) mod rows.
+int launch_tc_operand(const float* x, int64_t rows, int cols, int64_t ld, __nv_bfloat16* out, int kpad, int role,
+                      int metric, int64_t row_mult, cudaStream_t st);
 
 }  // namespace annb

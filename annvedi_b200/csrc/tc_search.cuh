@@ -1,0 +1,46 @@
+// Helpers of the tensor-core search around the GEMM (tc_search.cu): grouping filter survivors into
+// per-query streams, the bar check and re-run gather, and the row order of the BF16 base copy.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace annb {
+
+// The BF16 base copy stores row (p * mult) mod n at position p (a Weyl sequence with mult ~ 0.618 n,
+// coprime to n): any 256 consecutive positions cover the rows evenly, so a strided sample of whole
+// tiles is an even sample of the base whatever order the rows came in.
+int64_t tc_row_mult(int64_t n);
+
+struct TcGroupArgs {
+    // filter survivors: warp w holds entries [w * wcap, w * wcap + min(wcount[w], wcap))
+    const float* fkey;
+    const int* fcol;
+    const int* frow;
+    const int* wcount;
+    int nwarps;
+    int wcap;
+    int M;            // rows (queries) of the filter launch
+    int64_t n;        // base rows, for the position -> row map
+    int64_t mult;     // tc_row_mult(n)
+    // outputs
+    int* rowcnt;      // [M] survivors per row
+    int64_t* offs;    // [M] start of row m's stream in gkey / gid
+    int* cursor;      // [M] scratch
+    float* gkey;      // [nwarps * wcap]
+    int* gid;         // [nwarps * wcap] base row ids
+    int* max_wcount;  // [1] largest wcount (an overflow if > wcap)
+};
+int launch_tc_group(const TcGroupArgs& g, cudaStream_t st);
+
+// Rows with fewer than R survivors go to list (count in flags[0]).
+int launch_tc_bar_check(const int* rowcnt, int M, int R, int* list, int* flags, cudaStream_t st);
+// A2[j] = A[list[j]], tau2[j] = tau[list[j]], j < nb.
+int launch_tc_gather(const __nv_bfloat16* A, int kpad, const int* list, int nb, const float* tau, __nv_bfloat16* A2,
+                     float* tau2, cudaStream_t st);
+// ids[i] (positions of the BF16 copy) -> base rows, in place; kNoId stays.
+int launch_tc_map_ids(int* ids, int64_t count, int64_t n, int64_t mult, cudaStream_t st);
+// out[q][row(p)] = keys[q][p] for a [nq, n] key matrix in position order.
+int launch_tc_unpermute(const float* keys, int nq, int64_t n, int64_t mult, float* out, cudaStream_t st);
+
+}  // namespace annb

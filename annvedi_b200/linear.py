@@ -190,6 +190,15 @@ class LinearIndex:
         _lib.check(self._lib.ann_flat_profile(self._h, out))
         return {"scan_ms": out[0], "merge_ms": out[1], "scan_launches": int(out[2]), "query_calls": int(out[3])}
 
+    def get_stage_times(self) -> dict:
+        """Every stage total: the exact scan's and the tensor-core search's (GEMM passes, selections,
+        exact re-rank), with launch counts."""
+        out = (ctypes.c_double * 8)()
+        _lib.check(self._lib.ann_flat_profile_stages(self._h, out))
+        return {"scan_ms": out[0], "merge_ms": out[1], "tc_gemm_ms": out[2], "tc_select_ms": out[3],
+                "rerank_ms": out[4], "scan_launches": int(out[5]), "tc_gemm_launches": int(out[6]),
+                "query_calls": int(out[7])}
+
     def reset_profile_results(self) -> None:
         _lib.check(self._lib.ann_flat_reset_profile(self._h))
 

@@ -222,6 +222,38 @@ def run_ours(args, rank, world, local):
     del flat
     torch.cuda.empty_cache()
 
+    # ---- tensor-core exact search: BF16 tcgen05 keys, sampled bars, exact FP32 re-rank ----
+    tcx = LinearIndex(device=local, metric="l2", mode="exact")
+    tcx.fit(base)
+    t_ids = torch.empty(q, K_NN, dtype=torch.int64, device=dev)
+    t_d = torch.empty(q, K_NN, dtype=torch.float32, device=dev)
+
+    def tc_step():
+        tcx.search_tc(queries, K_NN, refine_r=args.tc_refine, out_ids=t_ids, out_dists=t_d)
+
+    for _ in range(max(3, args.warmup)):
+        tc_step()
+    torch.cuda.synchronize()
+    tc_recall = recall_evaluator(base, queries, t_ids, kth)
+    tcx.reset_profile_results()
+    tcx.set_profiling(True)
+    tsteps = max(2, min(args.steps, 5))
+    tc_ms = _time_steps(tc_step, tsteps, stream) / tsteps
+    tcx.set_profiling(False)
+    tst = tcx.get_stage_times()
+    tc_qps = q / (tc_ms / 1e3)
+    kpad = -(-(d + 3) // 64) * 64
+    gemm_ms = tst["tc_gemm_ms"] / tsteps
+    tc_line = {"qps": round(tc_qps, 1), "ms_per_batch": round(tc_ms, 3), "recall_at_100": round(tc_recall, 4),
+               "refine_r": args.tc_refine, "kernel": "tc_gemm_kernel",
+               "stage_ms_per_batch": {"gemm_passes": round(gemm_ms, 4),
+                                      "selections": round(tst["tc_select_ms"] / tsteps, 4),
+                                      "rerank": round(tst["rerank_ms"] / tsteps, 4)},
+               "gemm_launches_per_batch": round(tst["tc_gemm_launches"] / tsteps, 2),
+               "filter_tflops": round(2.0 * n * kpad * q / (gemm_ms / 1e3) / 1e12, 1) if gemm_ms > 0 else None}
+    del tcx
+    torch.cuda.empty_cache()
+
     # ---- IVF-SQ8: lists = the 2,048 L2-normalised generating centres ----
     ivf = IVFIndex(device=local, mode="exact")
     t0 = time.perf_counter()
@@ -313,6 +345,7 @@ def run_ours(args, rank, world, local):
         "recall_at_100": round(rec, 4),
         "speedup_vs_plain_fp32_scan": round(qps / (flat_qps * world), 2),
         "plain_fp32_scan": flat_line,
+        "tensor_core_exact_search": tc_line,
         "nprobe_sweep": sweep,
         "latency_ms_batch1": {"device_p50": round(float(np.percentile(lat_dev, 50)), 4),
                               "device_p99": round(float(np.percentile(lat_dev, 99)), 4),
@@ -441,6 +474,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--refine", type=int, default=300)
+    ap.add_argument("--tc-refine", type=int, default=400)
     ap.add_argument("--ref-nprobe", type=int, default=32)
     ap.add_argument("--cpu-sample", type=int, default=64)
     ap.add_argument("--latency-queries", type=int, default=200)

@@ -68,3 +68,60 @@ def test_tc_device_and_host_agree(cuda):
     b, bd = ix.search_tc(w.queries, 20)
     np.testing.assert_array_equal(a.cpu().numpy(), b)
     np.testing.assert_array_equal(ad.cpu().numpy(), bd)
+
+
+@pytest.mark.parametrize("metric", ["l2", "ip"])
+def test_tc_sampled_bar_path_is_exact(cuda, metric):
+    """Bases of >= 262,144 rows take the sampled-bar path (sample pass, fast bar, filtered full pass,
+    re-runs under the safe bar where needed); with R >= the BF16 error margin the result is the exact
+    top-k."""
+    import torch
+    from tests.helpers import check_exact_topk
+    from annvedi_b200.linear import LinearIndex
+    w = synth.mixture(300_000, 64, 96, c=256, sigma=0.35, seed=21, metric=metric)
+    ix = LinearIndex(device=0, metric=metric, mode="exact")
+    ix.fit(torch.from_numpy(w.base).cuda())
+    ids, d = ix.search_tc(torch.from_numpy(w.queries).cuda(), 20, refine_r=400)
+    torch.cuda.synchronize()
+    check_exact_topk(w.base, w.queries, ids.cpu().numpy(), d.cpu().numpy(), 20, metric=metric)
+
+
+def _weyl_mult(n):
+    """Row order of the BF16 base copy: position p holds row (p * g) mod n."""
+    g = max(1, int(0.6180339887498949 * n))
+    while np.gcd(g, n) != 1:
+        g += 1
+    return g
+
+
+def test_tc_rerun_under_safe_bar_is_exact(cuda):
+    """Queries whose nearest rows all sit at sampled positions of the base copy: the sample
+    over-represents them, the fast bar (the ~134th best sampled key) lets fewer than R = 400 keys through
+    over all rows, and the query is re-run under its safe bar. The result is still the exact top-k."""
+    import torch
+    from tests.helpers import check_exact_topk
+    from annvedi_b200.linear import LinearIndex
+    rng = np.random.default_rng(5)
+    n, dim, R = 300_032, 64, 400
+    g = _weyl_mult(n)
+    full_tiles = n // 256
+    stride = full_tiles // max(128, -(-16 * R // 256))  # sample: every stride-th 256-row tile
+    tiles = np.arange(full_tiles // stride) * stride
+    pos = (tiles[:, None] * 256 + np.arange(256)[None, :]).ravel()
+    sampled_rows = (pos.astype(object) * g % n).astype(np.int64)
+    base = rng.normal(size=(n, dim)).astype(np.float32)
+    nclu, size = 8, 300
+    centres = 4.0 * rng.normal(size=(nclu, dim)).astype(np.float32)
+    rows = rng.choice(sampled_rows, nclu * size, replace=False).reshape(nclu, size)
+    for i in range(nclu):
+        base[rows[i]] = centres[i] + 0.05 * rng.normal(size=(size, dim))
+    plain = rng.normal(size=(24, dim)).astype(np.float32)
+    queries = np.concatenate([centres + 0.05 * rng.normal(size=(nclu, dim)), plain]).astype(np.float32)
+    ix = LinearIndex(device=0, mode="exact")
+    ix.fit(torch.from_numpy(base).cuda())
+    ix.set_profiling(True)
+    ix.reset_profile_results()
+    ids, d = ix.search_tc(queries, 20, refine_r=R)
+    st = ix.get_stage_times()
+    check_exact_topk(base, queries, ids, d, 20)
+    assert st["tc_gemm_launches"] >= 3, st  # sample, filter and at least one re-run
