@@ -229,16 +229,26 @@ int ann_flat_fit(ann_flat* h, const float* data, int64_t n, int32_t dim, int64_t
 }  // extern "C"
 
 // Number of row splits for an exact scan of n rows by nq queries in tiles of bq.
-int annb::flat_choose_nsplit(int64_t n, int nq, int bq, int64_t* rows_per_split) {
-    const int n_qtiles = (int)ceil_div(nq, bq);
-    const int ctas_per_sm = bq <= 8 ? 2 : 1;
-    const int64_t target = (int64_t)kNumSMs * ctas_per_sm;
-    int64_t nsplit = ceil_div(target, n_qtiles);
+int annb::flat_choose_nsplit(int64_t n, int nq, int bq, int64_t* rows_per_split, int ctas_per_sm) {
+    // Choose the splits per query tile so that (query tiles x splits) fills whole waves of
+    // kNumSMs * ctas_per_sm CTAs, with a small charge per split for the merge.
+    const int64_t wave = (int64_t)kNumSMs * std::max(1, ctas_per_sm);
+    const int64_t n_qtiles = ceil_div(nq, bq);
     const int64_t tile = 256;
-    const int64_t max_split = std::max<int64_t>(1, ceil_div(n, 2 * tile));
-    nsplit = std::max<int64_t>(1, std::min(nsplit, max_split));
-    int64_t rps = ceil_div(ceil_div(n, nsplit), tile) * tile;
-    nsplit = ceil_div(n, rps);
+    const int64_t max_split = std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 2 * tile), 4 * wave));
+    int64_t best_s = 1;
+    double best = 1e300;
+    for (int64_t s = 1; s <= max_split; ++s) {
+        const int64_t ctas = n_qtiles * s;
+        const int64_t waves = ceil_div(ctas, wave);
+        const double cost = (double)waves * wave / (double)ctas * (1.0 + 0.002 * (double)s);
+        if (cost < best - 1e-12) {
+            best = cost;
+            best_s = s;
+        }
+    }
+    int64_t rps = ceil_div(ceil_div(n, best_s), tile) * tile;
+    const int64_t nsplit = ceil_div(n, rps);
     *rows_per_split = rps;
     return (int)nsplit;
 }
@@ -282,11 +292,18 @@ int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t
         sz.take<int64_t>((size_t)nq * kk);
         sz.take<float>((size_t)nq * kk);
     }
+    bool radix_merge = false;
     if (mode == ANN_MODE_EXACT) {
         bq = std::min(flat_scan_bq(nq), flat_scan_max_bq(kk));
-        nsplit = flat_choose_nsplit(h->n, nq, bq, &rps);
+        nsplit = flat_choose_nsplit(h->n, nq, bq, &rps, flat_scan_ctas_per_sm(bq, kk, dpad, h->metric));
         sz.take<float>((size_t)nq * nsplit * kk);
         sz.take<int>((size_t)nq * nsplit * kk);
+        // many splits per query: select the k best with the radix selection, then sort them
+        radix_merge = nsplit >= 16;
+        if (radix_merge) {
+            sz.take<float>((size_t)nq * kk);
+            sz.take<int>((size_t)nq * kk);
+        }
     } else {
         ncp = compat_num_checkpoints(h->dim);
         const size_t per_q = sizeof(float) * (size_t)h->n * (ncp + 1);
@@ -336,8 +353,22 @@ int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t
         rc = launch_flat_scan(a, bq, st);
         if (rc) return rc;
         h->prof.mark(prec, st);
-        MergeArgs m{skey, sid, nq, nsplit, kk, kk, h->metric == ANN_METRIC_IP ? 1 : 0, ids_dev, dists_dev};
-        rc = launch_merge_splits(m, st);
+        if (radix_merge) {
+            float* mkey = cv.take<float>((size_t)nq * kk);
+            int* mid = cv.take<int>((size_t)nq * kk);
+            RadixSelectArgs rs{};
+            rs.keys = skey;
+            rs.ld = (int64_t)nsplit * kk;
+            rs.ids = sid;
+            rs.R = kk;
+            rs.out_key = mkey;
+            rs.out_id = mid;
+            if ((rc = launch_radix_select(rs, nq, st))) return rc;
+            rc = launch_sort_topk(mkey, mid, nq, kk, h->metric == ANN_METRIC_IP ? 1 : 0, ids_dev, dists_dev, st);
+        } else {
+            MergeArgs m{skey, sid, nq, nsplit, kk, kk, h->metric == ANN_METRIC_IP ? 1 : 0, ids_dev, dists_dev};
+            rc = launch_merge_splits(m, st);
+        }
         if (rc) return rc;
         h->prof.mark(prec, st);
         if (prec >= 0) h->prof.launches += 1;

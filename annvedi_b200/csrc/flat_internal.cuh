@@ -25,5 +25,6 @@ struct ann_flat {
 
 namespace annb {
 // Number of row splits (and rows per split) for an exact scan of n rows by nq queries in tiles of bq.
-int flat_choose_nsplit(int64_t n, int nq, int bq, int64_t* rows_per_split);
+// ctas_per_sm: resident CTAs per SM of the scan form used (one wave = kNumSMs * ctas_per_sm CTAs).
+int flat_choose_nsplit(int64_t n, int nq, int bq, int64_t* rows_per_split, int ctas_per_sm = 1);
 }  // namespace annb

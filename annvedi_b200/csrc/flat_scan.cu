@@ -283,6 +283,41 @@ __global__ void __launch_bounds__(256) merge_splits_kernel(MergeArgs a) {
     }
 }
 
+// One warp per query sorts its set of k (key, id) pairs (any order, kNoId padding) by (key, id) and
+// writes the final top-k: int64 ids (-1 for padding) and distances (negated back for inner product).
+__global__ void sort_topk_kernel(const float* __restrict__ keys, const int* __restrict__ ids, int nq, int k, int negate,
+                                 int64_t* out_ids, float* out_dists) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int cap = topk_cap(k);
+    float* sKey = reinterpret_cast<float*>(smem_raw);
+    int* sId = reinterpret_cast<int*>(sKey + cap);
+    const int q = blockIdx.x;
+    const int lane = threadIdx.x;
+    for (int e = lane; e < cap; e += 32) {
+        const bool ok = e < k && ids[(int64_t)q * k + e] != kNoId;
+        sKey[e] = ok ? keys[(int64_t)q * k + e] : kInf;
+        sId[e] = ok ? ids[(int64_t)q * k + e] : kNoId;
+    }
+    __syncwarp();
+    warp_sort_smem(sKey, sId, cap);
+    for (int e = lane; e < k; e += 32) {
+        const bool ok = sId[e] != kNoId;
+        if (out_ids) out_ids[(int64_t)q * k + e] = ok ? (int64_t)sId[e] : -1;
+        if (out_dists) out_dists[(int64_t)q * k + e] = ok ? (negate ? -sKey[e] : sKey[e]) : (negate ? -kInf : kInf);
+    }
+}
+
+int launch_sort_topk(const float* keys, const int* ids, int nq, int k, int negate, int64_t* out_ids, float* out_dists,
+                     cudaStream_t st) {
+    if (nq == 0) return ANN_OK;
+    ANN_CHECK_ARG(k >= 1 && k <= 1024, "sort top-k: k=%d outside [1, 1024]", k);
+    const size_t smem = (size_t)topk_cap(k) * 8;
+    ANN_CUDA_TRY(cudaFuncSetAttribute(sort_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    sort_topk_kernel<<<nq, 32, smem, st>>>(keys, ids, nq, k, negate, out_ids, out_dists);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
 // Copies rows [n, dim] (row stride ld floats) into [n, dpad] with zero padding.
 __global__ void pad_rows_kernel(const float* __restrict__ src, int64_t n, int dim, int64_t ld, float* __restrict__ dst,
                                 int dpad) {
@@ -301,6 +336,176 @@ int launch_pad_rows(const float* src, int64_t n, int dim, int64_t ld, float* dst
     pad_rows_kernel<<<blocks, 256, 0, st>>>(src, n, dim, ld, dst, dpad);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Streaming form for 1, 2 or 4 queries per CTA, where the scan is HBM-bound: no shared-memory
+// staging of the base. Each warp reads 4 rows at a time, 8 lanes per row, each lane a 16-byte piece
+// of every 128-byte stretch of its row (coalesced 128-byte reads), straight into registers; the 8
+// lanes combine their partial sums with three shuffles. The queries sit in shared memory (read as
+// broadcasts). Every warp keeps its own top-k per query (WarpTopK, no block barriers while
+// scanning); at the end one warp per query merges the eight warps' lists into the split's top-k.
+// ---------------------------------------------------------------------------------------------
+constexpr int kStreamWarps = 8;
+constexpr int kStreamBatch = 12;  // 16-byte loads in flight per lane (a 384-float row in one batch)
+
+template <int BQ, int METRIC>
+__global__ void __launch_bounds__(32 * kStreamWarps) flat_stream_kernel(FlatScanArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int dpad = a.dpad, cap = a.cap, k = a.k;
+    float* sQ = reinterpret_cast<float*>(smem_raw);                 // [BQ][dpad]
+    float* bufK = sQ + BQ * dpad;                                   // [warps][BQ][cap]
+    int* bufI = reinterpret_cast<int*>(bufK + kStreamWarps * BQ * cap);
+    int* sCount = bufI + kStreamWarps * BQ * cap;                   // [warps][BQ]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int oct = lane >> 3, o = lane & 7;
+    const int q0 = blockIdx.x * BQ;
+    const int split = blockIdx.y;
+    const int64_t row_begin = (int64_t)split * a.rows_per_split;
+    const int64_t row_end = min(row_begin + a.rows_per_split, a.n);
+    for (int i = threadIdx.x; i < BQ * dpad; i += blockDim.x) {
+        const int qi = i / dpad;
+        sQ[i] = q0 + qi < a.nq ? a.q[(int64_t)(q0 + qi) * dpad + (i - qi * dpad)] : 0.f;
+    }
+    __syncthreads();
+    WarpTopK top[BQ];
+#pragma unroll
+    for (int qi = 0; qi < BQ; ++qi) top[qi].init(bufK + (warp * BQ + qi) * cap, bufI + (warp * BQ + qi) * cap, k);
+    const int nj = dpad / 32;
+    for (int64_t r0 = row_begin + warp * 4; r0 < row_end; r0 += 4 * kStreamWarps) {
+        const int64_t row = r0 + oct;
+        const bool valid = row < row_end;
+        const float4* x = reinterpret_cast<const float4*>(a.base + (valid ? row : row_begin) * (int64_t)dpad) + o;
+        const float4* qv4 = reinterpret_cast<const float4*>(sQ) + o;
+        float acc[BQ];
+#pragma unroll
+        for (int qi = 0; qi < BQ; ++qi) acc[qi] = 0.f;
+        for (int j0 = 0; j0 < nj; j0 += kStreamBatch) {
+            // every load of the batch is issued before the first is used
+            float4 xb[kStreamBatch];
+#pragma unroll
+            for (int u = 0; u < kStreamBatch; ++u)
+                if (j0 + u < nj) xb[u] = __ldcs(x + 8 * (j0 + u));
+#pragma unroll
+            for (int u = 0; u < kStreamBatch; ++u) {
+            if (j0 + u >= nj) break;
+            const int j = j0 + u;
+            const float4 xv = xb[u];
+#pragma unroll
+            for (int qi = 0; qi < BQ; ++qi) {
+                const float4 qv = qv4[qi * (dpad / 4) + 8 * j];
+                if (METRIC == ANN_METRIC_L2) {
+                    const float d0 = xv.x - qv.x, d1 = xv.y - qv.y, d2 = xv.z - qv.z, d3 = xv.w - qv.w;
+                    acc[qi] = fmaf(d0, d0, acc[qi]);
+                    acc[qi] = fmaf(d1, d1, acc[qi]);
+                    acc[qi] = fmaf(d2, d2, acc[qi]);
+                    acc[qi] = fmaf(d3, d3, acc[qi]);
+                } else {
+                    acc[qi] = fmaf(xv.x, qv.x, acc[qi]);
+                    acc[qi] = fmaf(xv.y, qv.y, acc[qi]);
+                    acc[qi] = fmaf(xv.z, qv.z, acc[qi]);
+                    acc[qi] = fmaf(xv.w, qv.w, acc[qi]);
+                }
+            }
+            }
+        }
+        float key = kInf;
+#pragma unroll
+        for (int qi = 0; qi < BQ; ++qi) {
+            float v = acc[qi];
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            v += __shfl_xor_sync(0xffffffffu, v, 2);
+            v += __shfl_xor_sync(0xffffffffu, v, 4);
+            if (o == qi) key = METRIC == ANN_METRIC_L2 ? v : -v;
+        }
+#pragma unroll
+        for (int qi = 0; qi < BQ; ++qi) top[qi].offer(key, (int)row, valid && o == qi && q0 + qi < a.nq);
+    }
+#pragma unroll
+    for (int qi = 0; qi < BQ; ++qi) {
+        top[qi].compact();
+        if (lane == 0) sCount[warp * BQ + qi] = top[qi].count;
+    }
+    __syncthreads();
+    // warp qi merges query qi's lists from the other warps into its own
+#pragma unroll
+    for (int qi = 0; qi < BQ; ++qi) {
+        if (warp != qi || q0 + qi >= a.nq) continue;
+        for (int w = 0; w < kStreamWarps; ++w) {
+            if (w == warp) continue;
+            const int cnt = sCount[w * BQ + qi];
+            const float* wk = bufK + (w * BQ + qi) * cap;
+            const int* wi = bufI + (w * BQ + qi) * cap;
+            for (int e0 = 0; e0 < cnt; e0 += 32) {
+                const int e = e0 + lane;
+                const bool ok = e < cnt;
+                top[qi].offer(ok ? wk[e] : kInf, ok ? wi[e] : kNoId, ok);
+            }
+        }
+        top[qi].compact();
+        const int cnt = top[qi].count;
+        float* okey = a.out_key + ((int64_t)(q0 + qi) * a.nsplit + split) * k;
+        int* oid = a.out_id + ((int64_t)(q0 + qi) * a.nsplit + split) * k;
+        for (int e = lane; e < k; e += 32) {
+            okey[e] = e < cnt ? top[qi].key[e] : kInf;
+            oid[e] = e < cnt ? top[qi].id[e] : kNoId;
+        }
+    }
+}
+
+static size_t stream_smem(int bq, int dpad, int cap) {
+    return sizeof(float) * (size_t)bq * dpad + (size_t)kStreamWarps * bq * cap * 8 + sizeof(int) * kStreamWarps * bq;
+}
+
+bool flat_stream_eligible(int bq, int k, int dpad) {
+    return (bq == 1 || bq == 2 || bq == 4) && stream_smem(bq, dpad, topk_cap(k)) <= 100 * 1024;
+}
+
+template <int BQ, int METRIC>
+static int stream_occupancy(int dpad, int cap) {
+    auto kern = flat_stream_kernel<BQ, METRIC>;
+    const size_t smem = stream_smem(BQ, dpad, cap);
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    int nb = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 32 * kStreamWarps, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return std::max(1, nb);
+}
+
+int flat_scan_ctas_per_sm(int bq, int k, int dpad, int metric) {
+    if (!flat_stream_eligible(bq, k, dpad)) return 1;
+    const int cap = topk_cap(k);
+    const bool l2 = metric == ANN_METRIC_L2;
+    switch (bq) {
+    case 1: return l2 ? stream_occupancy<1, ANN_METRIC_L2>(dpad, cap) : stream_occupancy<1, ANN_METRIC_IP>(dpad, cap);
+    case 2: return l2 ? stream_occupancy<2, ANN_METRIC_L2>(dpad, cap) : stream_occupancy<2, ANN_METRIC_IP>(dpad, cap);
+    default: return l2 ? stream_occupancy<4, ANN_METRIC_L2>(dpad, cap) : stream_occupancy<4, ANN_METRIC_IP>(dpad, cap);
+    }
+}
+
+template <int BQ, int METRIC>
+static int launch_stream_t(const FlatScanArgs& a, int n_qtiles, cudaStream_t st) {
+    auto kern = flat_stream_kernel<BQ, METRIC>;
+    const size_t smem = stream_smem(BQ, a.dpad, a.cap);
+    ANN_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid(n_qtiles, a.nsplit);
+    kern<<<grid, 32 * kStreamWarps, smem, st>>>(a);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+template <int METRIC>
+static int dispatch_stream(const FlatScanArgs& a, int bq, int n_qtiles, cudaStream_t st) {
+    switch (bq) {
+    case 1: return launch_stream_t<1, METRIC>(a, n_qtiles, st);
+    case 2: return launch_stream_t<2, METRIC>(a, n_qtiles, st);
+    default: return launch_stream_t<4, METRIC>(a, n_qtiles, st);
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -334,10 +539,10 @@ int flat_scan_bq(int nq) {
 template <int METRIC>
 static int dispatch_bq(const FlatScanArgs& a, int bq, int n_qtiles, cudaStream_t st) {
     switch (bq) {
-    case 1: return launch_scan_t<1, 1, 1, 2, METRIC>(a, n_qtiles, st);
-    case 2: return launch_scan_t<2, 2, 1, 2, METRIC>(a, n_qtiles, st);
-    case 4: return launch_scan_t<4, 4, 1, 2, METRIC>(a, n_qtiles, st);
-    case 8: return launch_scan_t<8, 8, 1, 2, METRIC>(a, n_qtiles, st);
+    case 1: return launch_scan_t<1, 1, 1, kSmallTileStages, METRIC>(a, n_qtiles, st);
+    case 2: return launch_scan_t<2, 2, 1, kSmallTileStages, METRIC>(a, n_qtiles, st);
+    case 4: return launch_scan_t<4, 4, 1, kSmallTileStages, METRIC>(a, n_qtiles, st);
+    case 8: return launch_scan_t<8, 8, 1, kSmallTileStages, METRIC>(a, n_qtiles, st);
     case 16: return launch_scan_t<16, 8, 2, 3, METRIC>(a, n_qtiles, st);
     default: return launch_scan_t<32, 8, 4, 3, METRIC>(a, n_qtiles, st);
     }
@@ -350,6 +555,10 @@ int launch_flat_scan(const FlatScanArgs& a0, int bq, cudaStream_t st) {
     a.cap = topk_cap(a.k);
     if (bq > flat_scan_max_bq(a.k)) bq = flat_scan_max_bq(a.k);
     const int n_qtiles = (int)ceil_div(a.nq, bq);
+    if (flat_stream_eligible(bq, a.k, a.dpad)) {
+        if (a.metric == ANN_METRIC_L2) return dispatch_stream<ANN_METRIC_L2>(a, bq, n_qtiles, st);
+        return dispatch_stream<ANN_METRIC_IP>(a, bq, n_qtiles, st);
+    }
     if (a.metric == ANN_METRIC_L2) return dispatch_bq<ANN_METRIC_L2>(a, bq, n_qtiles, st);
     return dispatch_bq<ANN_METRIC_IP>(a, bq, n_qtiles, st);
 }

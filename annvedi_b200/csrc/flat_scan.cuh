@@ -34,10 +34,21 @@ struct MergeArgs {
     float* out_key32 = nullptr; // [nq, k] raw keys (+inf where fewer), optional
 };
 
+// Pipeline depth of the query tiles of 1..8 queries (HBM-bound: four 36 KB stages keep enough bytes
+// in flight with one CTA per SM).
+constexpr int kSmallTileStages = 4;
+
 int flat_scan_bq(int nq);
+// Tiles of 1, 2 or 4 queries run the register-streaming form (several CTAs per SM, as the occupancy
+// calculator allows); the others the shared-memory pipeline (one CTA per SM).
+bool flat_stream_eligible(int bq, int k, int dpad);
+int flat_scan_ctas_per_sm(int bq, int k, int dpad, int metric);
 int flat_scan_max_bq(int k);
 int launch_flat_scan(const FlatScanArgs& a, int bq, cudaStream_t st);
 int launch_merge_splits(const MergeArgs& a, cudaStream_t st);
+// Sorts per-query sets of k pairs by (key, id) into the final top-k (see flat_scan.cu).
+int launch_sort_topk(const float* keys, const int* ids, int nq, int k, int negate, int64_t* out_ids, float* out_dists,
+                     cudaStream_t st);
 int launch_pad_rows(const float* src, int64_t n, int dim, int64_t ld, float* dst, int dpad, cudaStream_t st);
 
 }  // namespace annb

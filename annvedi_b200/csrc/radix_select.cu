@@ -134,27 +134,46 @@ __global__ void __launch_bounds__(kThreads) radix_select_kernel(RadixSelectArgs 
         if (two) a.out_kth2[orow] = len >= a.R2 ? unord(prefix[1] | low) : kInf;
     }
     if (!want_set) return;
-    // collect: all keys < t, then keys == t in stream order up to R (fewer than R keys: all, padded)
+    // collect: all keys < t, then keys == t in stream order (a block scan per chunk) up to R; fewer
+    // than R keys: all, padded
     const uint32_t t = prefix[0];
     const int need_ties = R - below_total;
+    __shared__ int sWarpTies[kThreads / 32];
     if (threadIdx.x == 0) {
         sCount = 0;
         sTies = 0;
     }
     __syncthreads();
-    for (int64_t p = threadIdx.x; p < len; p += kThreads) {
-        const float kv = kq[p];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int64_t base = 0; base < len; base += kThreads) {
+        const int64_t p = base + threadIdx.x;
+        const bool valid = p < len;
+        const float kv = valid ? kq[p] : 0.f;
         const uint32_t o = ord(kv);
-        int slot = -1;
-        if (o < t) {
-            slot = atomicAdd(&sCount, 1);
-        } else if (o == t) {
-            const int tie = atomicAdd(&sTies, 1);
-            if (tie < need_ties) slot = below_total + tie;
-        }
-        if (slot >= 0 && slot < R) {
+        const bool tie = valid && o == t;
+        if (valid && o < t) {
+            const int slot = atomicAdd(&sCount, 1);
             if (ok) ok[slot] = kv;
             if (oi) oi[slot] = id_of(p);
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, tie);
+        if (__syncthreads_or(bal != 0)) {  // uniform: some tie in this chunk
+            if (lane == 0) sWarpTies[warp] = __popc(bal);
+            __syncthreads();
+            int before = sTies;
+            for (int w = 0; w < warp; ++w) before += sWarpTies[w];
+            const int rank = before + __popc(bal & ((1u << lane) - 1u));
+            if (tie && rank < need_ties) {
+                if (ok) ok[below_total + rank] = kv;
+                if (oi) oi[below_total + rank] = id_of(p);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int tot = 0;
+                for (int w = 0; w < kThreads / 32; ++w) tot += sWarpTies[w];
+                sTies += tot;
+            }
+            __syncthreads();
         }
     }
     for (int64_t p = len + threadIdx.x; p < R; p += kThreads) {

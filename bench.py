@@ -219,6 +219,29 @@ def run_ours(args, rank, world, local):
     fp32_instr = 2.0 * n * d * q  # one sub + one fma per element pair
     flat_line = {"qps": round(flat_qps, 1), "ms_per_batch": round(flat_ms, 3), "recall_at_100": round(flat_recall, 4),
                  "kernel": "flat_scan_kernel", "fp32_instr_per_s": round(fp32_instr / (fscan_ms / 1e3), 1)}
+    # HBM-bound regime: one query per call streams the whole base once (flat_stream_kernel)
+    dpad = -(-d // 32) * 32
+    small = {}
+    for b in (1, 4):
+        qb = queries[:b].contiguous()
+        ib = torch.empty(b, K_NN, dtype=torch.int64, device=dev)
+        db = torch.empty(b, K_NN, dtype=torch.float32, device=dev)
+        for _ in range(3):
+            flat.search(qb, K_NN, mode="exact", out_ids=ib, out_dists=db)
+        torch.cuda.synchronize()
+        flat.reset_profile_results()
+        flat.set_profiling(True)
+        reps = 20
+        ms_b = _time_steps(lambda: flat.search(qb, K_NN, mode="exact", out_ids=ib, out_dists=db), reps, stream) / reps
+        flat.set_profiling(False)
+        pr = flat.get_profile_results()
+        scan_b = pr["scan_ms"] / max(1, pr["scan_launches"])
+        gbs = n * dpad * 4 / (scan_b / 1e3) / 1e9
+        small[f"batch{b}"] = {"ms_per_call": round(ms_b, 4), "scan_kernel_ms": round(scan_b, 4),
+                              "merge_ms": round(pr["merge_ms"] / max(1, pr["scan_launches"]), 4),
+                              "scan_gbs": round(gbs, 1), "hbm_frac": round(gbs / hbm_peak, 4),
+                              "kernel": "flat_stream_kernel", "bytes_per_launch": n * dpad * 4}
+    flat_line["small_batch_hbm"] = small
     del flat
     torch.cuda.empty_cache()
 

@@ -49,7 +49,7 @@ def test_reference_mode_single_query_drop_in(cuda, linear_fx):
         np.testing.assert_array_equal(got, linear_fx[f"{name}/ids"], err_msg=name)
 
 
-@pytest.mark.parametrize("nq", [1, 3, 8, 17, 64, 200])
+@pytest.mark.parametrize("nq", [1, 2, 3, 4, 8, 17, 64, 200])
 @pytest.mark.parametrize("k", [1, 10, 100, 257])
 def test_exact_mode_matches_fp64(cuda, nq, k):
     w = synth.flat_normal(20000, 384, nq, seed=nq * 31 + k)
@@ -65,6 +65,32 @@ def test_exact_mode_dims_and_ip(cuda, dim):
         ix = _index(w.base, mode="exact", metric=metric)
         ids, d = ix.search(w.queries, 50)
         check_exact_topk(w.base, w.queries, ids, d, 50, metric=metric)
+
+
+@pytest.mark.parametrize("nq", [1, 2, 4, 16])
+@pytest.mark.parametrize("metric", ["l2", "ip"])
+def test_exact_ties_break_by_lower_id(cuda, nq, metric):
+    """Rows that are exact copies have equal FP32 distances; the exact top-k orders them by lower id,
+    also where the tie straddles the k-th place (every split, the streaming form and the merge)."""
+    rng = np.random.default_rng(nq)
+    distinct = rng.normal(size=(150, 64)).astype(np.float32)
+    group = rng.integers(0, 150, 60000)
+    base = distinct[group]
+    queries = rng.normal(size=(nq, 64)).astype(np.float32)
+    ix = _index(base, mode="exact", metric=metric)
+    ids, _ = ix.search(queries, 100)
+    for qi in range(nq):
+        if metric == "l2":
+            score = ((distinct.astype(np.float64) - queries[qi]) ** 2).sum(1)
+        else:
+            score = -(distinct.astype(np.float64) @ queries[qi])
+        order = np.argsort(score, kind="stable")
+        want = []
+        for g in order:
+            want.extend(np.flatnonzero(group == g).tolist())
+            if len(want) >= 100:
+                break
+        np.testing.assert_array_equal(ids[qi], np.array(want[:100]), err_msg=f"query {qi}")
 
 
 def test_exact_mode_device_tensors_match_host(cuda):
