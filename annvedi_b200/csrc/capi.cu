@@ -424,14 +424,15 @@ int ann_flat_profile(ann_flat* h, double* out4) {
     return ANN_OK;
 }
 
-int ann_flat_profile_stages(ann_flat* h, double* out8) {
-    ANN_CHECK_ARG(h != nullptr && out8 != nullptr, "null argument");
+int ann_flat_profile_stages(ann_flat* h, double* out10) {
+    ANN_CHECK_ARG(h != nullptr && out10 != nullptr, "null argument");
     DeviceGuard g(h->device);
     h->prof.collect();
-    for (int i = 0; i < 5; ++i) out8[i] = h->prof.total_ms[i];
-    out8[5] = (double)h->prof.launches;
-    out8[6] = (double)h->prof.tc_launches;
-    out8[7] = (double)h->prof.calls;
+    for (int i = 0; i < 6; ++i) out10[i] = h->prof.total_ms[i];
+    out10[6] = (double)h->prof.launches;
+    out10[7] = (double)h->prof.tc_launches;
+    out10[8] = (double)h->prof.filter_launches;
+    out10[9] = (double)h->prof.calls;
     return ANN_OK;
 }
 
@@ -628,7 +629,8 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
             int* flags = cb.take<int>(4);
             __nv_bfloat16* A2 = cb.take<__nv_bfloat16>((size_t)kRerunBatch * kpad);
 
-            const int prec = h->prof.begin(st, 2);  // stages 2: tensor-core passes, 3: selections
+            // stages 2: sample pass and bars, 3: filter pass, 4: grouping, selections and re-runs
+            const int prec = h->prof.begin(st, 2);
             TcGemmArgs sa{nc, (int)S, kpad, nullptr, kA, S, h->d_err};
             sa.b_tile_stride = stride;
             sa.b_rows = n;
@@ -646,6 +648,7 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
                 bar.kth_upper = 1;
                 if ((rc = launch_radix_select(bar, nc, st))) return rc;
             }
+            h->prof.mark(prec, st);
             auto filter = [&](const __nv_bfloat16* A, int M, const float* tau) -> int {
                 TcGemmArgs fa{M, (int)n, kpad, nullptr, nullptr, n, h->d_err};
                 fa.tau = tau;
@@ -662,6 +665,7 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
             };
             if ((rc = filter(qbc, nc, tauF))) return rc;
             h->prof.mark(prec, st);
+            if (prec >= 0) h->prof.filter_launches += 1;
             ANN_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int), st));
             if ((rc = launch_tc_bar_check(rowcnt, nc, R, list, flags, st))) return rc;
             int hf[2] = {0, 0};  // re-runs, largest warp count
@@ -704,7 +708,7 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
             const int nf = std::min(qfull, nc - f0);
             if ((rc = ws_reserve_big(ws, sizeof(float) * (size_t)nf * n))) return rc;
             float* keys = reinterpret_cast<float*>(ws->big);
-            const int prec = h->prof.begin(st, 2);
+            const int prec = h->prof.begin(st, 3);  // stage 3: the full key matrix, 4: its selection
             TcGemmArgs a{nf, (int)n, kpad, nullptr, keys, n, h->d_err};
             if ((rc = launch_tc_gemm(qbc + (size_t)f0 * kpad, h->base_bf16, a, st))) return rc;
             h->prof.mark(prec, st);
@@ -720,7 +724,7 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
             if (prec >= 0) h->prof.tc_launches += 1;
         }
     }
-    const int prec = h->prof.begin(st, 4);  // stage 4: re-rank
+    const int prec = h->prof.begin(st, 5);  // stage 5: re-rank
     IvfQueryArgs ra{};
     ra.ix.n = h->n;
     ra.ix.dim = h->dim;

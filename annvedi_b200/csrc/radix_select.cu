@@ -267,11 +267,23 @@ __global__ void __launch_bounds__(kBarThreads) sample_bars_kernel(const float* _
     float4* sK4 = reinterpret_cast<float4*>(sK);
     const int S4 = S / 4;
     float lo = kInf, hi = -kInf;
-    for (int i = threadIdx.x; i < S4; i += kBarThreads) {
-        const float4 v = src[i];
-        sK4[i] = v;
-        lo = fminf(lo, fminf(fminf(v.x, v.y), fminf(v.z, v.w)));
-        hi = fmaxf(hi, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+    constexpr int kLoadBatch = 8;  // loads issued before the first is used
+    for (int i0 = threadIdx.x; i0 < S4; i0 += kLoadBatch * kBarThreads) {
+        float4 v[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int i = i0 + u * kBarThreads;
+            if (i < S4) v[u] = __ldcs(src + i);
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int i = i0 + u * kBarThreads;
+            if (i < S4) {
+                sK4[i] = v[u];
+                lo = fminf(lo, fminf(fminf(v[u].x, v[u].y), fminf(v[u].z, v[u].w)));
+                hi = fmaxf(hi, fmaxf(fmaxf(v[u].x, v[u].y), fmaxf(v[u].z, v[u].w)));
+            }
+        }
     }
     for (int i = threadIdx.x; i < kBins; i += kBarThreads) {
         hist[0][i] = 0;

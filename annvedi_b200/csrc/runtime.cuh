@@ -58,6 +58,7 @@ struct StageProfiler {
     double total_ms[kStages] = {0, 0, 0, 0, 0, 0};
     int64_t launches = 0;     // exact-scan launches
     int64_t tc_launches = 0;  // tensor-core GEMM launches
+    int64_t filter_launches = 0;  // tensor-core filter passes timed alone
     int64_t calls = 0;
     std::mutex mu;
 
@@ -111,6 +112,7 @@ struct StageProfiler {
         for (double& t : total_ms) t = 0;
         launches = 0;
         tc_launches = 0;
+        filter_launches = 0;
         calls = 0;
     }
     ~StageProfiler() {

@@ -148,7 +148,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     float* sT = reinterpret_cast<float*>(smem + kStages * (kABytes + kBBytes) + 256);  // [8 warps][32][33]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int mt = (int)ceil_div(a.M, kBM), nt = (int)ceil_div(a.N, kBN), kt = a.K / kBK;
+    const int mt = (int)ceil_div(a.M, kBM), nt = (int)ceil_div(a.N, kBN), kt = (int)ceil_div(a.K, kBK);
+    const int k16_last = (a.K - (kt - 1) * kBK) / 16;  // MMAs of the last k-block (K is a multiple of 16)
     const int64_t tiles = (int64_t)mt * nt;
 
     if (threadIdx.x == 0) {
@@ -205,10 +206,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                     const uint32_t ph = (uint32_t)((it / kStages) & 1);
                     if (!(ok = bar_wait(&full[s], ph, a.err))) break;
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    // the last k-block's box runs past K (zero fill); its zero columns are not multiplied
+                    const int n16 = kb == kt - 1 ? k16_last : kBK / 16;
 #pragma unroll
                     for (int k16 = 0; k16 < kBK / 16; ++k16)
-                        mma_bf16(d, sw128_desc(sA + s * kABytes + k16 * 32), sw128_desc(sB + s * kBBytes + k16 * 32),
-                                 (kb | k16) ? 1u : 0u);
+                        if (k16 < n16)
+                            mma_bf16(d, sw128_desc(sA + s * kABytes + k16 * 32),
+                                     sw128_desc(sB + s * kBBytes + k16 * 32), (kb | k16) ? 1u : 0u);
                     mma_commit(&empty[s]);
                 }
                 mma_commit(&tfull[b]);
@@ -347,13 +351,13 @@ int make_map(CUtensorMap* tm, const void* base, int64_t rows, int cols, int box_
 
 size_t tc_gemm_smem() { return (size_t)kStages * (kABytes + kBBytes) + 1024 + 256 + kEpiWarps * 32 * 33 * 4; }
 
-int tc_kpad(int dim, int metric) { return (int)ceil_div(dim + (metric == ANN_METRIC_L2 ? 3 : 0), kBK) * kBK; }
+int tc_kpad(int dim, int metric) { return (int)ceil_div(dim + (metric == ANN_METRIC_L2 ? 3 : 0), 16) * 16; }
 
 static int tc_grid(int M, int N) { return (int)std::min<int64_t>(ceil_div(M, kBM) * ceil_div(N, kBN), kNumSMs); }
 int tc_filter_warps(int M, int N) { return tc_grid(M, N) * kEpiWarps; }
 
 int launch_tc_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, const TcGemmArgs& a, cudaStream_t st) {
-    ANN_CHECK_ARG(a.K % kBK == 0 && a.K > 0, "tensor-core scan: K=%d not a positive multiple of %d", a.K, kBK);
+    ANN_CHECK_ARG(a.K % 16 == 0 && a.K > 0, "tensor-core scan: K=%d not a positive multiple of 16", a.K);
     ANN_CHECK_ARG((reinterpret_cast<uintptr_t>(A) & 15) == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0,
                   "tensor-core scan: operands must be 16-byte aligned");
     ANN_CHECK_ARG(a.out != nullptr || (a.tau && a.fkey && a.fcol && a.frow && a.wcount && a.wcap > 0),
@@ -409,7 +413,7 @@ __global__ void tc_operand_kernel(const float* __restrict__ x, int64_t rows, int
 
 int launch_tc_operand(const float* x, int64_t rows, int cols, int64_t ld, __nv_bfloat16* out, int kpad, int role,
                       int metric, int64_t row_mult, cudaStream_t st) {
-    ANN_CHECK_ARG(kpad >= tc_kpad(cols, metric) && kpad % kBK == 0, "tensor-core operand: kpad %d too small", kpad);
+    ANN_CHECK_ARG(kpad >= tc_kpad(cols, metric) && kpad % 16 == 0, "tensor-core operand: kpad %d too small", kpad);
     ANN_CHECK_ARG(row_mult == 0 || role == kTcBase, "tensor-core operand: only the base is reordered");
     if (rows == 0) return ANN_OK;
     const bool l2 = metric == ANN_METRIC_L2;

@@ -12,7 +12,7 @@ namespace annb {
 //   IP: base row [bf16(b)], query row [bf16(-a)]  ->  sum = -a.b
 // Smaller keys are better in both metrics.
 struct TcGemmArgs {
-    int M, N, K;           // A [M, K], B [N, K] BF16 row-major; K a multiple of 64
+    int M, N, K;           // A [M, K], B [N, K] BF16 row-major; K a multiple of 16
     const float* normA;    // [M] optional per-row addend (|a|^2 turns the L2 key into the squared distance)
     float* out;            // [M, ldo] keys; null in filter mode
     int64_t ldo;
@@ -33,7 +33,7 @@ struct TcGemmArgs {
 enum TcRole { kTcBase = 0, kTcQuery = 1 };
 
 // Columns of the BF16 operands for vectors of `dim` FP32 values: the key columns included, rounded up
-// to the 64-column k-block.
+// to the 16-column MMA step (the 64-column TMA boxes of the last k-block read zeros past it).
 int tc_kpad(int dim, int metric);
 // Epilogue warps of a filter launch over M x N keys (the size of the wcount array).
 int tc_filter_warps(int M, int N);

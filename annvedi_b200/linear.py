@@ -191,13 +191,13 @@ class LinearIndex:
         return {"scan_ms": out[0], "merge_ms": out[1], "scan_launches": int(out[2]), "query_calls": int(out[3])}
 
     def get_stage_times(self) -> dict:
-        """Every stage total: the exact scan's and the tensor-core search's (GEMM passes, selections,
-        exact re-rank), with launch counts."""
-        out = (ctypes.c_double * 8)()
+        """Every stage total: the exact scan's and the tensor-core search's (sample pass and bars, filter
+        pass, selections, exact re-rank), with launch counts."""
+        out = (ctypes.c_double * 10)()
         _lib.check(self._lib.ann_flat_profile_stages(self._h, out))
-        return {"scan_ms": out[0], "merge_ms": out[1], "tc_gemm_ms": out[2], "tc_select_ms": out[3],
-                "rerank_ms": out[4], "scan_launches": int(out[5]), "tc_gemm_launches": int(out[6]),
-                "query_calls": int(out[7])}
+        return {"scan_ms": out[0], "merge_ms": out[1], "tc_sample_ms": out[2], "tc_filter_ms": out[3],
+                "tc_select_ms": out[4], "rerank_ms": out[5], "scan_launches": int(out[6]),
+                "tc_gemm_launches": int(out[7]), "tc_filter_launches": int(out[8]), "query_calls": int(out[9])}
 
     def reset_profile_results(self) -> None:
         _lib.check(self._lib.ann_flat_reset_profile(self._h))

@@ -96,10 +96,11 @@ int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t
 int ann_flat_set_profiling(ann_flat* h, int32_t enable);
 int ann_flat_profile(ann_flat* h, double* out4);
 int ann_flat_reset_profile(ann_flat* h);
-/* All stage totals of the flat index: out[0] scan ms, out[1] merge ms, out[2] tensor-core GEMM passes
- * ms (ann_flat_query_tc), out[3] its selections ms, out[4] its exact re-rank ms, out[5] scan launches,
- * out[6] tensor-core GEMM launches, out[7] profiled calls. */
-int ann_flat_profile_stages(ann_flat* h, double* out8);
+/* All stage totals of the flat index: out[0] scan ms, out[1] merge ms; for ann_flat_query_tc out[2]
+ * sample pass and bars ms, out[3] filter pass (or full key matrix) ms, out[4] grouping, selections and
+ * re-runs ms, out[5] exact re-rank ms; out[6] scan launches, out[7] tensor-core GEMM launches, out[8]
+ * filter passes (each timed alone in out[3]), out[9] profiled calls. */
+int ann_flat_profile_stages(ann_flat* h, double* out10);
 
 /* Tensor-core form of ann_flat_query (no counterpart in the reference; the reference's only fast scan
  * is its CPU loop): keys for every (query, row) from a BF16 tcgen05 GEMM with FP32 accumulation
