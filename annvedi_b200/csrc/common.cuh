@@ -9,11 +9,36 @@
 #include <cfloat>
 #include <climits>
 #include <cstdio>
+#include <mutex>
+#include <set>
 #include <string>
+#include <utility>
 
 #include "../../include/annvedi_b200.h"
 
 namespace annb {
+
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in maximum, once per (kernel,
+// device). Launches of any size up to that limit then need no attribute call, so concurrent host
+// threads never change a kernel's attributes while another thread launches it.
+inline cudaError_t smem_optin(const void* func) {
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({func, dev})) return cudaSuccess;
+    cudaFuncAttributes fa;
+    if ((e = cudaFuncGetAttributes(&fa, func)) != cudaSuccess) return e;
+    int optin = 0;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes)) !=
+        cudaSuccess)
+        return e;
+    done.insert({func, dev});
+    return cudaSuccess;
+}
 
 // ---------------------------------------------------------------------------------------------
 // Host-side error state: the last failing call's message, per host thread.

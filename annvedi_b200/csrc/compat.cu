@@ -80,14 +80,14 @@ int launch_compat(CompatArgs a, int q_begin, int q_count, cudaStream_t st) {
     if (q_count <= 0 || a.n == 0) return ANN_OK;
     a.q_end = q_begin + q_count;
     const size_t smem = sizeof(float) * kCompatQG * a.dim;
-    ANN_CUDA_TRY(cudaFuncSetAttribute(compat_partials_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(compat_partials_kernel)));
     const int64_t rblocks = std::min<int64_t>(ceil_div(a.n, 16), kNumSMs * 8);
     dim3 g1((unsigned)rblocks, (unsigned)ceil_div(q_count, kCompatQG));
     compat_partials_kernel<<<g1, 256, smem, st>>>(a, q_begin);
     ANN_LAUNCH_CHECK();
     const unsigned g2 = (unsigned)ceil_div(q_count, 4);
     const size_t smem2 = (size_t)4 * topk_cap(a.k) * 8;
-    ANN_CUDA_TRY(cudaFuncSetAttribute(compat_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(compat_select_kernel)));
     compat_select_kernel<<<g2, 128, smem2, st>>>(a, q_begin);
     ANN_LAUNCH_CHECK();
     return ANN_OK;

@@ -312,7 +312,7 @@ int launch_sort_topk(const float* keys, const int* ids, int nq, int k, int negat
     if (nq == 0) return ANN_OK;
     ANN_CHECK_ARG(k >= 1 && k <= 1024, "sort top-k: k=%d outside [1, 1024]", k);
     const size_t smem = (size_t)topk_cap(k) * 8;
-    ANN_CUDA_TRY(cudaFuncSetAttribute(sort_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(sort_topk_kernel)));
     sort_topk_kernel<<<nq, 32, smem, st>>>(keys, ids, nq, k, negate, out_ids, out_dists);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
@@ -465,7 +465,7 @@ template <int BQ, int METRIC>
 static int stream_occupancy(int dpad, int cap) {
     auto kern = flat_stream_kernel<BQ, METRIC>;
     const size_t smem = stream_smem(BQ, dpad, cap);
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    if (smem_optin(reinterpret_cast<const void*>(kern)) != cudaSuccess) {
         cudaGetLastError();
         return 1;
     }
@@ -492,7 +492,7 @@ template <int BQ, int METRIC>
 static int launch_stream_t(const FlatScanArgs& a, int n_qtiles, cudaStream_t st) {
     auto kern = flat_stream_kernel<BQ, METRIC>;
     const size_t smem = stream_smem(BQ, a.dpad, a.cap);
-    ANN_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(kern)));
     dim3 grid(n_qtiles, a.nsplit);
     kern<<<grid, 32 * kStreamWarps, smem, st>>>(a);
     ANN_LAUNCH_CHECK();
@@ -517,7 +517,7 @@ static int launch_scan_t(FlatScanArgs a, int n_qtiles, cudaStream_t st) {
     auto kern = flat_scan_kernel<BQ, TQ, TR, STAGES, METRIC>;
     const size_t smem = C::smem(a.cap);
     ANN_CHECK_ARG(smem <= 227 * 1024, "flat scan: %zu bytes of shared memory for k=%d", smem, a.k);
-    ANN_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(kern)));
     dim3 grid(n_qtiles, a.nsplit);
     kern<<<grid, C::THREADS, smem, st>>>(a);
     ANN_LAUNCH_CHECK();
@@ -567,7 +567,7 @@ int launch_merge_splits(const MergeArgs& a, cudaStream_t st) {
     ANN_CHECK_ARG(a.k >= 1 && a.k <= 1024, "merge: k=%d outside [1, 1024]", a.k);
     if (a.nq == 0) return ANN_OK;
     const size_t smem = (size_t)8 * topk_cap(a.k) * 8;
-    ANN_CUDA_TRY(cudaFuncSetAttribute(merge_splits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(merge_splits_kernel)));
     merge_splits_kernel<<<a.nq, 256, smem, st>>>(a);
     ANN_LAUNCH_CHECK();
     return ANN_OK;

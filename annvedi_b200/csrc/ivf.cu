@@ -456,7 +456,7 @@ template <int W>
 static int launch_stream_t(const IvfQueryArgs& a, cudaStream_t st) {
     const int dpad8 = 16 * W;
     const size_t smem = stream_smem(dpad8, a.R, a.plan.npc);
-    ANN_CUDA_TRY(cudaFuncSetAttribute(ivf_sq8_stream_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(ivf_sq8_stream_kernel<W>)));
     dim3 grid(a.plan.nq, a.nsplit);
     ivf_sq8_stream_kernel<W><<<grid, 288, smem, st>>>(a, stream_tile_rows(dpad8));
     ANN_LAUNCH_CHECK();
@@ -494,7 +494,7 @@ int launch_ivf_sq8_scan(const IvfQueryArgs& a, cudaStream_t st) {
         set_error("sq8 scan: R=%d with dim %d needs %zu bytes of shared memory", a.R, a.ix.dim, smem);
         return ANN_ERR_UNSUPPORTED;
     }
-    ANN_CUDA_TRY(cudaFuncSetAttribute(ivf_sq8_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(ivf_sq8_scan_kernel)));
     dim3 grid(a.plan.nq, a.nsplit);
     ivf_sq8_scan_kernel<<<grid, 256, smem, st>>>(a);
     ANN_LAUNCH_CHECK();
@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(128) ivf_ref_replay_kernel(IvfQueryArgs a) {
 int launch_ivf_ref_sq8(const IvfQueryArgs& a, int64_t Lmax, cudaStream_t st) {
     if (a.plan.nq == 0 || Lmax == 0) return ANN_OK;
     const size_t smem = sizeof(float) * 2 * a.ix.dim;
-    ANN_CUDA_TRY(cudaFuncSetAttribute(ivf_ref_sq8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(ivf_ref_sq8_kernel)));
     const int64_t blocks = std::min<int64_t>(ceil_div(Lmax, 16), 4096);
     dim3 g1(a.plan.nq, (unsigned)blocks);
     ivf_ref_sq8_kernel<<<g1, 256, smem, st>>>(a);
@@ -618,7 +618,7 @@ int launch_select_topk(const float* keys, int64_t ld, const int64_t* lens, int n
     int warps = (int)std::max<size_t>(1, std::min<size_t>(8, (96 * 1024) / per_warp));
     const size_t smem = per_warp * warps;
     ANN_CHECK_ARG(smem <= 227 * 1024, "select: k=%d needs too much shared memory", kout);
-    ANN_CUDA_TRY(cudaFuncSetAttribute(select_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(select_topk_kernel)));
     IvfPlan p{};
     if (plan) p = *plan;
     select_topk_kernel<<<nq, warps * 32, smem, st>>>(keys, ld, offs, lens, kout, p, plan ? 1 : 0, out_key, out_id);
@@ -711,10 +711,10 @@ int launch_ivf_rerank(const IvfQueryArgs& a, const float* keyR, const int* idR, 
     const size_t smem = sizeof(float) * a.ix.dpad + (size_t)a.R * 8 + (size_t)topk_cap(a.k) * 8;
     ANN_CHECK_ARG(smem <= 227 * 1024, "re-rank: R=%d, k=%d need too much shared memory", a.R, a.k);
     if (reference) {
-        ANN_CUDA_TRY(cudaFuncSetAttribute(ivf_rerank_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(ivf_rerank_kernel<true>)));
         ivf_rerank_kernel<true><<<a.plan.nq, 256, smem, st>>>(a, keyR, idR);
     } else {
-        ANN_CUDA_TRY(cudaFuncSetAttribute(ivf_rerank_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(ivf_rerank_kernel<false>)));
         ivf_rerank_kernel<false><<<a.plan.nq, 256, smem, st>>>(a, keyR, idR);
     }
     ANN_LAUNCH_CHECK();
@@ -741,7 +741,7 @@ __global__ void __launch_bounds__(256) ref_centroid_kernel(IvfView ix, const flo
 int launch_ref_centroid_dists(const IvfView& ix, const float* q, int64_t ldq, int nq, float* Dc, cudaStream_t st) {
     if (nq == 0) return ANN_OK;
     const size_t smem = sizeof(float) * ix.dim;
-    ANN_CUDA_TRY(cudaFuncSetAttribute(ref_centroid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(ref_centroid_kernel)));
     dim3 g(nq, (unsigned)std::min<int64_t>(ceil_div(ix.C, 16), 64));
     ref_centroid_kernel<<<g, 256, smem, st>>>(ix, q, ldq, Dc);
     ANN_LAUNCH_CHECK();

@@ -311,7 +311,7 @@ int launch_batched(const IvfBatchArgs& b, const float* qdev, float* qs, float* D
     const size_t smem = sizeof(float) * ((size_t)kBQ * a.ix.dpad + (size_t)kBR * kPitch + a.ix.dpad) +
                         (size_t)2 * kBR * kKC + sizeof(int64_t) * kBQ + 16;
     ANN_CHECK_ARG(smem <= 227 * 1024, "batched SQ8 pass: dim %d needs %zu bytes of shared memory", a.ix.dim, smem);
-    ANN_CUDA_TRY(cudaFuncSetAttribute(ivf_batched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(ivf_batched_kernel)));
     int per_sm = 0;
     ANN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ivf_batched_kernel, kThreads, smem));
     const int grid = kNumSMs * std::max(1, per_sm);

@@ -352,7 +352,7 @@ int launch_sample_bars(const float* keys, int S, int nq, int r1, int r2, float* 
     ANN_CHECK_ARG(S > 0 && S % 4 == 0 && sample_bars_smem(S) <= kSampleBarsMaxSmem && r1 >= 1 && r2 >= 1,
                   "sample bars: S=%d, ranks %d, %d", S, r1, r2);
     const int smem = (int)sample_bars_smem(S);
-    ANN_CUDA_TRY(cudaFuncSetAttribute(sample_bars_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(sample_bars_kernel)));
     sample_bars_kernel<<<nq, kBarThreads, smem, st>>>(keys, S, r1, r2, bar1, bar2);
     ANN_LAUNCH_CHECK();
     return ANN_OK;

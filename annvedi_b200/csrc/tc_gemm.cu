@@ -374,7 +374,7 @@ int launch_tc_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, const TcGemmA
     rc = make_map(&tmB, B, b_rows, a.K, kBN);
     if (rc) return rc;
     const size_t smem = tc_gemm_smem();
-    ANN_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(tc_gemm_kernel)));
     tc_gemm_kernel<<<tc_grid(a.M, a.N), kThreads, smem, st>>>(tmA, tmB, a);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
