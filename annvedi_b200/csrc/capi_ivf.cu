@@ -6,6 +6,7 @@
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -13,8 +14,11 @@
 #include "flat_scan.cuh"
 #include "ivf.cuh"
 #include "ivf_batched.cuh"
+#include "radix_select.cuh"
 #include "refmath.cuh"
 #include "runtime.cuh"
+#include "tc_gemm.cuh"
+#include "tc_search.cuh"
 
 using namespace annb;
 
@@ -35,6 +39,10 @@ struct ann_ivf {
     std::vector<int64_t> sizes_desc;  // list sizes, largest first (bounds for planning)
     ann_workspace ws;
     StageProfiler prof;  // 0: coarse ranking, 1: plan, 2: SQ8 pass (+ merge), 3: re-rank
+    __nv_bfloat16* base_bf16 = nullptr;  // [n, kpad] BF16 operand form of the list-ordered rows (tensor-core form)
+    __nv_bfloat16* cent_bf16 = nullptr;  // [C, kpad] BF16 operand form of the centroids
+    int kpad = 0;
+    std::mutex tc_mu;
     int64_t query_count = 0;
 
     IvfView view() const {
@@ -57,8 +65,11 @@ struct ann_ivf {
 
 static void ivf_free_state(ann_ivf* h) {
     for (void* p : {(void*)h->centroids, (void*)h->original, (void*)h->codes, (void*)h->scale, (void*)h->offset,
-                    (void*)h->r2o, (void*)h->list_off})
+                    (void*)h->r2o, (void*)h->list_off, (void*)h->base_bf16, (void*)h->cent_bf16})
         if (p) cudaFree(p);
+    h->base_bf16 = nullptr;
+    h->cent_bf16 = nullptr;
+    h->kpad = 0;
     h->centroids = nullptr;
     h->original = nullptr;
     h->codes = nullptr;
@@ -397,9 +408,37 @@ const int g_scan_kind = [] {
 struct IvfQueryCfg {
     int k, npc, R, nsplit, num_threads, bqc, nsplit_c, ncp;
     int64_t max_c, ub, rps_c;
-    bool ref, coarse_flat, batched;
+    bool ref, coarse_flat, batched, tc;
     size_t sort_tmp, scan_tmp, bscratch;
 };
+
+// BF16 operand form of the list-ordered rows for the tensor-core form, built once.
+static int ivf_ensure_bf16(ann_ivf* h, cudaStream_t st) {
+    std::lock_guard<std::mutex> lk(h->tc_mu);
+    if (h->base_bf16) return ANN_OK;
+    const int kpad = tc_kpad(h->dim, ANN_METRIC_L2);
+    __nv_bfloat16 *b = nullptr, *cb = nullptr;
+    cudaError_t e = cudaMalloc(&b, sizeof(__nv_bfloat16) * (size_t)h->n * kpad);
+    if (e == cudaSuccess) e = cudaMalloc(&cb, sizeof(__nv_bfloat16) * (size_t)h->C * kpad);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (b) cudaFree(b);
+        set_error("tensor-core IVF: cannot allocate the BF16 copy of the lists (%s)", cudaGetErrorString(e));
+        return ANN_ERR_NOMEM;
+    }
+    int rc = launch_tc_operand(h->original, h->n, h->dim, h->dpad, b, kpad, kTcBase, ANN_METRIC_L2, 0, st);
+    if (!rc) rc = launch_tc_operand(h->centroids, h->C, h->dim, h->dpad, cb, kpad, kTcBase, ANN_METRIC_L2, 0, st);
+    if (rc) {
+        cudaFree(b);
+        cudaFree(cb);
+        return rc;
+    }
+    ANN_CUDA_TRY(cudaStreamSynchronize(st));
+    h->kpad = kpad;
+    h->cent_bf16 = cb;
+    h->base_bf16 = b;
+    return ANN_OK;
+}
 
 // Bytes of scratch one device-side query call of nq queries needs (mirrors the carving below).
 static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
@@ -424,6 +463,13 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
     if (c.batched) {
         sz.take<float>((size_t)nq * h->dpad);
         sz.take<char>(c.bscratch);
+    }
+    if (c.tc) {
+        sz.take<float>((size_t)nq * h->C);  // BF16 coarse keys
+        sz.take<__nv_bfloat16>((size_t)nq * h->kpad);
+        sz.take<__nv_bfloat16>((size_t)nq * c.npc * h->kpad);
+        sz.take<int64_t>((size_t)nq * c.npc);
+        sz.take<int64_t>((size_t)h->C + 1);
     }
     return sz.off;
 }
@@ -453,6 +499,11 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     float* DP = c.ref ? cv.take<float>((size_t)nq * c.ub * (c.ncp + 2)) : nullptr;
     float* qs = c.batched ? cv.take<float>((size_t)nq * h->dpad) : nullptr;
     void* bscratch = c.batched ? cv.take<char>(c.bscratch) : nullptr;
+    float* ckeys = c.tc ? cv.take<float>((size_t)nq * h->C) : nullptr;
+    __nv_bfloat16* qb = c.tc ? cv.take<__nv_bfloat16>((size_t)nq * h->kpad) : nullptr;
+    __nv_bfloat16* Apk = c.tc ? cv.take<__nv_bfloat16>((size_t)nq * c.npc * h->kpad) : nullptr;
+    int64_t* dbase = c.tc ? cv.take<int64_t>((size_t)nq * c.npc) : nullptr;
+    int64_t* titem = c.tc ? cv.take<int64_t>((size_t)h->C + 1) : nullptr;
 
     IvfQueryArgs a{};
     a.ix = h->view();
@@ -479,7 +530,14 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     int rc;
     const int prec = h->prof.begin(st);
     // 1. coarse ranking
-    if (c.coarse_flat) {
+    if (c.tc) {
+        // BF16 keys to every centroid, then the exact FP32 order of the best npc + 16
+        if ((rc = launch_tc_operand(qdev, nq, h->dim, h->dpad, qb, h->kpad, kTcQuery, ANN_METRIC_L2, 0, st))) return rc;
+        TcGemmArgs ca{nq, h->C, h->kpad, nullptr, ckeys, h->C, h->d_err};
+        if ((rc = launch_tc_gemm(qb, h->cent_bf16, ca, st))) return rc;
+        if ((rc = launch_tc_coarse(ckeys, h->C, nq, h->C, c.npc, 16, qdev, h->centroids, h->dpad, probes, st)))
+            return rc;
+    } else if (c.coarse_flat) {
         FlatScanArgs fa{h->centroids, h->C, h->dpad, qdev, nq, ANN_METRIC_L2, c.npc, c.rps_c, c.nsplit_c, ckey, cid};
         if ((rc = launch_flat_scan(fa, c.bqc, st))) return rc;
         MergeArgs m{ckey, cid, nq, c.nsplit_c, c.npc, c.npc, 0, nullptr, nullptr};
@@ -502,8 +560,37 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         if (tot[2] == 0) {  // no query fell back to scanning every row
             if ((rc = ws_reserve_big(ws, sizeof(float) * (size_t)std::max<int64_t>(tot[1], 1)))) return rc;
             float* D = reinterpret_cast<float*>(ws->big);
-            if ((rc = launch_batched(b, qdev, qs, D, st))) return rc;
-            if ((rc = launch_select_topk(D, 0, n_cands, nq, c.R, &a.plan, keyR, idR, st, b.cand_off))) return rc;
+            if (c.tc) {
+                // BF16 keys of every (pair, list row) from grouped tcgen05 GEMMs, the best R of each
+                // query's stream by radix selection
+                const int kpad = h->kpad;
+                const int64_t max_pairs = (int64_t)nq * c.npc;
+                if ((rc = launch_tc_ivf_pairs(qb, kpad, b.pair_vals, b.pair_lists, b.lq_off + h->C, max_pairs, c.npc,
+                                              b.cand_off, a.plan.seg_pref, h->list_off, Apk, dbase, st)))
+                    return rc;
+                if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, h->C, titem, st))) return rc;
+                TcGemmArgs g{(int)max_pairs, (int)h->n, kpad, nullptr, D, 0, h->d_err};
+                g.g_item_off = titem;
+                g.g_a_off = b.lq_off;
+                g.g_b_off = h->list_off;
+                g.g_dbase = dbase;
+                g.g_total = titem + h->C;
+                g.g_lists = h->C;
+                if ((rc = launch_tc_gemm(Apk, h->base_bf16, g, st))) return rc;
+                RadixSelectArgs rs{};
+                rs.keys = D;
+                rs.offs = b.cand_off;
+                rs.lens = n_cands;
+                rs.plan = a.plan;
+                rs.use_plan = 1;
+                rs.R = c.R;
+                rs.out_key = keyR;
+                rs.out_id = idR;
+                if ((rc = launch_radix_select(rs, nq, st))) return rc;
+            } else {
+                if ((rc = launch_batched(b, qdev, qs, D, st))) return rc;
+                if ((rc = launch_select_topk(D, 0, n_cands, nq, c.R, &a.plan, keyR, idR, st, b.cand_off))) return rc;
+            }
             done = true;
         }
     }
@@ -552,7 +639,8 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     }
     ANN_CHECK_ARG(nq >= 0 && k >= 1, "ann_ivf_query: nq=%d, k=%d", nq, k);
     ANN_CHECK_ARG(ldq >= h->dim, "ann_ivf_query: query stride < dim");
-    ANN_CHECK_ARG(mode == ANN_MODE_EXACT || mode == ANN_MODE_REFERENCE, "ann_ivf_query: unknown mode %d", mode);
+    ANN_CHECK_ARG(mode == ANN_MODE_EXACT || mode == ANN_MODE_REFERENCE || mode == ANN_MODE_TC,
+                  "ann_ivf_query: unknown mode %d", mode);
     ANN_CHECK_ARG(nq == 0 || (queries && out_ids), "ann_ivf_query: null pointer");
     ANN_CHECK_ARG(k <= 1024, "ann_ivf_query: k=%d > 1024", k);
     if (n_probes != 0) {
@@ -565,7 +653,9 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     cudaStream_t st = as_stream(stream);
 
     IvfQueryCfg c{};
+    int rc0 = ANN_OK;
     c.ref = mode == ANN_MODE_REFERENCE;
+    c.tc = mode == ANN_MODE_TC;
     c.k = k;
     c.npc = std::max(1, std::min(n_probe_clusters, h->C));  // active_clusters (:332)
     // R = max(k, refine_r > 0 ? refine_r : 4k) (:472-474); cap max(2000, 4 * target) (:357-358)
@@ -592,7 +682,8 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     c.ub = std::max<int64_t>(ub, 1);
     c.ncp = ref_num_checkpoints(h->dim);
     c.coarse_flat = !c.ref && c.npc <= 512;
-    c.batched = !c.ref && g_scan_kind == kScanBatched && nq >= kBatchedMinQueries;
+    c.batched = !c.ref && (c.tc || (g_scan_kind == kScanBatched && nq >= kBatchedMinQueries));
+    if (c.tc && (rc0 = ivf_ensure_bf16(h, st))) return rc0;
     const int dpad = h->dpad;
     const bool host = mem == ANN_MEM_HOST;
 

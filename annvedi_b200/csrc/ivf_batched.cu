@@ -291,6 +291,7 @@ int batched_prepare(const IvfQueryArgs& a, void* scratch, size_t sort_tmp, size_
     b.ix = a.ix;
     b.plan = a.plan;
     b.pair_vals = vout;
+    b.pair_lists = kout;
     b.lq_off = lq_off;
     b.item_off = item_off;
     b.total_items = item_off + C;

@@ -13,6 +13,7 @@ struct IvfBatchArgs {
     IvfView ix;
     IvfPlan plan;
     const int32_t* pair_vals;   // (q * npc + j) of each probe, grouped by list
+    const int32_t* pair_lists;  // the list of each pair (C past the valid pairs)
     const int64_t* lq_off;      // [C + 1] first pair of each list
     const int64_t* item_off;    // [C + 1] first work item of each list
     const int64_t* total_items; // device scalar (item_off[C])

@@ -67,8 +67,40 @@ __device__ int find_bin(const int* hist, int rank, int* below, int* sScan) {
     return bin;
 }
 
+__device__ __forceinline__ int lin_bin(float k, float lo, float scale) {
+    const float f = (k - lo) * scale;  // NaN (0 * inf) counts as bin 0
+    return !(f > 0.f) ? 0 : (f >= (float)(kBins - 1) ? kBins - 1 : (int)f);
+}
+
+// Block-wide min and max (kThreads threads); the results are visible to every thread on return.
+__device__ void block_minmax(float& lo, float& hi, float* sRed) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        sRed[warp] = lo;
+        sRed[32 + warp] = hi;
+    }
+    __syncthreads();
+    lo = kInf;
+    hi = -kInf;
+    for (int w = 0; w < kThreads / 32; ++w) {
+        lo = fminf(lo, sRed[w]);
+        hi = fmaxf(hi, sRed[32 + w]);
+    }
+    __syncthreads();
+}
+
+constexpr int kLinCap = 2048;  // keys of the final sub-bin sorted in shared memory
+
 __global__ void __launch_bounds__(kThreads) radix_select_kernel(RadixSelectArgs a) {
     __shared__ int hist[2][kBins];
+    __shared__ float sCandK[kLinCap];
+    __shared__ int sCandP[kLinCap];
+    __shared__ float sRed[64];
     __shared__ int sScan[kThreads];
     __shared__ int sCount, sTies;
     const int q = blockIdx.x;
@@ -100,6 +132,105 @@ __global__ void __launch_bounds__(kThreads) radix_select_kernel(RadixSelectArgs 
             if (two) a.out_kth2[orow] = kInf;
         }
         return;
+    }
+    if (want_set && !two && !a.kth_upper) {
+        // Linear bins over the stream's [min, max]: keys of similar magnitude spread over many bins
+        // (the integer image's top bits would put them all in one, serialising the histogram).
+        float lo = kInf, hi = -kInf;
+        for (int64_t p = threadIdx.x; p < len; p += kThreads) {
+            const float kv = kq[p];
+            lo = fminf(lo, kv);
+            hi = fmaxf(hi, kv);
+        }
+        block_minmax(lo, hi, sRed);
+        const float scale1 = (float)kBins / (hi - lo);
+        if (!(hi > lo) || !isfinite(scale1)) {  // all keys equal: the first R in stream order
+            for (int64_t p = threadIdx.x; p < R; p += kThreads) {
+                if (ok) ok[p] = kq[p];
+                if (oi) oi[p] = id_of(p);
+            }
+            return;
+        }
+        for (int i = threadIdx.x; i < kBins; i += kThreads) {
+            hist[0][i] = 0;
+            hist[1][i] = 0;
+        }
+        __syncthreads();
+        for (int64_t p = threadIdx.x; p < len; p += kThreads) atomicAdd(&hist[0][lin_bin(kq[p], lo, scale1)], 1);
+        __syncthreads();
+        int below1 = 0, below2 = 0;
+        const int b1 = find_bin(hist[0], R - 1, &below1, sScan);
+        const float w = (hi - lo) / (float)kBins;
+        const float lo2 = lo + w * (float)b1;
+        const float scale2 = (float)kBins / w;
+        for (int64_t p = threadIdx.x; p < len; p += kThreads) {
+            const float kv = kq[p];
+            if (lin_bin(kv, lo, scale1) == b1) atomicAdd(&hist[1][lin_bin(kv, lo2, scale2)], 1);
+        }
+        __syncthreads();
+        const int b2 = find_bin(hist[1], R - 1 - below1, &below2, sScan);
+        const int ncand = hist[1][b2];
+        const int fixed = below1 + below2;  // keys certainly in the set
+        if (ncand <= kLinCap) {
+            if (threadIdx.x == 0) {
+                sCount = 0;
+                sTies = 0;
+            }
+            __shared__ int sWarpC[kThreads / 32];
+            __syncthreads();
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            for (int64_t base = 0; base < len; base += kThreads) {
+                const int64_t p = base + threadIdx.x;
+                const bool valid = p < len;
+                const float kv = valid ? kq[p] : 0.f;
+                const int bk = valid ? lin_bin(kv, lo, scale1) : kBins;
+                const int sk = bk == b1 ? lin_bin(kv, lo2, scale2) : 0;
+                if (valid && (bk < b1 || (bk == b1 && sk < b2))) {
+                    const int slot = atomicAdd(&sCount, 1);
+                    if (ok) ok[slot] = kv;
+                    if (oi) oi[slot] = id_of(p);
+                }
+                const bool cand = valid && bk == b1 && sk == b2;
+                const unsigned bal = __ballot_sync(0xffffffffu, cand);
+                if (__syncthreads_or(bal != 0)) {  // uniform: gather the sub-bin's keys in stream order
+                    if (lane == 0) sWarpC[warp] = __popc(bal);
+                    __syncthreads();
+                    int before = sTies;
+                    for (int ww = 0; ww < warp; ++ww) before += sWarpC[ww];
+                    if (cand) {
+                        const int at = before + __popc(bal & ((1u << lane) - 1u));
+                        sCandK[at] = kv;
+                        sCandP[at] = (int)p;
+                    }
+                    __syncthreads();
+                    if (threadIdx.x == 0) {
+                        int tot = 0;
+                        for (int ww = 0; ww < kThreads / 32; ++ww) tot += sWarpC[ww];
+                        sTies += tot;
+                    }
+                    __syncthreads();
+                }
+            }
+            // the sub-bin's keys by (key, stream position); the first `need` complete the set
+            if (threadIdx.x < 32) {
+                int cap2 = 32;
+                while (cap2 < ncand) cap2 <<= 1;
+                for (int e = ncand + threadIdx.x; e < cap2; e += 32) {
+                    sCandK[e] = kInf;
+                    sCandP[e] = INT_MAX;
+                }
+                __syncwarp();
+                warp_sort_smem(sCandK, sCandP, cap2);
+            }
+            __syncthreads();
+            const int need = R - fixed;
+            for (int e = threadIdx.x; e < need; e += kThreads) {
+                if (ok) ok[fixed + e] = sCandK[e];
+                if (oi) oi[fixed + e] = id_of(sCandP[e]);
+            }
+            return;
+        }
+        __syncthreads();  // more equal keys than the buffer holds: the exact integer radix below
     }
     const int npass = (a.kth_upper && !want_set) ? 2 : 3;
     uint32_t prefix[2] = {0, 0}, mask = 0;
@@ -190,10 +321,6 @@ __global__ void __launch_bounds__(kThreads) radix_select_kernel(RadixSelectArgs 
 // them (a bar at or above the r-th smallest key, within a sub-bin of it).
 constexpr int kBarThreads = 1024;
 
-__device__ __forceinline__ int lin_bin(float k, float lo, float scale) {
-    const float f = (k - lo) * scale;  // NaN (0 * inf) counts as bin 0
-    return !(f > 0.f) ? 0 : (f >= (float)(kBins - 1) ? kBins - 1 : (int)f);
-}
 
 // rank-th smallest (0-based) bin of a histogram over kBins, kBarThreads threads.
 __device__ int find_bin_bar(const int* hist, int rank, int* below, int* sScan) {

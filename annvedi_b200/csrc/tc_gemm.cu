@@ -129,6 +129,33 @@ __device__ __forceinline__ void tmem_after_wait(uint32_t (&r)[32]) {
                  : "memory");
 }
 
+// A grouped-mode work item: A rows [a0, a0 + am), B rows [b0, b0 + bn).
+struct GroupTile {
+    int64_t a0, b0;
+    int am, bn;
+};
+__device__ __forceinline__ GroupTile group_tile(const TcGemmArgs& a, int64_t t) {
+    int lo = 0, hi = a.g_lists - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a.g_item_off[mid] <= t)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const int64_t np = a.g_a_off[lo + 1] - a.g_a_off[lo];
+    const int64_t nr = a.g_b_off[lo + 1] - a.g_b_off[lo];
+    const int64_t npt = (np + kBM - 1) / kBM;
+    const int64_t local = t - a.g_item_off[lo];
+    const int64_t g = local % npt, rt = local / npt;
+    GroupTile gt;
+    gt.a0 = a.g_a_off[lo] + g * kBM;
+    gt.b0 = a.g_b_off[lo] + rt * kBN;
+    gt.am = (int)min((int64_t)kBM, np - g * kBM);
+    gt.bn = (int)min((int64_t)kBN, nr - rt * kBN);
+    return gt;
+}
+
 constexpr int kEpiWarps = 8;
 constexpr int kThreads = 64 + 32 * kEpiWarps;
 
@@ -150,7 +177,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = (int)ceil_div(a.M, kBM), nt = (int)ceil_div(a.N, kBN), kt = (int)ceil_div(a.K, kBK);
     const int k16_last = (a.K - (kt - 1) * kBK) / 16;  // MMAs of the last k-block (K is a multiple of 16)
-    const int64_t tiles = (int64_t)mt * nt;
+    const bool grouped = a.g_item_off != nullptr;
+    const int64_t tiles = grouped ? *a.g_total : (int64_t)mt * nt;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -180,14 +208,22 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             int64_t it = 0;
             bool ok = true;
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-                const int m0 = (int)(t % mt) * kBM, n0 = (int)(t / mt) * kBN;
+                int64_t arow, brow;
+                if (grouped) {
+                    const GroupTile gt = group_tile(a, t);
+                    arow = gt.a0;
+                    brow = gt.b0;
+                } else {
+                    arow = (t % mt) * kBM;
+                    brow = (t / mt) * kBN * a.b_tile_stride;
+                }
                 for (int kb = 0; kb < kt; ++kb, ++it) {
                     const int s = (int)(it % kStages);
                     const uint32_t ph = (uint32_t)((it / kStages) & 1);
                     if (!(ok = bar_wait(&empty[s], ph ^ 1u, a.err))) break;
                     bar_expect(&full[s], kABytes + kBBytes);
-                    tma_load_2d(sA + s * kABytes, &tmA, kb * kBK, m0, &full[s]);
-                    tma_load_2d(sB + s * kBBytes, &tmB, kb * kBK, n0 * a.b_tile_stride, &full[s]);
+                    tma_load_2d(sA + s * kABytes, &tmA, kb * kBK, (int)arow, &full[s]);
+                    tma_load_2d(sB + s * kBBytes, &tmB, kb * kBK, (int)brow, &full[s]);
                 }
             }
         }
@@ -235,6 +271,40 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int m0 = (int)(t % mt) * kBM, n0 = (int)(t / mt) * kBN;
             const int m = m0 + lane_base + lane;
+            if (grouped) {  // keys of pair a0 + row, list rows b0 + column, to their stream positions
+                const GroupTile gt = group_tile(a, t);
+                const int ml = lane_base + lane;
+                // the stream position of list row b0 for each of the warp's 32 pairs (lane r holds row r's)
+                const int64_t dst_lane = (ml < gt.am ? a.g_dbase[gt.a0 + ml] : 0) + gt.b0;
+                const int rows = min(32, gt.am - lane_base);  // valid pairs of this warp
+                const uint32_t tb = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kBN + col0);
+#pragma unroll 1
+                for (int c = 0; c < 128; c += 64) {
+                    uint32_t r0[32], r1[32];
+                    tmem_ld32(tb + (uint32_t)c, r0);
+                    tmem_ld32(tb + (uint32_t)(c + 32), r1);
+                    tmem_wait(r0);
+                    tmem_after_wait(r1);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int cb = col0 + c + 32 * h;
+                        if (rows <= 0 || cb >= gt.bn) continue;  // uniform across the warp
+                        // transpose through shared memory: each store writes 32 consecutive keys of one pair
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) tw[lane * 33 + u] = __uint_as_float(h ? r1[u] : r0[u]);
+                        __syncwarp();
+                        const bool cok = cb + lane < gt.bn;
+                        for (int r = 0; r < rows; ++r) {
+                            const int64_t dr = __shfl_sync(0xffffffffu, dst_lane, r);
+                            if (cok) a.out[dr + cb + lane] = tw[r * 33 + lane];
+                        }
+                        __syncwarp();
+                    }
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                bar_arrive(&tempty[b]);
+                continue;
+            }
             const float an = (a.normA && m < a.M) ? a.normA[m] : 0.f;
             // rows past M (TMA zero fill) get a bar no key passes
             const float tau = (a.tau && m < a.M) ? a.tau[m] : -kInf;
@@ -362,11 +432,14 @@ int launch_tc_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, const TcGemmA
                   "tensor-core scan: operands must be 16-byte aligned");
     ANN_CHECK_ARG(a.out != nullptr || (a.tau && a.fkey && a.fcol && a.frow && a.wcount && a.wcap > 0),
                   "tensor-core scan: neither an output matrix nor a filter");
+    ANN_CHECK_ARG(a.g_item_off == nullptr ||
+                      (a.out && a.g_a_off && a.g_b_off && a.g_dbase && a.g_total && a.g_lists > 0 && a.tau == nullptr),
+                  "tensor-core scan: incomplete grouping");
     ANN_CHECK_ARG(a.b_tile_stride >= 1, "tensor-core scan: bad sample stride");
     if (a.M == 0 || a.N == 0) return ANN_OK;
     const int64_t b_rows = a.b_rows > 0 ? a.b_rows : a.N;
     // the last sampled tile must start inside B
-    ANN_CHECK_ARG((ceil_div(a.N, kBN) - 1) * kBN * (int64_t)a.b_tile_stride < b_rows,
+    ANN_CHECK_ARG(a.g_item_off != nullptr || (ceil_div(a.N, kBN) - 1) * kBN * (int64_t)a.b_tile_stride < b_rows,
                   "tensor-core scan: sample runs past the base");
     CUtensorMap tmA, tmB;
     int rc = make_map(&tmA, A, a.M, a.K, kBM);
@@ -375,7 +448,8 @@ int launch_tc_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, const TcGemmA
     if (rc) return rc;
     const size_t smem = tc_gemm_smem();
     ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(tc_gemm_kernel)));
-    tc_gemm_kernel<<<tc_grid(a.M, a.N), kThreads, smem, st>>>(tmA, tmB, a);
+    const int grid = a.g_item_off ? kNumSMs : tc_grid(a.M, a.N);  // grouped: persistent over the items
+    tc_gemm_kernel<<<grid, kThreads, smem, st>>>(tmA, tmB, a);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

@@ -28,6 +28,17 @@ struct TcGemmArgs {
     int* frow = nullptr;
     int* wcount = nullptr;
     int wcap = 0;
+    // Grouped mode (g_item_off != null; out receives the keys): tile t is work item t of a list-major
+    // grouping (an IVF batch). List l owns A rows [g_a_off[l], g_a_off[l+1]) (its (query, list) pairs)
+    // and B rows [g_b_off[l], g_b_off[l+1]) (its rows); its items are ceil(pairs/128) x ceil(rows/256)
+    // tiles, pair tiles fastest, numbered from g_item_off[l]; *g_total items in all (read on the
+    // device). The key of pair i and list row r goes to out[g_dbase[i] + r].
+    const int64_t* g_item_off = nullptr;
+    const int64_t* g_a_off = nullptr;
+    const int64_t* g_b_off = nullptr;
+    const int64_t* g_dbase = nullptr;
+    const int64_t* g_total = nullptr;
+    int g_lists = 0;
 };
 
 enum TcRole { kTcBase = 0, kTcQuery = 1 };

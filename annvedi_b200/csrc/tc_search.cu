@@ -107,7 +107,132 @@ __global__ void tc_unpermute_kernel(const float* keys, int64_t n, int64_t mult, 
         out[(int64_t)q * n + pos_to_row(p, n, mult)] = keys[(int64_t)q * n + p];
 }
 
+__global__ void __launch_bounds__(1024) tc_ivf_items_kernel(const int64_t* lq_off, const int64_t* list_off, int C,
+                                                            int64_t* item_off) {
+    __shared__ int64_t sPart[1024];
+    const int per = (C + 1023) / 1024;
+    const int l0 = threadIdx.x * per;
+    auto items = [&](int l) -> int64_t {
+        const int64_t np = lq_off[l + 1] - lq_off[l], nr = list_off[l + 1] - list_off[l];
+        return (np == 0 || nr == 0) ? 0 : ((np + 127) / 128) * ((nr + 255) / 256);
+    };
+    int64_t local = 0;
+    for (int i = 0; i < per; ++i)
+        if (l0 + i < C) local += items(l0 + i);
+    sPart[threadIdx.x] = local;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const int64_t v = threadIdx.x >= off ? sPart[threadIdx.x - off] : 0;
+        __syncthreads();
+        sPart[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int64_t run = sPart[threadIdx.x] - local;
+    for (int i = 0; i < per; ++i) {
+        const int l = l0 + i;
+        if (l < C) {
+            item_off[l] = run;
+            run += items(l);
+        }
+    }
+    if (threadIdx.x == 1023) item_off[C] = sPart[1023];
+}
+
+// one warp per pair
+__global__ void tc_ivf_pairs_kernel(const __nv_bfloat16* qb, int kpad, const int32_t* pair_vals,
+                                    const int32_t* pair_lists, const int64_t* n_pairs, int64_t max_pairs, int npc,
+                                    const int64_t* cand_off, const int64_t* seg_pref, const int64_t* list_off,
+                                    __nv_bfloat16* A, int64_t* dbase) {
+    const int64_t np = min(*n_pairs, max_pairs);
+    const int lane = threadIdx.x & 31;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < np;
+         i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int32_t v = pair_vals[i];
+        const int q = v / npc, j = v % npc;
+        const uint4* src = reinterpret_cast<const uint4*>(qb + (size_t)q * kpad);
+        uint4* dst = reinterpret_cast<uint4*>(A + (size_t)i * kpad);
+        for (int c = lane; c < kpad / 8; c += 32) dst[c] = src[c];
+        if (lane == 0) dbase[i] = cand_off[q] + seg_pref[(int64_t)q * (npc + 1) + j] - list_off[pair_lists[i]];
+    }
+}
+
+// one warp per query
+__global__ void __launch_bounds__(128) tc_coarse_kernel(const float* __restrict__ keys, int64_t ldk, int nq, int C,
+                                                       int npc, int m, const float* __restrict__ q,
+                                                       const float* __restrict__ cent, int dpad, int32_t* probes) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cap = topk_cap(m);
+    float* sK = reinterpret_cast<float*>(smem_raw) + warp * 2 * cap;
+    int* sI = reinterpret_cast<int*>(sK + cap);
+    const int qi = blockIdx.x * 4 + warp;
+    if (qi >= nq) return;
+    WarpTopK top;
+    top.init(sK, sI, m);
+    const float* kr = keys + (int64_t)qi * ldk;
+    for (int c0 = 0; c0 < C; c0 += 32) {
+        const int c = c0 + lane;
+        top.offer(c < C ? kr[c] : kInf, c < C ? c : kNoId, c < C);
+    }
+    top.compact();
+    const int cnt = top.count;
+    // exact FP32 squared distances of the m candidates
+    const float* qv = q + (int64_t)qi * dpad;
+    for (int e = 0; e < cnt; ++e) {
+        const int c = sI[e];
+        const float* x = cent + (int64_t)c * dpad;
+        float acc = 0.f;
+        for (int d = lane; d < dpad; d += 32) {
+            const float t = x[d] - qv[d];
+            acc = fmaf(t, t, acc);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) sK[e] = acc;
+        __syncwarp();
+    }
+    for (int e = cnt + lane; e < cap; e += 32) {
+        sK[e] = kInf;
+        sI[e] = kNoId;
+    }
+    __syncwarp();
+    warp_sort_smem(sK, sI, cap);
+    for (int j = lane; j < npc; j += 32) probes[(int64_t)qi * npc + j] = j < cnt ? sI[j] : 0;
+}
+
 }  // namespace
+
+int launch_tc_coarse(const float* keys, int64_t ldk, int nq, int C, int npc, int margin, const float* q,
+                     const float* centroids, int dpad, int32_t* probes, cudaStream_t st) {
+    if (nq == 0) return ANN_OK;
+    const int m = std::min(C, npc + margin);
+    ANN_CHECK_ARG(npc >= 1 && npc <= m && m <= 1024, "tensor-core coarse ranking: npc=%d, m=%d", npc, m);
+    const size_t smem = (size_t)4 * 2 * topk_cap(m) * 4;
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(tc_coarse_kernel)));
+    tc_coarse_kernel<<<(unsigned)ceil_div(nq, 4), 128, smem, st>>>(keys, ldk, nq, C, npc, m, q, centroids, dpad, probes);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int launch_tc_ivf_items(const int64_t* lq_off, const int64_t* list_off, int C, int64_t* item_off, cudaStream_t st) {
+    ANN_CHECK_ARG(C >= 1, "tensor-core IVF: no lists");
+    tc_ivf_items_kernel<<<1, 1024, 0, st>>>(lq_off, list_off, C, item_off);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int launch_tc_ivf_pairs(const __nv_bfloat16* qb, int kpad, const int32_t* pair_vals, const int32_t* pair_lists,
+                        const int64_t* n_pairs, int64_t max_pairs, int npc, const int64_t* cand_off,
+                        const int64_t* seg_pref, const int64_t* list_off, __nv_bfloat16* A, int64_t* dbase,
+                        cudaStream_t st) {
+    if (max_pairs == 0) return ANN_OK;
+    ANN_CHECK_ARG(kpad % 8 == 0, "tensor-core IVF: kpad %d", kpad);
+    const int grid = (int)std::min<int64_t>(ceil_div(max_pairs * 32, 256), 16 * kNumSMs);
+    tc_ivf_pairs_kernel<<<grid, 256, 0, st>>>(qb, kpad, pair_vals, pair_lists, n_pairs, max_pairs, npc, cand_off,
+                                              seg_pref, list_off, A, dbase);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
 
 int launch_tc_group(const TcGroupArgs& g, cudaStream_t st) {
     if (g.M == 0) return ANN_OK;

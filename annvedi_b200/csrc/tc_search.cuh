@@ -43,4 +43,23 @@ int launch_tc_map_ids(int* ids, int64_t count, int64_t n, int64_t mult, cudaStre
 // out[q][row(p)] = keys[q][p] for a [nq, n] key matrix in position order.
 int launch_tc_unpermute(const float* keys, int nq, int64_t n, int64_t mult, float* out, cudaStream_t st);
 
+// IVF batches on the tensor cores (a list-major grouping of (query, list) pairs, ivf_batched.cu):
+// items per list = ceil(pairs / 128) x ceil(rows / 256), exclusively scanned into item_off[0..C]
+// (item_off[C] = all items). One block.
+int launch_tc_ivf_items(const int64_t* lq_off, const int64_t* list_off, int C, int64_t* item_off, cudaStream_t st);
+// For each valid pair i (< lq_off[C]; pairs grouped by list, pair_vals = q * npc + j, pair_lists = the
+// list): A[i] = qb[q] (kpad BF16 columns) and dbase[i] = cand_off[q] + seg_pref[q][j] - list_off[list],
+// the stream position of the list's row 0 in the candidate array.
+int launch_tc_ivf_pairs(const __nv_bfloat16* qb, int kpad, const int32_t* pair_vals, const int32_t* pair_lists,
+                        const int64_t* n_pairs, int64_t max_pairs, int npc, const int64_t* cand_off,
+                        const int64_t* seg_pref, const int64_t* list_off, __nv_bfloat16* A, int64_t* dbase,
+                        cudaStream_t st);
+
+// Coarse ranking of the tensor-core IVF form from BF16 keys [nq, C] (ldk per row): per query, the best
+// m = min(C, npc + margin) centroids by key, their exact FP32 squared distances (FP32 queries and
+// centroids, row stride dpad), and the best npc of those by (distance, id) into probes [nq, npc],
+// best first.
+int launch_tc_coarse(const float* keys, int64_t ldk, int nq, int C, int npc, int margin, const float* q,
+                     const float* centroids, int dpad, int32_t* probes, cudaStream_t st);
+
 }  // namespace annb

@@ -40,6 +40,7 @@ extern "C" {
 /* search semantics */
 #define ANN_MODE_EXACT 0     /* the true top-k by (distance, id) */
 #define ANN_MODE_REFERENCE 1 /* the reference's ranking, incl. its 64-entry early-abandon heap */
+#define ANN_MODE_TC 2        /* IVF: candidates ranked by BF16 tensor-core keys, then the exact FP32 re-rank */
 
 /* where caller pointers live */
 #define ANN_MEM_HOST 0
@@ -173,7 +174,9 @@ int ann_ivf_info(const ann_ivf* h, int64_t* out4);
  * distances; the best k returned as original ids (-1 padded) with their squared distances.
  * ANN_MODE_REFERENCE reproduces the reference's own ranking, including the 64-entry early-abandon
  * heap of each of `num_threads` ThreadPool chunks (<= 0: this host's hardware concurrency, as the
- * reference sizes its pool); ANN_MODE_EXACT ranks by full SQ8 distances. `n_probes` (multiprobe
+ * reference sizes its pool); ANN_MODE_EXACT ranks by full SQ8 distances; ANN_MODE_TC ranks the same
+ * candidate streams by BF16 tcgen05 keys of the FP32 rows (|x|^2 - 2 x.q, FP32 accumulate), the lists
+ * scored list-major as grouped GEMMs (no counterpart in the reference). `n_probes` (multiprobe
  * LSH buckets) must be 0. Adds each query's candidate count to the distance counter (:459-460). */
 int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t nq, int64_t ldq, int32_t k,
                   int32_t n_probes, int32_t n_probe_clusters, int32_t refine_r, int64_t max_candidates, int32_t mode,
