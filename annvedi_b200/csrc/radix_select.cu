@@ -26,7 +26,7 @@ __device__ __forceinline__ float unord(uint32_t t) {
     return isnan(f) ? kInf : f;
 }
 
-constexpr int kThreads = 512;
+constexpr int kThreads = 256;
 constexpr int kBins = 2048;
 
 // The bin holding the rank-th smallest (0-based) element of the histogram, and the count of elements
@@ -72,6 +72,28 @@ __device__ __forceinline__ int lin_bin(float k, float lo, float scale) {
     return !(f > 0.f) ? 0 : (f >= (float)(kBins - 1) ? kBins - 1 : (int)f);
 }
 
+// Block-wide bitonic sort of n (a power of two) (key, val) pairs in shared memory by (key, val).
+__device__ void block_sort_pairs(float* key, int* val, int n) {
+    for (int size = 2; size <= n; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = threadIdx.x; t < (n >> 1); t += kThreads) {
+                const int lo = 2 * t - (t & (stride - 1));
+                const int hi = lo + stride;
+                const bool asc = (lo & size) == 0;
+                const float kl = key[lo], kh = key[hi];
+                const int vl = val[lo], vh = val[hi];
+                if (asc ? pair_less(kh, vh, kl, vl) : pair_less(kl, vl, kh, vh)) {
+                    key[lo] = kh;
+                    key[hi] = kl;
+                    val[lo] = vh;
+                    val[hi] = vl;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
 // Block-wide min and max (kThreads threads); the results are visible to every thread on return.
 __device__ void block_minmax(float& lo, float& hi, float* sRed) {
 #pragma unroll
@@ -94,7 +116,28 @@ __device__ void block_minmax(float& lo, float& hi, float* sRed) {
     __syncthreads();
 }
 
-constexpr int kLinCap = 2048;  // keys of the final sub-bin sorted in shared memory
+constexpr int kLinCap = 2048;  // keys sorted in shared memory (the final sub-bin, or a sampled bar's set)
+constexpr int kSamples = 1024; // keys of the stream sampled for a bar
+constexpr int kLoadBatch = 8;   // keys per thread loaded ahead of their use
+
+// f(p, key) for every position p < len of the stream (each thread a strided share), with kLoadBatch
+// loads in flight per thread.
+template <typename F>
+__device__ __forceinline__ void for_each_key(const float* __restrict__ kq, int64_t len, F&& f) {
+    for (int64_t base = threadIdx.x; base < len; base += (int64_t)kLoadBatch * kThreads) {
+        float v[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int64_t p = base + (int64_t)u * kThreads;
+            v[u] = p < len ? kq[p] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int64_t p = base + (int64_t)u * kThreads;
+            if (p < len) f(p, v[u]);
+        }
+    }
+}
 
 __global__ void __launch_bounds__(kThreads) radix_select_kernel(RadixSelectArgs a) {
     __shared__ int hist[2][kBins];
@@ -133,15 +176,58 @@ __global__ void __launch_bounds__(kThreads) radix_select_kernel(RadixSelectArgs 
         }
         return;
     }
+    if (want_set && !two && !a.kth_upper && (int64_t)R * 8 <= len && R <= 512) {
+        // Sampled bar: every s-th key, the bar at the ~1.3 R / s-th smallest sample; one pass gathers
+        // the keys at or below it with their positions, and if there are at least R of them (the R
+        // smallest keys then all are), a sort by (key, position) gives the set exactly.
+        const int64_t sstep = max((int64_t)1, len / kSamples);
+        const int ns = (int)min((int64_t)kSamples, (len + sstep - 1) / sstep);
+        const int r = min(ns, (int)(((int64_t)R * 13 + 10 * sstep - 1) / (10 * sstep)) + 4);
+        for (int i = threadIdx.x; i < kSamples; i += kThreads) {
+            sCandK[i] = i < ns ? kq[(int64_t)i * sstep] : kInf;
+            sCandP[i] = i;
+        }
+        if (threadIdx.x == 0) sCount = 0;
+        __syncthreads();
+        block_sort_pairs(sCandK, sCandP, kSamples);
+        const float bar = sCandK[r - 1];
+        __syncthreads();
+        for_each_key(kq, len, [&](int64_t p, float kv) {
+            if (kv <= bar) {
+                const int at = atomicAdd(&sCount, 1);
+                if (at < kLinCap) {
+                    sCandK[at] = kv;
+                    sCandP[at] = (int)p;
+                }
+            }
+        });
+        __syncthreads();
+        const int cnt = sCount;
+        if (cnt >= R && cnt <= kLinCap) {
+            int cap2 = 32;
+            while (cap2 < cnt) cap2 <<= 1;
+            for (int e = cnt + threadIdx.x; e < cap2; e += kThreads) {
+                sCandK[e] = kInf;
+                sCandP[e] = INT_MAX;
+            }
+            __syncthreads();
+            block_sort_pairs(sCandK, sCandP, cap2);
+            for (int e = threadIdx.x; e < R; e += kThreads) {
+                if (ok) ok[e] = sCandK[e];
+                if (oi) oi[e] = id_of(sCandP[e]);
+            }
+            return;
+        }
+        __syncthreads();  // too few or too many under the bar: the linear bins below
+    }
     if (want_set && !two && !a.kth_upper) {
         // Linear bins over the stream's [min, max]: keys of similar magnitude spread over many bins
         // (the integer image's top bits would put them all in one, serialising the histogram).
         float lo = kInf, hi = -kInf;
-        for (int64_t p = threadIdx.x; p < len; p += kThreads) {
-            const float kv = kq[p];
+        for_each_key(kq, len, [&](int64_t, float kv) {
             lo = fminf(lo, kv);
             hi = fmaxf(hi, kv);
-        }
+        });
         block_minmax(lo, hi, sRed);
         const float scale1 = (float)kBins / (hi - lo);
         if (!(hi > lo) || !isfinite(scale1)) {  // all keys equal: the first R in stream order
@@ -156,17 +242,16 @@ __global__ void __launch_bounds__(kThreads) radix_select_kernel(RadixSelectArgs 
             hist[1][i] = 0;
         }
         __syncthreads();
-        for (int64_t p = threadIdx.x; p < len; p += kThreads) atomicAdd(&hist[0][lin_bin(kq[p], lo, scale1)], 1);
+        for_each_key(kq, len, [&](int64_t, float kv) { atomicAdd(&hist[0][lin_bin(kv, lo, scale1)], 1); });
         __syncthreads();
         int below1 = 0, below2 = 0;
         const int b1 = find_bin(hist[0], R - 1, &below1, sScan);
         const float w = (hi - lo) / (float)kBins;
         const float lo2 = lo + w * (float)b1;
         const float scale2 = (float)kBins / w;
-        for (int64_t p = threadIdx.x; p < len; p += kThreads) {
-            const float kv = kq[p];
+        for_each_key(kq, len, [&](int64_t, float kv) {
             if (lin_bin(kv, lo, scale1) == b1) atomicAdd(&hist[1][lin_bin(kv, lo2, scale2)], 1);
-        }
+        });
         __syncthreads();
         const int b2 = find_bin(hist[1], R - 1 - below1, &below2, sScan);
         const int ncand = hist[1][b2];
@@ -176,41 +261,24 @@ __global__ void __launch_bounds__(kThreads) radix_select_kernel(RadixSelectArgs 
                 sCount = 0;
                 sTies = 0;
             }
-            __shared__ int sWarpC[kThreads / 32];
             __syncthreads();
-            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-            for (int64_t base = 0; base < len; base += kThreads) {
-                const int64_t p = base + threadIdx.x;
-                const bool valid = p < len;
-                const float kv = valid ? kq[p] : 0.f;
-                const int bk = valid ? lin_bin(kv, lo, scale1) : kBins;
-                const int sk = bk == b1 ? lin_bin(kv, lo2, scale2) : 0;
-                if (valid && (bk < b1 || (bk == b1 && sk < b2))) {
+            // keys below the final sub-bin go straight to the set; the final sub-bin's keys (few: the
+            // sub-bin is 2^-22 of the range) are gathered with their positions and sorted below, so
+            // their gathering order does not matter
+            for_each_key(kq, len, [&](int64_t p, float kv) {
+                const int bk = lin_bin(kv, lo, scale1);
+                const int sk = bk == b1 ? lin_bin(kv, lo2, scale2) : -1;
+                if (bk < b1 || (bk == b1 && sk < b2)) {
                     const int slot = atomicAdd(&sCount, 1);
                     if (ok) ok[slot] = kv;
                     if (oi) oi[slot] = id_of(p);
+                } else if (bk == b1 && sk == b2) {
+                    const int at = atomicAdd(&sTies, 1);
+                    sCandK[at] = kv;
+                    sCandP[at] = (int)p;
                 }
-                const bool cand = valid && bk == b1 && sk == b2;
-                const unsigned bal = __ballot_sync(0xffffffffu, cand);
-                if (__syncthreads_or(bal != 0)) {  // uniform: gather the sub-bin's keys in stream order
-                    if (lane == 0) sWarpC[warp] = __popc(bal);
-                    __syncthreads();
-                    int before = sTies;
-                    for (int ww = 0; ww < warp; ++ww) before += sWarpC[ww];
-                    if (cand) {
-                        const int at = before + __popc(bal & ((1u << lane) - 1u));
-                        sCandK[at] = kv;
-                        sCandP[at] = (int)p;
-                    }
-                    __syncthreads();
-                    if (threadIdx.x == 0) {
-                        int tot = 0;
-                        for (int ww = 0; ww < kThreads / 32; ++ww) tot += sWarpC[ww];
-                        sTies += tot;
-                    }
-                    __syncthreads();
-                }
-            }
+            });
+            __syncthreads();
             // the sub-bin's keys by (key, stream position); the first `need` complete the set
             if (threadIdx.x < 32) {
                 int cap2 = 32;
