@@ -35,7 +35,8 @@ import numpy as np
 class Route:
     """A resident index the server routes requests to.
 
-    search(queries_dev, k, stream, workspace) -> (ids_dev int64 [nq, k], dists_dev float32 [nq, k])
+    search(queries_dev, k, stream, workspace, out_ids, out_dists) -> (ids_dev int64 [nq, k], dists_dev
+        float32 [nq, k]), written into the given device tensors
     scratch_bytes(nq) -> device scratch (bytes) a call with nq queries needs in its workspace.
     """
     name: str
@@ -124,17 +125,17 @@ class Server:
         for r in self.routes.values():
             w = self._workers[0]
             x = torch.zeros(1, r.dim, dtype=torch.float32, device=dev)
-            r.search(x, 1, w["stream"], w["ws"])
+            r.search(x, 1, w["stream"], w["ws"], None, None)
             w["stream"].synchronize()
         if prewarm:
             g = torch.Generator(device=dev).manual_seed(0)
             for w in self._workers:
                 for r in self.routes.values():
-                    self._pinned(w, r, 100)
-                    x = torch.nn.functional.normalize(
-                        torch.randn(self.max_batch, r.dim, generator=g, device=dev), dim=1)
+                    _, _, _, dev_in, dev_ids, dev_d = self._pinned(w, r, 100)
+                    dev_in.copy_(torch.nn.functional.normalize(
+                        torch.randn(self.max_batch, r.dim, generator=g, device=dev), dim=1))
                     with torch.cuda.stream(w["stream"]):
-                        r.search(x, 100, w["stream"], w["ws"])
+                        r.search(dev_in, 100, w["stream"], w["ws"], dev_ids, dev_d)
                     w["stream"].synchronize()
         # Objects that live for the whole run (indexes, buffers, queued traffic) leave the collected
         # generations, so a full collection does not pause the workers for milliseconds.
@@ -233,14 +234,19 @@ class Server:
                     self._cv.notify_all()
 
     def _pinned(self, w, r: Route, k: int):
-        """The worker's pinned staging buffers for route r and k, max_batch rows (allocated once:
-        pinned allocations are slow and synchronise the device)."""
+        """The worker's staging buffers for route r and k, max_batch rows: pinned host input and
+        outputs, and the device input and outputs (allocated once: allocations mid-stream are slow,
+        and pinned ones synchronise the device)."""
         import torch
         key = (r.name, k)
         if key not in w["pin"]:
+            dev = f"cuda:{self.device}"
             w["pin"][key] = (torch.empty(self.max_batch, r.dim, dtype=torch.float32, pin_memory=True),
                              torch.empty(self.max_batch, k, dtype=torch.int64, pin_memory=True),
-                             torch.empty(self.max_batch, k, dtype=torch.float32, pin_memory=True))
+                             torch.empty(self.max_batch, k, dtype=torch.float32, pin_memory=True),
+                             torch.empty(self.max_batch, r.dim, dtype=torch.float32, device=dev),
+                             torch.empty(self.max_batch, k, dtype=torch.int64, device=dev),
+                             torch.empty(self.max_batch, k, dtype=torch.float32, device=dev))
         return w["pin"][key]
 
     def _run(self, w, dev, name, reqs):
@@ -249,7 +255,7 @@ class Server:
         r = self.routes[name]
         k = reqs[0].k
         nq = sum(q.queries.shape[0] for q in reqs)
-        pin_in_all, pin_ids_all, pin_d_all = self._pinned(w, r, k)
+        pin_in_all, pin_ids_all, pin_d_all, dev_in, dev_ids, dev_d = self._pinned(w, r, k)
         pin_in = pin_in_all[:nq]
         o = 0
         for req in reqs:
@@ -258,8 +264,9 @@ class Server:
             o += b
         st = w["stream"]
         with torch.cuda.stream(st):
-            qdev = pin_in.to(dev, non_blocking=True)
-            ids, dists = r.search(qdev, k, st, w["ws"])
+            qdev = dev_in[:nq]
+            qdev.copy_(pin_in, non_blocking=True)
+            ids, dists = r.search(qdev, k, st, w["ws"], dev_ids[:nq], dev_d[:nq])
             pin_ids_all[:nq].copy_(ids, non_blocking=True)
             pin_d_all[:nq].copy_(dists, non_blocking=True)
         st.synchronize()
@@ -308,8 +315,9 @@ class Server:
 # ---- routes over this package's indexes ------------------------------------------------------
 def tc_route(name: str, index, refine_r: int = 400) -> Route:
     """The tensor-core exact search of a LinearIndex (ann_flat_query_tc)."""
-    def search(x, k, stream, ws):
-        return index.search_tc(x, k, refine_r=refine_r, workspace=ws, stream=stream)
+    def search(x, k, stream, ws, out_ids=None, out_dists=None):
+        return index.search_tc(x, k, refine_r=refine_r, workspace=ws, stream=stream, out_ids=out_ids,
+                               out_dists=out_dists)
 
     def scratch(nq):
         # sampled keys (~32k FP32 per query) + survivor regions + per-query sets + queries
@@ -320,15 +328,18 @@ def tc_route(name: str, index, refine_r: int = 400) -> Route:
 
 def flat_route(name: str, index) -> Route:
     """The plain FP32 exact scan of a LinearIndex (ann_flat_query, exact mode)."""
-    def search(x, k, stream, ws):
-        return index.search(x, k, mode="exact", workspace=ws, stream=stream)
+    def search(x, k, stream, ws, out_ids=None, out_dists=None):
+        return index.search(x, k, mode="exact", workspace=ws, stream=stream, out_ids=out_ids, out_dists=out_dists)
     return Route(name, index.dim, search, lambda nq: nq * (200 * 8 * 100 + 8 * index.dim) + (16 << 20))
 
 
-def ivf_route(name: str, index, n_probe_clusters: int, refine_r: int = 300, max_list: int = 40_000) -> Route:
-    """The exact-selection IVF-SQ8 search of an IVFIndex (ann_ivf_query, no candidate cap)."""
-    def search(x, k, stream, ws):
-        return index.search(x, k, 0, n_probe_clusters, refine_r, max_candidates=0, workspace=ws, stream=stream)
+def ivf_route(name: str, index, n_probe_clusters: int, refine_r: int = 300, max_list: int = 40_000,
+              mode: str = "exact") -> Route:
+    """An IVFIndex search (ann_ivf_query, no candidate cap): mode "exact" ranks the candidates by SQ8
+    distances, "tc" by BF16 tensor-core keys; both re-rank in exact FP32."""
+    def search(x, k, stream, ws, out_ids=None, out_dists=None):
+        return index.search(x, k, 0, n_probe_clusters, refine_r, max_candidates=0, mode=mode, workspace=ws,
+                            stream=stream, out_ids=out_ids, out_dists=out_dists)
 
     def scratch(nq):
         # candidate keys over the probed lists (bounded by the largest lists) + selections

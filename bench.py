@@ -11,8 +11,10 @@ Forms: the plain FP32 exact scan (the correctness oracle of the GPU side and the
 denominator, also timed at 1 and 4 queries per call where it is HBM-bound); the tensor-core exact
 search (BF16 tcgen05 keys with FP32 accumulation, sampled bars, exact FP32 re-rank of the best 400);
 the batched IVF-SQ8 scan with exact FP32 re-rank at the smallest nprobe whose recall@100 against the
-FP64 exact top-100 is >= 0.95. The headline (`value`) is the fastest form at recall@100 >= 0.95
-(--form tc|ivf picks one); every form is reported under `forms`.
+FP64 exact top-100 is >= 0.95; and the same IVF lists on the tensor cores (grouped BF16 tcgen05 GEMMs
+over the batch's (query, list) pairs, exact FP32 re-rank), at its own smallest such nprobe. The
+headline (`value`) is the fastest form at recall@100 >= 0.95 (--form tc|ivf|ivf_tc picks one); every
+form is reported under `forms`.
 
 Timing: W untimed warm-up steps, then exactly K steps between a barrier + device synchronize on
 each side, timed with CUDA events on the search stream; max over ranks. The base (1.5 GB) is
@@ -346,10 +348,41 @@ def run_ours(args, rank, world, local):
                    "candidate_cap": "none"},
     }
 
+    # ---- IVF on the tensor cores: the same lists scored by grouped BF16 tcgen05 GEMMs ----
+    sweep_tc = []
+    chosen_tc = None
+    for npc_t in (8, 16, 32):
+        ivf.search(queries, K_NN, 0, npc_t, args.refine, max_candidates=0, mode="tc", out_ids=o_ids, out_dists=o_d)
+        torch.cuda.synchronize()
+        rec = recall_evaluator(base, queries, o_ids, kth)
+        ms = _time_steps(lambda: ivf.search(queries, K_NN, 0, npc_t, args.refine, max_candidates=0, mode="tc",
+                                            out_ids=o_ids, out_dists=o_d), 3, stream) / 3
+        sweep_tc.append({"nprobe": npc_t, "recall_at_100": round(rec, 4), "qps": round(q / (ms / 1e3), 1)})
+        if chosen_tc is None and rec >= 0.95:
+            chosen_tc = (npc_t, rec, q / (ms / 1e3))
+    if chosen_tc is None:
+        chosen_tc = (32, sweep_tc[-1]["recall_at_100"], sweep_tc[-1]["qps"])
+    npc_tc, tc_rec, tc_qps = chosen_tc
+
+    def ivf_tc_step():
+        ivf.search(queries, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc", out_ids=o_ids, out_dists=o_d)
+
+    forms["ivf_tc"] = {
+        "qps": tc_qps, "recall": tc_rec, "step": ivf_tc_step,
+        "host": lambda: ivf.search(qh, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc", with_dists=False),
+        "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc",
+                                        out_ids=o_ids[:1], with_dists=False),
+        "lat_host": lambda x: ivf.search(x, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc",
+                                         with_dists=False),
+        "dtype": "bf16 (tcgen05 list keys, fp32 accumulate, exact fp32 re-rank)",
+        "config": {"form": "ivf on tensor cores", "n_lists": 2048, "nprobe": npc_tc, "refine_r": args.refine,
+                   "candidate_cap": "none"},
+    }
+
     # ---- the headline: the fastest form at recall@100 >= 0.95 (or the one asked for) ----
     ok = {k2: v for k2, v in forms.items() if v["recall"] >= 0.95} or forms
-    if args.form in ("tc", "ivf"):
-        head = "tensor_core_exact" if args.form == "tc" else "ivf_sq8"
+    if args.form in ("tc", "ivf", "ivf_tc"):
+        head = {"tc": "tensor_core_exact", "ivf": "ivf_sq8", "ivf_tc": "ivf_tc"}[args.form]
     else:
         head = max(ok, key=lambda k2: ok[k2]["qps"])
     hf = forms[head]
@@ -362,7 +395,7 @@ def run_ours(args, rank, world, local):
     tcx.set_profiling(head == "tensor_core_exact")
     ivf.reset_profile_results()
     ivf.reset_distances_count()
-    ivf.set_profiling(head == "ivf_sq8")
+    ivf.set_profiling(head in ("ivf_sq8", "ivf_tc"))
     launches0 = _lib.kernel_launches()
     barrier(world)
     torch.cuda.synchronize()
@@ -371,13 +404,11 @@ def run_ours(args, rank, world, local):
     launches = _lib.kernel_launches() - launches0
     tcx.set_profiling(False)
     ivf.set_profiling(False)
+    cands_timed = ivf.total_distances_count()  # candidates of the timed steps (later calls add more)
     clk = clocks.stop()
     ms_max = max_over_ranks(ms, world)
     qps = world * q * args.steps / (ms_max / 1e3)
-    if head == "tensor_core_exact":
-        hf["recall"] = recall_evaluator(base, queries, t_ids, kth)
-    else:
-        hf["recall"] = recall_evaluator(base, queries, o_ids, kth)
+    hf["recall"] = recall_evaluator(base, queries, t_ids if head == "tensor_core_exact" else o_ids, kth)
 
     # ---- end to end through the public API with host buffers ----
     barrier(world)
@@ -407,12 +438,26 @@ def run_ours(args, rank, world, local):
                   "select": stt["tc_select_ms"], "rerank": stt["rerank_ms"]}
         stage_ms = {k2: round(v / args.steps, 4) for k2, v in stages.items()}
         extra = {"gemm_launches_per_batch": round(stt["tc_gemm_launches"] / args.steps, 2)}
+    elif head == "ivf_tc":
+        prof = ivf.get_profile_results()
+        stage = prof.get("stage_ms", {})
+        calls = max(1, prof.get("profiled_calls", 1))
+        rr_ms = stage.get("rerank", 0.0) / calls
+        r_eff = min(args.refine, int(cands_timed / max(1, args.steps) / q))
+        bytes_per_launch = q * r_eff * d * 4 + q * r_eff * 8  # the candidates' FP32 rows, their keys and ids
+        achieved = bytes_per_launch / (rr_ms / 1e3) / 1e9 if rr_ms > 0 else 0.0
+        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(achieved / hbm_peak, 4), "traffic": None, "peak_kind": peak_kind,
+                "kernel": "ivf_rerank_kernel (exact FP32 re-rank, the largest kernel of this form)",
+                "bytes_per_launch": int(bytes_per_launch), "kernel_ms": round(rr_ms, 4)}
+        stage_ms = {k2: round(v / calls, 4) for k2, v in stage.items()}
+        extra = {"candidates_per_query": round(cands_timed / max(1, args.steps) / q, 1)}
     else:
         prof = ivf.get_profile_results()
         stage = prof.get("stage_ms", {})
         calls = max(1, prof.get("profiled_calls", 1))
         sq8_ms = stage.get("sq8", 0.0) / calls
-        cands = ivf.total_distances_count()
+        cands = cands_timed
         bytes_per_launch = (cands / max(1, args.steps)) * d
         achieved = bytes_per_launch / (sq8_ms / 1e3) / 1e9 if sq8_ms > 0 else 0.0
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
@@ -435,7 +480,7 @@ def run_ours(args, rank, world, local):
         "speedup_vs_plain_fp32_scan": round(qps / (flat_qps * world), 2),
         "forms": summary,
         "plain_fp32_scan": flat_line,
-        "nprobe_sweep": sweep,
+        "nprobe_sweep": {"ivf_sq8": sweep, "ivf_tc": sweep_tc},
         "latency_ms_batch1": latency,
         "ivf_build_s": round(build_s, 3),
         "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": q * d * 4,
@@ -633,7 +678,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--refine", type=int, default=300)
     ap.add_argument("--tc-refine", type=int, default=400)
-    ap.add_argument("--form", choices=["auto", "tc", "ivf"], default="auto")
+    ap.add_argument("--form", choices=["auto", "tc", "ivf", "ivf_tc"], default="auto")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="per offered rate; 0 skips serving")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[2000, 10000, 50000])
     ap.add_argument("--ref-nprobe", type=int, default=32)
