@@ -194,6 +194,12 @@ def _time_steps(fn, steps, stream):
     return e0.elapsed_time(e1)
 
 
+# DRAM traffic per query of the dominant kernels, measured once with ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum, one launch) on this workload at its default sizes: the exact re-rank of the IVF
+# tensor-core form (4.00 GB per 10,000-query launch, R = 300) and the filter pass of the tensor-core exact
+# search (0.878 GB per 5,000-query launch). Other sizes report traffic as null.
+MEASURED_TRAFFIC_PER_QUERY = {"ivf_rerank": 4.00e9 / 10_000, "tc_filter": 0.878e9 / 5_000}
+
 WORKLOAD = "1M x 384 zipf mixture (2,048 centres, sigma 0.3, L2-normalised), 10k-query batches, k=100, squared L2"
 DATA = "synthetic (seeded zipf mixture, 2,048 centres, sigma 0.3, L2-normalised)"
 
@@ -237,151 +243,163 @@ def run_ours(args, rank, world, local):
     qpin.copy_(queries)
     qh = qpin.numpy()
 
+    sel = set(args.forms.split(","))
+    tcx = ivf = None
+    build_s, npc = None, None
     # ---- the plain FP32 exact scan (the denominator) ----
-    flat = LinearIndex(device=local, metric="l2", mode="exact")
-    flat.fit(base)
-    f_ids = torch.empty(q, K_NN, dtype=torch.int64, device=dev)
-    f_d = torch.empty(q, K_NN, dtype=torch.float32, device=dev)
+    flat_line, flat_qps = None, None
+    if "plain" in sel:
+        flat = LinearIndex(device=local, metric="l2", mode="exact")
+        flat.fit(base)
+        f_ids = torch.empty(q, K_NN, dtype=torch.int64, device=dev)
+        f_d = torch.empty(q, K_NN, dtype=torch.float32, device=dev)
 
-    def flat_step():
-        flat.search(queries, K_NN, mode="exact", out_ids=f_ids, out_dists=f_d)
+        def flat_step():
+            flat.search(queries, K_NN, mode="exact", out_ids=f_ids, out_dists=f_d)
 
-    flat_step()
-    torch.cuda.synchronize()
-    flat_recall = recall_evaluator(base, queries[:1000], f_ids[:1000], kth[:1000])
-    flat.reset_profile_results()
-    flat.set_profiling(True)
-    fsteps = max(2, min(args.steps, 3))
-    flat_ms = _time_steps(flat_step, fsteps, stream) / fsteps
-    flat.set_profiling(False)
-    fprof = flat.get_profile_results()
-    flat_qps = q / (flat_ms / 1e3)
-    fscan_ms = fprof["scan_ms"] / max(1, fprof["scan_launches"])
-    fp32_instr = 2.0 * n * d * q  # one sub + one fma per element pair
-    flat_line = {"qps": round(flat_qps, 1), "ms_per_batch": round(flat_ms, 3), "recall_at_100": round(flat_recall, 4),
-                 "kernel": "flat_scan_kernel", "fp32_instr_per_s": round(fp32_instr / (fscan_ms / 1e3), 1)}
-    # HBM-bound regime: a query per call streams the whole base once (flat_stream_kernel)
-    dpad = -(-d // 32) * 32
-    small = {}
-    for b in (1, 4):
-        qb = queries[:b].contiguous()
-        ib = torch.empty(b, K_NN, dtype=torch.int64, device=dev)
-        db = torch.empty(b, K_NN, dtype=torch.float32, device=dev)
-        for _ in range(3):
-            flat.search(qb, K_NN, mode="exact", out_ids=ib, out_dists=db)
+        flat_step()
         torch.cuda.synchronize()
+        flat_recall = recall_evaluator(base, queries[:1000], f_ids[:1000], kth[:1000])
         flat.reset_profile_results()
         flat.set_profiling(True)
-        reps = 20
-        ms_b = _time_steps(lambda: flat.search(qb, K_NN, mode="exact", out_ids=ib, out_dists=db), reps, stream) / reps
+        fsteps = max(2, min(args.steps, 3))
+        flat_ms = _time_steps(flat_step, fsteps, stream) / fsteps
         flat.set_profiling(False)
-        pr = flat.get_profile_results()
-        scan_b = pr["scan_ms"] / max(1, pr["scan_launches"])
-        gbs = n * dpad * 4 / (scan_b / 1e3) / 1e9
-        small[f"batch{b}"] = {"ms_per_call": round(ms_b, 4), "scan_kernel_ms": round(scan_b, 4),
-                              "merge_ms": round(pr["merge_ms"] / max(1, pr["scan_launches"]), 4),
-                              "scan_gbs": round(gbs, 1), "hbm_frac": round(gbs / hbm_peak, 4),
-                              "kernel": "flat_stream_kernel", "bytes_per_launch": n * dpad * 4}
-    flat_line["small_batch_hbm"] = small
-    del flat
-    torch.cuda.empty_cache()
+        fprof = flat.get_profile_results()
+        flat_qps = q / (flat_ms / 1e3)
+        fscan_ms = fprof["scan_ms"] / max(1, fprof["scan_launches"])
+        fp32_instr = 2.0 * n * d * q  # one sub + one fma per element pair
+        flat_line = {"qps": round(flat_qps, 1), "ms_per_batch": round(flat_ms, 3), "recall_at_100": round(flat_recall, 4),
+                     "kernel": "flat_scan_kernel", "fp32_instr_per_s": round(fp32_instr / (fscan_ms / 1e3), 1)}
+        # HBM-bound regime: a query per call streams the whole base once (flat_stream_kernel)
+        dpad = -(-d // 32) * 32
+        small = {}
+        for b in (1, 4):
+            qb = queries[:b].contiguous()
+            ib = torch.empty(b, K_NN, dtype=torch.int64, device=dev)
+            db = torch.empty(b, K_NN, dtype=torch.float32, device=dev)
+            for _ in range(3):
+                flat.search(qb, K_NN, mode="exact", out_ids=ib, out_dists=db)
+            torch.cuda.synchronize()
+            flat.reset_profile_results()
+            flat.set_profiling(True)
+            reps = 20
+            ms_b = _time_steps(lambda: flat.search(qb, K_NN, mode="exact", out_ids=ib, out_dists=db), reps, stream) / reps
+            flat.set_profiling(False)
+            pr = flat.get_profile_results()
+            scan_b = pr["scan_ms"] / max(1, pr["scan_launches"])
+            gbs = n * dpad * 4 / (scan_b / 1e3) / 1e9
+            small[f"batch{b}"] = {"ms_per_call": round(ms_b, 4), "scan_kernel_ms": round(scan_b, 4),
+                                  "merge_ms": round(pr["merge_ms"] / max(1, pr["scan_launches"]), 4),
+                                  "scan_gbs": round(gbs, 1), "hbm_frac": round(gbs / hbm_peak, 4),
+                                  "kernel": "flat_stream_kernel", "bytes_per_launch": n * dpad * 4}
+        flat_line["small_batch_hbm"] = small
+        del flat
+        torch.cuda.empty_cache()
 
     forms = {}
     # ---- tensor-core exact search: BF16 tcgen05 keys, sampled bars, exact FP32 re-rank ----
-    tcx = LinearIndex(device=local, metric="l2", mode="exact")
-    tcx.fit(base)
-    t_ids = torch.empty(q, K_NN, dtype=torch.int64, device=dev)
-    t_d = torch.empty(q, K_NN, dtype=torch.float32, device=dev)
+    if "tc" in sel:
+        tcx = LinearIndex(device=local, metric="l2", mode="exact")
+        tcx.fit(base)
+        t_ids = torch.empty(q, K_NN, dtype=torch.int64, device=dev)
+        t_d = torch.empty(q, K_NN, dtype=torch.float32, device=dev)
 
-    def tc_step():
-        tcx.search_tc(queries, K_NN, refine_r=args.tc_refine, out_ids=t_ids, out_dists=t_d)
+        def tc_step():
+            tcx.search_tc(queries, K_NN, refine_r=args.tc_refine, out_ids=t_ids, out_dists=t_d)
 
-    for _ in range(max(3, args.warmup)):
-        tc_step()
-    torch.cuda.synchronize()
-    tc_recall = recall_evaluator(base, queries, t_ids, kth)
-    tc_ms = _time_steps(tc_step, 2, stream) / 2
-    forms["tensor_core_exact"] = {
-        "qps": q / (tc_ms / 1e3), "recall": tc_recall, "step": tc_step,
-        "host": lambda: tcx.search_tc(qh, K_NN, refine_r=args.tc_refine, with_dists=False),
-        "lat_dev": lambda x: tcx.search_tc(x, K_NN, refine_r=args.tc_refine, out_ids=t_ids[:1], with_dists=False),
-        "lat_host": lambda x: tcx.search_tc(x, K_NN, refine_r=args.tc_refine, with_dists=False),
-        "dtype": "bf16 (tcgen05 keys, fp32 accumulate, exact fp32 re-rank)",
-        "config": {"form": "tensor-core exact search", "refine_r": args.tc_refine,
-                   "sample": "strided 256-row tiles of a Weyl-ordered BF16 copy, ~32k keys per query"},
-    }
+        for _ in range(max(3, args.warmup)):
+            tc_step()
+        torch.cuda.synchronize()
+        tc_recall = recall_evaluator(base, queries, t_ids, kth)
+        tc_ms = _time_steps(tc_step, 2, stream) / 2
+        forms["tensor_core_exact"] = {
+            "qps": q / (tc_ms / 1e3), "recall": tc_recall, "step": tc_step,
+            "host": lambda: tcx.search_tc(qh, K_NN, refine_r=args.tc_refine, with_dists=False),
+            "lat_dev": lambda x: tcx.search_tc(x, K_NN, refine_r=args.tc_refine, out_ids=t_ids[:1], with_dists=False),
+            "lat_host": lambda x: tcx.search_tc(x, K_NN, refine_r=args.tc_refine, with_dists=False),
+            "dtype": "bf16 (tcgen05 keys, fp32 accumulate, exact fp32 re-rank)",
+            "config": {"form": "tensor-core exact search", "refine_r": args.tc_refine,
+                       "sample": "strided 256-row tiles of a Weyl-ordered BF16 copy, ~32k keys per query"},
+        }
 
     # ---- IVF-SQ8: lists = the 2,048 L2-normalised generating centres ----
-    ivf = IVFIndex(device=local, mode="exact")
-    t0 = time.perf_counter()
-    ivf.fit(base, 1, 0, 2048, centroids=w.centres)
-    torch.cuda.synchronize()
-    build_s = time.perf_counter() - t0
-    o_ids = torch.empty(q, K_NN, dtype=torch.int64, device=dev)
-    o_d = torch.empty(q, K_NN, dtype=torch.float32, device=dev)
-    sweep = []
-    chosen = None
-    for npc in (8, 16, 32, 64, 128):
-        ivf.search(queries, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids, out_dists=o_d)
+    if "ivf" in sel or "ivf_tc" in sel:
+        ivf = IVFIndex(device=local, mode="exact")
+        t0 = time.perf_counter()
+        ivf.fit(base, 1, 0, 2048, centroids=w.centres)
         torch.cuda.synchronize()
-        rec = recall_evaluator(base, queries, o_ids, kth)
-        ms = _time_steps(lambda: ivf.search(queries, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids,
-                                            out_dists=o_d), 2, stream) / 2
-        sweep.append({"nprobe": npc, "recall_at_100": round(rec, 4), "qps": round(q / (ms / 1e3), 1)})
-        if chosen is None and rec >= 0.95:
-            chosen = (npc, rec, q / (ms / 1e3))
-    if chosen is None:
-        chosen = (128, sweep[-1]["recall_at_100"], sweep[-1]["qps"])
-    npc, ivf_rec, ivf_qps = chosen
+        build_s = time.perf_counter() - t0
+        o_ids = torch.empty(q, K_NN, dtype=torch.int64, device=dev)
+        o_d = torch.empty(q, K_NN, dtype=torch.float32, device=dev)
+    sweep = []
+    if "ivf" in sel:
+        sweep = []
+        chosen = None
+        for npc in (8, 16, 32, 64, 128):
+            ivf.search(queries, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids, out_dists=o_d)
+            torch.cuda.synchronize()
+            rec = recall_evaluator(base, queries, o_ids, kth)
+            ms = _time_steps(lambda: ivf.search(queries, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids,
+                                                out_dists=o_d), 2, stream) / 2
+            sweep.append({"nprobe": npc, "recall_at_100": round(rec, 4), "qps": round(q / (ms / 1e3), 1)})
+            if chosen is None and rec >= 0.95:
+                chosen = (npc, rec, q / (ms / 1e3))
+        if chosen is None:
+            chosen = (128, sweep[-1]["recall_at_100"], sweep[-1]["qps"])
+        npc, ivf_rec, ivf_qps = chosen
 
-    def ivf_step():
-        ivf.search(queries, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids, out_dists=o_d)
+        def ivf_step():
+            ivf.search(queries, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids, out_dists=o_d)
 
-    forms["ivf_sq8"] = {
-        "qps": ivf_qps, "recall": ivf_rec, "step": ivf_step,
-        "host": lambda: ivf.search(qh, K_NN, 0, npc, args.refine, max_candidates=0, with_dists=False),
-        "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids[:1],
-                                        with_dists=False),
-        "lat_host": lambda x: ivf.search(x, K_NN, 0, npc, args.refine, max_candidates=0, with_dists=False),
-        "dtype": "f32 (sq8 codes, fp32 re-rank)",
-        "config": {"form": "ivf-sq8 exact selection", "n_lists": 2048, "nprobe": npc, "refine_r": args.refine,
-                   "candidate_cap": "none"},
-    }
+        forms["ivf_sq8"] = {
+            "qps": ivf_qps, "recall": ivf_rec, "step": ivf_step,
+            "host": lambda: ivf.search(qh, K_NN, 0, npc, args.refine, max_candidates=0, with_dists=False),
+            "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids[:1],
+                                            with_dists=False),
+            "lat_host": lambda x: ivf.search(x, K_NN, 0, npc, args.refine, max_candidates=0, with_dists=False),
+            "dtype": "f32 (sq8 codes, fp32 re-rank)",
+            "config": {"form": "ivf-sq8 exact selection", "n_lists": 2048, "nprobe": npc, "refine_r": args.refine,
+                       "candidate_cap": "none"},
+        }
 
     # ---- IVF on the tensor cores: the same lists scored by grouped BF16 tcgen05 GEMMs ----
     sweep_tc = []
-    chosen_tc = None
-    for npc_t in (8, 16, 32):
-        ivf.search(queries, K_NN, 0, npc_t, args.refine, max_candidates=0, mode="tc", out_ids=o_ids, out_dists=o_d)
-        torch.cuda.synchronize()
-        rec = recall_evaluator(base, queries, o_ids, kth)
-        ms = _time_steps(lambda: ivf.search(queries, K_NN, 0, npc_t, args.refine, max_candidates=0, mode="tc",
-                                            out_ids=o_ids, out_dists=o_d), 3, stream) / 3
-        sweep_tc.append({"nprobe": npc_t, "recall_at_100": round(rec, 4), "qps": round(q / (ms / 1e3), 1)})
-        if chosen_tc is None and rec >= 0.95:
-            chosen_tc = (npc_t, rec, q / (ms / 1e3))
-    if chosen_tc is None:
-        chosen_tc = (32, sweep_tc[-1]["recall_at_100"], sweep_tc[-1]["qps"])
-    npc_tc, tc_rec, tc_qps = chosen_tc
+    if "ivf_tc" in sel:
+        sweep_tc = []
+        chosen_tc = None
+        for npc_t in (8, 16, 32):
+            ivf.search(queries, K_NN, 0, npc_t, args.refine, max_candidates=0, mode="tc", out_ids=o_ids, out_dists=o_d)
+            torch.cuda.synchronize()
+            rec = recall_evaluator(base, queries, o_ids, kth)
+            ms = _time_steps(lambda: ivf.search(queries, K_NN, 0, npc_t, args.refine, max_candidates=0, mode="tc",
+                                                out_ids=o_ids, out_dists=o_d), 3, stream) / 3
+            sweep_tc.append({"nprobe": npc_t, "recall_at_100": round(rec, 4), "qps": round(q / (ms / 1e3), 1)})
+            if chosen_tc is None and rec >= 0.95:
+                chosen_tc = (npc_t, rec, q / (ms / 1e3))
+        if chosen_tc is None:
+            chosen_tc = (32, sweep_tc[-1]["recall_at_100"], sweep_tc[-1]["qps"])
+        npc_tc, tc_rec, tc_qps = chosen_tc
 
-    def ivf_tc_step():
-        ivf.search(queries, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc", out_ids=o_ids, out_dists=o_d)
+        def ivf_tc_step():
+            ivf.search(queries, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc", out_ids=o_ids, out_dists=o_d)
 
-    forms["ivf_tc"] = {
-        "qps": tc_qps, "recall": tc_rec, "step": ivf_tc_step,
-        "host": lambda: ivf.search(qh, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc", with_dists=False),
-        "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc",
-                                        out_ids=o_ids[:1], with_dists=False),
-        "lat_host": lambda x: ivf.search(x, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc",
-                                         with_dists=False),
-        "dtype": "bf16 (tcgen05 list keys, fp32 accumulate, exact fp32 re-rank)",
-        "config": {"form": "ivf on tensor cores", "n_lists": 2048, "nprobe": npc_tc, "refine_r": args.refine,
-                   "candidate_cap": "none"},
-    }
+        forms["ivf_tc"] = {
+            "qps": tc_qps, "recall": tc_rec, "step": ivf_tc_step,
+            "host": lambda: ivf.search(qh, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc", with_dists=False),
+            "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc",
+                                            out_ids=o_ids[:1], with_dists=False),
+            "lat_host": lambda x: ivf.search(x, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc",
+                                             with_dists=False),
+            "dtype": "bf16 (tcgen05 list keys, fp32 accumulate, exact fp32 re-rank)",
+            "config": {"form": "ivf on tensor cores", "n_lists": 2048, "nprobe": npc_tc, "refine_r": args.refine,
+                       "candidate_cap": "none"},
+        }
 
     # ---- the headline: the fastest form at recall@100 >= 0.95 (or the one asked for) ----
     ok = {k2: v for k2, v in forms.items() if v["recall"] >= 0.95} or forms
-    if args.form in ("tc", "ivf", "ivf_tc"):
+    if args.form in ("tc", "ivf", "ivf_tc") and {"tc": "tensor_core_exact", "ivf": "ivf_sq8",
+                                                  "ivf_tc": "ivf_tc"}[args.form] in forms:
         head = {"tc": "tensor_core_exact", "ivf": "ivf_sq8", "ivf_tc": "ivf_tc"}[args.form]
     else:
         head = max(ok, key=lambda k2: ok[k2]["qps"])
@@ -391,20 +409,25 @@ def run_ours(args, rank, world, local):
         step()
     torch.cuda.synchronize()
     clocks = ClockSampler(local).start()
-    tcx.reset_profile_results()
-    tcx.set_profiling(head == "tensor_core_exact")
-    ivf.reset_profile_results()
-    ivf.reset_distances_count()
-    ivf.set_profiling(head in ("ivf_sq8", "ivf_tc"))
+    if tcx is not None:
+        tcx.reset_profile_results()
+        tcx.set_profiling(head == "tensor_core_exact")
+    if ivf is not None:
+        ivf.reset_profile_results()
+        ivf.reset_distances_count()
+        ivf.set_profiling(head in ("ivf_sq8", "ivf_tc"))
     launches0 = _lib.kernel_launches()
     barrier(world)
     torch.cuda.synchronize()
     ms = _time_steps(step, args.steps, stream)
     barrier(world)
     launches = _lib.kernel_launches() - launches0
-    tcx.set_profiling(False)
-    ivf.set_profiling(False)
-    cands_timed = ivf.total_distances_count()  # candidates of the timed steps (later calls add more)
+    if tcx is not None:
+        tcx.set_profiling(False)
+    cands_timed = 0
+    if ivf is not None:
+        ivf.set_profiling(False)
+        cands_timed = ivf.total_distances_count()  # candidates of the timed steps (later calls add more)
     clk = clocks.stop()
     ms_max = max_over_ranks(ms, world)
     qps = world * q * args.steps / (ms_max / 1e3)
@@ -430,8 +453,10 @@ def run_ours(args, rank, world, local):
         filt_ms = stt["tc_filter_ms"] / nfl
         flops = 2.0 * n * d * q * args.steps / nfl  # algorithmic: the 384-wide dot products of one filter pass
         achieved = flops / (filt_ms / 1e3) / 1e12
+        default_size = (n, d, q) == (1_000_000, 384, 10_000)
+        traffic = MEASURED_TRAFFIC_PER_QUERY["tc_filter"] * q * args.steps / nfl if default_size else None
         roof = {"bound": "tensor", "achieved": round(achieved, 1), "peak": bf16_sustained, "unit": "TFLOP/s",
-                "frac": round(achieved / bf16_sustained, 4), "traffic": None,
+                "frac": round(achieved / bf16_sustained, 4), "traffic": traffic, "traffic_unit": "bytes per launch",
                 "peak_kind": f"{peak_kind} bf16 sustained (kernel timed inside a long step)",
                 "kernel": "tc_gemm_kernel (filter pass)", "flops_per_launch": flops, "kernel_ms": round(filt_ms, 4)}
         stages = {"sample_and_bars": stt["tc_sample_ms"], "filter": stt["tc_filter_ms"],
@@ -446,8 +471,11 @@ def run_ours(args, rank, world, local):
         r_eff = min(args.refine, int(cands_timed / max(1, args.steps) / q))
         bytes_per_launch = q * r_eff * d * 4 + q * r_eff * 8  # the candidates' FP32 rows, their keys and ids
         achieved = bytes_per_launch / (rr_ms / 1e3) / 1e9 if rr_ms > 0 else 0.0
+        default_size = (n, d, q, args.refine) == (1_000_000, 384, 10_000, 300)
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(achieved / hbm_peak, 4), "traffic": None, "peak_kind": peak_kind,
+                "frac": round(achieved / hbm_peak, 4), "peak_kind": peak_kind,
+                "traffic": MEASURED_TRAFFIC_PER_QUERY["ivf_rerank"] * q if default_size else None,
+                "traffic_unit": "bytes per launch",
                 "kernel": "ivf_rerank_kernel (exact FP32 re-rank, the largest kernel of this form)",
                 "bytes_per_launch": int(bytes_per_launch), "kernel_ms": round(rr_ms, 4)}
         stage_ms = {k2: round(v / calls, 4) for k2, v in stage.items()}
@@ -467,7 +495,8 @@ def run_ours(args, rank, world, local):
         extra = {"candidates_per_query": round(cands / max(1, args.steps) / q, 1)}
 
     summary = {name: {"qps": round(f["qps"], 1), "recall_at_100": round(f["recall"], 4),
-                      "speedup_vs_plain_fp32_scan": round(f["qps"] / flat_qps, 2), **f["config"]}
+                      "speedup_vs_plain_fp32_scan": round(f["qps"] / flat_qps, 2) if flat_qps else None,
+                      **f["config"]}
                for name, f in forms.items()}
     cfg = {"workload": WORKLOAD, "n": n, "dim": d, "batch": q, "k": K_NN, "metric": "l2",
            "l2": "inputs larger than L2 (1.5 GB FP32 rows, 0.9 GB BF16 rows, 384 MB codes)",
@@ -477,12 +506,12 @@ def run_ours(args, rank, world, local):
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": hf["dtype"], "data": DATA, "config": cfg,
         "recall_at_100": round(hf["recall"], 4),
-        "speedup_vs_plain_fp32_scan": round(qps / (flat_qps * world), 2),
+        "speedup_vs_plain_fp32_scan": round(qps / (flat_qps * world), 2) if flat_qps else None,
         "forms": summary,
         "plain_fp32_scan": flat_line,
         "nprobe_sweep": {"ivf_sq8": sweep, "ivf_tc": sweep_tc},
         "latency_ms_batch1": latency,
-        "ivf_build_s": round(build_s, 3),
+        "ivf_build_s": round(build_s, 3) if build_s is not None else None,
         "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": q * d * 4,
                 "d2h_bytes_per_step": q * K_NN * 8},
         "gpu_launches": int(launches),
@@ -491,9 +520,9 @@ def run_ours(args, rank, world, local):
         "roofline": roof,
         "clocks": clk,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_ivf(ivf, queries, npc, args)
-    if rank == 0 and world == 1 and args.serve_seconds > 0:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and ivf is not None:
+        line["cpu_baseline"] = cpu_baseline_ivf(ivf, queries, npc if npc is not None else npc_tc, args)
+    if rank == 0 and world == 1 and args.serve_seconds > 0 and npc is not None:
         line["serving"] = serving_c5(args, local, ivf, npc, w)
     return line
 
@@ -679,6 +708,8 @@ def main():
     ap.add_argument("--refine", type=int, default=300)
     ap.add_argument("--tc-refine", type=int, default=400)
     ap.add_argument("--form", choices=["auto", "tc", "ivf", "ivf_tc"], default="auto")
+    ap.add_argument("--forms", default="plain,tc,ivf,ivf_tc",
+                    help="forms to measure (the default measures all; one form alone is for profiling it)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="per offered rate; 0 skips serving")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[2000, 10000, 50000])
     ap.add_argument("--ref-nprobe", type=int, default=32)
