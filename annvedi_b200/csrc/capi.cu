@@ -178,6 +178,8 @@ int ann_flat_destroy(ann_flat* h) {
         DeviceGuard g(h->device);
         if (h->base) cudaFree(h->base);
         if (h->base_bf16) cudaFree(h->base_bf16);
+        if (h->base_e4m3) cudaFree(h->base_e4m3);
+        if (h->fac_e4m3) cudaFree(h->fac_e4m3);
         if (h->d_err) cudaFree(h->d_err);
     }
     ws_release(&h->ws);
@@ -205,6 +207,12 @@ int ann_flat_fit(ann_flat* h, const float* data, int64_t n, int32_t dim, int64_t
     if (h->base_bf16) {
         ANN_CUDA_TRY(cudaFree(h->base_bf16));
         h->base_bf16 = nullptr;
+    }
+    if (h->base_e4m3) {
+        ANN_CUDA_TRY(cudaFree(h->base_e4m3));
+        ANN_CUDA_TRY(cudaFree(h->fac_e4m3));
+        h->base_e4m3 = nullptr;
+        h->fac_e4m3 = nullptr;
     }
     const size_t bytes = sizeof(float) * (size_t)n * dpad;
     cudaError_t e = cudaMalloc(&h->base, bytes);
@@ -473,6 +481,62 @@ static int flat_ensure_bf16(ann_flat* h, cudaStream_t st) {
     return ANN_OK;
 }
 
+// E4M3 operand form of the base (per-row scales, same Weyl order), built once.
+static int flat_ensure_e4m3(ann_flat* h, cudaStream_t st) {
+    if (h->base_e4m3) return ANN_OK;
+    int rc = flat_ensure_bf16(h, st);  // the row order and the error flag
+    if (rc) return rc;
+    const int kpad8 = (int)ceil_div(h->dim, 32) * 32;
+    uint8_t* b = nullptr;
+    float2* f = nullptr;
+    cudaError_t e = cudaMalloc(&b, (size_t)h->n * kpad8);
+    if (e == cudaSuccess) e = cudaMalloc(&f, sizeof(float2) * (size_t)h->n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (b) cudaFree(b);
+        set_error("tensor-core scan: cannot allocate the E4M3 copy of the base (%s)", cudaGetErrorString(e));
+        return ANN_ERR_NOMEM;
+    }
+    rc = launch_tc_operand_e4m3(h->base, h->n, h->dim, h->dpad, b, kpad8, kTcBase, h->metric, h->row_mult, nullptr, f,
+                                st);
+    if (rc) {
+        cudaFree(b);
+        cudaFree(f);
+        return rc;
+    }
+    ANN_CUDA_TRY(cudaStreamSynchronize(st));
+    h->base_e4m3 = b;
+    h->fac_e4m3 = f;
+    h->kpad8 = kpad8;
+    return ANN_OK;
+}
+
+// The tensor-core operands of the index's current element kind.
+struct FlatTc {
+    int kind, kpad;
+    size_t es;  // bytes per element
+    const void* base;
+    const float2* cfac;
+};
+static int flat_ensure_tc(ann_flat* h, cudaStream_t st, FlatTc* t) {
+    int rc = h->tc_kind == kTcE4M3 ? flat_ensure_e4m3(h, st) : flat_ensure_bf16(h, st);
+    if (rc) return rc;
+    t->kind = h->tc_kind;
+    t->kpad = t->kind == kTcE4M3 ? h->kpad8 : h->kpad;
+    t->es = t->kind == kTcE4M3 ? 1 : 2;
+    t->base = t->kind == kTcE4M3 ? (const void*)h->base_e4m3 : (const void*)h->base_bf16;
+    t->cfac = t->kind == kTcE4M3 ? h->fac_e4m3 : nullptr;
+    return ANN_OK;
+}
+// Queries to the operand form: E4M3 rows with their scales into rfac, or BF16 rows.
+static int flat_tc_queries(const ann_flat* h, const FlatTc& t, const float* q, int nq, int64_t ldq, void* out,
+                           float* rfac, cudaStream_t st) {
+    if (t.kind == kTcE4M3)
+        return launch_tc_operand_e4m3(q, nq, h->dim, ldq, static_cast<uint8_t*>(out), t.kpad, kTcQuery, h->metric, 0,
+                                      rfac, nullptr, st);
+    return launch_tc_operand(q, nq, h->dim, ldq, static_cast<__nv_bfloat16*>(out), t.kpad, kTcQuery, h->metric, 0, st);
+}
+
 static int flat_check_err(ann_flat* h) {
     int v = 0;
     if (!h->d_err) return ANN_OK;
@@ -492,21 +556,35 @@ int ann_flat_scores_tc(ann_flat* h, const float* queries, int32_t nq, int64_t ld
     if (nq == 0) return ANN_OK;
     DeviceGuard g(h->device);
     cudaStream_t st = as_stream(stream);
-    int rc = flat_ensure_bf16(h, st);
+    FlatTc t;
+    int rc = flat_ensure_tc(h, st, &t);
     if (rc) return rc;
     Sizer sz;
-    sz.take<__nv_bfloat16>((size_t)nq * h->kpad);
+    sz.take<unsigned char>((size_t)nq * t.kpad * t.es);
+    sz.take<float>((size_t)nq);
     if ((rc = ws_reserve_device(&h->ws, sz.bytes()))) return rc;
     if ((rc = ws_reserve_big(&h->ws, sizeof(float) * (size_t)nq * h->n))) return rc;
     Carver cv(h->ws.dev);
-    __nv_bfloat16* qb = cv.take<__nv_bfloat16>((size_t)nq * h->kpad);
+    unsigned char* qb = cv.take<unsigned char>((size_t)nq * t.kpad * t.es);
+    float* rfac = cv.take<float>((size_t)nq);
     float* tmp = reinterpret_cast<float*>(h->ws.big);
-    if ((rc = launch_tc_operand(queries, nq, h->dim, ldq, qb, h->kpad, kTcQuery, h->metric, 0, st))) return rc;
-    TcGemmArgs a{nq, (int)h->n, h->kpad, nullptr, tmp, h->n, h->d_err};
-    if ((rc = launch_tc_gemm(qb, h->base_bf16, a, st))) return rc;
+    if ((rc = flat_tc_queries(h, t, queries, nq, ldq, qb, rfac, st))) return rc;
+    TcGemmArgs a{nq, (int)h->n, t.kpad, nullptr, tmp, h->n, h->d_err};
+    a.kind = t.kind;
+    a.col_fac = t.cfac;
+    a.row_fac = t.kind == kTcE4M3 ? rfac : nullptr;
+    if ((rc = launch_tc_gemm(qb, t.base, a, st))) return rc;
     if ((rc = launch_tc_unpermute(tmp, nq, h->n, h->row_mult, out_keys, st))) return rc;
     ANN_CUDA_TRY(cudaStreamSynchronize(st));
     return flat_check_err(h);
+}
+
+int ann_flat_set_tc_precision(ann_flat* h, int32_t precision) {
+    clear_error();
+    ANN_CHECK_ARG(h != nullptr, "ann_flat_set_tc_precision: null index");
+    ANN_CHECK_ARG(precision == ANN_TC_BF16 || precision == ANN_TC_E4M3, "ann_flat_set_tc_precision: %d", precision);
+    h->tc_kind = precision == ANN_TC_E4M3 ? kTcE4M3 : kTcBF16;
+    return ANN_OK;
 }
 
 int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int32_t nq, int64_t ldq, int32_t k,
@@ -527,13 +605,17 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
     if (!ws) ws = &h->ws;
     DeviceGuard g(h->device);
     cudaStream_t st = as_stream(stream);
-    int rc = flat_ensure_bf16(h, st);
+    FlatTc t;
+    int rc = flat_ensure_tc(h, st, &t);
     if (rc) return rc;
-    const int dpad = h->dpad, kpad = h->kpad;
+    const int dpad = h->dpad, kpad = t.kpad;
+    const size_t rowb = (size_t)kpad * t.es;  // bytes of an operand row
+    const bool e4 = t.kind == kTcE4M3;
     const bool host = mem == ANN_MEM_HOST;
     Sizer sz;
     sz.take<float>((size_t)nq * dpad);
-    sz.take<__nv_bfloat16>((size_t)nq * kpad);
+    sz.take<unsigned char>((size_t)nq * rowb);
+    sz.take<float>((size_t)nq);
     sz.take<float>((size_t)nq * R);
     sz.take<int>((size_t)nq * R);
     if (host) {
@@ -543,7 +625,8 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
     if ((rc = ws_reserve_device(ws, sz.bytes()))) return rc;
     Carver cv(ws->dev);
     float* qdev = cv.take<float>((size_t)nq * dpad);
-    __nv_bfloat16* qb = cv.take<__nv_bfloat16>((size_t)nq * kpad);
+    unsigned char* qb = cv.take<unsigned char>((size_t)nq * rowb);
+    float* rfac = cv.take<float>((size_t)nq);
     float* keyR = cv.take<float>((size_t)nq * R);
     int* idR = cv.take<int>((size_t)nq * R);
     int64_t* ids_dev = out_ids;
@@ -562,7 +645,7 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
     } else {
         if ((rc = launch_pad_rows(queries, nq, h->dim, ldq, qdev, dpad, st))) return rc;
     }
-    if ((rc = launch_tc_operand(qdev, nq, h->dim, dpad, qb, kpad, kTcQuery, h->metric, 0, st))) return rc;
+    if ((rc = flat_tc_queries(h, t, qdev, nq, dpad, qb, rfac, st))) return rc;
     // Sampled bars: keys over a strided sample of S positions of the BF16 copy (an even sample of the
     // base, by its row order) give each query two bars. The safe bar, its R-th best sampled key, is at
     // or above its R-th best key over all rows (about n * R / S keys pass it). The fast bar, its rF-th
@@ -586,7 +669,8 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
     const int qc = (int)std::min<int64_t>(qmax, ceil_div(ceil_div(nq, nchunks), 128) * 128);
     for (int q0 = 0; q0 < nq; q0 += qc) {
         const int nc = std::min(qc, nq - q0);
-        const __nv_bfloat16* qbc = qb + (size_t)q0 * kpad;
+        const unsigned char* qbc = qb + (size_t)q0 * rowb;
+        const float* rfc = e4 ? rfac + q0 : nullptr;
         float* keyRc = keyR + (size_t)q0 * R;
         int* idRc = idR + (size_t)q0 * R;
         bool done = false;
@@ -609,7 +693,8 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
             for (int i = 0; i < 3; ++i) s2.take<int>((size_t)nc);    // row counts, cursors, re-run list
             s2.take<int64_t>((size_t)nc);              // stream offsets
             s2.take<int>(4);                           // flags
-            s2.take<__nv_bfloat16>((size_t)kRerunBatch * kpad);
+            s2.take<unsigned char>((size_t)kRerunBatch * rowb);
+            s2.take<float>((size_t)kRerunBatch);
             if ((rc = ws_reserve_big(ws, s2.bytes()))) return rc;
             Carver cb(ws->big);
             float* kA = cb.take<float>((size_t)nc * S);
@@ -627,14 +712,18 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
             int* list = cb.take<int>((size_t)nc);
             int64_t* offs = cb.take<int64_t>((size_t)nc);
             int* flags = cb.take<int>(4);
-            __nv_bfloat16* A2 = cb.take<__nv_bfloat16>((size_t)kRerunBatch * kpad);
+            unsigned char* A2 = cb.take<unsigned char>((size_t)kRerunBatch * rowb);
+            float* rfac2 = cb.take<float>((size_t)kRerunBatch);
 
             // stages 2: sample pass and bars, 3: filter pass, 4: grouping, selections and re-runs
             const int prec = h->prof.begin(st, 2);
             TcGemmArgs sa{nc, (int)S, kpad, nullptr, kA, S, h->d_err};
             sa.b_tile_stride = stride;
             sa.b_rows = n;
-            if ((rc = launch_tc_gemm(qbc, h->base_bf16, sa, st))) return rc;
+            sa.kind = t.kind;
+            sa.col_fac = t.cfac;
+            sa.row_fac = rfc;
+            if ((rc = launch_tc_gemm(qbc, t.base, sa, st))) return rc;
             if (sample_bars_smem((int)S) <= kSampleBarsMaxSmem) {
                 if ((rc = launch_sample_bars(kA, (int)S, nc, rF, R, tauF, tauS, st))) return rc;
             } else {
@@ -649,21 +738,24 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
                 if ((rc = launch_radix_select(bar, nc, st))) return rc;
             }
             h->prof.mark(prec, st);
-            auto filter = [&](const __nv_bfloat16* A, int M, const float* tau) -> int {
+            auto filter = [&](const void* A, int M, const float* tau, const float* rf) -> int {
                 TcGemmArgs fa{M, (int)n, kpad, nullptr, nullptr, n, h->d_err};
+                fa.kind = t.kind;
+                fa.col_fac = t.cfac;
+                fa.row_fac = rf;
                 fa.tau = tau;
                 fa.fkey = fkey;
                 fa.fcol = fcol;
                 fa.frow = frow;
                 fa.wcount = wcnt;
                 fa.wcap = wcap;
-                int r = launch_tc_gemm(A, h->base_bf16, fa, st);
+                int r = launch_tc_gemm(A, t.base, fa, st);
                 if (r) return r;
                 TcGroupArgs ga{fkey, fcol, frow, wcnt, tc_filter_warps(M, (int)n), wcap, M, n, h->row_mult,
                                rowcnt, offs, cursor, gkey, gid, flags + 1};
                 return launch_tc_group(ga, st);
             };
-            if ((rc = filter(qbc, nc, tauF))) return rc;
+            if ((rc = filter(qbc, nc, tauF, rfc))) return rc;
             h->prof.mark(prec, st);
             if (prec >= 0) h->prof.filter_launches += 1;
             ANN_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int), st));
@@ -686,8 +778,9 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
                 done = true;
                 for (int j0 = 0; j0 < hf[0] && done; j0 += kRerunBatch) {
                     const int nb = std::min(kRerunBatch, hf[0] - j0);
-                    if ((rc = launch_tc_gather(qbc, kpad, list + j0, nb, tauS, A2, tau2, st))) return rc;
-                    if ((rc = filter(A2, nb, tau2))) return rc;
+                    if ((rc = launch_tc_gather(qbc, (int)rowb, list + j0, nb, tauS, A2, tau2, rfc, rfac2, st)))
+                        return rc;
+                    if ((rc = filter(A2, nb, tau2, e4 ? rfac2 : nullptr))) return rc;
                     ++ngemm;
                     int hmax = 0;
                     ANN_CUDA_TRY(cudaMemcpyAsync(&hmax, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -710,7 +803,10 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
             float* keys = reinterpret_cast<float*>(ws->big);
             const int prec = h->prof.begin(st, 3);  // stage 3: the full key matrix, 4: its selection
             TcGemmArgs a{nf, (int)n, kpad, nullptr, keys, n, h->d_err};
-            if ((rc = launch_tc_gemm(qbc + (size_t)f0 * kpad, h->base_bf16, a, st))) return rc;
+            a.kind = t.kind;
+            a.col_fac = t.cfac;
+            a.row_fac = e4 ? rfc + f0 : nullptr;
+            if ((rc = launch_tc_gemm(qbc + (size_t)f0 * rowb, t.base, a, st))) return rc;
             h->prof.mark(prec, st);
             RadixSelectArgs fs{};
             fs.keys = keys;

@@ -21,6 +21,10 @@ struct ann_flat {
     int64_t row_mult = 1;                // position p of base_bf16 holds row (p * row_mult) mod n
     int kpad = 0;                        // operand columns: dim plus the key columns, rounded up to 64
     int* d_err = nullptr;                // device flag of bounded waits
+    int tc_kind = 0;                     // element kind of the tensor-core search (0 BF16, 1 E4M3)
+    uint8_t* base_e4m3 = nullptr;        // [n, kpad8] E4M3 operand form, Weyl order, built on first use
+    float2* fac_e4m3 = nullptr;          // [n] its per-row key factors
+    int kpad8 = 0;                       // dim rounded up to 32
 };
 
 namespace annb {

@@ -19,6 +19,7 @@
 //             region at slots from a warp prefix sum (no atomics, nothing waits on memory).
 // Every mbarrier wait is bounded (about 2 s); a timeout raises a device flag and the CTA winds down.
 #include <cuda.h>
+#include <cuda_fp8.h>
 
 #include "common.cuh"
 #include "tc_gemm.cuh"
@@ -27,9 +28,16 @@ namespace annb {
 
 namespace {
 
+// A k-block is one 128-byte row per operand row: 64 BF16 or 128 E4M3 elements.
 constexpr int kBM = 128, kBN = 256, kBK = 64, kStages = 4;
-constexpr int kABytes = kBM * kBK * 2;  // 16 KB
-constexpr int kBBytes = kBN * kBK * 2;  // 32 KB
+constexpr int kRowBytes = 128;
+constexpr int kABytes = kBM * kRowBytes;  // 16 KB
+constexpr int kBBytes = kBN * kRowBytes;  // 32 KB
+template <int KIND>
+struct KindOf {
+    static constexpr int kBlockK = KIND == kTcBF16 ? 64 : 128;  // elements per k-block
+    static constexpr int kMmaK = KIND == kTcBF16 ? 16 : 32;     // elements per MMA
+};
 constexpr int kTmemCols = 512;
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -81,15 +89,28 @@ __device__ __forceinline__ uint64_t sw128_desc(const void* p) {
     const uint64_t addr = (su32(p) >> 4) & 0x3FFFull;
     return addr | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
 }
-// Instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N = 256, M = 128.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kBN >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24);
+// Instruction descriptors: FP32 accumulator (bits 4-5 = 1), A and B K-major, N = 256 (bits 17-22 = N / 8),
+// M = 128 (bits 24-28 = M / 16); A and B types in bits 7-9 and 10-12: BF16 = 1 under kind::f16, E4M3 = 0
+// under kind::f8f6f4.
+constexpr uint32_t kIdescShape = (1u << 4) | ((uint32_t)(kBN >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24);
+constexpr uint32_t kIdescBF16 = kIdescShape | (1u << 7) | (1u << 10);
+constexpr uint32_t kIdescE4M3 = kIdescShape;
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t accumulate) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
-        "l"(ad), "l"(bd), "r"(kIdesc), "r"(accumulate)
-        : "memory");
+// One MMA of the 32 bytes of K that follow each descriptor's start: 16 BF16 or 32 E4M3 elements.
+template <int KIND>
+__device__ __forceinline__ void mma_issue(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t accumulate) {
+    if (KIND == kTcBF16)
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
+            "l"(ad), "l"(bd), "r"(kIdescBF16), "r"(accumulate)
+            : "memory");
+    else
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
+            "l"(ad), "l"(bd), "r"(kIdescE4M3), "r"(accumulate)
+            : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
@@ -159,6 +180,7 @@ __device__ __forceinline__ GroupTile group_tile(const TcGemmArgs& a, int64_t t) 
 constexpr int kEpiWarps = 8;
 constexpr int kThreads = 64 + 32 * kEpiWarps;
 
+template <int KIND>
 __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
                                                          const __grid_constant__ CUtensorMap tmB, TcGemmArgs a) {
     extern __shared__ unsigned char smem_raw[];
@@ -175,8 +197,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     float* sT = reinterpret_cast<float*>(smem + kStages * (kABytes + kBBytes) + 256);  // [8 warps][32][33]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int mt = (int)ceil_div(a.M, kBM), nt = (int)ceil_div(a.N, kBN), kt = (int)ceil_div(a.K, kBK);
-    const int k16_last = (a.K - (kt - 1) * kBK) / 16;  // MMAs of the last k-block (K is a multiple of 16)
+    constexpr int kBlockK = KindOf<KIND>::kBlockK, kMmaK = KindOf<KIND>::kMmaK;
+    const int mt = (int)ceil_div(a.M, kBM), nt = (int)ceil_div(a.N, kBN), kt = (int)ceil_div(a.K, kBlockK);
+    const int k16_last = (a.K - (kt - 1) * kBlockK) / kMmaK;  // MMAs of the last k-block
     const bool grouped = a.g_item_off != nullptr;
     const int64_t tiles = grouped ? *a.g_total : (int64_t)mt * nt;
 
@@ -222,8 +245,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                     const uint32_t ph = (uint32_t)((it / kStages) & 1);
                     if (!(ok = bar_wait(&empty[s], ph ^ 1u, a.err))) break;
                     bar_expect(&full[s], kABytes + kBBytes);
-                    tma_load_2d(sA + s * kABytes, &tmA, kb * kBK, (int)arow, &full[s]);
-                    tma_load_2d(sB + s * kBBytes, &tmB, kb * kBK, (int)brow, &full[s]);
+                    tma_load_2d(sA + s * kABytes, &tmA, kb * kBlockK, (int)arow, &full[s]);
+                    tma_load_2d(sB + s * kBBytes, &tmB, kb * kBlockK, (int)brow, &full[s]);
                 }
             }
         }
@@ -243,12 +266,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                     if (!(ok = bar_wait(&full[s], ph, a.err))) break;
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     // the last k-block's box runs past K (zero fill); its zero columns are not multiplied
-                    const int n16 = kb == kt - 1 ? k16_last : kBK / 16;
+                    const int n16 = kb == kt - 1 ? k16_last : kBlockK / kMmaK;
 #pragma unroll
-                    for (int k16 = 0; k16 < kBK / 16; ++k16)
+                    for (int k16 = 0; k16 < kBlockK / kMmaK; ++k16)
                         if (k16 < n16)
-                            mma_bf16(d, sw128_desc(sA + s * kABytes + k16 * 32),
-                                     sw128_desc(sB + s * kBBytes + k16 * 32), (kb | k16) ? 1u : 0u);
+                            mma_issue<KIND>(d, sw128_desc(sA + s * kABytes + k16 * 32),
+                                            sw128_desc(sB + s * kBBytes + k16 * 32), (kb | k16) ? 1u : 0u);
                     mma_commit(&empty[s]);
                 }
                 mma_commit(&tfull[b]);
@@ -306,9 +329,24 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                 continue;
             }
             const float an = (a.normA && m < a.M) ? a.normA[m] : 0.f;
+            const float rfac = (a.row_fac && m < a.M) ? a.row_fac[m] : 1.f;
             // rows past M (TMA zero fill) get a bar no key passes
             const float tau = (a.tau && m < a.M) ? a.tau[m] : -kInf;
             const uint32_t tbase = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kBN + col0);
+            // filter mode with scaled operands: the warp's 128 column factors staged once per tile in its
+            // (otherwise unused) transpose buffer, read back as broadcasts
+            const bool staged = a.col_fac != nullptr && a.out == nullptr;
+            float2* sf = reinterpret_cast<float2*>(tw);
+            if (staged) {
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int col = n0 + col0 + 32 * i + lane;
+                    const int64_t nrow = (int64_t)(col / kBN) * kBN * a.b_tile_stride + col % kBN;
+                    sf[32 * i + lane] = col < a.N ? a.col_fac[nrow] : make_float2(0.f, 0.f);
+                }
+                __syncwarp();
+            }
 #pragma unroll 1
             for (int c = 0; c < 128; c += 64) {
                 uint32_t r0[32], r1[32];
@@ -322,6 +360,20 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
 #pragma unroll
                     for (int u = 0; u < 32; ++u) v[u] = __uint_as_float(h ? r1[u] : r0[u]) + an;
                     const int nb = n0 + col0 + c + 32 * h;  // output column of v[0]
+                    if (staged) {  // scaled operands: key = f.y + f.x * (row scale * accumulator)
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) {
+                            const float2 f = sf[c + 32 * h + u];
+                            v[u] = fmaf(f.x, rfac * v[u], f.y);
+                        }
+                    } else if (a.col_fac) {
+                        const int col = nb + lane;  // output column -> base row (strided sample of 256-row tiles)
+                        const int64_t nrow = (int64_t)(col / kBN) * kBN * a.b_tile_stride + col % kBN;
+                        const float2 f = col < a.N ? a.col_fac[nrow] : make_float2(0.f, 0.f);
+#pragma unroll
+                        for (int u = 0; u < 32; ++u)
+                            v[u] = fmaf(__shfl_sync(0xffffffffu, f.x, u), rfac * v[u], __shfl_sync(0xffffffffu, f.y, u));
+                    }
                     if (nb + 32 > a.N) {  // ragged last tile: columns past N pass no bar (NaN) and are not stored
 #pragma unroll
                         for (int u = 0; u < 32; ++u)
@@ -397,21 +449,23 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-int make_map(CUtensorMap* tm, const void* base, int64_t rows, int cols, int box_rows) {
+int make_map(CUtensorMap* tm, const void* base, int64_t rows, int cols, int box_rows, int kind) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) {
         set_error("cuTensorMapEncodeTiled is not available from the driver");
         return ANN_ERR_CUDA;
     }
     const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-    const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+    const int esize = kind == kTcBF16 ? 2 : 1;
+    const cuuint64_t strides[1] = {(cuuint64_t)cols * esize};
+    const cuuint32_t box[2] = {(cuuint32_t)(kRowBytes / esize), (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
-    const CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+    const CUresult r = fn(tm, kind == kTcBF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 2,
+                          const_cast<void*>(base), dims, strides, box, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
-        set_error("cuTensorMapEncodeTiled failed (%d) for a [%lld, %d] bf16 matrix", (int)r, (long long)rows, cols);
+        set_error("cuTensorMapEncodeTiled failed (%d) for a [%lld, %d] matrix", (int)r, (long long)rows, cols);
         return ANN_ERR_CUDA;
     }
     return ANN_OK;
@@ -426,8 +480,12 @@ int tc_kpad(int dim, int metric) { return (int)ceil_div(dim + (metric == ANN_MET
 static int tc_grid(int M, int N) { return (int)std::min<int64_t>(ceil_div(M, kBM) * ceil_div(N, kBN), kNumSMs); }
 int tc_filter_warps(int M, int N) { return tc_grid(M, N) * kEpiWarps; }
 
-int launch_tc_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, const TcGemmArgs& a, cudaStream_t st) {
-    ANN_CHECK_ARG(a.K % 16 == 0 && a.K > 0, "tensor-core scan: K=%d not a positive multiple of 16", a.K);
+int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream_t st) {
+    const int step = a.kind == kTcBF16 ? 16 : 32;
+    ANN_CHECK_ARG(a.kind == kTcBF16 || a.kind == kTcE4M3, "tensor-core scan: element kind %d", a.kind);
+    ANN_CHECK_ARG(a.K % step == 0 && a.K > 0, "tensor-core scan: K=%d not a positive multiple of %d", a.K, step);
+    ANN_CHECK_ARG(a.kind == kTcBF16 || (a.col_fac && a.row_fac && a.g_item_off == nullptr),
+                  "tensor-core scan: E4M3 operands need their scale factors (and no grouping)");
     ANN_CHECK_ARG((reinterpret_cast<uintptr_t>(A) & 15) == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0,
                   "tensor-core scan: operands must be 16-byte aligned");
     ANN_CHECK_ARG(a.out != nullptr || (a.tau && a.fkey && a.fcol && a.frow && a.wcount && a.wcap > 0),
@@ -442,14 +500,19 @@ int launch_tc_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, const TcGemmA
     ANN_CHECK_ARG(a.g_item_off != nullptr || (ceil_div(a.N, kBN) - 1) * kBN * (int64_t)a.b_tile_stride < b_rows,
                   "tensor-core scan: sample runs past the base");
     CUtensorMap tmA, tmB;
-    int rc = make_map(&tmA, A, a.M, a.K, kBM);
+    int rc = make_map(&tmA, A, a.M, a.K, kBM, a.kind);
     if (rc) return rc;
-    rc = make_map(&tmB, B, b_rows, a.K, kBN);
+    rc = make_map(&tmB, B, b_rows, a.K, kBN, a.kind);
     if (rc) return rc;
     const size_t smem = tc_gemm_smem();
-    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(tc_gemm_kernel)));
     const int grid = a.g_item_off ? kNumSMs : tc_grid(a.M, a.N);  // grouped: persistent over the items
-    tc_gemm_kernel<<<grid, kThreads, smem, st>>>(tmA, tmB, a);
+    if (a.kind == kTcBF16) {
+        ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(tc_gemm_kernel<kTcBF16>)));
+        tc_gemm_kernel<kTcBF16><<<grid, kThreads, smem, st>>>(tmA, tmB, a);
+    } else {
+        ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(tc_gemm_kernel<kTcE4M3>)));
+        tc_gemm_kernel<kTcE4M3><<<grid, kThreads, smem, st>>>(tmA, tmB, a);
+    }
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }
@@ -483,6 +546,53 @@ __global__ void tc_operand_kernel(const float* __restrict__ x, int64_t rows, int
         out[p * kpad + cols + 1] = mid;
         out[p * kpad + cols + 2] = __float2bfloat16_rn(r2);
     }
+}
+
+// One warp per output row: the E4M3 operand form of an FP32 row with its own scale s = max|x| / 448
+// (1 for a zero row): out = e4m3(x / s), saturating; fac = s for a query row; for a base row
+// fac = (-2 s, |x|^2) under L2 and (-s, 0) under inner product, the key's per-column factors.
+__global__ void tc_operand_e4m3_kernel(const float* __restrict__ x, int64_t rows, int cols, int64_t ld, uint8_t* out,
+                                       int kpad, int base, int l2, int64_t row_mult, float* qfac, float2* bfac) {
+    const int64_t p = blockIdx.x * (int64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (p >= rows) return;
+    const int64_t r = row_mult > 0 ? (int64_t)(((unsigned __int128)p * (uint64_t)row_mult) % (uint64_t)rows) : p;
+    float mx = 0.f, ss = 0.f;
+    for (int c = lane; c < cols; c += 32) {
+        const float v = x[r * ld + c];
+        mx = fmaxf(mx, fabsf(v));
+        ss = fmaf(v, v, ss);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    }
+    const float sc = mx > 0.f ? mx / 448.f : 1.f;
+    const float inv = 1.f / sc;
+    for (int c = lane; c < kpad; c += 32) {
+        const float v = c < cols ? x[r * ld + c] * inv : 0.f;
+        out[p * kpad + c] = (uint8_t)__nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3);
+    }
+    if (lane == 0) {
+        if (base)
+            bfac[p] = l2 ? make_float2(-2.f * sc, ss) : make_float2(-sc, 0.f);
+        else
+            qfac[p] = sc;
+    }
+}
+
+int launch_tc_operand_e4m3(const float* x, int64_t rows, int cols, int64_t ld, uint8_t* out, int kpad, int role,
+                           int metric, int64_t row_mult, float* qfac, float2* bfac, cudaStream_t st) {
+    ANN_CHECK_ARG(kpad >= cols && kpad % 32 == 0, "E4M3 operand: kpad %d", kpad);
+    ANN_CHECK_ARG(role == kTcBase ? bfac != nullptr : (qfac != nullptr && row_mult == 0), "E4M3 operand: factors");
+    if (rows == 0) return ANN_OK;
+    tc_operand_e4m3_kernel<<<(unsigned)ceil_div(rows, 8), 256, 0, st>>>(x, rows, cols, ld, out, kpad,
+                                                                         role == kTcBase ? 1 : 0,
+                                                                         metric == ANN_METRIC_L2 ? 1 : 0, row_mult,
+                                                                         qfac, bfac);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
 }
 
 int launch_tc_operand(const float* x, int64_t rows, int cols, int64_t ld, __nv_bfloat16* out, int kpad, int role,

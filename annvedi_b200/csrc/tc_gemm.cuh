@@ -11,6 +11,8 @@ namespace annb {
 //       query row [bf16(-2a), 1, 1, 1]  ->  sum = |b|^2 - 2 a.b
 //   IP: base row [bf16(b)], query row [bf16(-a)]  ->  sum = -a.b
 // Smaller keys are better in both metrics.
+enum TcKind { kTcBF16 = 0, kTcE4M3 = 1 };
+
 struct TcGemmArgs {
     int M, N, K;           // A [M, K], B [N, K] BF16 row-major; K a multiple of 16
     const float* normA;    // [M] optional per-row addend (|a|^2 turns the L2 key into the squared distance)
@@ -39,6 +41,11 @@ struct TcGemmArgs {
     const int64_t* g_dbase = nullptr;
     const int64_t* g_total = nullptr;
     int g_lists = 0;
+    // Element kind of A and B. E4M3 operands carry a scale per row (launch_tc_operand_e4m3): the key is
+    // col_fac[n].y + col_fac[n].x * row_fac[m] * accumulator (key-matrix and filter modes).
+    int kind = kTcBF16;
+    const float2* col_fac = nullptr;  // per B row, indexed like B's rows
+    const float* row_fac = nullptr;   // per A row
 };
 
 enum TcRole { kTcBase = 0, kTcQuery = 1 };
@@ -49,7 +56,11 @@ int tc_kpad(int dim, int metric);
 // Epilogue warps of a filter launch over M x N keys (the size of the wcount array).
 int tc_filter_warps(int M, int N);
 size_t tc_gemm_smem();
-int launch_tc_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, const TcGemmArgs& a, cudaStream_t st);
+int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream_t st);
+// FP32 rows -> E4M3 [rows, kpad] (kpad >= cols, a multiple of 32) with a per-row scale: a query row's
+// scale into qfac[row]; a base row's key factors into bfac[row] (row_mult as for launch_tc_operand).
+int launch_tc_operand_e4m3(const float* x, int64_t rows, int cols, int64_t ld, uint8_t* out, int kpad, int role,
+                           int metric, int64_t row_mult, float* qfac, float2* bfac, cudaStream_t st);
 // FP32 [rows, ld] (first `cols` columns) -> the BF16 operand form of `role` for `metric`, [rows, kpad].
 // With row_mult > 0 (base only), output row p holds input row (p * row_mult) mod rows.
 int launch_tc_operand(const float* x, int64_t rows, int cols, int64_t ld, __nv_bfloat16* out, int kpad, int role,

@@ -83,15 +83,18 @@ __global__ void tc_bar_check_kernel(const int* rowcnt, int M, int R, int* list, 
     if (q < M && rowcnt[q] < R) list[atomicAdd(&flags[0], 1)] = q;
 }
 
-__global__ void tc_gather_kernel(const __nv_bfloat16* A, int kpad, const int* list, int nb, const float* tau,
-                                 __nv_bfloat16* A2, float* tau2) {
+__global__ void tc_gather_kernel(const unsigned char* A, int row_bytes, const int* list, int nb, const float* tau,
+                                 unsigned char* A2, float* tau2, const float* rfac, float* rfac2) {
     const int j = blockIdx.x;
     if (j >= nb) return;
     const int q = list[j];
-    const uint4* src = reinterpret_cast<const uint4*>(A + (size_t)q * kpad);
-    uint4* dst = reinterpret_cast<uint4*>(A2 + (size_t)j * kpad);
-    for (int c = threadIdx.x; c < kpad / 8; c += blockDim.x) dst[c] = src[c];
-    if (threadIdx.x == 0) tau2[j] = tau[q];
+    const uint4* src = reinterpret_cast<const uint4*>(A + (size_t)q * row_bytes);
+    uint4* dst = reinterpret_cast<uint4*>(A2 + (size_t)j * row_bytes);
+    for (int c = threadIdx.x; c < row_bytes / 16; c += blockDim.x) dst[c] = src[c];
+    if (threadIdx.x == 0) {
+        tau2[j] = tau[q];
+        if (rfac) rfac2[j] = rfac[q];
+    }
 }
 
 __global__ void tc_map_ids_kernel(int* ids, int64_t count, int64_t n, int64_t mult) {
@@ -254,11 +257,12 @@ int launch_tc_bar_check(const int* rowcnt, int M, int R, int* list, int* flags, 
     return ANN_OK;
 }
 
-int launch_tc_gather(const __nv_bfloat16* A, int kpad, const int* list, int nb, const float* tau, __nv_bfloat16* A2,
-                     float* tau2, cudaStream_t st) {
+int launch_tc_gather(const void* A, int row_bytes, const int* list, int nb, const float* tau, void* A2, float* tau2,
+                     const float* rfac, float* rfac2, cudaStream_t st) {
     if (nb == 0) return ANN_OK;
-    ANN_CHECK_ARG(kpad % 8 == 0, "gather: kpad %d", kpad);
-    tc_gather_kernel<<<nb, 128, 0, st>>>(A, kpad, list, nb, tau, A2, tau2);
+    ANN_CHECK_ARG(row_bytes % 16 == 0, "gather: row of %d bytes", row_bytes);
+    tc_gather_kernel<<<nb, 128, 0, st>>>(static_cast<const unsigned char*>(A), row_bytes, list, nb, tau,
+                                         static_cast<unsigned char*>(A2), tau2, rfac, rfac2);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

@@ -35,9 +35,9 @@ int launch_tc_group(const TcGroupArgs& g, cudaStream_t st);
 
 // Rows with fewer than R survivors go to list (count in flags[0]).
 int launch_tc_bar_check(const int* rowcnt, int M, int R, int* list, int* flags, cudaStream_t st);
-// A2[j] = A[list[j]], tau2[j] = tau[list[j]], j < nb.
-int launch_tc_gather(const __nv_bfloat16* A, int kpad, const int* list, int nb, const float* tau, __nv_bfloat16* A2,
-                     float* tau2, cudaStream_t st);
+// A2[j] = A[list[j]] (rows of row_bytes), tau2[j] = tau[list[j]] and, if given, rfac2[j] = rfac[list[j]].
+int launch_tc_gather(const void* A, int row_bytes, const int* list, int nb, const float* tau, void* A2, float* tau2,
+                     const float* rfac, float* rfac2, cudaStream_t st);
 // ids[i] (positions of the BF16 copy) -> base rows, in place; kNoId stays.
 int launch_tc_map_ids(int* ids, int64_t count, int64_t n, int64_t mult, cudaStream_t st);
 // out[q][row(p)] = keys[q][p] for a [nq, n] key matrix in position order.

@@ -172,6 +172,14 @@ class LinearIndex:
                                                _lib.MEM_HOST, _lib.ptr(ids), _lib.ptr(dists), None))
         return ids, dists
 
+    def set_tc_precision(self, precision: str = "bf16") -> None:
+        """Element kind of search_tc / scores_tc: "bf16" (default) or "e4m3" (scaled FP8: twice the tensor
+        rate, a coarser key; pair it with a deeper refine_r)."""
+        kinds = {"bf16": 0, "e4m3": 1}
+        if precision not in kinds:
+            raise ValueError(f"unknown precision {precision!r}")
+        _lib.check(self._lib.ann_flat_set_tc_precision(self._h, kinds[precision]))
+
     def scores_tc(self, queries):
         """Diagnostic: the tensor-core key matrix [nq, N] (device tensor in, device tensor out)."""
         import torch

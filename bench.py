@@ -522,6 +522,8 @@ def run_ours(args, rank, world, local):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and ivf is not None:
         line["cpu_baseline"] = cpu_baseline_ivf(ivf, queries, npc if npc is not None else npc_tc, args)
+    if rank == 0 and world == 1 and args.fp8:
+        line["scaled_fp8_4m_256"] = scaled_fp8_c4(args, local)
     if rank == 0 and world == 1 and args.serve_seconds > 0 and npc is not None:
         line["serving"] = serving_c5(args, local, ivf, npc, w)
     return line
@@ -551,6 +553,25 @@ def serving_c5(args, local, ivf, npc, w3):
     kth_ip = torch.cat(kth_ip)
     del xb
     kth_l2 = ground_truth(w3.base, w3.queries, K_NN)
+    # the exact IP index's own batch figure (the 1M x 768 configuration): 10k-query batches
+    stream = torch.cuda.current_stream()
+    c2_ids = torch.empty(10_000, K_NN, dtype=torch.int64, device=dev)
+    c2_d = torch.empty(10_000, K_NN, dtype=torch.float32, device=dev)
+    c2_step = lambda: exact.search_tc(w2.queries, K_NN, refine_r=400, out_ids=c2_ids, out_dists=c2_d)
+    for _ in range(3):
+        c2_step()
+    torch.cuda.synchronize()
+    c2_ms = _time_steps(c2_step, 5, stream) / 5
+    xq = w2.queries.double()
+    hit = []
+    for s0 in range(0, 10_000, 1000):
+        x = w2.base[c2_ids[s0:s0 + 1000]].double()
+        sc = (x * xq[s0:s0 + 1000, None, :]).sum(-1)
+        hit.append((sc >= kth_ip[s0:s0 + 1000, None] * (1 - 1e-9) - 1e-12).double().mean().item())
+    c2 = {"workload": "1M x 768 mixture (1,024 centres, sigma 0.35, normalised), inner product, k=100, "
+                      "10k-query batches", "form": "tensor-core exact search, R = 400",
+          "qps": round(10_000 / (c2_ms / 1e3), 1), "ms_per_batch": round(c2_ms, 3),
+          "recall_at_100": round(float(np.mean(hit)), 4)}
     pools = {"ivf_sq8_384": w3.queries.cpu().numpy(), "exact_ip_768": w2.queries.cpu().numpy()}
     routes = [serving.ivf_route("ivf_sq8_384", ivf, npc, args.refine),
               serving.tc_route("exact_ip_768", exact, refine_r=400)]
@@ -598,7 +619,51 @@ def serving_c5(args, local, ivf, npc, w3):
     torch.cuda.empty_cache()
     return {"config": "IVF-SQ8 1M x 384 (70%) + exact IP 1M x 768 tensor-core form (30%); Poisson arrivals, "
                       "request sizes geometric(0.1) capped at 256, k=100, 3 workers, admission by free HBM",
-            "runs": out}
+            "runs": out, "exact_ip_768_batch": c2}
+
+
+def scaled_fp8_c4(args, local):
+    """The scaled-FP8 configuration: 4,000,000 x 256, 4,096-centre mixture (sigma 0.4), not normalised
+    (norms spread 0.5-2.0), 20,000 queries, squared L2, k = 100, exact FP32 re-rank of the best 500.
+    The tensor-core exact search with E4M3 operands (a scale per vector, FP32 accumulation) beside the
+    same search with BF16 operands; recall@100 against the FP64 exact top-100 of the first 500 queries."""
+    import torch
+    from annvedi_b200 import synth
+    from annvedi_b200.linear import LinearIndex
+    dev = f"cuda:{local}"
+    n, d, nq, R = 4_000_000, 256, 20_000, 500
+    w = synth.scaled_mixture(n, d, nq, c=4096, sigma=0.4, seed=5, backend="torch", device=dev)
+    xb = w.base.double()
+    qs = w.queries[:500].double()
+    dd = (xb * xb).sum(1)[None] - 2 * qs @ xb.T + (qs * qs).sum(1)[:, None]
+    kth = torch.topk(dd, K_NN, dim=1, largest=False).values[:, -1]
+    del dd, xb
+    ix = LinearIndex(device=local, metric="l2", mode="exact")
+    ix.fit(w.base)
+    stream = torch.cuda.current_stream()
+    ids = torch.empty(nq, K_NN, dtype=torch.int64, device=dev)
+    dist = torch.empty(nq, K_NN, dtype=torch.float32, device=dev)
+    out = {"workload": "4M x 256 scaled mixture (4,096 centres, sigma 0.4, norms 0.5-2.0), 20k-query batches, "
+                       "squared L2, k=100, re-rank of the best 500"}
+    for prec in ("e4m3", "bf16"):
+        ix.set_tc_precision(prec)
+        step = lambda: ix.search_tc(w.queries, K_NN, refine_r=R, out_ids=ids, out_dists=dist)
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        ix.reset_profile_results()
+        ix.set_profiling(True)
+        ms = _time_steps(step, 3, stream) / 3
+        ix.set_profiling(False)
+        st = ix.get_stage_times()
+        x = w.base[ids[:500]].double()
+        pd = ((x - qs[:, None]) ** 2).sum(-1)
+        rec = float((pd <= kth[:, None] * (1 + 1e-9) + 1e-12).double().mean())
+        out[prec] = {"qps": round(nq / (ms / 1e3), 1), "ms_per_batch": round(ms, 3), "recall_at_100": round(rec, 4),
+                     "filter_ms_per_batch": round(st["tc_filter_ms"] / 3, 3)}
+    del ix, w
+    torch.cuda.empty_cache()
+    return out
 
 
 def _reference_ivf_from(ivf):
@@ -711,6 +776,7 @@ def main():
     ap.add_argument("--forms", default="plain,tc,ivf,ivf_tc",
                     help="forms to measure (the default measures all; one form alone is for profiling it)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="per offered rate; 0 skips serving")
+    ap.add_argument("--no-fp8", dest="fp8", action="store_false", help="skip the scaled-FP8 configuration")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[2000, 10000, 50000])
     ap.add_argument("--ref-nprobe", type=int, default=32)
     ap.add_argument("--cpu-sample", type=int, default=64)

@@ -111,6 +111,15 @@ int ann_flat_profile_stages(ann_flat* h, double* out10);
 int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int32_t nq, int64_t ldq, int32_t k,
                       int32_t refine_r, int32_t mem, int64_t* out_ids, float* out_dists, void* stream);
 
+/* Element kind of the tensor-core search (no counterpart in the reference): ANN_TC_BF16 (default) or
+ * ANN_TC_E4M3 -- FP8 operands with a scale per vector (s = max|x| / 448), FP32 accumulation, the key
+ * |x|^2 - 2 s_x s_q acc (or -s_x s_q acc for inner product) formed in the GEMM's epilogue; twice the tensor
+ * rate of BF16 and half the bytes, with a coarser key that a deeper re-rank (refine_r) wins back. The
+ * operand copy of a kind is built on its first query. */
+#define ANN_TC_BF16 0
+#define ANN_TC_E4M3 1
+int ann_flat_set_tc_precision(ann_flat* h, int32_t precision);
+
 /* Diagnostic: the tensor-core key matrix out_keys[nq][n] (device pointers; synchronous). */
 int ann_flat_scores_tc(ann_flat* h, const float* queries, int32_t nq, int64_t ldq, float* out_keys, void* stream);
 

@@ -125,3 +125,63 @@ def test_tc_rerun_under_safe_bar_is_exact(cuda):
     st = ix.get_stage_times()
     check_exact_topk(base, queries, ids, d, 20)
     assert st["tc_gemm_launches"] >= 3, st  # sample, filter and at least one re-run
+
+
+def _ref_keys_e4m3(base, queries, metric):
+    """Keys from the same E4M3 operands: each row over its own scale max|x| / 448, rounded to nearest."""
+    import torch
+
+    def quant(x):
+        s = x.abs().amax(1, keepdim=True) / 448.0
+        s = torch.where(s > 0, s, torch.ones_like(s))
+        xq = (x / s).clamp(-448.0, 448.0).to(torch.float8_e4m3fn).float()
+        return xq, s[:, 0]
+
+    xb, sb = quant(base)
+    qb, sq = quant(queries)
+    dot = (qb.double() @ xb.double().T) * sq[:, None].double() * sb[None, :].double()
+    if metric == "ip":
+        return -dot
+    return (base.double() ** 2).sum(1)[None, :] - 2.0 * dot
+
+
+@pytest.mark.parametrize("n,dim,nq", [(1000, 100, 200), (5000, 256, 130), (4096, 768, 64)])
+@pytest.mark.parametrize("metric", ["l2", "ip"])
+def test_tc_e4m3_key_matrix(cuda, n, dim, nq, metric):
+    """E4M3 operands (a scale per vector), FP32 accumulation: the keys equal an FP64 computation on the same
+    E4M3-rounded operands up to the accumulation's rounding. The tensor cores' E4M3 accumulation keeps fewer
+    bits than FP32 over long K (measured: 2e-5 of the key scale at K = 256, 1.6e-4 at K = 768), far below the
+    E4M3 rounding of the operands themselves (2^-4 per element); the bound is 4e-4 of the key scale."""
+    import torch
+    from annvedi_b200.linear import LinearIndex
+    w = synth.scaled_mixture(n, dim, nq, c=64, seed=n + dim)
+    base = torch.from_numpy(w.base).cuda()
+    q = torch.from_numpy(w.queries).cuda()
+    ix = LinearIndex(device=0, metric=metric, mode="exact")
+    ix.fit(base)
+    ix.set_tc_precision("e4m3")
+    keys = ix.scores_tc(q).double()
+    torch.cuda.synchronize()
+    ref = _ref_keys_e4m3(base, q, metric)
+    scale = ref.abs().max().item()
+    err = (keys - ref).abs().max().item()
+    assert err < 4e-4 * scale + 1e-5, f"max |key - ref| = {err} (key scale {scale})"
+
+
+@pytest.mark.parametrize("metric", ["l2", "ip"])
+def test_tc_e4m3_search_recovers_exact(cuda, metric):
+    """The scaled-FP8 form with a deep re-rank returns exact FP32 distances for its ids and nearly all of
+    the exact top-k (the sampled-bar path: 300,000 rows)."""
+    import torch
+    from oracle.refmod import exact_topk_f64
+    from tests.helpers import fp64_dists
+    from annvedi_b200.linear import LinearIndex
+    w = synth.scaled_mixture(300_000, 128, 96, c=256, seed=31)
+    ix = LinearIndex(device=0, metric=metric, mode="exact")
+    ix.fit(torch.from_numpy(w.base).cuda())
+    ix.set_tc_precision("e4m3")
+    ids, d = ix.search_tc(w.queries, 50, refine_r=1000)
+    if metric == "l2":
+        np.testing.assert_allclose(d, fp64_dists(w.base, w.queries, ids), rtol=1e-5, atol=1e-5)
+    gt, _ = exact_topk_f64(w.base, w.queries, 50, metric)
+    assert np.mean([len(set(a) & set(b)) / 50 for a, b in zip(ids, gt)]) > 0.99
