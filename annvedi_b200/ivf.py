@@ -152,6 +152,14 @@ class IVFIndex:
         _lib.check(self._lib.ann_ivf_reset_profile(self._h))
 
     # ---- batched API -----------------------------------------------------------------------------
+    @property
+    def dim(self) -> int:
+        return self._dim
+
+    @property
+    def ntotal(self) -> int:
+        return self._n
+
     def search(self, queries, k: int, n_probes: int = 0, n_probe_clusters: int = 8, refine_r: int = -1,
                max_candidates: int | None = None, mode: str | None = None, workspace=None, out_ids=None,
                out_dists=None, stream=None, with_dists: bool = True):

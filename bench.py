@@ -173,14 +173,8 @@ def ground_truth(base, queries, k):
 
 def recall_evaluator(base, queries, ids, kth):
     """mean(pred_d[:k] <= true_d[k-1]) with FP64 distances (orthogonal-competition/evaluator.py:149-157)."""
-    hits = 0.0
-    for s in range(0, queries.shape[0], 1000):
-        ii = ids[s:s + 1000]
-        ok = ii >= 0
-        x = base[ii.clamp(min=0)].double()
-        d = ((x - queries[s:s + 1000].double()[:, None, :]) ** 2).sum(-1)
-        hits += float(((d <= kth[s:s + 1000, None] * (1 + 1e-9) + 1e-12) & ok).double().sum().item())
-    return hits / ids.numel()
+    from annvedi_b200.autotune import recall_at_k
+    return recall_at_k(base, queries, ids, kth)
 
 
 def _time_steps(fn, steps, stream):
@@ -294,6 +288,20 @@ def run_ours(args, rank, world, local):
                                   "scan_gbs": round(gbs, 1), "hbm_frac": round(gbs / hbm_peak, 4),
                                   "kernel": "flat_stream_kernel", "bytes_per_launch": n * dpad * 4}
         flat_line["small_batch_hbm"] = small
+        # batch-1 latency of the plain scan as a replayed CUDA graph
+        from annvedi_b200 import graphs
+        gs = graphs.flat_exact(flat, 1, K_NN, local)
+        lat = []
+        for i in range(args.latency_queries):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            gs(queries[i:i + 1])
+            b.record(stream)
+            b.synchronize()
+            lat.append(a.elapsed_time(b))
+        flat_line["batch1_graph_ms"] = {"p50": round(float(np.percentile(lat, 50)), 4),
+                                        "p99": round(float(np.percentile(lat, 99)), 4)}
+        del gs
         del flat
         torch.cuda.empty_cache()
 
@@ -332,22 +340,23 @@ def run_ours(args, rank, world, local):
         build_s = time.perf_counter() - t0
         o_ids = torch.empty(q, K_NN, dtype=torch.int64, device=dev)
         o_d = torch.empty(q, K_NN, dtype=torch.float32, device=dev)
-    sweep = []
+    # nprobe for each IVF form: the autotuner's cheapest probe count with recall@100 >= 0.95 (re-rank
+    # depth fixed at the configuration's R)
+    sweep, sweep_tc = [], []
+    if "ivf" in sel or "ivf_tc" in sel:
+        from annvedi_b200 import autotune
+        modes = [m for m, f in (("exact", "ivf"), ("tc", "ivf_tc")) if f in sel]
+        tuned = autotune.tune_ivf(ivf, base, queries, kth, K_NN, 0.95, modes=modes, nprobes=(8, 16, 32, 64, 128),
+                                  refines=(args.refine,), reps=2)
+
+        def pick(mode):
+            rows = [r for r in tuned["table"] if r["mode"] == mode]
+            ok = [r for r in rows if r["recall"] >= 0.95]
+            r = ok[0] if ok else rows[-1]
+            return r["nprobe"], r["recall"], r["qps"], [{"nprobe": x["nprobe"], "recall_at_100": x["recall"],
+                                                         "qps": x["qps"]} for x in rows]
     if "ivf" in sel:
-        sweep = []
-        chosen = None
-        for npc in (8, 16, 32, 64, 128):
-            ivf.search(queries, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids, out_dists=o_d)
-            torch.cuda.synchronize()
-            rec = recall_evaluator(base, queries, o_ids, kth)
-            ms = _time_steps(lambda: ivf.search(queries, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids,
-                                                out_dists=o_d), 2, stream) / 2
-            sweep.append({"nprobe": npc, "recall_at_100": round(rec, 4), "qps": round(q / (ms / 1e3), 1)})
-            if chosen is None and rec >= 0.95:
-                chosen = (npc, rec, q / (ms / 1e3))
-        if chosen is None:
-            chosen = (128, sweep[-1]["recall_at_100"], sweep[-1]["qps"])
-        npc, ivf_rec, ivf_qps = chosen
+        npc, ivf_rec, ivf_qps, sweep = pick("exact")
 
         def ivf_step():
             ivf.search(queries, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids, out_dists=o_d)
@@ -364,22 +373,8 @@ def run_ours(args, rank, world, local):
         }
 
     # ---- IVF on the tensor cores: the same lists scored by grouped BF16 tcgen05 GEMMs ----
-    sweep_tc = []
     if "ivf_tc" in sel:
-        sweep_tc = []
-        chosen_tc = None
-        for npc_t in (8, 16, 32):
-            ivf.search(queries, K_NN, 0, npc_t, args.refine, max_candidates=0, mode="tc", out_ids=o_ids, out_dists=o_d)
-            torch.cuda.synchronize()
-            rec = recall_evaluator(base, queries, o_ids, kth)
-            ms = _time_steps(lambda: ivf.search(queries, K_NN, 0, npc_t, args.refine, max_candidates=0, mode="tc",
-                                                out_ids=o_ids, out_dists=o_d), 3, stream) / 3
-            sweep_tc.append({"nprobe": npc_t, "recall_at_100": round(rec, 4), "qps": round(q / (ms / 1e3), 1)})
-            if chosen_tc is None and rec >= 0.95:
-                chosen_tc = (npc_t, rec, q / (ms / 1e3))
-        if chosen_tc is None:
-            chosen_tc = (32, sweep_tc[-1]["recall_at_100"], sweep_tc[-1]["qps"])
-        npc_tc, tc_rec, tc_qps = chosen_tc
+        npc_tc, tc_rec, tc_qps, sweep_tc = pick("tc")
 
         def ivf_tc_step():
             ivf.search(queries, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc", out_ids=o_ids, out_dists=o_d)
@@ -445,6 +440,21 @@ def run_ours(args, rank, world, local):
     # ---- batch-1 latency of both forms ----
     latency = {name: _latency(f["lat_dev"], f["lat_host"], queries, qh, args.latency_queries, stream)
                for name, f in forms.items()}
+    if "ivf" in sel:  # the IVF-SQ8 query of one query replayed as a CUDA graph
+        from annvedi_b200 import graphs
+        gi = graphs.ivf_exact(ivf, 1, K_NN, npc, args.refine, local)
+        lat = []
+        for i in range(args.latency_queries):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            gi(queries[i:i + 1])
+            b.record(stream)
+            b.synchronize()
+            lat.append(a.elapsed_time(b))
+        latency["ivf_sq8_graph"] = {"device_p50": round(float(np.percentile(lat, 50)), 4),
+                                    "device_p99": round(float(np.percentile(lat, 99)), 4),
+                                    "queries": args.latency_queries}
+        del gi
 
     # ---- roofline of the headline's dominant kernel ----
     if head == "tensor_core_exact":
@@ -509,7 +519,8 @@ def run_ours(args, rank, world, local):
         "speedup_vs_plain_fp32_scan": round(qps / (flat_qps * world), 2) if flat_qps else None,
         "forms": summary,
         "plain_fp32_scan": flat_line,
-        "nprobe_sweep": {"ivf_sq8": sweep, "ivf_tc": sweep_tc},
+        "nprobe_sweep": {"ivf_sq8": sweep, "ivf_tc": sweep_tc,
+                         "chosen_by": "annvedi_b200.autotune.tune_ivf (cheapest nprobe with recall@100 >= 0.95)"},
         "latency_ms_batch1": latency,
         "ivf_build_s": round(build_s, 3) if build_s is not None else None,
         "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": q * d * 4,
