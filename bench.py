@@ -115,27 +115,38 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup():
+def dist_setup(backend: str = "nccl"):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE); the process group with a short
+    timeout, so that ranks waiting for a rank that failed end with an error."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
+        if backend == "nccl":
+            torch.cuda.set_device(local)
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
     return rank, world, local
 
 
 def max_over_ranks(x: float, world: int) -> float:
+    """The slowest rank's figure (every rank takes part; a MAX all-reduce of one float)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_qps(queries_per_rank: int, steps: int, ms_this_rank: float, world: int) -> float:
+    """value = all ranks' queries / the slowest rank's time (weak scaling: every rank its own batch)."""
+    ms = max_over_ranks(ms_this_rank, world)
+    return world * queries_per_rank * steps / (ms / 1e3)
 
 
 def barrier(world):
@@ -425,7 +436,7 @@ def run_ours(args, rank, world, local):
         cands_timed = ivf.total_distances_count()  # candidates of the timed steps (later calls add more)
     clk = clocks.stop()
     ms_max = max_over_ranks(ms, world)
-    qps = world * q * args.steps / (ms_max / 1e3)
+    qps = whole_job_qps(q, args.steps, ms, world)
     hf["recall"] = recall_evaluator(base, queries, t_ids if head == "tensor_core_exact" else o_ids, kth)
 
     # ---- end to end through the public API with host buffers ----
