@@ -93,6 +93,9 @@ SIGNATURES = [
     ("ann_ivf_query", ctypes.c_int, [_vp, _vp, _vp, _i32, _i64, _i32, _i32, _i32, _i32, _i64, _i32, _i32, _i32,
                                      _vp, _vp, _vp]),
     ("ann_ivf_device_status", ctypes.c_int, [_vp]),
+    ("ann_ivf_import_tables", ctypes.c_int, [_vp, _i32, _i32, _vp, _vp, _vp, _vp]),
+    ("ann_ivf_build_tables", ctypes.c_int, [_vp, _i32, _i32, _vp]),
+    ("ann_ivf_export_tables", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("ann_ivf_total_distances", _i64, [_vp]),
     ("ann_ivf_reset_distances", ctypes.c_int, [_vp]),
     ("ann_ivf_set_profiling", ctypes.c_int, [_vp, _i32]),

@@ -6,7 +6,9 @@
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <cmath>
 #include <mutex>
+#include <random>
 #include <thread>
 #include <vector>
 
@@ -14,6 +16,7 @@
 #include "flat_scan.cuh"
 #include "ivf.cuh"
 #include "ivf_batched.cuh"
+#include "ivf_lsh.cuh"
 #include "radix_select.cuh"
 #include "refmath.cuh"
 #include "runtime.cuh"
@@ -39,6 +42,14 @@ struct ann_ivf {
     std::vector<int64_t> sizes_desc;  // list sizes, largest first (bounds for planning)
     ann_workspace ws;
     StageProfiler prof;  // 0: coarse ranking, 1: plan, 2: SQ8 pass (+ merge), 3: re-rank
+    // LSH bucket tables (n_bits > 0, or several tables); T = 1, B = 0 is the plain inverted-list index
+    int T = 1, B = 0;
+    float* proj = nullptr;        // [T * B, dpad]
+    float* lsh_mean = nullptr;    // [dpad]
+    int64_t* tab_off = nullptr;   // [T * C * 2^B + 1]
+    int32_t* tab_ids = nullptr;   // [T * n]
+    bool lsh() const { return tab_off != nullptr && (B > 0 || T > 1); }
+    LshView lsh_view() const { return LshView{T, B, proj, lsh_mean, tab_off, tab_ids}; }
     __nv_bfloat16* base_bf16 = nullptr;  // [n, kpad] BF16 operand form of the list-ordered rows (tensor-core form)
     __nv_bfloat16* cent_bf16 = nullptr;  // [C, kpad] BF16 operand form of the centroids
     int kpad = 0;
@@ -65,10 +76,16 @@ struct ann_ivf {
 
 static void ivf_free_state(ann_ivf* h) {
     for (void* p : {(void*)h->centroids, (void*)h->original, (void*)h->codes, (void*)h->scale, (void*)h->offset,
-                    (void*)h->r2o, (void*)h->list_off, (void*)h->base_bf16, (void*)h->cent_bf16})
+                    (void*)h->r2o, (void*)h->list_off, (void*)h->base_bf16, (void*)h->cent_bf16, (void*)h->proj,
+                    (void*)h->lsh_mean, (void*)h->tab_off, (void*)h->tab_ids})
         if (p) cudaFree(p);
     h->base_bf16 = nullptr;
     h->cent_bf16 = nullptr;
+    h->proj = h->lsh_mean = nullptr;
+    h->tab_off = nullptr;
+    h->tab_ids = nullptr;
+    h->T = 1;
+    h->B = 0;
     h->kpad = 0;
     h->centroids = nullptr;
     h->original = nullptr;
@@ -389,6 +406,164 @@ int ann_ivf_info(const ann_ivf* h, int64_t* out4) {
     return ANN_OK;
 }
 
+static void lsh_free(ann_ivf* h) {
+    for (void* p : {(void*)h->proj, (void*)h->lsh_mean, (void*)h->tab_off, (void*)h->tab_ids})
+        if (p) cudaFree(p);
+    h->proj = h->lsh_mean = nullptr;
+    h->tab_off = nullptr;
+    h->tab_ids = nullptr;
+    h->T = 1;
+    h->B = 0;
+}
+
+static int lsh_alloc(ann_ivf* h, int T, int B) {
+    const int64_t nbk = (int64_t)T * h->C * ((int64_t)1 << B);
+    cudaError_t e = cudaSuccess;
+    e = cudaMalloc(&h->proj, sizeof(float) * (size_t)std::max(1, T * B) * h->dpad);
+    if (e == cudaSuccess) e = cudaMalloc(&h->lsh_mean, sizeof(float) * h->dpad);
+    if (e == cudaSuccess) e = cudaMalloc(&h->tab_off, sizeof(int64_t) * (size_t)(nbk + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&h->tab_ids, sizeof(int32_t) * (size_t)std::max<int64_t>(1, T * h->n));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        lsh_free(h);
+        set_error("LSH tables: cannot allocate (%s)", cudaGetErrorString(e));
+        return ANN_ERR_NOMEM;
+    }
+    h->T = T;
+    h->B = B;
+    return ANN_OK;
+}
+
+int ann_ivf_import_tables(ann_ivf* h, int32_t n_tables, int32_t n_bits, const float* projections, const float* mean,
+                          const int64_t* table_offsets, const int32_t* table_ids) {
+    clear_error();
+    ANN_CHECK_ARG(h != nullptr && h->n > 0, "ann_ivf_import_tables: index not imported");
+    ANN_CHECK_ARG(n_tables >= 1 && n_tables <= 64 && n_bits >= 0 && n_bits <= 16,
+                  "ann_ivf_import_tables: %d tables of %d bits", n_tables, n_bits);
+    ANN_CHECK_ARG(table_offsets && table_ids && mean && (n_bits == 0 || projections), "ann_ivf_import_tables: null");
+    DeviceGuard g(h->device);
+    lsh_free(h);
+    int rc = lsh_alloc(h, n_tables, n_bits);
+    if (rc) return rc;
+    const int dim = h->dim;
+    const int64_t nbk = (int64_t)n_tables * h->C * ((int64_t)1 << n_bits);
+    ANN_CUDA_TRY(cudaMemset(h->proj, 0, sizeof(float) * (size_t)std::max(1, n_tables * n_bits) * h->dpad));
+    ANN_CUDA_TRY(cudaMemset(h->lsh_mean, 0, sizeof(float) * h->dpad));
+    if (n_bits > 0)
+        ANN_CUDA_TRY(cudaMemcpy2D(h->proj, sizeof(float) * h->dpad, projections, sizeof(float) * dim,
+                                  sizeof(float) * dim, (size_t)n_tables * n_bits, cudaMemcpyHostToDevice));
+    ANN_CUDA_TRY(cudaMemcpy(h->lsh_mean, mean, sizeof(float) * dim, cudaMemcpyHostToDevice));
+    ANN_CUDA_TRY(cudaMemcpy(h->tab_off, table_offsets, sizeof(int64_t) * (size_t)(nbk + 1), cudaMemcpyHostToDevice));
+    ANN_CUDA_TRY(cudaMemcpy(h->tab_ids, table_ids, sizeof(int32_t) * (size_t)n_tables * h->n, cudaMemcpyHostToDevice));
+    return ANN_OK;
+}
+
+int ann_ivf_export_tables(ann_ivf* h, int32_t* out2, float* projections, float* mean, int64_t* table_offsets,
+                          int32_t* table_ids) {
+    clear_error();
+    ANN_CHECK_ARG(h != nullptr, "ann_ivf_export_tables: null index");
+    DeviceGuard g(h->device);
+    if (out2) {
+        out2[0] = h->tab_off ? h->T : 1;
+        out2[1] = h->tab_off ? h->B : 0;
+    }
+    if (!h->tab_off) return ANN_OK;
+    const int dim = h->dim;
+    const int64_t nbk = (int64_t)h->T * h->C * ((int64_t)1 << h->B);
+    if (projections && h->B > 0)
+        ANN_CUDA_TRY(cudaMemcpy2D(projections, sizeof(float) * dim, h->proj, sizeof(float) * h->dpad,
+                                  sizeof(float) * dim, (size_t)h->T * h->B, cudaMemcpyDeviceToHost));
+    if (mean) ANN_CUDA_TRY(cudaMemcpy(mean, h->lsh_mean, sizeof(float) * dim, cudaMemcpyDeviceToHost));
+    if (table_offsets)
+        ANN_CUDA_TRY(cudaMemcpy(table_offsets, h->tab_off, sizeof(int64_t) * (size_t)(nbk + 1), cudaMemcpyDeviceToHost));
+    if (table_ids)
+        ANN_CUDA_TRY(cudaMemcpy(table_ids, h->tab_ids, sizeof(int32_t) * (size_t)h->T * h->n, cudaMemcpyDeviceToHost));
+    return ANN_OK;
+}
+
+int ann_ivf_build_tables(ann_ivf* h, int32_t n_tables, int32_t n_bits, void* stream) {
+    clear_error();
+    ANN_CHECK_ARG(h != nullptr && h->n > 0, "ann_ivf_build_tables: index not fitted");
+    ANN_CHECK_ARG(n_tables >= 1 && n_tables <= 64 && n_bits >= 0 && n_bits <= 16,
+                  "ann_ivf_build_tables: %d tables of %d bits", n_tables, n_bits);
+    DeviceGuard g(h->device);
+    cudaStream_t st = as_stream(stream);
+    lsh_free(h);
+    int rc = lsh_alloc(h, n_tables, n_bits);
+    if (rc) return rc;
+    const int dim = h->dim, T = n_tables, B = n_bits;
+    // projections: mt19937(42), N(0, 1) floats, row by row (:216-225); Gram-Schmidt within each table
+    // when B <= dim (:228-257), in FP32 in the reference's loop order
+    std::vector<float> proj((size_t)T * B * dim);
+    {
+        std::mt19937 gen(42);
+        std::normal_distribution<float> dist(0.0f, 1.0f);
+        for (auto& v : proj) v = dist(gen);
+        if (B <= dim)
+            for (int t = 0; t < T; ++t)
+                for (int b = 0; b < B; ++b) {
+                    float* pi = proj.data() + (size_t)(t * B + b) * dim;
+                    for (int bp = 0; bp < b; ++bp) {
+                        const float* pp = proj.data() + (size_t)(t * B + bp) * dim;
+                        float dot = 0.f;
+                        for (int d = 0; d < dim; ++d) dot += pi[d] * pp[d];
+                        for (int d = 0; d < dim; ++d) pi[d] -= dot * pp[d];
+                    }
+                    float nrm = 0.f;
+                    for (int d = 0; d < dim; ++d) nrm += pi[d] * pi[d];
+                    nrm = std::sqrt(nrm);
+                    if (nrm > 1e-8f)
+                        for (int d = 0; d < dim; ++d) pi[d] /= nrm;
+                }
+    }
+    ANN_CUDA_TRY(cudaMemsetAsync(h->proj, 0, sizeof(float) * (size_t)std::max(1, T * B) * h->dpad, st));
+    if (B > 0)
+        ANN_CUDA_TRY(cudaMemcpy2DAsync(h->proj, sizeof(float) * h->dpad, proj.data(), sizeof(float) * dim,
+                                       sizeof(float) * dim, (size_t)T * B, cudaMemcpyHostToDevice, st));
+    if ((rc = launch_lsh_mean(h->original, h->n, dim, h->dpad, h->lsh_mean, st))) return rc;
+    // bucket keys (list, signature) of every row per table, stably sorted: members ascend by row
+    const int64_t n = h->n;
+    const int nb = 1 << B;
+    int32_t *keys = nullptr, *kout = nullptr, *vin = nullptr;
+    void* tmp = nullptr;
+    size_t tb = 0;
+    int end_bit = 1;
+    while (((int64_t)1 << end_bit) <= (int64_t)h->C * nb) ++end_bit;
+    ANN_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, (int32_t*)nullptr, (int32_t*)nullptr, (int32_t*)nullptr,
+                                                 (int32_t*)nullptr, (int)n, 0, end_bit, st));
+    cudaError_t e = cudaMalloc(&keys, sizeof(int32_t) * (size_t)T * n);
+    if (e == cudaSuccess) e = cudaMalloc(&kout, sizeof(int32_t) * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&vin, sizeof(int32_t) * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, tb);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        for (void* p : {(void*)keys, (void*)kout, (void*)vin, tmp})
+            if (p) cudaFree(p);
+        set_error("LSH build: cannot allocate scratch (%s)", cudaGetErrorString(e));
+        return ANN_ERR_NOMEM;
+    }
+    rc = launch_lsh_row_keys(h->view(), h->lsh_view(), keys, st);
+    if (!rc) rc = launch_iota(vin, n, st);
+    for (int t = 0; t < T && !rc; ++t) {
+        size_t tb2 = tb;
+        cudaError_t e2 = cub::DeviceRadixSort::SortPairs(tmp, tb2, keys + (size_t)t * n, kout, vin,
+                                                         h->tab_ids + (size_t)t * n, (int)n, 0, end_bit, st);
+        if (e2 != cudaSuccess) {
+            set_error("LSH build: sort failed (%s)", cudaGetErrorString(e2));
+            rc = ANN_ERR_CUDA;
+            break;
+        }
+        rc = launch_list_offsets(kout, n, h->C * nb, h->tab_off + (size_t)t * h->C * nb, st);
+        if (!rc && t > 0) rc = launch_add_offset(h->tab_off + (size_t)t * h->C * nb, (int64_t)h->C * nb + 1,
+                                                 (int64_t)t * n, st);
+    }
+    cudaError_t e3 = cudaStreamSynchronize(st);
+    for (void* p : {(void*)keys, (void*)kout, (void*)vin, tmp}) cudaFree(p);
+    if (rc) return rc;
+    ANN_CUDA_TRY(e3);
+    return ANN_OK;
+}
+
 }  // extern "C"
 
 namespace {
@@ -408,7 +583,9 @@ const int g_scan_kind = [] {
 struct IvfQueryCfg {
     int k, npc, R, nsplit, num_threads, bqc, nsplit_c, ncp;
     int64_t max_c, ub, rps_c;
-    bool ref, coarse_flat, batched, tc;
+    bool ref, coarse_flat, batched, tc, lsh;
+    int64_t ub_cand;  // longest explicit candidate stream (LSH buckets; a fallback to every row needs none)
+    int n_probes;
     size_t sort_tmp, scan_tmp, bscratch;
 };
 
@@ -464,6 +641,7 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
         sz.take<float>((size_t)nq * h->dpad);
         sz.take<char>(c.bscratch);
     }
+    if (c.lsh) sz.take<int32_t>((size_t)nq * c.ub_cand);
     if (c.tc) {
         sz.take<float>((size_t)nq * h->C);  // BF16 coarse keys
         sz.take<__nv_bfloat16>((size_t)nq * h->kpad);
@@ -499,6 +677,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     float* DP = c.ref ? cv.take<float>((size_t)nq * c.ub * (c.ncp + 2)) : nullptr;
     float* qs = c.batched ? cv.take<float>((size_t)nq * h->dpad) : nullptr;
     void* bscratch = c.batched ? cv.take<char>(c.bscratch) : nullptr;
+    int32_t* cand = c.lsh ? cv.take<int32_t>((size_t)nq * c.ub_cand) : nullptr;
     float* ckeys = c.tc ? cv.take<float>((size_t)nq * h->C) : nullptr;
     __nv_bfloat16* qb = c.tc ? cv.take<__nv_bfloat16>((size_t)nq * h->kpad) : nullptr;
     __nv_bfloat16* Apk = c.tc ? cv.take<__nv_bfloat16>((size_t)nq * c.npc * h->kpad) : nullptr;
@@ -548,8 +727,32 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         if ((rc = launch_select_topk(Dc, h->C, nullptr, nq, c.npc, nullptr, pkey, probes, st))) return rc;
     }
     h->prof.mark(prec, st);
-    // 2. plan
-    if ((rc = launch_ivf_plan(a, st))) return rc;
+    // 2. plan: whole lists, or the LSH buckets' explicit streams
+    if (c.lsh) {
+        LshCandArgs la{};
+        la.ix = a.ix;
+        la.lsh = h->lsh_view();
+        la.probes = probes;
+        la.npc = c.npc;
+        la.q = qdev;
+        la.ldq = h->dpad;
+        la.nq = nq;
+        la.k = c.k;
+        la.n_probes = c.n_probes;
+        la.max_c = c.max_c;
+        la.ld = c.ub_cand;
+        la.largest_list = h->sizes_desc.empty() ? 1 : h->sizes_desc[0];
+        la.cand_ids = cand;
+        la.n_cands = n_cands;
+        la.n_seg = n_seg;
+        la.ndist = h->d_ndist;
+        if ((rc = launch_lsh_candidates(la, st))) return rc;
+        a.plan.cand_ids = cand;
+        a.plan.cand_ld = c.ub_cand;
+        a.use_stream = false;
+    } else if ((rc = launch_ivf_plan(a, st))) {
+        return rc;
+    }
     h->prof.mark(prec, st);
     // 3. SQ8 pass -> best R per query
     bool done = false;
@@ -643,10 +846,7 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
                   "ann_ivf_query: unknown mode %d", mode);
     ANN_CHECK_ARG(nq == 0 || (queries && out_ids), "ann_ivf_query: null pointer");
     ANN_CHECK_ARG(k <= 1024, "ann_ivf_query: k=%d > 1024", k);
-    if (n_probes != 0) {
-        set_error("ann_ivf_query: multiprobe LSH buckets (n_probes > 0) need n_bits > 0 tables, not built here");
-        return ANN_ERR_UNSUPPORTED;
-    }
+    ANN_CHECK_ARG(n_probes >= 0, "ann_ivf_query: n_probes=%d < 0", n_probes);
     if (nq == 0) return ANN_OK;
     if (!ws) ws = &h->ws;
     DeviceGuard g(h->device);
@@ -679,18 +879,28 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     if (c.max_c != INT64_MAX) ub = std::min(ub, c.max_c - 1 + h->sizes_desc[0]);
     for (int j = 0; j < c.npc; ++j) smallest += h->sizes_desc[h->C - 1 - j];
     if (smallest < k) ub = std::max(ub, h->n);
+    c.lsh = h->lsh();
+    c.n_probes = c.lsh ? n_probes : 0;
+    c.ub_cand = std::max<int64_t>(ub, 1);
+    // an LSH stream can fall short of k however large its lists: then it is every row
+    if (c.lsh) ub = std::max(ub, h->n);
     c.ub = std::max<int64_t>(ub, 1);
+    if (c.lsh && mode == ANN_MODE_TC) {
+        set_error("ann_ivf_query: the tensor-core form scores whole lists; LSH bucket tables use the SQ8 forms");
+        return ANN_ERR_UNSUPPORTED;
+    }
     c.ncp = ref_num_checkpoints(h->dim);
     c.coarse_flat = !c.ref && c.npc <= 512;
-    c.batched = !c.ref && (c.tc || (g_scan_kind == kScanBatched && nq >= kBatchedMinQueries));
+    c.batched = !c.ref && !c.lsh && (c.tc || (g_scan_kind == kScanBatched && nq >= kBatchedMinQueries));
     if (c.tc && (rc0 = ivf_ensure_bf16(h, st))) return rc0;
     const int dpad = h->dpad;
     const bool host = mem == ANN_MEM_HOST;
 
     // queries per device call: bounded scratch in reference mode
     int qc = nq;
-    if (c.ref) {
-        const size_t per_q = sizeof(float) * (size_t)c.ub * (c.ncp + 2) + 4096;
+    if (c.ref || c.lsh) {
+        const size_t per_q = (c.ref ? sizeof(float) * (size_t)c.ub * (c.ncp + 2) : 0) +
+                             (c.lsh ? sizeof(int32_t) * (size_t)c.ub_cand : 0) + 4096;
         qc = (int)std::max<size_t>(1, std::min<size_t>(nq, ((size_t)2 << 30) / per_q));
     }
     c.nsplit = c.ref ? 1 : (int)std::max<int64_t>(1, std::min<int64_t>(64, ceil_div(2 * kNumSMs, qc)));

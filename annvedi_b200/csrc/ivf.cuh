@@ -32,12 +32,15 @@ struct IvfPlan {
     int64_t* seg_pref;         // [nq, npc + 1]
     int32_t* n_seg;            // [nq] lists used; -1 = all rows
     int64_t* n_cands;          // [nq]
+    const int32_t* cand_ids = nullptr;  // [nq, cand_ld] explicit streams (LSH buckets) instead of whole lists
+    int64_t cand_ld = 0;
 };
 
 // Position p of query q's candidate stream -> list-order row.
 __device__ __forceinline__ int64_t plan_row(const IvfPlan& p, int q, int64_t pos) {
     const int ns = p.n_seg[q];
     if (ns < 0) return pos;
+    if (p.cand_ids) return p.cand_ids[(int64_t)q * p.cand_ld + pos];
     const int64_t* pref = p.seg_pref + (int64_t)q * (p.npc + 1);
     int lo = 0, hi = ns - 1;
     while (lo < hi) {
@@ -93,6 +96,8 @@ int launch_sq8_encode(const float* x, int64_t n, int dim, int ld, const float* s
 int launch_gather_rows(const float* src, int64_t n, int ld_src, const int32_t* rows, float* dst, int ld_dst,
                        cudaStream_t st);
 int launch_list_offsets(const int32_t* sorted_assign, int64_t n, int C, int64_t* off, cudaStream_t st);
+int launch_iota(int32_t* v, int64_t n, cudaStream_t st);                 // v[i] = i
+int launch_add_offset(int64_t* v, int64_t n, int64_t add, cudaStream_t st);  // v[i] += add
 int launch_centroid_update(const float* x, int ld, int dim, const int32_t* order, const int64_t* off, int C,
                            float* centroids, int ldc, const float* fallback_rows, cudaStream_t st);
 

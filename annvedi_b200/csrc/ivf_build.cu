@@ -159,6 +159,30 @@ __global__ void list_offsets_kernel(const int32_t* __restrict__ a, int64_t n, in
     off[c] = lo;
 }
 
+__global__ void iota_kernel(int32_t* v, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v[i] = (int32_t)i;
+}
+
+__global__ void add_offset_kernel(int64_t* v, int64_t n, int64_t add) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v[i] += add;
+}
+
+int launch_iota(int32_t* v, int64_t n, cudaStream_t st) {
+    if (n == 0) return ANN_OK;
+    iota_kernel<<<(unsigned)std::min<int64_t>(ceil_div(n, 256), 16 * kNumSMs), 256, 0, st>>>(v, n);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int launch_add_offset(int64_t* v, int64_t n, int64_t add, cudaStream_t st) {
+    if (n == 0) return ANN_OK;
+    add_offset_kernel<<<(unsigned)std::min<int64_t>(ceil_div(n, 256), 16 * kNumSMs), 256, 0, st>>>(v, n, add);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
 int launch_list_offsets(const int32_t* sorted_assign, int64_t n, int C, int64_t* off, cudaStream_t st) {
     list_offsets_kernel<<<(unsigned)ceil_div(C + 1, 128), 128, 0, st>>>(sorted_assign, n, C, off);
     ANN_LAUNCH_CHECK();

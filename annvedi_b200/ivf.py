@@ -1,4 +1,5 @@
-"""IVF-SQ8 index on the GPU: the drop-in for ivf_lsh_cpp.LSHIndex with n_tables = 1, n_bits = 0.
+"""IVF-SQ8 index on the GPU: the drop-in for ivf_lsh_cpp.LSHIndex (inverted lists, optionally with
+LSH bucket tables over them: n_tables >= 1, n_bits in [0, 16]).
 
 Surface of the reference (competitors/ivf_lsh/src/lsh_index_optimized.cpp:658-666):
 ``fit(data, n_tables, n_bits, n_clusters=256)``, ``query(query, k, n_probes=0, n_probe_clusters=8,
@@ -45,9 +46,8 @@ class IVFIndex:
     # ---- build -----------------------------------------------------------------------------------
     def fit(self, data, n_tables: int = 1, n_bits: int = 0, n_clusters: int = 256, kmeans_iters: int = 15,
             centroids=None, assign=None) -> None:
-        if int(n_tables) != 1 or int(n_bits) != 0:
-            raise NotImplementedError("LSH bucket tables (n_tables > 1 or n_bits > 0) are not built on the GPU; "
-                                      "use n_tables=1, n_bits=0 (inverted lists)")
+        if int(n_tables) < 1 or not 0 <= int(n_bits) <= 16:
+            raise RuntimeError("n_tables must be >= 1 and n_bits in [0, 16]")
         if _lib.is_torch(data):
             x = _lib.as_f32_2d(data, "data")
             mem = _lib.MEM_DEVICE if x.is_cuda else _lib.MEM_HOST
@@ -77,6 +77,8 @@ class IVFIndex:
                                          _lib.ptr(asg), int(kmeans_iters), mem, st))
         self._n, self._dim = n, d
         self._C = min(int(n_clusters), n)
+        if int(n_tables) != 1 or int(n_bits) != 0:  # LSH bucket tables over the lists
+            _lib.check(self._lib.ann_ivf_build_tables(self._h, int(n_tables), int(n_bits), st))
 
     @staticmethod
     def _like(v, mem, dtype, x):
@@ -87,22 +89,36 @@ class IVFIndex:
         return np.ascontiguousarray(v.cpu().numpy() if _lib.is_torch(v) else v, dtype)
 
     def import_state(self, state: dict) -> None:
-        """Loads a state in the reference's layout (n_tables = 1, n_bits = 0): keys npts, dim,
-        n_clusters, centroids, original_data, quantized_data, scale, offset,
-        reordered_to_original, table_offsets (= list offsets)."""
-        if int(state.get("n_tables", 1)) != 1 or int(state.get("n_bits", 0)) != 0:
-            raise NotImplementedError("only inverted-list states (n_tables = 1, n_bits = 0) can be imported")
+        """Loads a state in the reference's layout: keys npts, dim, n_clusters, n_tables, n_bits,
+        centroids, original_data, quantized_data, scale, offset, mean, reordered_to_original,
+        projections, table_offsets, table_ids. With n_tables = 1 and n_bits = 0 the table offsets are the
+        list offsets; otherwise they index the buckets (t, list, signature) and the list offsets follow from
+        table 0."""
         n, d, c = int(state["npts"]), int(state["dim"]), int(state["n_clusters"])
+        T, B = int(state.get("n_tables", 1)), int(state.get("n_bits", 0))
+        toff = np.ascontiguousarray(state["table_offsets"], np.int64)
+        if T == 1 and B == 0:
+            list_off = toff
+        else:
+            list_off = np.ascontiguousarray(toff[: c * (1 << B) + 1: 1 << B], np.int64)
         arrs = [np.ascontiguousarray(state[k], t) for k, t in (
             ("centroids", np.float32), ("original_data", np.float32), ("quantized_data", np.uint8),
-            ("scale", np.float32), ("offset", np.float32), ("reordered_to_original", np.int32),
-            ("table_offsets", np.int64))]
-        _lib.check(self._lib.ann_ivf_import(self._h, n, d, c, *[_lib.ptr(a) for a in arrs]))
+            ("scale", np.float32), ("offset", np.float32), ("reordered_to_original", np.int32))]
+        _lib.check(self._lib.ann_ivf_import(self._h, n, d, c, *[_lib.ptr(a) for a in arrs], _lib.ptr(list_off)))
         self._n, self._dim, self._C = n, d, c
+        if T != 1 or B != 0:
+            proj = np.ascontiguousarray(state["projections"], np.float32).reshape(T * B, d) if B else None
+            mean = np.ascontiguousarray(state["mean"], np.float32)
+            ids = np.ascontiguousarray(state["table_ids"], np.int32)
+            _lib.check(self._lib.ann_ivf_import_tables(self._h, T, B, _lib.ptr(proj), _lib.ptr(mean), _lib.ptr(toff),
+                                                       _lib.ptr(ids)))
 
     def export_state(self) -> dict:
         n, d, c = self._n, self._dim, self._C
-        out = {"npts": n, "dim": d, "n_clusters": c, "n_tables": 1, "n_bits": 0,
+        tb = (ctypes.c_int32 * 2)()
+        _lib.check(self._lib.ann_ivf_export_tables(self._h, tb, None, None, None, None))
+        T, B = int(tb[0]), int(tb[1])
+        out = {"npts": n, "dim": d, "n_clusters": c, "n_tables": T, "n_bits": B,
                "centroids": np.empty((c, d), np.float32), "original_data": np.empty((n, d), np.float32),
                "quantized_data": np.empty((n, d), np.uint8), "scale": np.empty(d, np.float32),
                "offset": np.empty(d, np.float32), "reordered_to_original": np.empty(n, np.int32),
@@ -110,9 +126,18 @@ class IVFIndex:
         _lib.check(self._lib.ann_ivf_export(self._h, *[_lib.ptr(out[k]) for k in (
             "centroids", "original_data", "quantized_data", "scale", "offset", "reordered_to_original",
             "table_offsets")]))
-        out["mean"] = np.zeros(d, np.float32)
-        out["projections"] = np.zeros((0, d), np.float32)
-        out["table_ids"] = np.arange(n, dtype=np.int32)
+        if T == 1 and B == 0:
+            out["mean"] = np.zeros(d, np.float32)
+            out["projections"] = np.zeros((0, d), np.float32)
+            out["table_ids"] = np.arange(n, dtype=np.int32)
+        else:
+            out["projections"] = np.empty((T * B, d), np.float32)
+            out["mean"] = np.empty(d, np.float32)
+            out["table_offsets"] = np.empty(T * c * (1 << B) + 1, np.int64)
+            out["table_ids"] = np.empty(T * n, np.int32)
+            _lib.check(self._lib.ann_ivf_export_tables(self._h, None, _lib.ptr(out["projections"]),
+                                                       _lib.ptr(out["mean"]), _lib.ptr(out["table_offsets"]),
+                                                       _lib.ptr(out["table_ids"])))
         return out
 
     # ---- reference surface -----------------------------------------------------------------------

@@ -175,6 +175,19 @@ int ann_ivf_export(ann_ivf* h, float* centroids, float* original, uint8_t* codes
 /* out4 = {n, dim, n_clusters, largest list}. */
 int ann_ivf_info(const ann_ivf* h, int64_t* out4);
 
+/* LSH bucket tables of IVFLSHIndex (lsh_index_optimized.cpp:216-283): n_tables tables of 2^n_bits
+ * buckets per list; bucket (t, c, sig) holds table_ids[table_offsets[(t*C + c)*2^n_bits + sig] ..] (list-
+ * order rows, ascending), signatures the signs of (x - mean) . p over the table's n_bits projections.
+ * Queries then walk the buckets as LSHIndex::query does (:352-457), n_probes multiprobe flips included.
+ * import: the reference's arrays (after ann_ivf_import); build: the reference's projections (mt19937(42),
+ * N(0,1), Gram-Schmidt per table) and tables from the fitted lists; export: out2 = {n_tables, n_bits},
+ * then the arrays (NULL skips one). */
+int ann_ivf_import_tables(ann_ivf* h, int32_t n_tables, int32_t n_bits, const float* projections, const float* mean,
+                          const int64_t* table_offsets, const int32_t* table_ids);
+int ann_ivf_build_tables(ann_ivf* h, int32_t n_tables, int32_t n_bits, void* stream);
+int ann_ivf_export_tables(ann_ivf* h, int32_t* out2, float* projections, float* mean, int64_t* table_offsets,
+                          int32_t* table_ids);
+
 /* LSHIndex::query (lsh_index_optimized.cpp:304-516), batched over `nq` queries:
  * lists ranked by centroid distance, the first `n_probe_clusters` probed whole, in order, until the
  * candidate stream reaches `max_candidates` (-1: the reference's max(2000, 4 * refine target);
@@ -185,8 +198,9 @@ int ann_ivf_info(const ann_ivf* h, int64_t* out4);
  * heap of each of `num_threads` ThreadPool chunks (<= 0: this host's hardware concurrency, as the
  * reference sizes its pool); ANN_MODE_EXACT ranks by full SQ8 distances; ANN_MODE_TC ranks the same
  * candidate streams by BF16 tcgen05 keys of the FP32 rows (|x|^2 - 2 x.q, FP32 accumulate), the lists
- * scored list-major as grouped GEMMs (no counterpart in the reference). `n_probes` (multiprobe
- * LSH buckets) must be 0. Adds each query's candidate count to the distance counter (:459-460). */
+ * scored list-major as grouped GEMMs (no counterpart in the reference; whole lists only). With
+ * bucket tables (ann_ivf_import_tables / ann_ivf_build_tables) the candidate streams are the buckets'
+ * and `n_probes` flips widen each table's probe. Adds each query's candidate count to the distance counter (:459-460). */
 int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t nq, int64_t ldq, int32_t k,
                   int32_t n_probes, int32_t n_probe_clusters, int32_t refine_r, int64_t max_candidates, int32_t mode,
                   int32_t num_threads, int32_t mem, int64_t* out_ids, float* out_dists, void* stream);

@@ -32,10 +32,10 @@ def _ivf(mode="reference", threads=8):
 def test_reference_mode_matches_golden(cuda, ivf_fx):
     cases, _ = mg.ivf_cases()
     for name, spec, cfgs in cases:
-        if spec["n_bits"]:
-            continue  # LSH bucket tables are not built on the GPU
         w = mg.make_workload(spec["workload"])
-        st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
+        proj = mg.projections_from_reference(spec["n_tables"], spec["n_bits"], w.base.shape[1]) if spec["n_bits"] \
+            else None
+        st = ivf_state.build_state(w.base, w.centres, w.assign, spec["n_tables"], spec["n_bits"], proj)
         for ci, (k, n_probes, npc, rr, nt) in enumerate(cfgs):
             ix = _ivf(threads=nt)
             ix.import_state(st)
@@ -179,18 +179,19 @@ def test_exact_mode_device_tensors_and_counter(cuda):
 
 
 def test_ivf_errors_and_facade(cuda):
-    from annvedi_b200 import _lib
     from annvedi_b200.algorithm import Algorithm
     from annvedi_b200.ivf import IVFIndex
     w = synth.zipf_mixture(5000, 32, 6, c=16, lo=20, hi=800, seed=1)
     ix = IVFIndex(device=0)
     with pytest.raises(RuntimeError):
         ix.query(w.queries[0], 5)
-    with pytest.raises(NotImplementedError):
-        ix.fit(w.base, 10, 8, 16)
+    with pytest.raises(RuntimeError):  # the reference's LSHIndex accepts n_bits in [0, 16] only
+        ix.fit(w.base, 1, 17, 16)
+    with pytest.raises(RuntimeError):
+        ix.fit(w.base, 0, 8, 16)
     ix.fit(w.base, 1, 0, 16, centroids=w.centres, assign=w.assign)
-    with pytest.raises(_lib.AnnUnsupported):
-        ix.query(w.queries[0], 5, n_probes=2)
+    # n_bits = 0 leaves no bit to flip (lsh_index_optimized.cpp:408-426): multi-probe changes nothing
+    np.testing.assert_array_equal(ix.query(w.queries[0], 5, n_probes=2), ix.query(w.queries[0], 5))
     with pytest.raises(RuntimeError):
         ix.query(w.queries[0][:5], 5)
     algo = Algorithm()
@@ -246,3 +247,70 @@ def test_tc_mode_over_all_lists_is_exact(cuda):
     ids, d = ix.search(torch.from_numpy(w.queries).cuda(), 50, 0, 64, 400)
     torch.cuda.synchronize()
     check_exact_topk(w.base, w.queries, ids.cpu().numpy(), d.cpu().numpy(), 50)
+
+
+def _lsh_state(seed=3, n=12000, d=64, c=24, T=3, B=4):
+    w = synth.zipf_mixture(n, d, 40, c=c, lo=20, hi=2000, seed=seed)
+    proj = mg.projections_from_reference(T, B, d)
+    return w, ivf_state.build_state(w.base, w.centres, w.assign, T, B, proj)
+
+
+def test_lsh_reference_mode_matches_oracle(cuda):
+    """Bucket tables (3 tables of 4 bits) in the reference's semantics: the candidate streams (exact and
+    multiprobe buckets, caps at bucket granularity, fallback to every row), the per-chunk heaps and the
+    re-rank give the oracle's ids, distances and counter."""
+    w, st = _lsh_state()
+    for k, n_probes, npc, rr, nt, cap in ((10, 0, 4, 40, 4, -1), (50, 3, 6, 200, 8, -1), (20, 6, 3, -1, 3, 0),
+                                          (100, 2, 2, 300, 16, -1)):
+        ix = _ivf(threads=nt)
+        ix.import_state(st)
+        ids, dd = ix.search(w.queries, k, n_probes, npc, rr, max_candidates=cap)
+        nd = 0
+        for i, q in enumerate(w.queries):
+            oi, od, nc = refmod.ivf_query(st, q, k, n_probes, npc, rr, num_threads=nt, lanes=16, max_cands=cap)
+            np.testing.assert_array_equal(ids[i], oi, err_msg=f"k={k} probes={n_probes} npc={npc} q={i}")
+            np.testing.assert_array_equal(dd[i], od)
+            nd += nc
+        assert ix.total_distances_count() == nd
+
+
+def test_lsh_exact_mode_and_state_round_trip(cuda):
+    """Exact selection over the bucket streams: exact FP32 distances for the ids returned, and the ids of
+    an exact selection over the same candidates; export gives back the imported tables."""
+    w, st = _lsh_state(seed=8)
+    ix = _ivf(mode="exact")
+    ix.import_state(st)
+    got = ix.export_state()
+    for key in ("projections", "mean", "table_offsets", "table_ids", "original_data"):
+        np.testing.assert_array_equal(got[key], st[key], err_msg=key)
+    k, n_probes, npc, rr = 20, 3, 6, 200
+    ids, d = ix.search(w.queries, k, n_probes, npc, rr, max_candidates=0)
+    from tests.helpers import fp64_dists
+    np.testing.assert_allclose(d, fp64_dists(w.base, w.queries, ids), rtol=1e-5, atol=1e-6)
+    # the reference semantics over the same streams, with the 64-heap, keeps a subset of what exact keeps
+    ref = _ivf(mode="reference", threads=1)
+    ref.import_state(st)
+    rid, _ = ref.search(w.queries, k, n_probes, npc, rr, max_candidates=0)
+    assert np.mean([len(set(a) & set(b)) / k for a, b in zip(ids, rid)]) > 0.9
+
+
+def test_lsh_gpu_build_matches_reference_tables(cuda):
+    """The GPU build of 3 tables of 4 bits over given lists: the reference's projections (mt19937(42),
+    N(0,1), Gram-Schmidt) and bucket tables, up to rows on a hyperplane within rounding."""
+    from annvedi_b200.ivf import IVFIndex
+    w = synth.zipf_mixture(12000, 64, 8, c=24, lo=20, hi=2000, seed=3)
+    ix = IVFIndex(device=0)
+    ix.fit(w.base, 3, 4, 24, centroids=w.centres, assign=w.assign)
+    got = ix.export_state()
+    want = ivf_state.build_state(w.base, w.centres, w.assign, 3, 4, mg.projections_from_reference(3, 4, 64))
+    np.testing.assert_allclose(got["projections"], want["projections"], atol=1e-5)
+    np.testing.assert_allclose(got["mean"], want["mean"], atol=1e-6)
+
+    def bucket_of_row(stt):
+        off, ids = stt["table_offsets"], stt["table_ids"]
+        out = np.empty(ids.shape[0], np.int64)
+        out[ids + np.repeat(np.arange(3) * 12000, 12000)] = np.repeat(np.arange(off.shape[0] - 1), np.diff(off))
+        return out
+
+    same = np.mean(bucket_of_row(got) == bucket_of_row(want))
+    assert same > 0.999, same
