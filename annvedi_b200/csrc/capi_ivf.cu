@@ -45,11 +45,12 @@ struct ann_ivf {
     // LSH bucket tables (n_bits > 0, or several tables); T = 1, B = 0 is the plain inverted-list index
     int T = 1, B = 0;
     float* proj = nullptr;        // [T * B, dpad]
+    float* projT = nullptr;       // [dim, T * B]
     float* lsh_mean = nullptr;    // [dpad]
     int64_t* tab_off = nullptr;   // [T * C * 2^B + 1]
     int32_t* tab_ids = nullptr;   // [T * n]
     bool lsh() const { return tab_off != nullptr && (B > 0 || T > 1); }
-    LshView lsh_view() const { return LshView{T, B, proj, lsh_mean, tab_off, tab_ids}; }
+    LshView lsh_view() const { return LshView{T, B, proj, projT, lsh_mean, tab_off, tab_ids}; }
     __nv_bfloat16* base_bf16 = nullptr;  // [n, kpad] BF16 operand form of the list-ordered rows (tensor-core form)
     __nv_bfloat16* cent_bf16 = nullptr;  // [C, kpad] BF16 operand form of the centroids
     int kpad = 0;
@@ -77,11 +78,11 @@ struct ann_ivf {
 static void ivf_free_state(ann_ivf* h) {
     for (void* p : {(void*)h->centroids, (void*)h->original, (void*)h->codes, (void*)h->scale, (void*)h->offset,
                     (void*)h->r2o, (void*)h->list_off, (void*)h->base_bf16, (void*)h->cent_bf16, (void*)h->proj,
-                    (void*)h->lsh_mean, (void*)h->tab_off, (void*)h->tab_ids})
+                    (void*)h->projT, (void*)h->lsh_mean, (void*)h->tab_off, (void*)h->tab_ids})
         if (p) cudaFree(p);
     h->base_bf16 = nullptr;
     h->cent_bf16 = nullptr;
-    h->proj = h->lsh_mean = nullptr;
+    h->proj = h->projT = h->lsh_mean = nullptr;
     h->tab_off = nullptr;
     h->tab_ids = nullptr;
     h->T = 1;
@@ -407,9 +408,9 @@ int ann_ivf_info(const ann_ivf* h, int64_t* out4) {
 }
 
 static void lsh_free(ann_ivf* h) {
-    for (void* p : {(void*)h->proj, (void*)h->lsh_mean, (void*)h->tab_off, (void*)h->tab_ids})
+    for (void* p : {(void*)h->proj, (void*)h->projT, (void*)h->lsh_mean, (void*)h->tab_off, (void*)h->tab_ids})
         if (p) cudaFree(p);
-    h->proj = h->lsh_mean = nullptr;
+    h->proj = h->projT = h->lsh_mean = nullptr;
     h->tab_off = nullptr;
     h->tab_ids = nullptr;
     h->T = 1;
@@ -420,6 +421,7 @@ static int lsh_alloc(ann_ivf* h, int T, int B) {
     const int64_t nbk = (int64_t)T * h->C * ((int64_t)1 << B);
     cudaError_t e = cudaSuccess;
     e = cudaMalloc(&h->proj, sizeof(float) * (size_t)std::max(1, T * B) * h->dpad);
+    if (e == cudaSuccess) e = cudaMalloc(&h->projT, sizeof(float) * (size_t)std::max(1, T * B) * h->dim);
     if (e == cudaSuccess) e = cudaMalloc(&h->lsh_mean, sizeof(float) * h->dpad);
     if (e == cudaSuccess) e = cudaMalloc(&h->tab_off, sizeof(int64_t) * (size_t)(nbk + 1));
     if (e == cudaSuccess) e = cudaMalloc(&h->tab_ids, sizeof(int32_t) * (size_t)std::max<int64_t>(1, T * h->n));
@@ -441,6 +443,28 @@ int ann_ivf_import_tables(ann_ivf* h, int32_t n_tables, int32_t n_bits, const fl
     ANN_CHECK_ARG(n_tables >= 1 && n_tables <= 64 && n_bits >= 0 && n_bits <= 16,
                   "ann_ivf_import_tables: %d tables of %d bits", n_tables, n_bits);
     ANN_CHECK_ARG(table_offsets && table_ids && mean && (n_bits == 0 || projections), "ann_ivf_import_tables: null");
+    {
+        // every bucket (t, c, sig) a range of table t's n ids, in order, each a row of list c
+        const int64_t nbl = (int64_t)1 << n_bits;
+        ANN_CHECK_ARG(table_offsets[0] == 0, "ann_ivf_import_tables: table offsets do not start at 0");
+        for (int t = 0; t < n_tables; ++t)
+            for (int64_t c = 0; c < h->C; ++c) {
+                const int64_t lo = h->h_list_off[c], hi = h->h_list_off[c + 1];
+                for (int64_t sg = 0; sg < nbl; ++sg) {
+                    const int64_t bkt = ((int64_t)t * h->C + c) * nbl + sg;
+                    const int64_t b0 = table_offsets[bkt], b1 = table_offsets[bkt + 1];
+                    ANN_CHECK_ARG(b0 <= b1 && b0 >= (int64_t)t * h->n && b1 <= (int64_t)(t + 1) * h->n,
+                                  "ann_ivf_import_tables: bucket %lld has offsets [%lld, %lld)", (long long)bkt,
+                                  (long long)b0, (long long)b1);
+                    for (int64_t j = b0; j < b1; ++j)
+                        ANN_CHECK_ARG(table_ids[j] >= lo && table_ids[j] < hi,
+                                      "ann_ivf_import_tables: bucket %lld holds row %d outside its list",
+                                      (long long)bkt, table_ids[j]);
+                }
+            }
+        ANN_CHECK_ARG(table_offsets[(int64_t)n_tables * h->C * nbl] == (int64_t)n_tables * h->n,
+                      "ann_ivf_import_tables: table offsets do not span n per table");
+    }
     DeviceGuard g(h->device);
     lsh_free(h);
     int rc = lsh_alloc(h, n_tables, n_bits);
@@ -455,6 +479,8 @@ int ann_ivf_import_tables(ann_ivf* h, int32_t n_tables, int32_t n_bits, const fl
     ANN_CUDA_TRY(cudaMemcpy(h->lsh_mean, mean, sizeof(float) * dim, cudaMemcpyHostToDevice));
     ANN_CUDA_TRY(cudaMemcpy(h->tab_off, table_offsets, sizeof(int64_t) * (size_t)(nbk + 1), cudaMemcpyHostToDevice));
     ANN_CUDA_TRY(cudaMemcpy(h->tab_ids, table_ids, sizeof(int32_t) * (size_t)n_tables * h->n, cudaMemcpyHostToDevice));
+    if ((rc = launch_lsh_transpose(h->proj, n_tables * n_bits, dim, h->dpad, h->projT, nullptr))) return rc;
+    ANN_CUDA_TRY(cudaDeviceSynchronize());
     return ANN_OK;
 }
 
@@ -520,6 +546,7 @@ int ann_ivf_build_tables(ann_ivf* h, int32_t n_tables, int32_t n_bits, void* str
     if (B > 0)
         ANN_CUDA_TRY(cudaMemcpy2DAsync(h->proj, sizeof(float) * h->dpad, proj.data(), sizeof(float) * dim,
                                        sizeof(float) * dim, (size_t)T * B, cudaMemcpyHostToDevice, st));
+    if ((rc = launch_lsh_transpose(h->proj, T * B, dim, h->dpad, h->projT, st))) return rc;
     if ((rc = launch_lsh_mean(h->original, h->n, dim, h->dpad, h->lsh_mean, st))) return rc;
     // bucket keys (list, signature) of every row per table, stably sorted: members ascend by row
     const int64_t n = h->n;
@@ -572,6 +599,8 @@ namespace {
 // smaller ones query by query (ivf.cu). ANNB_IVF_SCAN=cpasync or =stream forces a per-query kernel
 // (for comparisons).
 constexpr int kBatchedMinQueries = 32;
+constexpr int kQueryOrderMinBatch = 256;  // smaller batches have no shared candidates worth grouping
+constexpr int kEveryRowMinSplit = 8;      // exact batches split fewer ways redo every-row queries apart
 enum { kScanBatched = 0, kScanCpAsync = 1, kScanStream = 2 };
 const int g_scan_kind = [] {
     const char* v = getenv("ANNB_IVF_SCAN");
@@ -584,6 +613,8 @@ struct IvfQueryCfg {
     int k, npc, R, nsplit, num_threads, bqc, nsplit_c, ncp;
     int64_t max_c, ub, rps_c;
     bool ref, coarse_flat, batched, tc, lsh;
+    bool fallback;    // a query's stream can fall short of k points and become every row
+    bool lsh_keys;    // exact LSH batch: SQ8 keys of the whole streams, then selection
     int64_t ub_cand;  // longest explicit candidate stream (LSH buckets; a fallback to every row needs none)
     int n_probes;
     size_t sort_tmp, scan_tmp, bscratch;
@@ -642,6 +673,7 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
         sz.take<char>(c.bscratch);
     }
     if (c.lsh) sz.take<int32_t>((size_t)nq * c.ub_cand);
+    if (c.lsh_keys) sz.take<float>((size_t)nq * c.ub_cand);
     if (c.tc) {
         sz.take<float>((size_t)nq * h->C);  // BF16 coarse keys
         sz.take<__nv_bfloat16>((size_t)nq * h->kpad);
@@ -649,6 +681,9 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
         sz.take<int64_t>((size_t)nq * c.npc);
         sz.take<int64_t>((size_t)h->C + 1);
     }
+    sz.take<int32_t>((size_t)nq);  // re-rank query order
+    sz.take<int64_t>(1);           // an every-row stream: its length
+    sz.take<int32_t>(1);           // and its segment flag
     return sz.off;
 }
 
@@ -678,11 +713,15 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     float* qs = c.batched ? cv.take<float>((size_t)nq * h->dpad) : nullptr;
     void* bscratch = c.batched ? cv.take<char>(c.bscratch) : nullptr;
     int32_t* cand = c.lsh ? cv.take<int32_t>((size_t)nq * c.ub_cand) : nullptr;
+    float* lkeys = c.lsh_keys ? cv.take<float>((size_t)nq * c.ub_cand) : nullptr;
     float* ckeys = c.tc ? cv.take<float>((size_t)nq * h->C) : nullptr;
     __nv_bfloat16* qb = c.tc ? cv.take<__nv_bfloat16>((size_t)nq * h->kpad) : nullptr;
     __nv_bfloat16* Apk = c.tc ? cv.take<__nv_bfloat16>((size_t)nq * c.npc * h->kpad) : nullptr;
     int64_t* dbase = c.tc ? cv.take<int64_t>((size_t)nq * c.npc) : nullptr;
     int64_t* titem = c.tc ? cv.take<int64_t>((size_t)h->C + 1) : nullptr;
+    int32_t* qorder = cv.take<int32_t>((size_t)nq);
+    int64_t* every_len = cv.take<int64_t>(1);
+    int32_t* every_seg = cv.take<int32_t>(1);
 
     IvfQueryArgs a{};
     a.ix = h->view();
@@ -754,6 +793,26 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         return rc;
     }
     h->prof.mark(prec, st);
+    // The queries whose stream is every row (fewer than k candidates, :453-457): in reference mode they do
+    // not fit the per-query scratch of L = ub positions, and in a large exact batch one CTA would scan all
+    // n rows. The main pass sees them as empty streams; each is redone below on its own, split over the
+    // whole GPU. (Small exact batches already split every query that widely and skip the host read.)
+    std::vector<int> every_row;
+    if (c.fallback && (c.ref || c.nsplit < kEveryRowMinSplit)) {
+        std::vector<int32_t> ns(nq);
+        ANN_CUDA_TRY(cudaMemcpyAsync(ns.data(), n_seg, sizeof(int32_t) * (size_t)nq, cudaMemcpyDeviceToHost, st));
+        ANN_CUDA_TRY(cudaStreamSynchronize(st));
+        for (int i = 0; i < nq; ++i)
+            if (ns[i] < 0) every_row.push_back(i);
+        if (!every_row.empty()) {
+            if ((rc = launch_clear_every_row(a.plan, st))) return rc;
+            const int64_t len = h->n;
+            const int32_t seg = -1;
+            ANN_CUDA_TRY(cudaMemcpyAsync(every_len, &len, sizeof(len), cudaMemcpyHostToDevice, st));
+            ANN_CUDA_TRY(cudaMemcpyAsync(every_seg, &seg, sizeof(seg), cudaMemcpyHostToDevice, st));
+            ANN_CUDA_TRY(cudaStreamSynchronize(st));  // the host values above live on this frame
+        }
+    }
     // 3. SQ8 pass -> best R per query
     bool done = false;
     if (!c.ref && c.batched) {
@@ -797,6 +856,11 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
             done = true;
         }
     }
+    if (!done && c.lsh_keys) {
+        if ((rc = launch_ivf_sq8_dists(a, lkeys, c.ub_cand, st))) return rc;
+        if ((rc = launch_select_topk(lkeys, c.ub_cand, n_cands, nq, c.R, &a.plan, keyR, idR, st))) return rc;
+        done = true;
+    }
     if (done) {
     } else if (!c.ref) {
         a.keyR = keyS;
@@ -821,8 +885,55 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         if ((rc = launch_select_topk(a.V, c.ub, n_cands, nq, c.R, &a.plan, keyR, idR, st))) return rc;
     }
     h->prof.mark(prec, st);
-    // 4. FP32 re-rank and the final top-k
+    // 4. FP32 re-rank and the final top-k; batches run their queries grouped by first probed list, so that
+    // CTAs resident together gather rows of the same lists (shared candidates come from L2)
+    if (!c.ref && nq >= kQueryOrderMinBatch && h->C <= kQueryOrderMaxLists) {
+        if ((rc = launch_query_order(probes, c.npc, nq, (int)h->C, qorder, st))) return rc;
+        a.qorder = qorder;
+    }
     if ((rc = launch_ivf_rerank(a, keyR, idR, c.ref ? 1 : 0, st))) return rc;
+    if (!every_row.empty()) {
+        const int64_t L = h->n;
+        const int nsp = (int)std::min<int64_t>(2 * kNumSMs, std::max<int64_t>(1, ceil_div(L, 2048)));
+        const size_t need = c.ref ? sizeof(float) * (size_t)L * (c.ncp + 2) : (size_t)8 * nsp * c.R;
+        if ((rc = ws_reserve_big(ws, need))) return rc;
+        float* big = reinterpret_cast<float*>(ws->big);
+        for (int q : every_row) {
+            IvfQueryArgs b = a;
+            b.qorder = nullptr;
+            b.plan.nq = 1;
+            b.plan.probes = probes + (size_t)q * c.npc;
+            b.plan.seg_start = seg_start + (size_t)q * c.npc;
+            b.plan.seg_pref = seg_pref + (size_t)q * (c.npc + 1);
+            b.plan.n_seg = every_seg;
+            b.plan.n_cands = every_len;
+            b.plan.cand_ids = nullptr;
+            b.q = qdev + (size_t)q * h->dpad;
+            b.out_ids = ids_dev + (size_t)q * c.k;
+            b.out_dists = dists_dev ? dists_dev + (size_t)q * c.k : nullptr;
+            float* kq = keyR + (size_t)q * c.R;
+            int* iq = idR + (size_t)q * c.R;
+            if (c.ref) {
+                b.L = L;
+                b.D = big;
+                b.V = big + L;
+                b.P = big + 2 * L;
+                if ((rc = launch_ivf_ref_sq8(b, L, st))) return rc;
+                if ((rc = launch_select_topk(b.V, L, b.plan.n_cands, 1, c.R, &b.plan, kq, iq, st))) return rc;
+            } else {
+                b.use_stream = false;
+                b.nsplit = nsp;
+                b.keyR = big;
+                b.idR = reinterpret_cast<int*>(big + (size_t)nsp * c.R);
+                if ((rc = launch_ivf_sq8_scan(b, st))) return rc;
+                MergeArgs m{b.keyR, b.idR, 1, nsp, c.R, c.R, 0, nullptr, nullptr};
+                m.out_id32 = iq;
+                m.out_key32 = kq;
+                if ((rc = launch_merge_splits(m, st))) return rc;
+            }
+            if ((rc = launch_ivf_rerank(b, kq, iq, c.ref ? 1 : 0, st))) return rc;
+        }
+    }
     h->prof.mark(prec, st);
     return ANN_OK;
 }
@@ -878,13 +989,13 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     for (int j = 0; j < c.npc; ++j) ub += h->sizes_desc[j];
     if (c.max_c != INT64_MAX) ub = std::min(ub, c.max_c - 1 + h->sizes_desc[0]);
     for (int j = 0; j < c.npc; ++j) smallest += h->sizes_desc[h->C - 1 - j];
-    if (smallest < k) ub = std::max(ub, h->n);
     c.lsh = h->lsh();
     c.n_probes = c.lsh ? n_probes : 0;
+    // an LSH stream can fall short of k however large its lists; reference-mode scratch is sized for the
+    // capped streams and a query that scans every row is redone on its own (ivf_query_device)
+    c.fallback = c.lsh || smallest < k;
     c.ub_cand = std::max<int64_t>(ub, 1);
-    // an LSH stream can fall short of k however large its lists: then it is every row
-    if (c.lsh) ub = std::max(ub, h->n);
-    c.ub = std::max<int64_t>(ub, 1);
+    c.ub = c.ub_cand;
     if (c.lsh && mode == ANN_MODE_TC) {
         set_error("ann_ivf_query: the tensor-core form scores whole lists; LSH bucket tables use the SQ8 forms");
         return ANN_ERR_UNSUPPORTED;
@@ -899,11 +1010,14 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     // queries per device call: bounded scratch in reference mode
     int qc = nq;
     if (c.ref || c.lsh) {
+        const bool keys = c.lsh && !c.ref && nq >= 64;  // the lsh_keys path, decided below
         const size_t per_q = (c.ref ? sizeof(float) * (size_t)c.ub * (c.ncp + 2) : 0) +
-                             (c.lsh ? sizeof(int32_t) * (size_t)c.ub_cand : 0) + 4096;
+                             (c.lsh ? sizeof(int32_t) * (size_t)c.ub_cand : 0) +
+                             (keys ? sizeof(float) * (size_t)c.ub_cand : 0) + 4096;
         qc = (int)std::max<size_t>(1, std::min<size_t>(nq, ((size_t)2 << 30) / per_q));
     }
     c.nsplit = c.ref ? 1 : (int)std::max<int64_t>(1, std::min<int64_t>(64, ceil_div(2 * kNumSMs, qc)));
+    c.lsh_keys = c.lsh && !c.ref && c.nsplit < kEveryRowMinSplit;
     c.bqc = std::min(flat_scan_bq(qc), flat_scan_max_bq(c.npc));
     {
         const int n_qt = (int)ceil_div(qc, c.bqc);

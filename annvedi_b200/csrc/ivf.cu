@@ -501,6 +501,80 @@ int launch_ivf_sq8_scan(const IvfQueryArgs& a, cudaStream_t st) {
     return ANN_OK;
 }
 
+// ---- 3a'. exact-mode SQ8 keys of whole candidate streams --------------------------------------------
+// D[q * ld + p] = the SQ8 distance of position p of query q's stream, for p < min(n_cands[q], ld): the
+// arithmetic of ivf_sq8_scan_kernel (two threads per row, each a fused multiply-add chain over its half of
+// the bytes in order, then the halves added), so either kernel gives a candidate the same key. grid:
+// (queries, tile slices); a tile is 128 positions; each thread's twelve 16-byte loads (dim 384) are
+// independent, so many are in flight.
+constexpr int kDistGroup = 6;  // 16-byte chunks in flight per thread (dim 384: two groups per half row)
+
+__global__ void __launch_bounds__(256) ivf_sq8_dists_kernel(IvfQueryArgs a, float* __restrict__ D, int64_t ld) {
+    extern __shared__ __align__(16) float sh_qs[];  // qs [dpad8], scale [dpad8]
+    const int dpad8 = a.ix.dpad8;
+    float* sQs = sh_qs;
+    float* sSc = sh_qs + dpad8;
+    const int q = blockIdx.x, tid = threadIdx.x;
+    const float* qv = a.q + (int64_t)q * a.ldq;
+    for (int d = tid; d < dpad8; d += 256) {
+        sQs[d] = d < a.ix.dim ? __fsub_rn(qv[d], a.ix.offset[d]) : 0.f;
+        sSc[d] = d < a.ix.dim ? a.ix.scale[d] : 0.f;
+    }
+    __syncthreads();
+    const int64_t L = min(a.plan.n_cands[q], ld);
+    const int r = tid >> 1, h = tid & 1;
+    const int half = dpad8 >> 1;
+    const float* qs = sQs + h * half;
+    const float* sc = sSc + h * half;
+    float* Dq = D + (int64_t)q * ld;
+    for (int64_t p0 = (int64_t)blockIdx.y * kSq8Tile; p0 < L; p0 += (int64_t)gridDim.y * kSq8Tile) {
+        const int64_t p = p0 + r;
+        const bool valid = p < L;
+        const int64_t row = valid ? plan_row(a.plan, q, p) : 0;
+        const uint4* src = reinterpret_cast<const uint4*>(a.ix.codes + row * dpad8 + h * half);
+        float acc = 0.f;
+        // chunks of 16 bytes, loaded kDistGroup at a time so that they are in flight together
+        for (int b0 = 0; valid && b0 < half; b0 += 16 * kDistGroup) {
+            uint4 cw[kDistGroup];
+#pragma unroll
+            for (int i = 0; i < kDistGroup; ++i)
+                if (b0 + 16 * i < half) cw[i] = src[(b0 >> 4) + i];
+#pragma unroll
+            for (int i = 0; i < kDistGroup; ++i) {
+                if (b0 + 16 * i >= half) break;
+                const int b = b0 + 16 * i;
+                const uint32_t w[4] = {cw[i].x, cw[i].y, cw[i].z, cw[i].w};
+#pragma unroll
+                for (int wi = 0; wi < 4; ++wi) {
+                    const float4 s4 = *reinterpret_cast<const float4*>(sc + b + wi * 4);
+                    const float4 q4 = *reinterpret_cast<const float4*>(qs + b + wi * 4);
+                    const float d0 = __fmaf_rn(u8_to_f32(w[wi], 0), s4.x, -q4.x);
+                    const float d1 = __fmaf_rn(u8_to_f32(w[wi], 1), s4.y, -q4.y);
+                    const float d2 = __fmaf_rn(u8_to_f32(w[wi], 2), s4.z, -q4.z);
+                    const float d3 = __fmaf_rn(u8_to_f32(w[wi], 3), s4.w, -q4.w);
+                    acc = __fmaf_rn(d0, d0, acc);
+                    acc = __fmaf_rn(d1, d1, acc);
+                    acc = __fmaf_rn(d2, d2, acc);
+                    acc = __fmaf_rn(d3, d3, acc);
+                }
+            }
+        }
+        const float other = __shfl_xor_sync(0xffffffffu, acc, 1);  // every lane runs each trip of the loop
+        if (valid && h == 0) Dq[p] = acc + other;
+    }
+}
+
+int launch_ivf_sq8_dists(const IvfQueryArgs& a, float* D, int64_t ld, cudaStream_t st) {
+    if (a.plan.nq == 0) return ANN_OK;
+    ANN_CHECK_ARG(a.ix.dpad8 % 32 == 0, "sq8 keys: code stride %d not a multiple of 32", a.ix.dpad8);
+    const size_t smem = sizeof(float) * 2 * a.ix.dpad8;
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(ivf_sq8_dists_kernel)));
+    const int slices = (int)std::min<int64_t>(8, std::max<int64_t>(1, ceil_div(ld, kSq8Tile)));
+    ivf_sq8_dists_kernel<<<dim3(a.plan.nq, slices), 256, smem, st>>>(a, D, ld);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
 // ---- 3b. reference-mode SQ8 pass ----------------------------------------------------------------
 // grid: (queries, position blocks); block: 16 groups of 16 lanes, one candidate per group.
 __global__ void __launch_bounds__(256) ivf_ref_sq8_kernel(IvfQueryArgs a) {
@@ -515,7 +589,7 @@ __global__ void __launch_bounds__(256) ivf_ref_sq8_kernel(IvfQueryArgs a) {
         sSc[d] = a.ix.scale[d];
     }
     __syncthreads();
-    const int64_t L = a.plan.n_cands[q];
+    const int64_t L = min(a.plan.n_cands[q], a.L);  // a longer stream (every row) is redone on its own
     const int grp = threadIdx.x >> 4;
     const bool leader = (threadIdx.x & 15) == 0;
     float* D = a.D + (int64_t)q * a.L;
@@ -537,7 +611,7 @@ __global__ void __launch_bounds__(256) ivf_ref_sq8_kernel(IvfQueryArgs a) {
 __global__ void __launch_bounds__(128) ivf_ref_replay_kernel(IvfQueryArgs a) {
     const int q = blockIdx.x;
     const int warp = threadIdx.x >> 5;
-    const int64_t L = a.plan.n_cands[q];
+    const int64_t L = min(a.plan.n_cands[q], a.L);
     const int T = (a.num_threads > 0 && L >= 2 * (int64_t)a.num_threads) ? a.num_threads : 1;
     const int lim = a.k < 64 ? a.k : 64;
     float* V = a.V + (int64_t)q * a.L;
@@ -566,7 +640,8 @@ int launch_ivf_ref_sq8(const IvfQueryArgs& a, int64_t Lmax, cudaStream_t st) {
 }
 
 // ---- generic per-query top-k selection over a dense key array -----------------------------------
-// keys[q * ld + p] (keys[offs[q] + p] when offs is given) for p < lens[q] (or ld when lens is null);
+// keys[q * ld + p] (keys[offs[q] + p] when offs is given) for p < lens[q] (at most ld without offs; ld when
+// lens is null);
 // id = plan_row(q, p) when a plan is
 // given, else p. Keeps the best kout (key, id) pairs, sorted, padded with (+inf, INT_MAX).
 __global__ void __launch_bounds__(256) select_topk_kernel(const float* __restrict__ keys, int64_t ld,
@@ -581,7 +656,7 @@ __global__ void __launch_bounds__(256) select_topk_kernel(const float* __restric
     float* sKey = reinterpret_cast<float*>(smem_raw);
     int* sId = reinterpret_cast<int*>(sKey + warps * cap);
     const int q = blockIdx.x;
-    const int64_t len = lens ? lens[q] : ld;
+    const int64_t len = lens ? (offs || ld <= 0 ? lens[q] : min(lens[q], ld)) : ld;
     WarpTopK top;
     top.init(sKey + warp * cap, sId + warp * cap, kout);
     const float* kq = keys + (offs ? offs[q] : (int64_t)q * ld);
@@ -642,7 +717,7 @@ __global__ void __launch_bounds__(256) ivf_rerank_kernel(IvfQueryArgs a, const f
     int* sRow = reinterpret_cast<int*>(sD + R);       // [R]
     float* sKey = reinterpret_cast<float*>(sRow + R); // [cap]
     int* sId = reinterpret_cast<int*>(sKey + cap);    // [cap]
-    const int q = blockIdx.x;
+    const int q = a.qorder ? a.qorder[blockIdx.x] : blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const float* qv = a.q + (int64_t)q * a.ldq;
     for (int d = threadIdx.x; d < dpad; d += blockDim.x) sQ[d] = d < a.ix.dim ? qv[d] : 0.f;
@@ -717,6 +792,91 @@ int launch_ivf_rerank(const IvfQueryArgs& a, const float* keyR, const int* idR, 
         ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(ivf_rerank_kernel<false>)));
         ivf_rerank_kernel<false><<<a.plan.nq, 256, smem, st>>>(a, keyR, idR);
     }
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+__global__ void clear_every_row_kernel(IvfPlan plan) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < plan.nq && plan.n_seg[q] < 0) {
+        plan.n_seg[q] = 0;
+        plan.n_cands[q] = 0;
+    }
+}
+
+int launch_clear_every_row(const IvfPlan& plan, cudaStream_t st) {
+    if (plan.nq == 0) return ANN_OK;
+    clear_every_row_kernel<<<(unsigned)ceil_div(plan.nq, 256), 256, 0, st>>>(plan);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+// Counting sort of the queries by first probed list, in one CTA: counts in shared memory, an
+// exclusive scan, then each query placed at its list's cursor. The order inside a list follows the
+// shared-memory atomics (the re-rank's results do not depend on it).
+__global__ void __launch_bounds__(1024) query_order_kernel(const int32_t* __restrict__ probes, int npc, int nq, int C,
+                                                           int32_t* __restrict__ order) {
+    extern __shared__ int sCnt[];  // [C]
+    __shared__ int sWarp[32];
+    for (int c = threadIdx.x; c < C; c += blockDim.x) sCnt[c] = 0;
+    __syncthreads();
+    for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        const int c = probes[(int64_t)q * npc];
+        if (c >= 0 && c < C) atomicAdd(&sCnt[c], 1);
+    }
+    __syncthreads();
+    // exclusive scan of sCnt: each thread a contiguous run of lists
+    const int per = (C + blockDim.x - 1) / blockDim.x;
+    const int c0 = threadIdx.x * per, c1 = min(C, c0 + per);
+    int run = 0;
+    for (int c = c0; c < c1; ++c) run += sCnt[c];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int inc = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    if (lane == 31) sWarp[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < (int)(blockDim.x >> 5) ? sWarp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += v;
+        }
+        sWarp[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    int acc = inc - run + (warp > 0 ? sWarp[warp - 1] : 0);
+    for (int c = c0; c < c1; ++c) {
+        const int v = sCnt[c];
+        sCnt[c] = acc;
+        acc += v;
+    }
+    __syncthreads();
+    // queries without a valid first list go last, in order
+    const int n_valid = sWarp[(blockDim.x >> 5) - 1];
+    for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+        const int c = probes[(int64_t)q * npc];
+        if (c >= 0 && c < C) order[atomicAdd(&sCnt[c], 1)] = q;
+    }
+    if (n_valid < nq && threadIdx.x == 0) {
+        int pos = n_valid;
+        for (int q = 0; q < nq; ++q) {
+            const int c = probes[(int64_t)q * npc];
+            if (!(c >= 0 && c < C)) order[pos++] = q;
+        }
+    }
+}
+
+int launch_query_order(const int32_t* probes, int npc, int nq, int C, int32_t* order, cudaStream_t st) {
+    ANN_CHECK_ARG(C >= 1 && C <= kQueryOrderMaxLists && npc >= 1, "query order: %d lists", C);
+    if (nq == 0) return ANN_OK;
+    const size_t smem = sizeof(int) * (size_t)C;
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(query_order_kernel)));
+    query_order_kernel<<<1, 1024, smem, st>>>(probes, npc, nq, C, order);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

@@ -76,10 +76,13 @@ struct IvfQueryArgs {
     int metric;                // re-rank metric: ANN_METRIC_L2 (default) or ANN_METRIC_IP
     int64_t* out_ids;          // [nq, k]
     float* out_dists;          // [nq, k]
+    const int32_t* qorder;     // re-rank: CTA b takes query qorder[b] (NULL: query b)
 };
 
 int launch_ivf_plan(const IvfQueryArgs& a, cudaStream_t st);
 int launch_ivf_sq8_scan(const IvfQueryArgs& a, cudaStream_t st);
+// SQ8 keys of whole candidate streams, D[q * ld + p] (the scan's arithmetic, no selection).
+int launch_ivf_sq8_dists(const IvfQueryArgs& a, float* D, int64_t ld, cudaStream_t st);
 int launch_ivf_ref_sq8(const IvfQueryArgs& a, int64_t Lmax, cudaStream_t st);
 int launch_select_topk(const float* keys, int64_t ld_keys, const int64_t* lens, int nq, int kout,
                        const IvfPlan* plan, float* out_key, int* out_id, cudaStream_t st,
@@ -97,6 +100,12 @@ int launch_gather_rows(const float* src, int64_t n, int ld_src, const int32_t* r
                        cudaStream_t st);
 int launch_list_offsets(const int32_t* sorted_assign, int64_t n, int C, int64_t* off, cudaStream_t st);
 int launch_iota(int32_t* v, int64_t n, cudaStream_t st);                 // v[i] = i
+// Every query whose stream is every row (n_seg < 0) becomes an empty stream: n_seg = n_cands = 0.
+int launch_clear_every_row(const IvfPlan& plan, cudaStream_t st);
+// order[0..nq) = the queries grouped by their first probed list (probes[q * npc], in [0, C)), so that
+// neighbouring re-rank CTAs gather rows of the same lists; one CTA, C <= kQueryOrderMaxLists.
+constexpr int kQueryOrderMaxLists = 32768;
+int launch_query_order(const int32_t* probes, int npc, int nq, int C, int32_t* order, cudaStream_t st);
 int launch_add_offset(int64_t* v, int64_t n, int64_t add, cudaStream_t st);  // v[i] += add
 int launch_centroid_update(const float* x, int ld, int dim, const int32_t* order, const int64_t* off, int C,
                            float* centroids, int ldc, const float* fallback_rows, cudaStream_t st);

@@ -11,6 +11,7 @@ namespace annb {
 struct LshView {
     int T, B;                 // tables, bits per signature (B = 0: one bucket per list)
     const float* proj;        // [T * B, dpad] projections (zero past dim)
+    const float* projT;       // [dim, T * B] the same, transposed (the query signatures read it)
     const float* mean;        // [dpad] mean of the rows (zero past dim)
     const int64_t* tab_off;   // [T * C * 2^B + 1]: bucket (t, c, sig) holds tab_ids[off .. off')
     const int32_t* tab_ids;   // [T * n] list-order row ids, ascending within a bucket
@@ -33,9 +34,13 @@ struct LshCandArgs {
     unsigned long long* ndist;  // distance counter (+= n_cands)
 };
 
-// LSHIndex::query's candidate stream (competitors/ivf_lsh/src/lsh_index_optimized.cpp:352-457), one CTA
+// LSHIndex::query's candidate stream (competitors/ivf_lsh/src/lsh_index_optimized.cpp:352-457), one warp
 // per query.
 int launch_lsh_candidates(const LshCandArgs& a, cudaStream_t st);
+// Flips probed per table: min(n_probes, m + m(m-1)/2), m = min(B, n_probes) (:407-426).
+int lsh_flips_kept(int B, int n_probes);
+// projT [dim, rows] from proj [rows, dpad].
+int launch_lsh_transpose(const float* proj, int rows, int dim, int dpad, float* projT, cudaStream_t st);
 
 // Signature of every list-order row in every table (the bucket build of IVFLSHIndex::fit, :260-283):
 // key[t * n + i] = cluster_of(i) * 2^B + sig_t(i).

@@ -80,6 +80,17 @@ class IVFIndex:
         if int(n_tables) != 1 or int(n_bits) != 0:  # LSH bucket tables over the lists
             _lib.check(self._lib.ann_ivf_build_tables(self._h, int(n_tables), int(n_bits), st))
 
+    def build_tables(self, n_tables: int, n_bits: int, stream=None) -> None:
+        """(Re)builds the LSH bucket tables over the fitted lists, as fit does for n_bits > 0 or several
+        tables (lsh_index_optimized.cpp:207-283): projections from mt19937(42), Gram-Schmidt per table,
+        buckets (table, list, signature) of list-order ids. n_tables = 1, n_bits = 0 drops the tables."""
+        if self._n == 0:
+            raise RuntimeError("index not fitted")
+        if int(n_tables) < 1 or not 0 <= int(n_bits) <= 16:
+            raise RuntimeError("n_tables must be >= 1 and n_bits in [0, 16]")
+        st = _lib.stream_ptr(None, stream)
+        _lib.check(self._lib.ann_ivf_build_tables(self._h, int(n_tables), int(n_bits), st))
+
     @staticmethod
     def _like(v, mem, dtype, x):
         if mem == _lib.MEM_DEVICE:

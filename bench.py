@@ -548,6 +548,8 @@ def run_ours(args, rank, world, local):
         line["scaled_fp8_4m_256"] = scaled_fp8_c4(args, local)
     if rank == 0 and world == 1 and args.serve_seconds > 0 and npc is not None:
         line["serving"] = serving_c5(args, local, ivf, npc, w)
+    if rank == 0 and world == 1 and args.lsh and ivf is not None:
+        line["ivf_lsh_tables"] = lsh_tables_c3(args, ivf, w)
     return line
 
 
@@ -688,6 +690,64 @@ def scaled_fp8_c4(args, local):
     return out
 
 
+# competitors/ivf_lsh/scenarios.yaml: (scenario, n_tables, n_bits, n_probes, n_probe_clusters, refine_r)
+LSH_SCENARIOS = (("memory", 25, 10, 12, 24, 100), ("fast", 15, 8, 6, 12, 50), ("high_recall", 30, 12, 20, 32, 150))
+LSH_REF_MAX_BUCKETS = 64 << 20  # the reference holds one std::vector per (table, list, signature)
+
+
+def lsh_tables_c3(args, ivf, w3):
+    """IVF-LSH bucket tables at the three settings of the reference bundle's scenarios (tables, bits,
+    multi-probe flips, probed lists, re-rank depth) over the 1M x 384 lists (2,048 lists; the
+    scenarios' own list counts suit smaller sets). Per setting: the tables built on the GPU; the
+    10k-query batch in the reference's semantics (its candidate cap and per-chunk early-abandon
+    ranking) and in exact selection (the same capped candidate streams, full SQ8 distances), both
+    with recall@100; and, where the reference's nested bucket vectors stay below 64M, its own LSHIndex
+    on the host cores over the same state on a bounded sample, its ids compared with the GPU's."""
+    import torch
+    stream = torch.cuda.current_stream()
+    q = w3.queries
+    nq = q.shape[0]
+    kth = ground_truth(w3.base, q, K_NN)
+    ids = torch.empty(nq, K_NN, dtype=torch.int64, device=q.device)
+    dists = torch.empty(nq, K_NN, dtype=torch.float32, device=q.device)
+    out = {"workload": "the 1M x 384 lists (2,048) with LSH bucket tables; 10k-query batches, k=100, "
+                       "the reference's candidate cap max(2000, 4 * refine_r)"}
+    try:
+        for name, T, B, npr, npc, rr in LSH_SCENARIOS:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ivf.build_tables(T, B)
+            row = {"n_tables": T, "n_bits": B, "n_probes": npr, "n_probe_clusters": npc, "refine_r": rr,
+                   "table_build_s": round(time.perf_counter() - t0, 3)}
+            for mode in ("reference", "exact"):
+                fn = lambda: ivf.search(q, K_NN, npr, npc, rr, max_candidates=-1, mode=mode, out_ids=ids,
+                                        out_dists=dists)
+                fn()
+                torch.cuda.synchronize()
+                ms = _time_steps(fn, 3, stream) / 3
+                row[mode] = {"qps": round(nq / (ms / 1e3), 1), "ms_per_batch": round(ms, 3),
+                             "recall_at_100": round(recall_evaluator(w3.base, q, ids, kth), 4)}
+            if args.no_cpu_baseline or T * ivf.n_lists * (1 << B) > LSH_REF_MAX_BUCKETS:
+                row["reference_cpu"] = None
+            else:
+                ref, _ = _reference_ivf_from(ivf)
+                qs = q[: args.cpu_sample].cpu().numpy()
+                ref.query(qs[0], K_NN, npr, npc, rr)
+                t0 = time.perf_counter()
+                rids = np.stack([ref.query(qq, K_NN, npr, npc, rr) for qq in qs])
+                dt = time.perf_counter() - t0
+                gids, _ = ivf.search(q[: len(qs)], K_NN, npr, npc, rr, max_candidates=-1, mode="reference")
+                row["reference_cpu"] = {"qps": round(len(qs) / dt, 2), "cores": os.cpu_count() or 1,
+                                        "sample": f"{len(qs)} queries one at a time",
+                                        "ids_identical_to_gpu_reference_mode": bool(np.array_equal(
+                                            rids, gids.cpu().numpy()))}
+                del ref
+            out[name] = row
+    finally:
+        ivf.build_tables(1, 0)
+    return out
+
+
 def _reference_ivf_from(ivf):
     """The reference's own LSHIndex (oracle/_ref, built from its sources) loaded with this index's
     state, its ThreadPool sized to every host core as the reference sizes it."""
@@ -799,6 +859,7 @@ def main():
                     help="forms to measure (the default measures all; one form alone is for profiling it)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="per offered rate; 0 skips serving")
     ap.add_argument("--no-fp8", dest="fp8", action="store_false", help="skip the scaled-FP8 configuration")
+    ap.add_argument("--no-lsh", dest="lsh", action="store_false", help="skip the LSH bucket-table settings")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[2000, 10000, 50000])
     ap.add_argument("--ref-nprobe", type=int, default=32)
     ap.add_argument("--cpu-sample", type=int, default=64)

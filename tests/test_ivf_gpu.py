@@ -274,6 +274,45 @@ def test_lsh_reference_mode_matches_oracle(cuda):
         assert ix.total_distances_count() == nd
 
 
+def test_lsh_reference_mode_every_row_fallback(cuda):
+    """Sparse buckets (8 bits over ~500-row lists): streams shorter than k become every row
+    (lsh_index_optimized.cpp:453-457). Those queries are redone with a full-length scratch; a batch with
+    both kinds matches the oracle query by query."""
+    w, st = _lsh_state(seed=5, T=1, B=8)
+    n = w.base.shape[0]
+    for k, n_probes, npc, rr, nt in ((40, 0, 1, 60, 4), (100, 0, 2, -1, 16), (30, 1, 1, 60, 8)):
+        ix = _ivf(threads=nt)
+        ix.import_state(st)
+        ids, dd = ix.search(w.queries, k, n_probes, npc, rr)
+        counts = []
+        for i, q in enumerate(w.queries):
+            oi, od, nc = refmod.ivf_query(st, q, k, n_probes, npc, rr, num_threads=nt, lanes=16)
+            np.testing.assert_array_equal(ids[i], oi, err_msg=f"k={k} probes={n_probes} q={i}")
+            np.testing.assert_array_equal(dd[i], od)
+            counts.append(nc)
+        assert ix.total_distances_count() == sum(counts)
+        assert any(c == n for c in counts) and any(c < n for c in counts), "not a mixed batch"
+
+
+def test_lsh_exact_mode_every_row_batch_equals_alone(cuda):
+    """Exact selection in a large batch redoes its every-row queries apart, split over the whole GPU:
+    each query's ids and distances equal those of the query run alone."""
+    w = synth.zipf_mixture(12000, 64, 120, c=24, lo=20, hi=2000, seed=5)
+    st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 8, mg.projections_from_reference(1, 8, 64))
+    ix = _ivf(mode="exact")
+    ix.import_state(st)
+    k, n_probes, npc, rr = 40, 0, 1, 60
+    ids, d = ix.search(w.queries, k, n_probes, npc, rr, max_candidates=-1)
+    every = 0
+    for i in range(len(w.queries)):
+        ix.reset_distances_count()
+        oi, od = ix.search(w.queries[i:i + 1], k, n_probes, npc, rr, max_candidates=-1)
+        every += ix.total_distances_count() == w.base.shape[0]
+        np.testing.assert_array_equal(ids[i], oi[0], err_msg=f"q={i}")
+        np.testing.assert_array_equal(d[i], od[0])
+    assert 0 < every < len(w.queries), every
+
+
 def test_lsh_exact_mode_and_state_round_trip(cuda):
     """Exact selection over the bucket streams: exact FP32 distances for the ids returned, and the ids of
     an exact selection over the same candidates; export gives back the imported tables."""
