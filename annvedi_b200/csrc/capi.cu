@@ -858,6 +858,15 @@ int ann_flat_device_status(ann_flat* h) {
     return flat_check_err(h);
 }
 
+int ann_merge_topk(const float* dists, const int64_t* ids, int32_t nq, int32_t parts, int32_t k, int32_t metric,
+                   int64_t* out_ids, float* out_dists, void* stream) {
+    clear_error();
+    ANN_CHECK_ARG(nq >= 0 && (nq == 0 || (dists && ids && out_ids)), "ann_merge_topk: null pointer");
+    ANN_CHECK_ARG(metric == ANN_METRIC_L2 || metric == ANN_METRIC_IP, "ann_merge_topk: metric %d", metric);
+    return launch_merge_parts(dists, ids, nq, parts, k, metric == ANN_METRIC_IP ? 1 : 0, out_ids, out_dists,
+                              as_stream(stream));
+}
+
 int64_t ann_flat_total_distances(const ann_flat* h) { return h ? h->ndist.load() : 0; }
 int32_t ann_flat_dim(const ann_flat* h) { return h ? h->dim : 0; }
 int64_t ann_flat_size(const ann_flat* h) { return h ? h->n : 0; }

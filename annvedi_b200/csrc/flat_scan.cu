@@ -573,4 +573,49 @@ int launch_merge_splits(const MergeArgs& a, cudaStream_t st) {
     return ANN_OK;
 }
 
+// ---- merge of per-shard top-k lists --------------------------------------------------------------------
+// One warp per query: the parts' k pairs each (sorted by (key, id), id < 0 = empty) offered as (key, slot)
+// with slot = part * k + position, the best k kept, slots mapped back to the parts' int64 ids. Parts hold
+// increasing id ranges, so (key, slot) order is (key, id) order.
+__global__ void __launch_bounds__(128) merge_parts_kernel(const float* __restrict__ d, const int64_t* __restrict__ ids,
+                                                          int nq, int parts, int k, int ip, int64_t* __restrict__ out_ids,
+                                                          float* __restrict__ out_d) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (q >= nq) return;  // the whole warp; no block barrier follows
+    const int cap = topk_cap(k);
+    float* key = reinterpret_cast<float*>(smem_raw) + (size_t)warp * 2 * cap;
+    int* slot = reinterpret_cast<int*>(key + cap);
+    WarpTopK top;
+    top.init(key, slot, k);
+    const int64_t total = (int64_t)parts * k;
+    const float* dq = d + (int64_t)q * total;
+    const int64_t* iq = ids + (int64_t)q * total;
+    for (int64_t e0 = 0; e0 < total; e0 += 32) {
+        const int64_t e = e0 + lane;
+        const bool ok = e < total && iq[e] >= 0;
+        const float kv = ok ? (ip ? -dq[e] : dq[e]) : kInf;
+        top.offer(kv, ok ? (int)e : kNoId, ok);
+    }
+    top.compact();
+    for (int e = lane; e < k; e += 32) {
+        const bool ok = e < top.count;
+        out_ids[(int64_t)q * k + e] = ok ? iq[slot[e]] : -1;
+        if (out_d) out_d[(int64_t)q * k + e] = ok ? (ip ? -key[e] : key[e]) : (ip ? -kInf : kInf);
+    }
+}
+
+int launch_merge_parts(const float* d, const int64_t* ids, int nq, int parts, int k, int ip, int64_t* out_ids,
+                       float* out_d, cudaStream_t st) {
+    ANN_CHECK_ARG(k >= 1 && k <= 1024 && parts >= 1 && (int64_t)parts * k < INT32_MAX,
+                  "merge: %d parts of k=%d", parts, k);
+    if (nq == 0) return ANN_OK;
+    const size_t smem = (size_t)4 * topk_cap(k) * 8;
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(merge_parts_kernel)));
+    merge_parts_kernel<<<(unsigned)ceil_div(nq, 4), 128, smem, st>>>(d, ids, nq, parts, k, ip, out_ids, out_d);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
 }  // namespace annb

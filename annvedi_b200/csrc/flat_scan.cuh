@@ -51,4 +51,9 @@ int launch_sort_topk(const float* keys, const int* ids, int nq, int k, int negat
                      cudaStream_t st);
 int launch_pad_rows(const float* src, int64_t n, int dim, int64_t ld, float* dst, int dpad, cudaStream_t st);
 
+// Best k of `parts` per-shard top-k lists per query: d / ids [nq, parts, k], each part sorted by (key, id)
+// (key = distance, or -score when ip), ids < 0 empty, parts in increasing id ranges. out [nq, k].
+int launch_merge_parts(const float* d, const int64_t* ids, int nq, int parts, int k, int ip, int64_t* out_ids,
+                       float* out_d, cudaStream_t st);
+
 }  // namespace annb

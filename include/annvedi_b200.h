@@ -126,6 +126,15 @@ int ann_flat_scores_tc(ann_flat* h, const float* queries, int32_t nq, int64_t ld
 /* Reads and clears the index's device error flag (ANN_ERR_TIMEOUT if a bounded device wait gave up). */
 int ann_flat_device_status(ann_flat* h);
 
+/* Merge of per-shard results (row sharding over ranks: each rank searches its rows, adds its first
+ * row to the ids, and the ranks' lists are all-gathered): dists / ids [nq, parts, k] device arrays,
+ * each part as ann_flat_query returns it (sorted, ids < 0 empty; squared L2 distances, or inner-product
+ * scores when metric = ANN_METRIC_IP), parts in increasing id ranges; out_ids / out_dists [nq, k]
+ * (out_dists may be NULL) get the best k by (distance, id). Asynchronous on `stream`. No counterpart in
+ * the reference, whose indexes live in one process (the exchange step of a sharded linear_index). */
+int ann_merge_topk(const float* dists, const int64_t* ids, int32_t nq, int32_t parts, int32_t k, int32_t metric,
+                   int64_t* out_ids, float* out_dists, void* stream);
+
 /* Exact-mode ann_flat_query for callers that cannot let a library allocate device memory (an
  * application that owns every device allocation through its own pool, or a serving thread that must
  * not call cudaMalloc/cudaFree because they can synchronise the device). No counterpart in the
