@@ -148,7 +148,7 @@ int ann_workspace_destroy(ann_workspace* ws) {
     return ANN_OK;
 }
 
-int64_t ann_workspace_bytes(const ann_workspace* ws) { return ws ? (int64_t)ws->dev_cap : 0; }
+int64_t ann_workspace_bytes(const ann_workspace* ws) { return ws ? (int64_t)(ws->dev_cap + ws->big_cap) : 0; }
 
 int ann_flat_create(ann_flat** out, int device) {
     clear_error();

@@ -733,6 +733,67 @@ __global__ void __launch_bounds__(256) ivf_rerank_kernel(IvfQueryArgs a, const f
             const float d = ref_l2_f32(x, sQ, a.ix.dim, NoEmit{});
             if ((lane & 15) == 0 && e < R) sD[e] = ok ? d : kInf;
         }
+    } else if (dpad <= 512) {
+        // two rows per warp step; each lane's (up to four) 16-byte pieces of both rows are loaded before they
+        // are used, so eight loads per lane are in flight. Per lane the sum runs over d in the same order as
+        // below, so the distances are the same.
+        for (int e0 = warp; e0 < R; e0 += 16) {
+            const int e1 = e0 + 8;
+            const int rowA = sRow[e0];
+            const int rowB = e1 < R ? sRow[e1] : kNoId;
+            const bool okA = rowA != kNoId, okB = rowB != kNoId;
+            const float* pa = a.ix.original + (int64_t)(okA ? rowA : 0) * dpad;
+            const float* pb = a.ix.original + (int64_t)(okB ? rowB : 0) * dpad;
+            float4 xa[4], xb[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int d = lane * 4 + 128 * i;
+                xa[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+                xb[i] = xa[i];
+                if (d < dpad) {
+                    if (okA) xa[i] = *reinterpret_cast<const float4*>(pa + d);
+                    if (okB) xb[i] = *reinterpret_cast<const float4*>(pb + d);
+                }
+            }
+            float accA = 0.f, accB = 0.f;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int d = lane * 4 + 128 * i;
+                if (d < dpad) {
+                    const float4 q4 = *reinterpret_cast<const float4*>(sQ + d);
+                    if (a.metric == ANN_METRIC_IP) {
+                        accA = fmaf(xa[i].x, q4.x, accA);
+                        accA = fmaf(xa[i].y, q4.y, accA);
+                        accA = fmaf(xa[i].z, q4.z, accA);
+                        accA = fmaf(xa[i].w, q4.w, accA);
+                        accB = fmaf(xb[i].x, q4.x, accB);
+                        accB = fmaf(xb[i].y, q4.y, accB);
+                        accB = fmaf(xb[i].z, q4.z, accB);
+                        accB = fmaf(xb[i].w, q4.w, accB);
+                    } else {
+                        float t0 = xa[i].x - q4.x, t1 = xa[i].y - q4.y, t2 = xa[i].z - q4.z, t3 = xa[i].w - q4.w;
+                        accA = fmaf(t0, t0, accA);
+                        accA = fmaf(t1, t1, accA);
+                        accA = fmaf(t2, t2, accA);
+                        accA = fmaf(t3, t3, accA);
+                        t0 = xb[i].x - q4.x, t1 = xb[i].y - q4.y, t2 = xb[i].z - q4.z, t3 = xb[i].w - q4.w;
+                        accB = fmaf(t0, t0, accB);
+                        accB = fmaf(t1, t1, accB);
+                        accB = fmaf(t2, t2, accB);
+                        accB = fmaf(t3, t3, accB);
+                    }
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                accA += __shfl_xor_sync(0xffffffffu, accA, o);
+                accB += __shfl_xor_sync(0xffffffffu, accB, o);
+            }
+            if (lane == 0) {
+                sD[e0] = okA ? (a.metric == ANN_METRIC_IP ? -accA : accA) : kInf;
+                if (e1 < R) sD[e1] = okB ? (a.metric == ANN_METRIC_IP ? -accB : accB) : kInf;
+            }
+        }
     } else {
         for (int e = warp; e < R; e += 8) {
             const int row = sRow[e];

@@ -92,6 +92,13 @@ class Server:
         self.completed: list[Request] = []
         self.batches: list[tuple[str, int, int, float, float]] = []  # (route, queries, requests, start, end)
         self.admission_waits = 0
+        # Free device memory as admission sees it: read from the driver at start and after a batch that
+        # grew its workspace (outside the scheduling lock), lowered by the growth granted meanwhile. A
+        # driver query under the lock on every batch stalled every worker whenever it was slow (tens of
+        # ms while other threads launch and synchronise).
+        self._free_seen = 0
+        self._free_read_at = 0.0
+        self.free_reads = 0
         self.in_flight = 0
         self.max_in_flight = 0  # most batches on the GPU at once
         self.errors: list[BaseException] = []
@@ -141,6 +148,7 @@ class Server:
         # generations, so a full collection does not pause the workers for milliseconds.
         gc.collect()
         gc.freeze()
+        self._refresh_free()
         self._running = True
         for i in range(len(self._workers)):
             t = threading.Thread(target=self._work, args=(i,), daemon=True, name=f"ann-serve-{i}")
@@ -159,10 +167,17 @@ class Server:
             raise self.errors[0]
 
     # ---- scheduling ------------------------------------------------------------------------
-    def _free_hbm(self) -> int:
+    def _refresh_free(self) -> None:
+        """Reads free device memory from the driver; never called with the scheduling lock held."""
         import torch
         free, _ = torch.cuda.mem_get_info(self.device)
-        return int(free)
+        with self._cv:
+            self._free_seen = int(free)
+            self._free_read_at = time.perf_counter()
+            self.free_reads += 1
+
+    def _free_hbm(self) -> int:
+        return self._free_seen
 
     def _take(self, w) -> tuple[str, list[Request], int] | None:
         """Under the lock: the next batch for worker w, admitted against free device memory."""
@@ -178,7 +193,7 @@ class Server:
                 reqs.append(req)
                 nq += req.queries.shape[0]
             have = w["ws"].nbytes()
-            avail = None  # free device memory is read only when a batch must grow the workspace
+            avail = None  # the admission figure is consulted only when a batch must grow the workspace
             while reqs:
                 growth = max(0, int(r.scratch_bytes(nq)) - have)
                 if growth > 0 and avail is None:
@@ -220,6 +235,7 @@ class Server:
                 self._growth_in_flight += growth
                 self.in_flight += 1
                 self.max_in_flight = max(self.max_in_flight, self.in_flight)
+            before = w["ws"].nbytes()
             try:
                 self._run(w, dev, name, reqs)
             except BaseException as e:  # surfaced by stop()
@@ -228,6 +244,9 @@ class Server:
                     req.done_at = time.perf_counter()
                     req._event.set()
             finally:
+                grew = w["ws"].nbytes() > before
+                if grew:
+                    self._refresh_free()  # the granted growth is now in the driver's figure
                 with self._cv:
                     self._growth_in_flight -= growth
                     self.in_flight -= 1

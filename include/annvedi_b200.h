@@ -63,7 +63,7 @@ int64_t ann_kernel_launches(void);
 /* ---- workspaces -------------------------------------------------------------------------- */
 int ann_workspace_create(ann_workspace** out, int device);
 int ann_workspace_destroy(ann_workspace* ws);
-/* Bytes of device scratch currently reserved. */
+/* Bytes of device scratch currently reserved (both of the workspace's device arenas). */
 int64_t ann_workspace_bytes(const ann_workspace* ws);
 
 /* ---- flat (linear) index -------------------------------------------------------------------
