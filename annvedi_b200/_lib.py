@@ -78,6 +78,7 @@ SIGNATURES = [
     ("ann_flat_set_tc_precision", ctypes.c_int, [_vp, _i32]),
     ("ann_flat_device_status", ctypes.c_int, [_vp]),
     ("ann_merge_topk", ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp, _vp]),
+    ("ann_select_smallest", ctypes.c_int, [_vp, _i64, _vp, _i32, _i32, _vp, _vp, _vp]),
     ("ann_flat_set_profiling", ctypes.c_int, [_vp, _i32]),
     ("ann_flat_profile", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     ("ann_flat_reset_profile", ctypes.c_int, [_vp]),

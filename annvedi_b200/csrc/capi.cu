@@ -867,6 +867,22 @@ int ann_merge_topk(const float* dists, const int64_t* ids, int32_t nq, int32_t p
                               as_stream(stream));
 }
 
+int ann_select_smallest(const float* keys, int64_t ld, const int64_t* lens, int32_t nq, int32_t r, float* out_keys,
+                        int32_t* out_pos, void* stream) {
+    clear_error();
+    ANN_CHECK_ARG(nq >= 0 && r >= 1 && ld >= 0 && ld < INT32_MAX, "ann_select_smallest: nq=%d r=%d ld=%lld", nq, r,
+                  (long long)ld);
+    ANN_CHECK_ARG(nq == 0 || (keys && out_keys && out_pos), "ann_select_smallest: null pointer");
+    RadixSelectArgs a{};
+    a.keys = keys;
+    a.ld = ld;
+    a.lens = lens;
+    a.R = r;
+    a.out_key = out_keys;
+    a.out_id = out_pos;
+    return launch_radix_select(a, nq, as_stream(stream));
+}
+
 int64_t ann_flat_total_distances(const ann_flat* h) { return h ? h->ndist.load() : 0; }
 int32_t ann_flat_dim(const ann_flat* h) { return h ? h->dim : 0; }
 int64_t ann_flat_size(const ann_flat* h) { return h ? h->n : 0; }

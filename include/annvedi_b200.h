@@ -135,6 +135,14 @@ int ann_flat_device_status(ann_flat* h);
 int ann_merge_topk(const float* dists, const int64_t* ids, int32_t nq, int32_t parts, int32_t k, int32_t metric,
                    int64_t* out_ids, float* out_dists, void* stream);
 
+/* The r smallest keys of each of nq device rows keys[q * ld + p], p < lens[q] (ld when lens is NULL),
+ * by (key, position): out_keys / out_pos [nq, r] device arrays, padded with +inf / INT32_MAX where a
+ * row holds fewer than r keys. The set is exact; its order is unspecified. This is the selection of the
+ * tensor-core forms (the best R candidates before the exact re-rank); the reference partially sorts
+ * its candidate pairs for the same purpose (lsh_index_optimized.cpp:471-480). Asynchronous on `stream`. */
+int ann_select_smallest(const float* keys, int64_t ld, const int64_t* lens, int32_t nq, int32_t r, float* out_keys,
+                        int32_t* out_pos, void* stream);
+
 /* Exact-mode ann_flat_query for callers that cannot let a library allocate device memory (an
  * application that owns every device allocation through its own pool, or a serving thread that must
  * not call cudaMalloc/cudaFree because they can synchronise the device). No counterpart in the
