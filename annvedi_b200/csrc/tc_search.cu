@@ -159,6 +159,8 @@ __global__ void tc_ivf_pairs_kernel(const __nv_bfloat16* qb, int kpad, const int
     }
 }
 
+constexpr int kCoarseChunks = 16;  // dims up to 512 take the register path of the exact distances
+
 // one warp per query
 __global__ void __launch_bounds__(128) tc_coarse_kernel(const float* __restrict__ keys, int64_t ldk, int nq, int C,
                                                        int npc, int m, const float* __restrict__ q,
@@ -173,15 +175,62 @@ __global__ void __launch_bounds__(128) tc_coarse_kernel(const float* __restrict_
     WarpTopK top;
     top.init(sK, sI, m);
     const float* kr = keys + (int64_t)qi * ldk;
-    for (int c0 = 0; c0 < C; c0 += 32) {
-        const int c = c0 + lane;
-        top.offer(c < C ? kr[c] : kInf, c < C ? c : kNoId, c < C);
+    for (int c0 = 0; c0 < C; c0 += 128) {  // four loads in flight, offered in key order
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int c = c0 + 32 * u + lane;
+            v[u] = c < C ? kr[c] : kInf;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int c = c0 + 32 * u + lane;
+            top.offer(v[u], c < C ? c : kNoId, c < C);
+        }
     }
     top.compact();
     const int cnt = top.count;
     // exact FP32 squared distances of the m candidates
     const float* qv = q + (int64_t)qi * dpad;
-    for (int e = 0; e < cnt; ++e) {
+    if (dpad <= 32 * kCoarseChunks) {
+        // the query's pieces in registers; two centroids at a time with all their pieces loaded before
+        // use; per lane the sum runs over d = lane, lane + 32, ... as in the loop below
+        float qr[kCoarseChunks];
+#pragma unroll
+        for (int i = 0; i < kCoarseChunks; ++i) qr[i] = lane + 32 * i < dpad ? qv[lane + 32 * i] : 0.f;
+        for (int e = 0; e < cnt; e += 2) {
+            const bool two = e + 1 < cnt;
+            const float* xa = cent + (int64_t)sI[e] * dpad;
+            const float* xb = cent + (int64_t)(two ? sI[e + 1] : sI[e]) * dpad;
+            float va[kCoarseChunks], vb[kCoarseChunks];
+#pragma unroll
+            for (int i = 0; i < kCoarseChunks; ++i) {
+                const int d = lane + 32 * i;
+                va[i] = d < dpad ? xa[d] : 0.f;
+                vb[i] = d < dpad ? xb[d] : 0.f;
+            }
+            float accA = 0.f, accB = 0.f;
+#pragma unroll
+            for (int i = 0; i < kCoarseChunks; ++i) {
+                if (lane + 32 * i < dpad) {
+                    const float ta = va[i] - qr[i], tb = vb[i] - qr[i];
+                    accA = fmaf(ta, ta, accA);
+                    accB = fmaf(tb, tb, accB);
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                accA += __shfl_xor_sync(0xffffffffu, accA, o);
+                accB += __shfl_xor_sync(0xffffffffu, accB, o);
+            }
+            if (lane == 0) {
+                sK[e] = accA;
+                if (two) sK[e + 1] = accB;
+            }
+            __syncwarp();
+        }
+    }
+    for (int e = 0; e < cnt && dpad > 32 * kCoarseChunks; ++e) {
         const int c = sI[e];
         const float* x = cent + (int64_t)c * dpad;
         float acc = 0.f;
