@@ -203,7 +203,7 @@ def _time_steps(fn, steps, stream):
 # dram__bytes_write.sum, one launch) on this workload at its default sizes: the exact re-rank of the IVF
 # tensor-core form (4.00 GB per 10,000-query launch, R = 300) and the filter pass of the tensor-core exact
 # search (0.878 GB per 5,000-query launch). Other sizes report traffic as null.
-MEASURED_TRAFFIC_PER_QUERY = {"ivf_rerank": 4.00e9 / 10_000, "tc_filter": 0.878e9 / 5_000}
+MEASURED_TRAFFIC_PER_QUERY = {"ivf_rerank": 1.40e9 / 10_000, "tc_filter": 0.878e9 / 5_000}
 
 WORKLOAD = "1M x 384 zipf mixture (2,048 centres, sigma 0.3, L2-normalised), 10k-query batches, k=100, squared L2"
 DATA = "synthetic (seeded zipf mixture, 2,048 centres, sigma 0.3, L2-normalised)"
