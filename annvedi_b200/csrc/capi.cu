@@ -8,6 +8,7 @@
 #include <cstring>
 #include <algorithm>
 #include <atomic>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -31,6 +32,42 @@ void set_error(const char* fmt, ...) {
     va_end(ap);
 }
 void clear_error() { g_err[0] = 0; }
+
+namespace {
+// threads for a host copy of `bytes`: one per 2 MB, at most 8 and the host's core count
+int copy_threads(size_t bytes) {
+    static const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    return (int)std::max<size_t>(1, std::min<size_t>({(size_t)8, (size_t)hw, bytes >> 21}));
+}
+
+template <typename F>
+void split_rows(int64_t rows, int threads, F&& f) {
+    if (threads <= 1) {
+        f((int64_t)0, rows);
+        return;
+    }
+    std::vector<std::thread> ts;
+    ts.reserve(threads - 1);
+    for (int t = 1; t < threads; ++t) ts.emplace_back(f, rows * t / threads, rows * (t + 1) / threads);
+    f((int64_t)0, rows / threads);
+    for (auto& t : ts) t.join();
+}
+}  // namespace
+
+void host_copy(void* dst, const void* src, size_t bytes) {
+    char* d = static_cast<char*>(dst);
+    const char* s = static_cast<const char*>(src);
+    split_rows((int64_t)bytes, copy_threads(bytes), [&](int64_t b0, int64_t b1) { std::memcpy(d + b0, s + b0, b1 - b0); });
+}
+
+void host_pad_rows(float* dst, int64_t dst_ld, const float* src, int64_t src_ld, int64_t rows, int cols) {
+    split_rows(rows, copy_threads(sizeof(float) * (size_t)rows * dst_ld), [&](int64_t r0, int64_t r1) {
+        for (int64_t i = r0; i < r1; ++i) {
+            std::memcpy(dst + i * dst_ld, src + i * src_ld, sizeof(float) * cols);
+            if (dst_ld > cols) std::memset(dst + i * dst_ld + cols, 0, sizeof(float) * (dst_ld - cols));
+        }
+    });
+}
 
 static std::atomic<int64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
@@ -342,10 +379,7 @@ int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t
         rc = ws_reserve_host(ws, std::max(qbytes, (sizeof(int64_t) + sizeof(float)) * (size_t)nq * kk));
         if (rc) return rc;
         float* hq = reinterpret_cast<float*>(ws->host);
-        for (int i = 0; i < nq; ++i) {
-            std::memcpy(hq + (size_t)i * dpad, queries + (size_t)i * ldq, sizeof(float) * h->dim);
-            if (dpad > h->dim) std::memset(hq + (size_t)i * dpad + h->dim, 0, sizeof(float) * (dpad - h->dim));
-        }
+        host_pad_rows(hq, dpad, queries, ldq, nq, h->dim);
         ANN_CUDA_TRY(cudaMemcpyAsync(qdev, hq, qbytes, cudaMemcpyHostToDevice, st));
     } else if (need_pad) {
         rc = launch_pad_rows(queries, nq, h->dim, ldq, qdev, dpad, st);
@@ -409,8 +443,8 @@ int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t
         if (out_dists)
             ANN_CUDA_TRY(cudaMemcpyAsync(hd, dists_dev, sizeof(float) * (size_t)nq * kk, cudaMemcpyDeviceToHost, st));
         ANN_CUDA_TRY(cudaStreamSynchronize(st));
-        std::memcpy(out_ids, hid, sizeof(int64_t) * (size_t)nq * kk);
-        if (out_dists) std::memcpy(out_dists, hd, sizeof(float) * (size_t)nq * kk);
+        host_copy(out_ids, hid, sizeof(int64_t) * (size_t)nq * kk);
+        if (out_dists) host_copy(out_dists, hd, sizeof(float) * (size_t)nq * kk);
     }
     return ANN_OK;
 }
@@ -637,10 +671,7 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
         if ((rc = ws_reserve_host(ws, std::max(sizeof(float) * (size_t)nq * dpad, (sizeof(int64_t) + 4) * (size_t)nq * kk))))
             return rc;
         float* hq = reinterpret_cast<float*>(ws->host);
-        for (int i = 0; i < nq; ++i) {
-            std::memcpy(hq + (size_t)i * dpad, queries + (size_t)i * ldq, sizeof(float) * h->dim);
-            if (dpad > h->dim) std::memset(hq + (size_t)i * dpad + h->dim, 0, sizeof(float) * (dpad - h->dim));
-        }
+        host_pad_rows(hq, dpad, queries, ldq, nq, h->dim);
         ANN_CUDA_TRY(cudaMemcpyAsync(qdev, hq, sizeof(float) * (size_t)nq * dpad, cudaMemcpyHostToDevice, st));
     } else {
         if ((rc = launch_pad_rows(queries, nq, h->dim, ldq, qdev, dpad, st))) return rc;
@@ -845,8 +876,8 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
         if (out_dists)
             ANN_CUDA_TRY(cudaMemcpyAsync(hd, dists_dev, sizeof(float) * (size_t)nq * kk, cudaMemcpyDeviceToHost, st));
         ANN_CUDA_TRY(cudaStreamSynchronize(st));
-        std::memcpy(out_ids, hid, sizeof(int64_t) * (size_t)nq * kk);
-        if (out_dists) std::memcpy(out_dists, hd, sizeof(float) * (size_t)nq * kk);
+        host_copy(out_ids, hid, sizeof(int64_t) * (size_t)nq * kk);
+        if (out_dists) host_copy(out_dists, hd, sizeof(float) * (size_t)nq * kk);
         return flat_check_err(h);
     }
     return ANN_OK;

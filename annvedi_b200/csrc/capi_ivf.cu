@@ -1048,10 +1048,7 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
         rc = ws_reserve_host(ws, std::max(sizeof(float) * (size_t)nq * dpad, (sizeof(int64_t) + 4) * (size_t)nq * k));
         if (rc) return rc;
         float* hq = reinterpret_cast<float*>(ws->host);
-        for (int i = 0; i < nq; ++i) {
-            std::memcpy(hq + (size_t)i * dpad, queries + (size_t)i * ldq, sizeof(float) * h->dim);
-            if (dpad > h->dim) std::memset(hq + (size_t)i * dpad + h->dim, 0, sizeof(float) * (dpad - h->dim));
-        }
+        host_pad_rows(hq, dpad, queries, ldq, nq, h->dim);
         ANN_CUDA_TRY(cudaMemcpyAsync(qdev, hq, sizeof(float) * (size_t)nq * dpad, cudaMemcpyHostToDevice, st));
     } else {
         rc = launch_pad_rows(queries, nq, h->dim, ldq, qdev, dpad, st);
@@ -1071,8 +1068,8 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
         if (out_dists)
             ANN_CUDA_TRY(cudaMemcpyAsync(hd, dists_dev, sizeof(float) * (size_t)nq * k, cudaMemcpyDeviceToHost, st));
         ANN_CUDA_TRY(cudaStreamSynchronize(st));
-        std::memcpy(out_ids, hid, sizeof(int64_t) * (size_t)nq * k);
-        if (out_dists) std::memcpy(out_dists, hd, sizeof(float) * (size_t)nq * k);
+        host_copy(out_ids, hid, sizeof(int64_t) * (size_t)nq * k);
+        if (out_dists) host_copy(out_dists, hd, sizeof(float) * (size_t)nq * k);
         return ann_ivf_device_status(h);
     }
     return ANN_OK;

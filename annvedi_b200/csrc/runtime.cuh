@@ -150,4 +150,10 @@ struct Sizer {
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Host-side staging copies of queries with host buffers, split over up to 8 threads when large (one thread
+// copies a 10,000 x 384 batch more slowly than the GPU searches it). host_pad_rows writes `rows` rows of
+// `cols` floats from src (stride src_ld) to dst (stride dst_ld), zero-filling each row past cols.
+void host_copy(void* dst, const void* src, size_t bytes);
+void host_pad_rows(float* dst, int64_t dst_ld, const float* src, int64_t src_ld, int64_t rows, int cols);
+
 }  // namespace annb

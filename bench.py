@@ -439,7 +439,10 @@ def run_ours(args, rank, world, local):
     qps = whole_job_qps(q, args.steps, ms, world)
     hf["recall"] = recall_evaluator(base, queries, t_ids if head == "tensor_core_exact" else o_ids, kth)
 
-    # ---- end to end through the public API with host buffers ----
+    # ---- end to end through the public API with host buffers (warmed up like the device steps: the first
+    # call sizes the index's own workspace and pinned staging buffers) ----
+    for _ in range(args.warmup):
+        hf["host"]()
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
