@@ -702,6 +702,21 @@ int launch_select_topk(const float* keys, int64_t ld, const int64_t* lens, int n
 }
 
 // ---- 4. FP32 re-rank and final top-k -------------------------------------------------------------
+constexpr int kRerankRankMax = 1024;  // R up to this: the final top-k by block-wide ranks
+
+// Sum of v over the block (every thread gets it); scratch: >= blockDim.x / 32 floats of shared memory, free
+// for the caller's use again after the call.
+__device__ __forceinline__ int block_sum_int(int v, float* scratch) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    int* s = reinterpret_cast<int*>(scratch);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+    __syncthreads();
+    int t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s[w];
+    return t;
+}
 // One CTA per query: exact distances of its R candidates to the original rows (the reference's
 // arithmetic in reference mode, lsh_index_optimized.cpp:481-486), then the best k by (distance, row)
 // and the mapping back to original ids (:503-512).
@@ -823,6 +838,31 @@ __global__ void __launch_bounds__(256) ivf_rerank_kernel(IvfQueryArgs a, const f
         }
     }
     __syncthreads();
+    const float kEmpty = a.metric == ANN_METRIC_IP ? -kInf : kInf;
+    if (R <= kRerankRankMax) {
+        // every thread ranks its entries by (distance, row) among the R (the rows are distinct, so the ranks
+        // are); an entry of rank < k goes to out[rank]: the best k in order, without leaving seven warps idle
+        // behind one that sorts
+        int nvalid = 0;
+        for (int e = threadIdx.x; e < R; e += blockDim.x) {
+            const int row = sRow[e];
+            if (row == kNoId) continue;
+            ++nvalid;
+            const float key = sD[e];
+            int rank = 0;
+            for (int j = 0; j < R; ++j) rank += pair_less(sD[j], sRow[j], key, row);
+            if (rank < k) {
+                a.out_ids[(int64_t)q * k + rank] = (int64_t)(a.ix.r2o ? a.ix.r2o[row] : row);
+                if (a.out_dists) a.out_dists[(int64_t)q * k + rank] = a.metric == ANN_METRIC_IP ? -key : key;
+            }
+        }
+        nvalid = block_sum_int(nvalid, sKey);
+        for (int e = nvalid + threadIdx.x; e < k; e += blockDim.x) {
+            a.out_ids[(int64_t)q * k + e] = -1;
+            if (a.out_dists) a.out_dists[(int64_t)q * k + e] = kEmpty;
+        }
+        return;
+    }
     if (warp == 0) {
         WarpTopK top;
         top.init(sKey, sId, k);
@@ -837,7 +877,7 @@ __global__ void __launch_bounds__(256) ivf_rerank_kernel(IvfQueryArgs a, const f
             a.out_ids[(int64_t)q * k + e] = ok ? (int64_t)(a.ix.r2o ? a.ix.r2o[sId[e]] : sId[e]) : -1;
             if (a.out_dists)
                 a.out_dists[(int64_t)q * k + e] =
-                    ok ? (a.metric == ANN_METRIC_IP ? -sKey[e] : sKey[e]) : (a.metric == ANN_METRIC_IP ? -kInf : kInf);
+                    ok ? (a.metric == ANN_METRIC_IP ? -sKey[e] : sKey[e]) : kEmpty;
         }
     }
 }
