@@ -67,6 +67,41 @@ __device__ int find_bin(const int* hist, int rank, int* below, int* sScan) {
     return bin;
 }
 
+// The bin holding the rank-th smallest (0-based) element of a kBins histogram, by a warp-shuffle block
+// scan (two barriers). Whole block; every thread gets the bin. sScan: >= kThreads / 32 + 1 ints.
+__device__ int find_bin_scan(const int* hist, int rank, int* sScan) {
+    constexpr int per = kBins / kThreads;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int local = 0;
+#pragma unroll
+    for (int i = 0; i < per; ++i) local += hist[threadIdx.x * per + i];
+    int incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) sScan[warp] = incl;
+    __syncthreads();
+    int before = 0;
+    for (int w = 0; w < warp; ++w) before += sScan[w];
+    incl += before;
+    const int excl = incl - local;
+    if (rank >= excl && rank < incl) {
+        int c = excl;
+        for (int i = 0; i < per; ++i) {
+            const int h = hist[threadIdx.x * per + i];
+            if (rank < c + h) {
+                sScan[kThreads / 32] = threadIdx.x * per + i;
+                break;
+            }
+            c += h;
+        }
+    }
+    __syncthreads();
+    return sScan[kThreads / 32];
+}
+
 __device__ __forceinline__ int lin_bin(float k, float lo, float scale) {
     const float f = (k - lo) * scale;  // NaN (0 * inf) counts as bin 0
     return !(f > 0.f) ? 0 : (f >= (float)(kBins - 1) ? kBins - 1 : (int)f);
@@ -183,17 +218,35 @@ __global__ void __launch_bounds__(kThreads) radix_select_kernel(RadixSelectArgs 
         const int64_t sstep = max((int64_t)1, len / kSamples);
         const int ns = (int)min((int64_t)kSamples, (len + sstep - 1) / sstep);
         const int r = min(ns, (int)(((int64_t)R * 13 + 10 * sstep - 1) / (10 * sstep)) + 4);
-        for (int i = threadIdx.x; i < kSamples; i += kThreads) {
-            sCandK[i] = i < ns ? kq[(int64_t)i * sstep] : kInf;
-            sCandP[i] = i;
+        // the bar: the linear bin (2,048 over the samples' [min, max]) holding the r-th smallest sample;
+        // the gather below keeps every key of that bin or a lower one (the same bin function), so at
+        // least r samples' worth of keys pass, and few more (about half a sample per bin)
+        constexpr int kPer = kSamples / kThreads;
+        float sv[kPer];
+        float slo = kInf, shi = -kInf;
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int i = threadIdx.x + u * kThreads;
+            sv[u] = i < ns ? kq[(int64_t)i * sstep] : kInf;
+            if (i < ns) {
+                slo = fminf(slo, sv[u]);
+                shi = fmaxf(shi, sv[u]);
+            }
         }
+        for (int i = threadIdx.x; i < kBins; i += kThreads) hist[0][i] = 0;
         if (threadIdx.x == 0) sCount = 0;
+        block_minmax(slo, shi, sRed);  // (its barriers also publish the zeroed bins)
+        const float sscale = (float)kBins / (shi - slo);
+        const bool spread = shi > slo && isfinite(sscale);
+        if (spread) {
+#pragma unroll
+            for (int u = 0; u < kPer; ++u)
+                if (threadIdx.x + u * kThreads < ns) atomicAdd(&hist[0][lin_bin(sv[u], slo, sscale)], 1);
+        }
         __syncthreads();
-        block_sort_pairs(sCandK, sCandP, kSamples);
-        const float bar = sCandK[r - 1];
-        __syncthreads();
+        const int bb = spread ? find_bin_scan(hist[0], r - 1, sScan) : kBins - 1;
         for_each_key(kq, len, [&](int64_t p, float kv) {
-            if (kv <= bar) {
+            if (lin_bin(kv, slo, sscale) <= bb || !spread) {
                 const int at = atomicAdd(&sCount, 1);
                 if (at < kLinCap) {
                     sCandK[at] = kv;
