@@ -8,7 +8,6 @@
 #include <cstring>
 #include <algorithm>
 #include <atomic>
-#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -33,40 +32,13 @@ void set_error(const char* fmt, ...) {
 }
 void clear_error() { g_err[0] = 0; }
 
-namespace {
-// threads for a host copy of `bytes`: one per 2 MB, at most 8 and the host's core count
-int copy_threads(size_t bytes) {
-    static const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-    return (int)std::max<size_t>(1, std::min<size_t>({(size_t)8, (size_t)hw, bytes >> 21}));
-}
-
-template <typename F>
-void split_rows(int64_t rows, int threads, F&& f) {
-    if (threads <= 1) {
-        f((int64_t)0, rows);
-        return;
-    }
-    std::vector<std::thread> ts;
-    ts.reserve(threads - 1);
-    for (int t = 1; t < threads; ++t) ts.emplace_back(f, rows * t / threads, rows * (t + 1) / threads);
-    f((int64_t)0, rows / threads);
-    for (auto& t : ts) t.join();
-}
-}  // namespace
-
-void host_copy(void* dst, const void* src, size_t bytes) {
-    char* d = static_cast<char*>(dst);
-    const char* s = static_cast<const char*>(src);
-    split_rows((int64_t)bytes, copy_threads(bytes), [&](int64_t b0, int64_t b1) { std::memcpy(d + b0, s + b0, b1 - b0); });
-}
-
-void host_pad_rows(float* dst, int64_t dst_ld, const float* src, int64_t src_ld, int64_t rows, int cols) {
-    split_rows(rows, copy_threads(sizeof(float) * (size_t)rows * dst_ld), [&](int64_t r0, int64_t r1) {
-        for (int64_t i = r0; i < r1; ++i) {
-            std::memcpy(dst + i * dst_ld, src + i * src_ld, sizeof(float) * cols);
-            if (dst_ld > cols) std::memset(dst + i * dst_ld + cols, 0, sizeof(float) * (dst_ld - cols));
-        }
-    });
+int queries_in(float* dev, int64_t dpad, const float* host, int64_t ld, int64_t rows, int cols, cudaStream_t st) {
+    if (rows == 0) return ANN_OK;
+    ANN_CUDA_TRY(cudaMemcpy2DAsync(dev, sizeof(float) * dpad, host, sizeof(float) * ld, sizeof(float) * cols, rows,
+                                   cudaMemcpyHostToDevice, st));
+    if (dpad > cols)
+        ANN_CUDA_TRY(cudaMemset2DAsync(dev + cols, sizeof(float) * dpad, 0, sizeof(float) * (dpad - cols), rows, st));
+    return ANN_OK;
 }
 
 static std::atomic<int64_t> g_launches{0};
@@ -124,26 +96,6 @@ int ws_reserve_big(ann_workspace* ws, size_t bytes) {
     return ANN_OK;
 }
 
-int ws_reserve_host(ann_workspace* ws, size_t bytes) {
-    std::lock_guard<std::mutex> lk(ws->mu);
-    if (ws->host_cap >= bytes) return ANN_OK;
-    size_t cap = std::max(bytes, ws->host_cap + ws->host_cap / 2);
-    if (ws->host) {
-        ANN_CUDA_TRY(cudaDeviceSynchronize());
-        ANN_CUDA_TRY(cudaFreeHost(ws->host));
-        ws->host = nullptr;
-        ws->host_cap = 0;
-    }
-    cudaError_t e = cudaMallocHost(&ws->host, cap);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        set_error("workspace: cannot allocate %zu bytes of pinned host memory (%s)", cap, cudaGetErrorString(e));
-        return ANN_ERR_NOMEM;
-    }
-    ws->host_cap = cap;
-    return ANN_OK;
-}
-
 }  // namespace annb
 
 using namespace annb;
@@ -170,12 +122,10 @@ int ann_workspace_create(ann_workspace** out, int device) {
 static void ws_release(ann_workspace* ws) {
     DeviceGuard g(ws->device);
     if (ws->dev) cudaFree(ws->dev);
-    if (ws->host) cudaFreeHost(ws->host);
     if (ws->big) cudaFree(ws->big);
     ws->dev = nullptr;
-    ws->host = nullptr;
     ws->big = nullptr;
-    ws->dev_cap = ws->host_cap = ws->big_cap = 0;
+    ws->dev_cap = ws->big_cap = 0;
 }
 
 int ann_workspace_destroy(ann_workspace* ws) {
@@ -375,12 +325,7 @@ int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t
 
     // ---- queries in ----
     if (host) {
-        const size_t qbytes = sizeof(float) * (size_t)nq * dpad;
-        rc = ws_reserve_host(ws, std::max(qbytes, (sizeof(int64_t) + sizeof(float)) * (size_t)nq * kk));
-        if (rc) return rc;
-        float* hq = reinterpret_cast<float*>(ws->host);
-        host_pad_rows(hq, dpad, queries, ldq, nq, h->dim);
-        ANN_CUDA_TRY(cudaMemcpyAsync(qdev, hq, qbytes, cudaMemcpyHostToDevice, st));
+        if ((rc = queries_in(qdev, dpad, queries, ldq, nq, h->dim, st))) return rc;
     } else if (need_pad) {
         rc = launch_pad_rows(queries, nq, h->dim, ldq, qdev, dpad, st);
         if (rc) return rc;
@@ -437,14 +382,10 @@ int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t
 
     // ---- results out ----
     if (host) {
-        int64_t* hid = reinterpret_cast<int64_t*>(ws->host);
-        float* hd = reinterpret_cast<float*>(ws->host + sizeof(int64_t) * (size_t)nq * kk);
-        ANN_CUDA_TRY(cudaMemcpyAsync(hid, ids_dev, sizeof(int64_t) * (size_t)nq * kk, cudaMemcpyDeviceToHost, st));
+        ANN_CUDA_TRY(cudaMemcpyAsync(out_ids, ids_dev, sizeof(int64_t) * (size_t)nq * kk, cudaMemcpyDeviceToHost, st));
         if (out_dists)
-            ANN_CUDA_TRY(cudaMemcpyAsync(hd, dists_dev, sizeof(float) * (size_t)nq * kk, cudaMemcpyDeviceToHost, st));
+            ANN_CUDA_TRY(cudaMemcpyAsync(out_dists, dists_dev, sizeof(float) * (size_t)nq * kk, cudaMemcpyDeviceToHost, st));
         ANN_CUDA_TRY(cudaStreamSynchronize(st));
-        host_copy(out_ids, hid, sizeof(int64_t) * (size_t)nq * kk);
-        if (out_dists) host_copy(out_dists, hd, sizeof(float) * (size_t)nq * kk);
     }
     return ANN_OK;
 }
@@ -668,11 +609,7 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
     if (host) {
         ids_dev = cv.take<int64_t>((size_t)nq * kk);
         dists_dev = cv.take<float>((size_t)nq * kk);
-        if ((rc = ws_reserve_host(ws, std::max(sizeof(float) * (size_t)nq * dpad, (sizeof(int64_t) + 4) * (size_t)nq * kk))))
-            return rc;
-        float* hq = reinterpret_cast<float*>(ws->host);
-        host_pad_rows(hq, dpad, queries, ldq, nq, h->dim);
-        ANN_CUDA_TRY(cudaMemcpyAsync(qdev, hq, sizeof(float) * (size_t)nq * dpad, cudaMemcpyHostToDevice, st));
+        if ((rc = queries_in(qdev, dpad, queries, ldq, nq, h->dim, st))) return rc;
     } else {
         if ((rc = launch_pad_rows(queries, nq, h->dim, ldq, qdev, dpad, st))) return rc;
     }
@@ -870,14 +807,10 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
     h->prof.mark(prec, st);
     h->ndist.fetch_add(h->n * (int64_t)nq);
     if (host) {
-        int64_t* hid = reinterpret_cast<int64_t*>(ws->host);
-        float* hd = reinterpret_cast<float*>(ws->host + sizeof(int64_t) * (size_t)nq * kk);
-        ANN_CUDA_TRY(cudaMemcpyAsync(hid, ids_dev, sizeof(int64_t) * (size_t)nq * kk, cudaMemcpyDeviceToHost, st));
+        ANN_CUDA_TRY(cudaMemcpyAsync(out_ids, ids_dev, sizeof(int64_t) * (size_t)nq * kk, cudaMemcpyDeviceToHost, st));
         if (out_dists)
-            ANN_CUDA_TRY(cudaMemcpyAsync(hd, dists_dev, sizeof(float) * (size_t)nq * kk, cudaMemcpyDeviceToHost, st));
+            ANN_CUDA_TRY(cudaMemcpyAsync(out_dists, dists_dev, sizeof(float) * (size_t)nq * kk, cudaMemcpyDeviceToHost, st));
         ANN_CUDA_TRY(cudaStreamSynchronize(st));
-        host_copy(out_ids, hid, sizeof(int64_t) * (size_t)nq * kk);
-        if (out_dists) host_copy(out_dists, hd, sizeof(float) * (size_t)nq * kk);
         return flat_check_err(h);
     }
     return ANN_OK;

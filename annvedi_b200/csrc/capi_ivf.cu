@@ -190,9 +190,9 @@ int ann_ivf_destroy(ann_ivf* h) {
         if (h->d_ndist) cudaFree(h->d_ndist);
         if (h->d_err) cudaFree(h->d_err);
         if (h->ws.dev) cudaFree(h->ws.dev);
-        if (h->ws.host) cudaFreeHost(h->ws.host);
+        if (h->ws.big) cudaFree(h->ws.big);
         h->ws.dev = nullptr;
-        h->ws.host = nullptr;
+        h->ws.big = nullptr;
     }
     delete h;
     return ANN_OK;
@@ -1045,11 +1045,7 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     }
     char* scratch = ws->dev + head_bytes;
     if (host) {
-        rc = ws_reserve_host(ws, std::max(sizeof(float) * (size_t)nq * dpad, (sizeof(int64_t) + 4) * (size_t)nq * k));
-        if (rc) return rc;
-        float* hq = reinterpret_cast<float*>(ws->host);
-        host_pad_rows(hq, dpad, queries, ldq, nq, h->dim);
-        ANN_CUDA_TRY(cudaMemcpyAsync(qdev, hq, sizeof(float) * (size_t)nq * dpad, cudaMemcpyHostToDevice, st));
+        if ((rc = queries_in(qdev, dpad, queries, ldq, nq, h->dim, st))) return rc;
     } else {
         rc = launch_pad_rows(queries, nq, h->dim, ldq, qdev, dpad, st);
         if (rc) return rc;
@@ -1062,14 +1058,10 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     }
     h->query_count += nq;
     if (host) {
-        int64_t* hid = reinterpret_cast<int64_t*>(ws->host);
-        float* hd = reinterpret_cast<float*>(ws->host + sizeof(int64_t) * (size_t)nq * k);
-        ANN_CUDA_TRY(cudaMemcpyAsync(hid, ids_dev, sizeof(int64_t) * (size_t)nq * k, cudaMemcpyDeviceToHost, st));
+        ANN_CUDA_TRY(cudaMemcpyAsync(out_ids, ids_dev, sizeof(int64_t) * (size_t)nq * k, cudaMemcpyDeviceToHost, st));
         if (out_dists)
-            ANN_CUDA_TRY(cudaMemcpyAsync(hd, dists_dev, sizeof(float) * (size_t)nq * k, cudaMemcpyDeviceToHost, st));
+            ANN_CUDA_TRY(cudaMemcpyAsync(out_dists, dists_dev, sizeof(float) * (size_t)nq * k, cudaMemcpyDeviceToHost, st));
         ANN_CUDA_TRY(cudaStreamSynchronize(st));
-        host_copy(out_ids, hid, sizeof(int64_t) * (size_t)nq * k);
-        if (out_dists) host_copy(out_dists, hd, sizeof(float) * (size_t)nq * k);
         return ann_ivf_device_status(h);
     }
     return ANN_OK;

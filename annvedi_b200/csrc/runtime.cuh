@@ -13,8 +13,6 @@ struct ann_workspace {
     int device = 0;
     char* dev = nullptr;
     size_t dev_cap = 0;
-    char* host = nullptr;  // pinned
-    size_t host_cap = 0;
     char* big = nullptr;   // second device arena for large per-batch buffers sized after planning
     size_t big_cap = 0;
     std::mutex mu;         // serialises growth; concurrent calls must still use separate workspaces
@@ -39,7 +37,6 @@ struct DeviceGuard {
 // Grows the workspace's device arena to at least `bytes` (drains the device first, since the old
 // block may be in use by earlier asynchronous work).
 int ws_reserve_device(ann_workspace* ws, size_t bytes);
-int ws_reserve_host(ann_workspace* ws, size_t bytes);
 int ws_reserve_big(ann_workspace* ws, size_t bytes);
 
 // Stage timer: records CUDA events around consecutive stages of a call on its stream; totals are
@@ -150,10 +147,9 @@ struct Sizer {
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
-// Host-side staging copies of queries with host buffers, split over up to 8 threads when large (one thread
-// copies a 10,000 x 384 batch more slowly than the GPU searches it). host_pad_rows writes `rows` rows of
-// `cols` floats from src (stride src_ld) to dst (stride dst_ld), zero-filling each row past cols.
-void host_copy(void* dst, const void* src, size_t bytes);
-void host_pad_rows(float* dst, int64_t dst_ld, const float* src, int64_t src_ld, int64_t rows, int cols);
+// Queries and results of calls with host buffers move straight between the caller's memory and the device
+// (the driver stages pageable memory itself; a copy through the library's own pinned buffer measured slower).
+// queries_in: rows of `cols` floats (host stride ld) into dev rows of stride dpad, columns past cols zeroed.
+int queries_in(float* dev, int64_t dpad, const float* host, int64_t ld, int64_t rows, int cols, cudaStream_t st);
 
 }  // namespace annb
