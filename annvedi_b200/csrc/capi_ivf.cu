@@ -680,6 +680,7 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
         sz.take<__nv_bfloat16>((size_t)nq * c.npc * h->kpad);
         sz.take<int64_t>((size_t)nq * c.npc);
         sz.take<int64_t>((size_t)h->C + 1);
+        sz.take<int32_t>((size_t)tc_items_bound((int64_t)nq * c.npc, (int)h->C, h->sizes_desc[0]));
     }
     sz.take<int32_t>((size_t)nq);  // re-rank query order
     sz.take<int64_t>(1);           // an every-row stream: its length
@@ -719,6 +720,8 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     __nv_bfloat16* Apk = c.tc ? cv.take<__nv_bfloat16>((size_t)nq * c.npc * h->kpad) : nullptr;
     int64_t* dbase = c.tc ? cv.take<int64_t>((size_t)nq * c.npc) : nullptr;
     int64_t* titem = c.tc ? cv.take<int64_t>((size_t)h->C + 1) : nullptr;
+    const int64_t items_cap = c.tc ? tc_items_bound((int64_t)nq * c.npc, (int)h->C, h->sizes_desc[0]) : 0;
+    int32_t* titem_list = c.tc ? cv.take<int32_t>((size_t)items_cap) : nullptr;
     int32_t* qorder = cv.take<int32_t>((size_t)nq);
     int64_t* every_len = cv.take<int64_t>(1);
     int32_t* every_seg = cv.take<int32_t>(1);
@@ -831,6 +834,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                                               b.cand_off, a.plan.seg_pref, h->list_off, Apk, dbase, st)))
                     return rc;
                 if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, h->C, titem, st))) return rc;
+                if ((rc = launch_tc_item_lists(titem, (int)h->C, titem_list, items_cap, st))) return rc;
                 TcGemmArgs g{(int)max_pairs, (int)h->n, kpad, nullptr, D, 0, h->d_err};
                 g.g_item_off = titem;
                 g.g_a_off = b.lq_off;
@@ -838,6 +842,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                 g.g_dbase = dbase;
                 g.g_total = titem + h->C;
                 g.g_lists = h->C;
+                g.g_item_list = titem_list;
                 if ((rc = launch_tc_gemm(Apk, h->base_bf16, g, st))) return rc;
                 RadixSelectArgs rs{};
                 rs.keys = D;

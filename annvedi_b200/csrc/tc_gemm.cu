@@ -157,12 +157,16 @@ struct GroupTile {
 };
 __device__ __forceinline__ GroupTile group_tile(const TcGemmArgs& a, int64_t t) {
     int lo = 0, hi = a.g_lists - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (a.g_item_off[mid] <= t)
-            lo = mid;
-        else
-            hi = mid - 1;
+    if (a.g_item_list) {
+        lo = a.g_item_list[t];  // one load, where a search would chain a dozen
+    } else {
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.g_item_off[mid] <= t)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
     }
     const int64_t np = a.g_a_off[lo + 1] - a.g_a_off[lo];
     const int64_t nr = a.g_b_off[lo + 1] - a.g_b_off[lo];

@@ -41,6 +41,7 @@ struct TcGemmArgs {
     const int64_t* g_dbase = nullptr;
     const int64_t* g_total = nullptr;
     int g_lists = 0;
+    const int32_t* g_item_list = nullptr;  // optional: the list of each item (else a search of g_item_off)
     // Element kind of A and B. E4M3 operands carry a scale per row (launch_tc_operand_e4m3): the key is
     // col_fac[n].y + col_fac[n].x * row_fac[m] * accumulator (key-matrix and filter modes).
     int kind = kTcBF16;

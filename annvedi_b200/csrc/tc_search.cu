@@ -273,6 +273,22 @@ int launch_tc_ivf_items(const int64_t* lq_off, const int64_t* list_off, int C, i
     return ANN_OK;
 }
 
+namespace {
+// item_list[t] = l for every item t of list l (t < cap)
+__global__ void tc_item_lists_kernel(const int64_t* __restrict__ item_off, int C, int32_t* __restrict__ item_list,
+                                     int64_t cap) {
+    for (int l = blockIdx.x; l < C; l += gridDim.x)
+        for (int64_t t = item_off[l] + threadIdx.x; t < item_off[l + 1] && t < cap; t += blockDim.x) item_list[t] = l;
+}
+}  // namespace
+
+int launch_tc_item_lists(const int64_t* item_off, int C, int32_t* item_list, int64_t cap, cudaStream_t st) {
+    ANN_CHECK_ARG(C >= 1, "tensor-core IVF: no lists");
+    tc_item_lists_kernel<<<(unsigned)std::min(C, 4 * kNumSMs), 128, 0, st>>>(item_off, C, item_list, cap);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
 int launch_tc_ivf_pairs(const __nv_bfloat16* qb, int kpad, const int32_t* pair_vals, const int32_t* pair_lists,
                         const int64_t* n_pairs, int64_t max_pairs, int npc, const int64_t* cand_off,
                         const int64_t* seg_pref, const int64_t* list_off, __nv_bfloat16* A, int64_t* dbase,
