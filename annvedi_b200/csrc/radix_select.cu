@@ -69,7 +69,7 @@ __device__ int find_bin(const int* hist, int rank, int* below, int* sScan) {
 
 // The bin holding the rank-th smallest (0-based) element of a kBins histogram, by a warp-shuffle block
 // scan (two barriers). Whole block; every thread gets the bin. sScan: >= kThreads / 32 + 1 ints.
-__device__ int find_bin_scan(const int* hist, int rank, int* sScan) {
+__device__ int find_bin_scan(const int* hist, int rank, int* sScan, int* below = nullptr) {
     constexpr int per = kBins / kThreads;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int local = 0;
@@ -93,12 +93,14 @@ __device__ int find_bin_scan(const int* hist, int rank, int* sScan) {
             const int h = hist[threadIdx.x * per + i];
             if (rank < c + h) {
                 sScan[kThreads / 32] = threadIdx.x * per + i;
+                sScan[kThreads / 32 + 1] = c;  // elements in lower bins
                 break;
             }
             c += h;
         }
     }
     __syncthreads();
+    if (below) *below = sScan[kThreads / 32 + 1];
     return sScan[kThreads / 32];
 }
 
@@ -151,6 +153,7 @@ __device__ void block_minmax(float& lo, float& hi, float* sRed) {
     __syncthreads();
 }
 
+constexpr int kTieCap = 256;   // pairs of a sampled set's boundary bin sorted by one warp
 constexpr int kLinCap = 2048;  // keys sorted in shared memory (the final sub-bin, or a sampled bar's set)
 constexpr int kSamples = 1024; // keys of the stream sampled for a bar
 constexpr int kLoadBatch = 8;   // keys per thread loaded ahead of their use
@@ -181,6 +184,8 @@ __global__ void __launch_bounds__(kThreads) radix_select_kernel(RadixSelectArgs 
     __shared__ float sRed[64];
     __shared__ int sScan[kThreads];
     __shared__ int sCount, sTies;
+    __shared__ float sTieK[kTieCap];
+    __shared__ int sTieP[kTieCap];
     const int q = blockIdx.x;
     const int64_t off = a.offs ? a.offs[q] : (int64_t)q * a.ld;
     int64_t len = a.lens ? a.lens[q] : a.ld;
@@ -214,7 +219,7 @@ __global__ void __launch_bounds__(kThreads) radix_select_kernel(RadixSelectArgs 
     if (want_set && !two && !a.kth_upper && (int64_t)R * 8 <= len && R <= 512) {
         // Sampled bar: every s-th key, the bar at the ~1.3 R / s-th smallest sample; one pass gathers
         // the keys at or below it with their positions, and if there are at least R of them (the R
-        // smallest keys then all are), a sort by (key, position) gives the set exactly.
+        // smallest keys then all are), the set is resolved among them exactly (below).
         const int64_t sstep = max((int64_t)1, len / kSamples);
         const int ns = (int)min((int64_t)kSamples, (len + sstep - 1) / sstep);
         const int r = min(ns, (int)(((int64_t)R * 13 + 10 * sstep - 1) / (10 * sstep)) + 4);
@@ -257,6 +262,61 @@ __global__ void __launch_bounds__(kThreads) radix_select_kernel(RadixSelectArgs 
         __syncthreads();
         const int cnt = sCount;
         if (cnt >= R && cnt <= kLinCap) {
+            // The set (unordered) of the R smallest of the cnt gathered pairs: linear bins over their range;
+            // every pair in a bin below the one holding the R-th is in, and that bin's pairs (few) are
+            // sorted by (key, position) by one warp to fill the set. Equal keys throughout, or a crowded
+            // boundary bin, take the full sort below.
+            float clo = kInf, chi = -kInf;
+            for (int e = threadIdx.x; e < cnt; e += kThreads) {
+                clo = fminf(clo, sCandK[e]);
+                chi = fmaxf(chi, sCandK[e]);
+            }
+            for (int i = threadIdx.x; i < kBins; i += kThreads) hist[1][i] = 0;
+            block_minmax(clo, chi, sRed);  // its barriers also order every read of sCount before the resets
+            const float csc = (float)kBins / (chi - clo);
+            if (chi > clo && isfinite(csc)) {
+                if (threadIdx.x == 0) {
+                    sCount = 0;
+                    sTies = 0;
+                }
+                for (int e = threadIdx.x; e < cnt; e += kThreads) atomicAdd(&hist[1][lin_bin(sCandK[e], clo, csc)], 1);
+                __syncthreads();
+                int below = 0;
+                const int bb = find_bin_scan(hist[1], R - 1, sScan, &below);
+                const int nb = hist[1][bb];
+                if (nb <= kTieCap) {
+                    for (int e = threadIdx.x; e < cnt; e += kThreads) {
+                        const float kv = sCandK[e];
+                        const int bin = lin_bin(kv, clo, csc);
+                        if (bin < bb) {
+                            const int slot = atomicAdd(&sCount, 1);
+                            if (ok) ok[slot] = kv;
+                            if (oi) oi[slot] = id_of(sCandP[e]);
+                        } else if (bin == bb) {
+                            const int at = atomicAdd(&sTies, 1);
+                            sTieK[at] = kv;
+                            sTieP[at] = sCandP[e];
+                        }
+                    }
+                    __syncthreads();
+                    if (threadIdx.x < 32) {
+                        int cap2 = 32;
+                        while (cap2 < nb) cap2 <<= 1;
+                        for (int e = nb + threadIdx.x; e < cap2; e += 32) {
+                            sTieK[e] = kInf;
+                            sTieP[e] = INT_MAX;
+                        }
+                        __syncwarp();
+                        warp_sort_smem(sTieK, sTieP, cap2);
+                        for (int e = threadIdx.x; e < R - below; e += 32) {
+                            if (ok) ok[below + e] = sTieK[e];
+                            if (oi) oi[below + e] = id_of(sTieP[e]);
+                        }
+                    }
+                    return;
+                }
+            }
+            __syncthreads();
             int cap2 = 32;
             while (cap2 < cnt) cap2 <<= 1;
             for (int e = cnt + threadIdx.x; e < cap2; e += kThreads) {
