@@ -721,7 +721,7 @@ __device__ __forceinline__ int block_sum_int(int v, float* scratch) {
 // arithmetic in reference mode, lsh_index_optimized.cpp:481-486), then the best k by (distance, row)
 // and the mapping back to original ids (:503-512).
 template <bool REF>
-__global__ void __launch_bounds__(256) ivf_rerank_kernel(IvfQueryArgs a, const float* __restrict__ keyR,
+__global__ void __launch_bounds__(256, 5) ivf_rerank_kernel(IvfQueryArgs a, const float* __restrict__ keyR,
                                                           const int* __restrict__ idR) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int R = a.R, k = a.k;
