@@ -703,6 +703,7 @@ int launch_select_topk(const float* keys, int64_t ld, const int64_t* lens, int n
 
 // ---- 4. FP32 re-rank and final top-k -------------------------------------------------------------
 constexpr int kRerankRankMax = 1024;  // R up to this: the final top-k by block-wide ranks
+constexpr int kRerankBins = 256;      // bins of the distances that narrow the ranking down
 
 // Sum of v over the block (every thread gets it); scratch: >= blockDim.x / 32 floats of shared memory, free
 // for the caller's use again after the call.
@@ -840,9 +841,95 @@ __global__ void __launch_bounds__(256, 5) ivf_rerank_kernel(IvfQueryArgs a, cons
     __syncthreads();
     const float kEmpty = a.metric == ANN_METRIC_IP ? -kInf : kInf;
     if (R <= kRerankRankMax) {
-        // every thread ranks its entries by (distance, row) among the R (the rows are distinct, so the ranks
-        // are); an entry of rank < k goes to out[rank]: the best k in order, without leaving seven warps idle
-        // behind one that sorts
+        // The best k in order, every warp working: entries are ranked by (distance, row) (the rows are
+        // distinct, so the ranks are) and an entry of rank < k goes to out[rank]. Ranking every entry
+        // against all R costs R^2 comparisons; first, 256 linear bins over the valid distances find the bin
+        // holding the k-th, and only the entries of that bin or lower (about k) are ranked, among themselves.
+        __shared__ int sHist[kRerankBins];
+        __shared__ float sRedF[2 * 32];
+        __shared__ int sRedI[32 + 3];
+        {
+            float lo = kInf, hi = -kInf;
+            int nv = 0;
+            for (int e = threadIdx.x; e < R; e += blockDim.x)
+                if (sRow[e] != kNoId) {
+                    lo = fminf(lo, sD[e]);
+                    hi = fmaxf(hi, sD[e]);
+                    ++nv;
+                }
+            for (int i = threadIdx.x; i < kRerankBins; i += blockDim.x) sHist[i] = 0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+                nv += __shfl_xor_sync(0xffffffffu, nv, o);
+            }
+            const int nw = (int)(blockDim.x >> 5);
+            if (lane == 0) {
+                sRedF[warp] = lo;
+                sRedF[32 + warp] = hi;
+                sRedI[warp] = nv;
+            }
+            if (threadIdx.x == 0) sRedI[32] = 0;  // list length
+            __syncthreads();
+            lo = kInf;
+            hi = -kInf;
+            nv = 0;
+            for (int w = 0; w < nw; ++w) {
+                lo = fminf(lo, sRedF[w]);
+                hi = fmaxf(hi, sRedF[32 + w]);
+                nv += sRedI[w];
+            }
+            const float sc = (float)kRerankBins / (hi - lo);
+            if (nv > k && hi > lo && isfinite(sc)) {  // uniform across the block
+                auto bin_of = [&](float d) {
+                    const float f = (d - lo) * sc;
+                    return !(f > 0.f) ? 0 : (f >= (float)(kRerankBins - 1) ? kRerankBins - 1 : (int)f);
+                };
+                for (int e = threadIdx.x; e < R; e += blockDim.x)
+                    if (sRow[e] != kNoId) atomicAdd(&sHist[bin_of(sD[e])], 1);
+                __syncthreads();
+                // the bin holding rank k - 1: one bin per thread, a warp-shuffle scan
+                int incl = 0, own = 0;
+                for (int b = threadIdx.x; b < kRerankBins; b += blockDim.x) own = sHist[b];
+                incl = own;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                if (lane == 31) sRedI[warp] = incl;
+                __syncthreads();
+                for (int w = 0; w < warp; ++w) incl += sRedI[w];
+                if (threadIdx.x < kRerankBins && k - 1 >= incl - own && k - 1 < incl) {
+                    sRedI[33] = threadIdx.x;
+                    sRedI[34] = incl;  // entries in this bin or lower
+                }
+                __syncthreads();
+                const int bb = sRedI[33], m = sRedI[34];
+                if (m <= topk_cap(k)) {
+                    for (int e = threadIdx.x; e < R; e += blockDim.x)
+                        if (sRow[e] != kNoId && bin_of(sD[e]) <= bb) {
+                            const int slot = atomicAdd(&sRedI[32], 1);
+                            sKey[slot] = sD[e];
+                            sId[slot] = sRow[e];
+                        }
+                    __syncthreads();
+                    for (int e = threadIdx.x; e < m; e += blockDim.x) {
+                        const float key = sKey[e];
+                        const int row = sId[e];
+                        int rank = 0;
+                        for (int j = 0; j < m; ++j) rank += pair_less(sKey[j], sId[j], key, row);
+                        if (rank < k) {
+                            a.out_ids[(int64_t)q * k + rank] = (int64_t)(a.ix.r2o ? a.ix.r2o[row] : row);
+                            if (a.out_dists) a.out_dists[(int64_t)q * k + rank] = a.metric == ANN_METRIC_IP ? -key : key;
+                        }
+                    }
+                    return;  // nv > k: all k slots written
+                }
+            }
+            __syncthreads();
+        }
         int nvalid = 0;
         for (int e = threadIdx.x; e < R; e += blockDim.x) {
             const int row = sRow[e];
