@@ -175,6 +175,31 @@ __global__ void __launch_bounds__(128) tc_coarse_kernel(const float* __restrict_
     WarpTopK top;
     top.init(sK, sI, m);
     const float* kr = keys + (int64_t)qi * ldk;
+    // A bar that keeps the offers few: each lane's smallest key, and the m-th smallest of those 32 minima
+    // (m <= 32). At least m keys lie at or below it, so the m-th smallest key does, and with it every key of
+    // the best m (ties included): offering only keys <= bar gives the same best m.
+    float bar = kInf;
+    if (m <= 32) {
+        float mn = kInf;
+        for (int c0 = 0; c0 < C; c0 += 128) {
+            float v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int c = c0 + 32 * u + lane;
+                v[u] = c < C ? kr[c] : kInf;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) mn = fminf(mn, v[u]);
+        }
+        int rank = 0;  // among the lane minima, ties by lane
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const float o = __shfl_sync(0xffffffffu, mn, j);
+            rank += (o < mn) || (o == mn && j < lane);
+        }
+        const unsigned sel = __ballot_sync(0xffffffffu, rank == m - 1);
+        bar = __shfl_sync(0xffffffffu, mn, __ffs(sel) - 1);
+    }
     for (int c0 = 0; c0 < C; c0 += 128) {  // four loads in flight, offered in key order
         float v[4];
 #pragma unroll
@@ -185,7 +210,7 @@ __global__ void __launch_bounds__(128) tc_coarse_kernel(const float* __restrict_
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int c = c0 + 32 * u + lane;
-            top.offer(v[u], c < C ? c : kNoId, c < C);
+            top.offer(v[u], c < C ? c : kNoId, c < C && v[u] <= bar);
         }
     }
     top.compact();
