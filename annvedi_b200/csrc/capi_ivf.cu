@@ -856,7 +856,17 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                 if ((rc = launch_radix_select(rs, nq, st))) return rc;
             } else {
                 if ((rc = launch_batched(b, qdev, qs, D, st))) return rc;
-                if ((rc = launch_select_topk(D, 0, n_cands, nq, c.R, &a.plan, keyR, idR, st, b.cand_off))) return rc;
+                // the best R of each stream as a set (ties by stream position); the re-rank orders them
+                RadixSelectArgs rs{};
+                rs.keys = D;
+                rs.offs = b.cand_off;
+                rs.lens = n_cands;
+                rs.plan = a.plan;
+                rs.use_plan = 1;
+                rs.R = c.R;
+                rs.out_key = keyR;
+                rs.out_id = idR;
+                if ((rc = launch_radix_select(rs, nq, st))) return rc;
             }
             done = true;
         }
