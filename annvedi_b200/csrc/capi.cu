@@ -301,11 +301,14 @@ int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t
         }
     } else {
         ncp = compat_num_checkpoints(h->dim);
-        const size_t per_q = sizeof(float) * (size_t)h->n * (ncp + 1);
+        const size_t per_q = sizeof(float) * (size_t)h->n * (ncp + 2) + (size_t)8 * kk;
         const size_t budget = (size_t)1 << 30;
         qc = (int)std::max<size_t>(1, std::min<size_t>((size_t)nq, budget / per_q));
         sz.take<float>((size_t)qc * h->n);
         sz.take<float>((size_t)qc * h->n * ncp);
+        sz.take<float>((size_t)qc * h->n);
+        sz.take<float>((size_t)qc * kk);
+        sz.take<int>((size_t)qc * kk);
     }
     int rc = ws_reserve_device(ws, sz.bytes());
     if (rc) return rc;
@@ -371,6 +374,9 @@ int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t
         a.ncp = ncp;
         a.D = cv.take<float>((size_t)qc * h->n);
         a.P = cv.take<float>((size_t)qc * h->n * ncp);
+        a.T = cv.take<float>((size_t)qc * h->n);
+        a.kbuf = cv.take<float>((size_t)qc * kk);
+        a.ibuf = cv.take<int>((size_t)qc * kk);
         a.out_ids = ids_dev;
         a.out_dists = dists_dev;
         for (int q0 = 0; q0 < nq; q0 += qc) {

@@ -14,11 +14,15 @@
 // compiled reference too: one fused 8-wide chunk folded the same way, then scalar fused steps.
 // It writes the full distance D[q][i] and the checkpoint values P[q][c][i].
 //
-// Pass 2 (compat_select_kernel) is one warp per query walking the rows in order: the running
-// 64-heap is replayed only at insertions (rows with D < T, which are rare once T settles), each
-// row's T_i is known exactly, v_i is picked from P, and the warp keeps the k best (v_i, i) pairs.
+// Pass 2 (compat_threshold_kernel) is one warp per query walking the rows in order: the running
+// 64-heap is replayed only at insertions (rows with D < T, which are rare once T settles), and each
+// row's threshold T_i is recorded. Pass 3 (compat_values_kernel), parallel over rows, picks v_i from D,
+// P and T_i. The k best (v_i, i) pairs come from the radix selection (the exact set, ties by row) and
+// a sort of those k.
 #include "common.cuh"
 #include "compat.cuh"
+#include "flat_scan.cuh"
+#include "radix_select.cuh"
 #include "refmath.cuh"
 
 namespace annb {
@@ -48,27 +52,77 @@ __global__ void __launch_bounds__(256) compat_partials_kernel(CompatArgs a, int 
     }
 }
 
-__global__ void __launch_bounds__(128) compat_select_kernel(CompatArgs a, int q_begin) {
+constexpr int kCompatAhead = 8;  // 32-row steps of distances loaded ahead of the walk
+
+__global__ void __launch_bounds__(128) compat_threshold_kernel(CompatArgs a, int q_begin) {
     constexpr int WARPS = 4;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int cap = topk_cap(a.k);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* sKey = reinterpret_cast<float*>(smem_raw) + warp * cap;
-    int* sId = reinterpret_cast<int*>(reinterpret_cast<float*>(smem_raw) + WARPS * cap) + warp * cap;
     const int qi = blockIdx.x * WARPS + warp;  // within chunk
-    if (q_begin + qi >= a.q_end) return;
-    const int k = a.k;
-    WarpTopK top;
-    top.init(sKey, sId, k);
-    ref_replay(a.D + (int64_t)qi * a.n, a.P + (int64_t)qi * a.ncp * a.n, a.n, a.ncp, 0, a.n, k < 64 ? k : 64,
-               [&](int64_t i, float v, bool valid) { top.offer(v, (int)i, valid); });
-    top.compact();
-    const int cnt = top.count;
-    const int64_t qo = q_begin + qi;
-    for (int e = lane; e < k; e += 32) {
-        const bool ok = e < cnt;
-        if (a.out_ids) a.out_ids[qo * k + e] = ok ? (int64_t)sId[e] : -1;
-        if (a.out_dists) a.out_dists[qo * k + e] = ok ? sKey[e] : kInf;
+    if (q_begin + qi >= a.q_end) return;       // the whole warp; no block barrier follows
+    const int lim = a.k < 64 ? a.k : 64;
+    const int64_t n = a.n;
+    const float* D = a.D + (int64_t)qi * n;
+    float* T = a.T + (int64_t)qi * n;
+    const float inf = __int_as_float(0x7f800000);
+    WarpHeap64 heap;
+    heap.init(lim);
+    float Tcur = 3.402823466e+38f;  // FLT_MAX until the heap holds lim distances
+    float nxt[kCompatAhead];
+#pragma unroll
+    for (int j = 0; j < kCompatAhead; ++j) {
+        const int64_t i = (int64_t)j * 32 + lane;
+        nxt[j] = i < n ? D[i] : inf;
+    }
+    for (int64_t base = 0; base < n; base += 32 * kCompatAhead) {
+        float cur[kCompatAhead];
+#pragma unroll
+        for (int j = 0; j < kCompatAhead; ++j) {
+            cur[j] = nxt[j];
+            const int64_t i = base + 32 * kCompatAhead + (int64_t)j * 32 + lane;
+            nxt[j] = i < n ? D[i] : inf;
+        }
+#pragma unroll
+        for (int j = 0; j < kCompatAhead; ++j) {
+            const int64_t i = base + (int64_t)j * 32 + lane;
+            const bool valid = i < n;
+            const float d = cur[j];
+            // rows enter the heap in row order; a row's threshold is the heap's before its own insertion
+            float myT = Tcur;
+            int last = -1;
+            while (true) {
+                const unsigned cand = __ballot_sync(0xffffffffu, valid && lane > last && d < myT);
+                if (cand == 0) break;
+                const int l0 = __ffs(cand) - 1;
+                heap.insert(__shfl_sync(0xffffffffu, d, l0));
+                Tcur = heap.worst();
+                if (lane > l0) myT = Tcur;
+                last = l0;
+            }
+            if (valid) T[i] = myT;
+        }
+    }
+}
+
+// v_i = d_i when d_i < T_i, else the first checkpoint value >= T_i (d_i if none), written over T_i.
+__global__ void __launch_bounds__(256) compat_values_kernel(CompatArgs a, int q_count) {
+    const int64_t n = a.n;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)q_count * n;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t qi = e / n, i = e - qi * n;
+        const float d = a.D[e];
+        const float t = a.T[e];
+        float v = d;
+        if (!(d < t)) {
+            const float* P = a.P + qi * a.ncp * n + i;
+            for (int c = 0; c < a.ncp; ++c) {
+                const float p = P[(int64_t)c * n];
+                if (p >= t) {
+                    v = p;
+                    break;
+                }
+            }
+        }
+        a.T[e] = v;
     }
 }
 
@@ -85,12 +139,21 @@ int launch_compat(CompatArgs a, int q_begin, int q_count, cudaStream_t st) {
     dim3 g1((unsigned)rblocks, (unsigned)ceil_div(q_count, kCompatQG));
     compat_partials_kernel<<<g1, 256, smem, st>>>(a, q_begin);
     ANN_LAUNCH_CHECK();
-    const unsigned g2 = (unsigned)ceil_div(q_count, 4);
-    const size_t smem2 = (size_t)4 * topk_cap(a.k) * 8;
-    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(compat_select_kernel)));
-    compat_select_kernel<<<g2, 128, smem2, st>>>(a, q_begin);
+    compat_threshold_kernel<<<(unsigned)ceil_div(q_count, 4), 128, 0, st>>>(a, q_begin);
     ANN_LAUNCH_CHECK();
-    return ANN_OK;
+    compat_values_kernel<<<(unsigned)std::min<int64_t>(ceil_div((int64_t)q_count * a.n, 256), 16 * kNumSMs), 256, 0,
+                           st>>>(a, q_count);
+    ANN_LAUNCH_CHECK();
+    RadixSelectArgs rs{};
+    rs.keys = a.T;
+    rs.ld = a.n;
+    rs.R = a.k;
+    rs.out_key = a.kbuf;
+    rs.out_id = a.ibuf;
+    int rc = launch_radix_select(rs, q_count, st);
+    if (rc) return rc;
+    return launch_sort_topk(a.kbuf, a.ibuf, q_count, a.k, 0, a.out_ids ? a.out_ids + (int64_t)q_begin * a.k : nullptr,
+                            a.out_dists ? a.out_dists + (int64_t)q_begin * a.k : nullptr, st);
 }
 
 }  // namespace annb

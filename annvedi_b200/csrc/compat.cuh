@@ -19,6 +19,9 @@ struct CompatArgs {
     int ncp;            // compat_num_checkpoints(dim)
     float* D;           // [chunk, n] scratch: full distances
     float* P;           // [chunk, ncp, n] scratch: checkpoint values
+    float* T;           // [chunk, n] scratch: each row's heap threshold, then its ranking value
+    float* kbuf;        // [chunk, k] scratch: the selected values
+    int* ibuf;          // [chunk, k] scratch: their rows
     int64_t* out_ids;   // [nq, k]
     float* out_dists;   // [nq, k] ranking values, or nullptr
 };
