@@ -559,6 +559,8 @@ def run_ours(args, rank, world, local):
         line["serving"] = serving_c5(args, local, ivf, npc, w)
     if rank == 0 and world == 1 and args.lsh and ivf is not None:
         line["ivf_lsh_tables"] = lsh_tables_c3(args, ivf, w)
+    if rank == 0 and world == 1 and args.dropin:
+        line["dropin_linear_100k"] = dropin_linear_c1(args)
     return line
 
 
@@ -696,6 +698,36 @@ def scaled_fp8_c4(args, local):
                      "filter_ms_per_batch": round(st["tc_filter_ms"] / 3, 3)}
     del ix, w
     torch.cuda.empty_cache()
+    return out
+
+
+def dropin_linear_c1(args):
+    """The drop-in as the competition harness drives it (Algorithm.query, one query per call, the
+    reference's semantics and distance counter) on the reference's CPU-runnable configuration: 100,000 x
+    384 unit rows, k = 100. Beside it, the reference's own linear_ann_cpp on the same rows and queries."""
+    from annvedi_b200 import harness, synth
+    from annvedi_b200.algorithm import Algorithm
+    w = synth.flat_normal(100_000, 384, 300, seed=0)
+    data = {"train": w.base, "test": w.queries}
+    res = harness.run(Algorithm, data, {"index_params": {"backend": "linear"}, "query_params": {}}, k=K_NN,
+                      log=lambda *_: None)
+    lat = res["query_times"][20:] * 1e3  # after the first calls' set-up
+    out = {"workload": "100k x 384 unit rows (N(0,1), normalised), 300 queries one at a time, k=100, backend linear",
+           "qps": round(len(lat) / (lat.sum() / 1e3), 1), "p50_ms": round(float(np.median(lat)), 3),
+           "p99_ms": round(float(np.percentile(lat, 99)), 3),
+           "distances_per_query": res["n_dist_queries"] // w.queries.shape[0]}
+    if not args.no_cpu_baseline:
+        from oracle import refmod
+        ix = refmod.load_ref("linear_ann_cpp").LinearIndex()
+        ix.fit(w.base)
+        qs = w.queries[:16]
+        ix.query(qs[0], K_NN)
+        t0 = time.perf_counter()
+        for qq in qs:
+            ix.query(qq, K_NN)
+        dt = (time.perf_counter() - t0) / len(qs) * 1e3
+        out["reference_cpu_ms_per_query"] = round(dt, 3)
+        out["reference_cpu_sample"] = "16 queries, one thread (linear_ann_cpp queries are serial)"
     return out
 
 
@@ -869,6 +901,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="per offered rate; 0 skips serving")
     ap.add_argument("--no-fp8", dest="fp8", action="store_false", help="skip the scaled-FP8 configuration")
     ap.add_argument("--no-lsh", dest="lsh", action="store_false", help="skip the LSH bucket-table settings")
+    ap.add_argument("--no-dropin", dest="dropin", action="store_false",
+                    help="skip the one-query-per-call drop-in measurement (100k x 384, backend linear)")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[2000, 10000, 50000])
     ap.add_argument("--ref-nprobe", type=int, default=8,
                     help="lists the reference arm probes: the headline form's (the autotuner's cheapest nprobe with "
