@@ -873,7 +873,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     }
     if (!done && c.lsh_keys) {
         if ((rc = launch_ivf_sq8_dists(a, lkeys, c.ub_cand, st))) return rc;
-        if ((rc = launch_select_topk(lkeys, c.ub_cand, n_cands, nq, c.R, &a.plan, keyR, idR, st))) return rc;
+        if ((rc = launch_select_topk(lkeys, c.ub_cand, n_cands, nq, c.R, &a.plan, keyR, idR, st, nullptr, true))) return rc;
         done = true;
     }
     if (done) {
@@ -897,7 +897,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         a.V = DP + (size_t)nq * c.ub;
         a.P = DP + (size_t)2 * nq * c.ub;
         if ((rc = launch_ivf_ref_sq8(a, c.ub, st))) return rc;
-        if ((rc = launch_select_topk(a.V, c.ub, n_cands, nq, c.R, &a.plan, keyR, idR, st))) return rc;
+        if ((rc = launch_select_topk(a.V, c.ub, n_cands, nq, c.R, &a.plan, keyR, idR, st, nullptr, true))) return rc;
     }
     h->prof.mark(prec, st);
     // 4. FP32 re-rank and the final top-k; batches run their queries grouped by first probed list, so that
@@ -934,7 +934,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                 b.V = big + L;
                 b.P = big + 2 * L;
                 if ((rc = launch_ivf_ref_sq8(b, L, st))) return rc;
-                if ((rc = launch_select_topk(b.V, L, b.plan.n_cands, 1, c.R, &b.plan, kq, iq, st))) return rc;
+                if ((rc = launch_select_topk(b.V, L, b.plan.n_cands, 1, c.R, &b.plan, kq, iq, st, nullptr, true))) return rc;
             } else {
                 b.use_stream = false;
                 b.nsplit = nsp;

@@ -608,7 +608,7 @@ __global__ void __launch_bounds__(256) ivf_ref_sq8_kernel(IvfQueryArgs a) {
 // One warp per ThreadPool chunk (src/thread_pool.h:93-124): chunk c of T covers
 // [c*(L/T) + min(c, L%T), ...), the first L%T chunks one longer; T = 1 when L < 2*num_threads
 // (lsh_index_optimized.cpp:465-469).
-__global__ void __launch_bounds__(128) ivf_ref_replay_kernel(IvfQueryArgs a) {
+__global__ void __launch_bounds__(1024) ivf_ref_replay_kernel(IvfQueryArgs a) {
     const int q = blockIdx.x;
     const int warp = threadIdx.x >> 5;
     const int64_t L = min(a.plan.n_cands[q], a.L);
@@ -634,21 +634,27 @@ int launch_ivf_ref_sq8(const IvfQueryArgs& a, int64_t Lmax, cudaStream_t st) {
     dim3 g1(a.plan.nq, (unsigned)blocks);
     ivf_ref_sq8_kernel<<<g1, 256, smem, st>>>(a);
     ANN_LAUNCH_CHECK();
-    ivf_ref_replay_kernel<<<a.plan.nq, 128, 0, st>>>(a);
+    // one warp per ThreadPool chunk (up to 32 in a block; more chunks loop)
+    const int rwarps = std::max(1, std::min(32, a.num_threads > 0 ? a.num_threads : 1));
+    ivf_ref_replay_kernel<<<a.plan.nq, 32 * rwarps, 0, st>>>(a);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }
 
 // ---- generic per-query top-k selection over a dense key array -----------------------------------
+constexpr int kSelBins = 1024;  // set-only selection: linear bins (4 per thread of a 256-thread block)
+constexpr int kSelTie = 256;    // boundary-bin pairs sorted by one warp
+
 // keys[q * ld + p] (keys[offs[q] + p] when offs is given) for p < lens[q] (at most ld without offs; ld when
 // lens is null);
 // id = plan_row(q, p) when a plan is
-// given, else p. Keeps the best kout (key, id) pairs, sorted, padded with (+inf, INT_MAX).
+// given, else p. Keeps the best kout (key, id) pairs, sorted, padded with (+inf, INT_MAX); with set_only
+// the same pairs in no particular order.
 __global__ void __launch_bounds__(256) select_topk_kernel(const float* __restrict__ keys, int64_t ld,
                                                           const int64_t* __restrict__ offs,
                                                           const int64_t* __restrict__ lens, int kout,
                                                           IvfPlan plan, int use_plan, float* out_key,
-                                                          int* out_id) {
+                                                          int* out_id, int set_only) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warps = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -657,14 +663,124 @@ __global__ void __launch_bounds__(256) select_topk_kernel(const float* __restric
     int* sId = reinterpret_cast<int*>(sKey + warps * cap);
     const int q = blockIdx.x;
     const int64_t len = lens ? (offs || ld <= 0 ? lens[q] : min(lens[q], ld)) : ld;
+    const float* kq = keys + (offs ? offs[q] : (int64_t)q * ld);
+    auto id_at = [&](int64_t p) { return (int)(use_plan ? plan_row(plan, q, p) : p); };
+    if (set_only && blockDim.x == kSelBins / 4 && len > kout) {
+        // The set only (unordered): kSelBins linear bins over the stream's keys find the bin holding the
+        // kout-th; every pair in a lower bin is in, and the boundary bin's pairs (few) are sorted by (key, id)
+        // by one warp -- the set the sorted path keeps, ties by id. Equal keys throughout, or a crowded
+        // boundary bin, take the sorted path below.
+        int* sHist = reinterpret_cast<int*>(smem_raw);                      // [kSelBins]
+        float* sBK = reinterpret_cast<float*>(sHist + kSelBins);             // [kSelTie]
+        int* sBI = reinterpret_cast<int*>(sBK + kSelTie);                    // [kSelTie]
+        __shared__ float sRf[64];
+        __shared__ int sRi[40];
+        float lo = kInf, hi = -kInf;
+        for (int64_t p = threadIdx.x; p < len; p += blockDim.x) {
+            const float kv = kq[p];
+            lo = fminf(lo, kv);
+            hi = fmaxf(hi, kv);
+        }
+        for (int i = threadIdx.x; i < kSelBins; i += blockDim.x) sHist[i] = 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (lane == 0) {
+            sRf[warp] = lo;
+            sRf[32 + warp] = hi;
+        }
+        if (threadIdx.x == 0) {
+            sRi[32] = 0;  // slots of the lower bins
+            sRi[33] = 0;  // boundary pairs
+        }
+        __syncthreads();
+        lo = kInf;
+        hi = -kInf;
+        for (int w = 0; w < warps; ++w) {
+            lo = fminf(lo, sRf[w]);
+            hi = fmaxf(hi, sRf[32 + w]);
+        }
+        const float sc = (float)kSelBins / (hi - lo);
+        if (hi > lo && isfinite(sc)) {  // uniform
+            auto bin_of = [&](float kv) {
+                const float f = (kv - lo) * sc;
+                return !(f > 0.f) ? 0 : (f >= (float)(kSelBins - 1) ? kSelBins - 1 : (int)f);
+            };
+            for (int64_t p = threadIdx.x; p < len; p += blockDim.x) atomicAdd(&sHist[bin_of(kq[p])], 1);
+            __syncthreads();
+            // the bin holding rank kout - 1: kSelBins / blockDim bins per thread, a warp-shuffle scan
+            constexpr int per = 4;
+            int own = 0;
+#pragma unroll
+            for (int i = 0; i < per; ++i) own += sHist[threadIdx.x * per + i];
+            int incl = own;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            if (lane == 31) sRi[warp] = incl;
+            __syncthreads();
+            for (int w = 0; w < warp; ++w) incl += sRi[w];
+            const int excl = incl - own;
+            if (kout - 1 >= excl && kout - 1 < incl) {
+                int c = excl;
+                for (int i = 0; i < per; ++i) {
+                    const int h = sHist[threadIdx.x * per + i];
+                    if (kout - 1 < c + h) {
+                        sRi[34] = threadIdx.x * per + i;
+                        sRi[35] = c;
+                        sRi[36] = h;
+                        break;
+                    }
+                    c += h;
+                }
+            }
+            __syncthreads();
+            const int bb = sRi[34], below = sRi[35], nb = sRi[36];
+            if (nb <= kSelTie) {
+                for (int64_t p = threadIdx.x; p < len; p += blockDim.x) {
+                    const float kv = kq[p];
+                    const int bin = bin_of(kv);
+                    if (bin < bb) {
+                        const int slot = atomicAdd(&sRi[32], 1);
+                        out_key[(int64_t)q * kout + slot] = kv;
+                        out_id[(int64_t)q * kout + slot] = id_at(p);
+                    } else if (bin == bb) {
+                        const int at = atomicAdd(&sRi[33], 1);
+                        sBK[at] = kv;
+                        sBI[at] = id_at(p);
+                    }
+                }
+                __syncthreads();
+                if (warp == 0) {
+                    int cap2 = 32;
+                    while (cap2 < nb) cap2 <<= 1;
+                    for (int e = nb + lane; e < cap2; e += 32) {
+                        sBK[e] = kInf;
+                        sBI[e] = kNoId;
+                    }
+                    __syncwarp();
+                    warp_sort_smem(sBK, sBI, cap2);
+                    for (int e = lane; e < kout - below; e += 32) {
+                        out_key[(int64_t)q * kout + below + e] = sBK[e];
+                        out_id[(int64_t)q * kout + below + e] = sBI[e];
+                    }
+                }
+                return;
+            }
+        }
+        __syncthreads();  // the sorted path reuses the shared memory
+    }
     WarpTopK top;
     top.init(sKey + warp * cap, sId + warp * cap, kout);
-    const float* kq = keys + (offs ? offs[q] : (int64_t)q * ld);
     for (int64_t base = (int64_t)warp * 32; base < len; base += (int64_t)warps * 32) {
         const int64_t p = base + lane;
         const bool ok = p < len;
         const float kv = ok ? kq[p] : kInf;
-        const int iv = ok ? (int)(use_plan ? plan_row(plan, q, p) : p) : kNoId;
+        const int iv = ok ? id_at(p) : kNoId;
         top.offer(kv, iv, ok);
     }
     top.compact();
@@ -686,17 +802,19 @@ __global__ void __launch_bounds__(256) select_topk_kernel(const float* __restric
 }
 
 int launch_select_topk(const float* keys, int64_t ld, const int64_t* lens, int nq, int kout, const IvfPlan* plan,
-                       float* out_key, int* out_id, cudaStream_t st, const int64_t* offs) {
+                       float* out_key, int* out_id, cudaStream_t st, const int64_t* offs, bool set_only) {
     if (nq == 0) return ANN_OK;
     ANN_CHECK_ARG(kout >= 1 && kout <= 8192, "select: k=%d outside [1, 8192]", kout);
     const size_t per_warp = (size_t)topk_cap(kout) * 8;
     int warps = (int)std::max<size_t>(1, std::min<size_t>(8, (96 * 1024) / per_warp));
-    const size_t smem = per_warp * warps;
+    size_t smem = per_warp * warps;
+    if (set_only) smem = std::max(smem, sizeof(int) * kSelBins + (size_t)8 * kSelTie);
     ANN_CHECK_ARG(smem <= 227 * 1024, "select: k=%d needs too much shared memory", kout);
     ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(select_topk_kernel)));
     IvfPlan p{};
     if (plan) p = *plan;
-    select_topk_kernel<<<nq, warps * 32, smem, st>>>(keys, ld, offs, lens, kout, p, plan ? 1 : 0, out_key, out_id);
+    select_topk_kernel<<<nq, warps * 32, smem, st>>>(keys, ld, offs, lens, kout, p, plan ? 1 : 0, out_key, out_id,
+                                                      set_only ? 1 : 0);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

@@ -86,7 +86,7 @@ int launch_ivf_sq8_dists(const IvfQueryArgs& a, float* D, int64_t ld, cudaStream
 int launch_ivf_ref_sq8(const IvfQueryArgs& a, int64_t Lmax, cudaStream_t st);
 int launch_select_topk(const float* keys, int64_t ld_keys, const int64_t* lens, int nq, int kout,
                        const IvfPlan* plan, float* out_key, int* out_id, cudaStream_t st,
-                       const int64_t* offs = nullptr);
+                       const int64_t* offs = nullptr, bool set_only = false);
 int launch_ivf_rerank(const IvfQueryArgs& a, const float* keyR, const int* idR, int reference, cudaStream_t st);
 int launch_ref_centroid_dists(const IvfView& ix, const float* q, int64_t ldq, int nq, float* Dc, cudaStream_t st);
 
