@@ -294,6 +294,25 @@ def test_lsh_reference_mode_every_row_fallback(cuda):
         assert any(c == n for c in counts) and any(c < n for c in counts), "not a mixed batch"
 
 
+def test_lsh_candidate_walks_agree(cuda):
+    """A query's candidate stream, and so its result, does not depend on its batch: a batch of 700 and the
+    same queries 50 at a time return identical ids, distances and counts (reference semantics: caps, flips,
+    per-chunk heaps)."""
+    w = synth.zipf_mixture(12000, 64, 700, c=24, lo=20, hi=2000, seed=6)
+    st = ivf_state.build_state(w.base, w.centres, w.assign, 3, 6, mg.projections_from_reference(3, 6, 64))
+    for n_probes, npc, rr, cap in ((3, 6, 40, -1), (0, 10, -1, -1), (6, 4, 100, 0)):
+        big = _ivf(threads=8)
+        big.import_state(st)
+        ids, d = big.search(w.queries, 20, n_probes, npc, rr, max_candidates=cap)
+        small = _ivf(threads=8)
+        small.import_state(st)
+        for s0 in range(0, 700, 50):
+            i2, d2 = small.search(w.queries[s0:s0 + 50], 20, n_probes, npc, rr, max_candidates=cap)
+            np.testing.assert_array_equal(ids[s0:s0 + 50], i2, err_msg=f"probes={n_probes} npc={npc} s0={s0}")
+            np.testing.assert_array_equal(d[s0:s0 + 50], d2)
+        assert big.total_distances_count() == small.total_distances_count()
+
+
 def test_lsh_exact_mode_every_row_batch_equals_alone(cuda):
     """Exact selection in a large batch redoes its every-row queries apart, split over the whole GPU:
     each query's ids and distances equal those of the query run alone."""
