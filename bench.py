@@ -440,7 +440,7 @@ def run_ours(args, rank, world, local):
     hf["recall"] = recall_evaluator(base, queries, t_ids if head == "tensor_core_exact" else o_ids, kth)
 
     # ---- end to end through the public API with host buffers (warmed up like the device steps: the first
-    # call sizes the index's own workspace and pinned staging buffers) ----
+    # call sizes the index's own device workspace) ----
     for _ in range(args.warmup):
         hf["host"]()
     barrier(world)
