@@ -7,16 +7,19 @@
 //
 // Structure (one CTA per SM, persistent over 128 x 256 output tiles, query tiles fastest so a base
 // tile is fetched from HBM once and reused from L2 by the query tiles that follow it):
-//   warp 0    TMA producer: 128x64 A and 256x64 B boxes (128-byte swizzle) into a 4-stage ring,
-//             mbarrier expect-tx completion; no multicast;
+//   warp 0    TMA producer: 128x64 A and 256x64 B boxes (128-byte swizzle) into a 4-stage ring
+//             (3 stages in the filter form), mbarrier expect-tx completion; no multicast;
 //   warp 1    allocates 512 TMEM columns (two 128 x 256 FP32 accumulators) and, from one thread,
 //             issues tcgen05.mma (kind::f16, BF16 in, FP32 out, M = 128, N = 256, K = 16 per
 //             instruction, 4 per stage); tcgen05.commit frees each stage and publishes each tile;
-//   warps 2-9 epilogue, two warps per TMEM lane quarter (warp w reads lanes 32 * (w % 4)), each
-//             taking half of the 256 columns: tcgen05.ld 2 x 32 columns per wait, then either store
-//             the keys (transposed through shared memory into coalesced rows) or, in filter mode,
-//             one predicate test per key against the row's bar; survivors go to the warp's own
-//             region at slots from a warp prefix sum (no atomics, nothing waits on memory).
+//   warps 2.. epilogue: 8 warps, two per TMEM lane quarter (warp w reads lanes 32 * (w % 4)), each
+//             taking half of the 256 columns, for the key-matrix and grouped forms; 16 warps, four
+//             per quarter taking 64 columns each, for the filter form, whose per-key test and
+//             survivor compaction are bound by issue latency at two warps per scheduler.
+//             tcgen05.ld 2 x 32 columns per wait, then either store the keys (transposed through
+//             shared memory into coalesced rows) or, in filter mode, one predicate test per key
+//             against the row's bar; survivors go to the warp's own region at slots from a warp
+//             prefix sum (no atomics, nothing waits on memory).
 // Every mbarrier wait is bounded (about 2 s); a timeout raises a device flag and the CTA winds down.
 #include <cuda.h>
 #include <cuda_fp8.h>
@@ -29,7 +32,7 @@ namespace annb {
 namespace {
 
 // A k-block is one 128-byte row per operand row: 64 BF16 or 128 E4M3 elements.
-constexpr int kBM = 128, kBN = 256, kBK = 64, kStages = 4;
+constexpr int kBM = 128, kBN = 256, kBK = 64;
 constexpr int kRowBytes = 128;
 constexpr int kABytes = kBM * kRowBytes;  // 16 KB
 constexpr int kBBytes = kBN * kRowBytes;  // 32 KB
@@ -57,10 +60,21 @@ __device__ __forceinline__ bool bar_try(uint64_t* b, uint32_t parity) {
                  : "memory");
     return ok != 0;
 }
+// try_wait that may suspend the thread for up to 0.1 ms (woken early when the phase completes), so a
+// waiting warp takes few issue slots from the epilogue warps that share its scheduler
+__device__ __forceinline__ bool bar_try_sleep(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity), "r"(100000u)
+        : "memory");
+    return ok != 0;
+}
 __device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, int* err) {
     if (bar_try(b, parity)) return true;
     const uint64_t t0 = gtimer();
-    while (!bar_try(b, parity))
+    while (!bar_try_sleep(b, parity))
         if (gtimer() - t0 > 2000000000ull) {
             if (err) atomicExch(err, 2);
             return false;
@@ -181,12 +195,23 @@ __device__ __forceinline__ GroupTile group_tile(const TcGemmArgs& a, int64_t t) 
     return gt;
 }
 
-constexpr int kEpiWarps = 8;
-constexpr int kThreads = 64 + 32 * kEpiWarps;
+// Epilogue warps of the key-matrix and grouped forms, and of the filter form; threads, pipeline stages
+// and shared memory (stages, 1 KB alignment slack, barriers, a 32 x 33 transpose area per warp) follow.
+constexpr int kKeyEpi = 8, kFilterEpi = 16;
+constexpr int epi_threads(int epi) { return 64 + 32 * epi; }
+constexpr int epi_stages(int epi) { return epi == kFilterEpi ? 3 : 4; }
+constexpr size_t epi_smem(int epi) {
+    return (size_t)epi_stages(epi) * (kABytes + kBBytes) + 1024 + 256 + (size_t)epi * 32 * 33 * 4;
+}
+static_assert(epi_smem(kKeyEpi) <= 232448 && epi_smem(kFilterEpi) <= 232448, "shared memory per CTA");
 
-template <int KIND>
-__global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
-                                                         const __grid_constant__ CUtensorMap tmB, TcGemmArgs a) {
+template <int KIND, int EPI>
+__global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                                     const __grid_constant__ CUtensorMap tmB,
+                                                                     TcGemmArgs a) {
+    constexpr int kStages = epi_stages(EPI);
+    constexpr int kCols = kBN / (EPI / 4);  // columns of a tile per epilogue warp
+    constexpr bool kFilterOnly = EPI == kFilterEpi;
     extern __shared__ unsigned char smem_raw[];
     // 1024-byte alignment for the swizzled tiles
     unsigned char* smem = smem_raw + ((1024 - (su32(smem_raw) & 1023)) & 1023);
@@ -198,7 +223,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     uint64_t* tempty = tfull + 2;
     uint64_t* done = tempty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
-    float* sT = reinterpret_cast<float*>(smem + kStages * (kABytes + kBBytes) + 256);  // [8 warps][32][33]
+    float* sT = reinterpret_cast<float*>(smem + kStages * (kABytes + kBBytes) + 256);  // [EPI warps][32][33]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int kBlockK = KindOf<KIND>::kBlockK, kMmaK = KindOf<KIND>::kMmaK;
@@ -214,7 +239,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         }
         for (int b = 0; b < 2; ++b) {
             bar_init(&tfull[b], 1);
-            bar_init(&tempty[b], 32 * kEpiWarps);
+            bar_init(&tempty[b], 32 * EPI);
         }
         bar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -287,9 +312,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     } else {  // epilogue warps 2..9
         const int lane_base = 32 * (warp & 3);
         const int ew = warp - 2;
-        const int col0 = 128 * (ew >> 2);  // this warp's half of the tile's columns
+        const int col0 = kCols * (ew >> 2);  // this warp's share of the tile's columns
         float* tw = sT + ew * 32 * 33;
-        const int64_t wbase = ((int64_t)blockIdx.x * kEpiWarps + ew) * a.wcap;
+        const int64_t wbase = ((int64_t)blockIdx.x * EPI + ew) * a.wcap;
         int wcount = 0;  // survivors met by this warp (uniform across the warp)
         int64_t acc = 0;
         for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x, ++acc) {
@@ -298,7 +323,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int m0 = (int)(t % mt) * kBM, n0 = (int)(t / mt) * kBN;
             const int m = m0 + lane_base + lane;
-            if (grouped) {  // keys of pair a0 + row, list rows b0 + column, to their stream positions
+            if (!kFilterOnly && grouped) {  // keys of pair a0 + row, list rows b0 + column, to their stream positions
                 const GroupTile gt = group_tile(a, t);
                 const int ml = lane_base + lane;
                 // the stream position of list row b0 for each of the warp's 32 pairs (lane r holds row r's)
@@ -306,7 +331,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                 const int rows = min(32, gt.am - lane_base);  // valid pairs of this warp
                 const uint32_t tb = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kBN + col0);
 #pragma unroll 1
-                for (int c = 0; c < 128; c += 64) {
+                for (int c = 0; c < kCols; c += 64) {
                     uint32_t r0[32], r1[32];
                     tmem_ld32(tb + (uint32_t)c, r0);
                     tmem_ld32(tb + (uint32_t)(c + 32), r1);
@@ -336,23 +361,30 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             const float rfac = (a.row_fac && m < a.M) ? a.row_fac[m] : 1.f;
             // rows past M (TMA zero fill) get a bar no key passes
             const float tau = (a.tau && m < a.M) ? a.tau[m] : -kInf;
+            const float tau_up = nextafterf(tau, kInf);
+            const float2 ntau2 = make_float2(-tau_up, -tau_up);
             const uint32_t tbase = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kBN + col0);
-            // filter mode with scaled operands: the warp's 128 column factors staged once per tile in its
-            // (otherwise unused) transpose buffer, read back as broadcasts
-            const bool staged = a.col_fac != nullptr && a.out == nullptr;
-            float2* sf = reinterpret_cast<float2*>(tw);
+            // filter mode with scaled operands: the warp's kCols column factors staged once per tile in
+            // its (otherwise unused) transpose buffer as two arrays (x then y), so that the factors of
+            // two adjacent columns load as one float2 broadcast
+            const bool staged = a.col_fac != nullptr && (kFilterOnly || a.out == nullptr);
+            float* sfx = tw;
+            float* sfy = tw + kCols;
             if (staged) {
                 __syncwarp();
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
+                for (int i = 0; i < kCols / 32; ++i) {
                     const int col = n0 + col0 + 32 * i + lane;
                     const int64_t nrow = (int64_t)(col / kBN) * kBN * a.b_tile_stride + col % kBN;
-                    sf[32 * i + lane] = col < a.N ? a.col_fac[nrow] : make_float2(0.f, 0.f);
+                    const float2 f = col < a.N ? a.col_fac[nrow] : make_float2(0.f, 0.f);
+                    sfx[32 * i + lane] = f.x;
+                    sfy[32 * i + lane] = f.y;
                 }
                 __syncwarp();
             }
+            const bool has_an = a.normA != nullptr;  // uniform
 #pragma unroll 1
-            for (int c = 0; c < 128; c += 64) {
+            for (int c = 0; c < kCols; c += 64) {
                 uint32_t r0[32], r1[32];
                 tmem_ld32(tbase + (uint32_t)c, r0);
                 tmem_ld32(tbase + (uint32_t)(c + 32), r1);
@@ -361,16 +393,30 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     float v[32];
+                    if (has_an) {
 #pragma unroll
-                    for (int u = 0; u < 32; ++u) v[u] = __uint_as_float(h ? r1[u] : r0[u]) + an;
+                        for (int u = 0; u < 32; ++u) v[u] = __uint_as_float(h ? r1[u] : r0[u]) + an;
+                    } else {
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) v[u] = __uint_as_float(h ? r1[u] : r0[u]);
+                    }
                     const int nb = n0 + col0 + c + 32 * h;  // output column of v[0]
-                    if (staged) {  // scaled operands: key = f.y + f.x * (row scale * accumulator)
+                    if (staged) {  // scaled operands: key = f.y + f.x * (row scale * accumulator), two at a time
+                        const float2 r2 = make_float2(rfac, rfac);
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) {
-                            const float2 f = sf[c + 32 * h + u];
-                            v[u] = fmaf(f.x, rfac * v[u], f.y);
+                        for (int u = 0; u < 32; u += 4) {
+                            const float4 fx = *reinterpret_cast<const float4*>(sfx + c + 32 * h + u);
+                            const float4 fy = *reinterpret_cast<const float4*>(sfy + c + 32 * h + u);
+                            const float2 t0 = __fmul2_rn(r2, make_float2(v[u], v[u + 1]));
+                            const float2 t1 = __fmul2_rn(r2, make_float2(v[u + 2], v[u + 3]));
+                            const float2 k0 = __ffma2_rn(make_float2(fx.x, fx.y), t0, make_float2(fy.x, fy.y));
+                            const float2 k1 = __ffma2_rn(make_float2(fx.z, fx.w), t1, make_float2(fy.z, fy.w));
+                            v[u] = k0.x;
+                            v[u + 1] = k0.y;
+                            v[u + 2] = k1.x;
+                            v[u + 3] = k1.y;
                         }
-                    } else if (a.col_fac) {
+                    } else if (!kFilterOnly && a.col_fac) {
                         const int col = nb + lane;  // output column -> base row (strided sample of 256-row tiles)
                         const int64_t nrow = (int64_t)(col / kBN) * kBN * a.b_tile_stride + col % kBN;
                         const float2 f = col < a.N ? a.col_fac[nrow] : make_float2(0.f, 0.f);
@@ -383,7 +429,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                         for (int u = 0; u < 32; ++u)
                             if (nb + u >= a.N) v[u] = __int_as_float(0x7fffffff);
                     }
-                    if (a.out) {
+                    if (!kFilterOnly && a.out) {
                         // transpose through shared memory so each store covers 32 consecutive columns
 #pragma unroll
                         for (int u = 0; u < 32; ++u) tw[lane * 33 + u] = v[u];
@@ -394,9 +440,21 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                         }
                         __syncwarp();
                     } else {
-                        uint32_t msk = 0;
+                        // v[u] <= tau exactly when v[u] - tau_up < 0 (tau_up the next float above tau: a
+                        // difference of two distinct floats is never +0, equal ones give +0, a NaN key
+                        // gives the positive default NaN), so the sign bits of packed differences, shifted
+                        // in by funnel shifts in four independent 8-key chains, form the mask
+                        uint32_t mq[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) msk |= (v[u] <= tau ? 1u : 0u) << u;
+                        for (int j = 0; j < 4; ++j) {
+#pragma unroll
+                            for (int u = 7; u >= 1; u -= 2) {
+                                const float2 d = __fadd2_rn(make_float2(v[8 * j + u - 1], v[8 * j + u]), ntau2);
+                                mq[j] = __funnelshift_l(__float_as_uint(d.y), mq[j], 1);
+                                mq[j] = __funnelshift_l(__float_as_uint(d.x), mq[j], 1);
+                            }
+                        }
+                        uint32_t msk = (mq[0] | (mq[1] << 8)) | ((mq[2] << 16) | (mq[3] << 24));
                         if (__any_sync(0xffffffffu, msk != 0)) {
                             const int cnt = __popc(msk);
                             int incl = cnt;
@@ -411,10 +469,17 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                                 const int u = __ffs(msk) - 1;
                                 msk &= msk - 1;
                                 if (slot < a.wcap) {
-                                    float kv = 0.f;
+                                    // v[u] for a run-time u: a five-level select tree on u's bits
+                                    float s16[16], s8[8], s4[4], s2[2];
 #pragma unroll
-                                    for (int z = 0; z < 32; ++z)
-                                        if (z == u) kv = v[z];
+                                    for (int z = 0; z < 16; ++z) s16[z] = (u & 16) ? v[z + 16] : v[z];
+#pragma unroll
+                                    for (int z = 0; z < 8; ++z) s8[z] = (u & 8) ? s16[z + 8] : s16[z];
+#pragma unroll
+                                    for (int z = 0; z < 4; ++z) s4[z] = (u & 4) ? s8[z + 4] : s8[z];
+#pragma unroll
+                                    for (int z = 0; z < 2; ++z) s2[z] = (u & 2) ? s4[z + 2] : s4[z];
+                                    const float kv = (u & 1) ? s2[1] : s2[0];
                                     a.fkey[wbase + slot] = kv;
                                     a.fcol[wbase + slot] = nb + u;
                                     a.frow[wbase + slot] = m;
@@ -428,7 +493,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             bar_arrive(&tempty[b]);
         }
-        if (a.wcount && lane == 0) a.wcount[(int64_t)blockIdx.x * kEpiWarps + ew] = wcount;
+        if (a.wcount && lane == 0) a.wcount[(int64_t)blockIdx.x * EPI + ew] = wcount;
     }
     __syncthreads();
     if (warp == 1) {
@@ -477,12 +542,21 @@ int make_map(CUtensorMap* tm, const void* base, int64_t rows, int cols, int box_
 
 }  // namespace
 
-size_t tc_gemm_smem() { return (size_t)kStages * (kABytes + kBBytes) + 1024 + 256 + kEpiWarps * 32 * 33 * 4; }
+size_t tc_gemm_smem() { return std::max(epi_smem(kKeyEpi), epi_smem(kFilterEpi)); }
 
 int tc_kpad(int dim, int metric) { return (int)ceil_div(dim + (metric == ANN_METRIC_L2 ? 3 : 0), 16) * 16; }
 
 static int tc_grid(int M, int N) { return (int)std::min<int64_t>(ceil_div(M, kBM) * ceil_div(N, kBN), kNumSMs); }
-int tc_filter_warps(int M, int N) { return tc_grid(M, N) * kEpiWarps; }
+int tc_filter_warps(int M, int N) { return tc_grid(M, N) * kFilterEpi; }
+
+template <int KIND, int EPI>
+static cudaError_t run_tc_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcGemmArgs& a, int grid,
+                               cudaStream_t st) {
+    const cudaError_t e = smem_optin(reinterpret_cast<const void*>(tc_gemm_kernel<KIND, EPI>));
+    if (e != cudaSuccess) return e;
+    tc_gemm_kernel<KIND, EPI><<<grid, epi_threads(EPI), epi_smem(EPI), st>>>(tmA, tmB, a);
+    return cudaSuccess;
+}
 
 int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream_t st) {
     const int step = a.kind == kTcBF16 ? 16 : 32;
@@ -508,15 +582,16 @@ int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream
     if (rc) return rc;
     rc = make_map(&tmB, B, b_rows, a.K, kBN, a.kind);
     if (rc) return rc;
-    const size_t smem = tc_gemm_smem();
     const int grid = a.g_item_off ? kNumSMs : tc_grid(a.M, a.N);  // grouped: persistent over the items
-    if (a.kind == kTcBF16) {
-        ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(tc_gemm_kernel<kTcBF16>)));
-        tc_gemm_kernel<kTcBF16><<<grid, kThreads, smem, st>>>(tmA, tmB, a);
-    } else {
-        ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(tc_gemm_kernel<kTcE4M3>)));
-        tc_gemm_kernel<kTcE4M3><<<grid, kThreads, smem, st>>>(tmA, tmB, a);
-    }
+    const bool filter = a.out == nullptr;
+    cudaError_t e;
+    if (a.kind == kTcBF16)
+        e = filter ? run_tc_gemm<kTcBF16, kFilterEpi>(tmA, tmB, a, grid, st)
+                   : run_tc_gemm<kTcBF16, kKeyEpi>(tmA, tmB, a, grid, st);
+    else
+        e = filter ? run_tc_gemm<kTcE4M3, kFilterEpi>(tmA, tmB, a, grid, st)
+                   : run_tc_gemm<kTcE4M3, kKeyEpi>(tmA, tmB, a, grid, st);
+    ANN_CUDA_TRY(e);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }
