@@ -659,14 +659,15 @@ def serving_c5(args, local, ivf, npc, w3):
 
 def scaled_fp8_c4(args, local):
     """The scaled-FP8 configuration: 4,000,000 x 256, 4,096-centre mixture (sigma 0.4), not normalised
-    (norms spread 0.5-2.0), 20,000 queries, squared L2, k = 100, exact FP32 re-rank of the best 500.
+    (norms spread 0.5-2.0), 20,000 queries, squared L2, k = 100, exact FP32 re-rank of the best 500
+    (--fp8-rows / --fp8-batch give a smaller case of the same data, for profiling).
     The tensor-core exact search with E4M3 operands (a scale per vector, FP32 accumulation) beside the
     same search with BF16 operands; recall@100 against the FP64 exact top-100 of the first 500 queries."""
     import torch
     from annvedi_b200 import synth
     from annvedi_b200.linear import LinearIndex
     dev = f"cuda:{local}"
-    n, d, nq, R = 4_000_000, 256, 20_000, 500
+    n, d, nq, R = getattr(args, "fp8_rows", 4_000_000), 256, getattr(args, "fp8_batch", 20_000), 500
     w = synth.scaled_mixture(n, d, nq, c=4096, sigma=0.4, seed=5, backend="torch", device=dev)
     xb = w.base.double()
     qs = w.queries[:500].double()
@@ -678,8 +679,8 @@ def scaled_fp8_c4(args, local):
     stream = torch.cuda.current_stream()
     ids = torch.empty(nq, K_NN, dtype=torch.int64, device=dev)
     dist = torch.empty(nq, K_NN, dtype=torch.float32, device=dev)
-    out = {"workload": "4M x 256 scaled mixture (4,096 centres, sigma 0.4, norms 0.5-2.0), 20k-query batches, "
-                       "squared L2, k=100, re-rank of the best 500"}
+    out = {"workload": f"{n:,} x 256 scaled mixture (4,096 centres, sigma 0.4, norms 0.5-2.0), {nq:,}-query "
+                       "batches, squared L2, k=100, re-rank of the best 500"}
     for prec in ("e4m3", "bf16"):
         ix.set_tc_precision(prec)
         step = lambda: ix.search_tc(w.queries, K_NN, refine_r=R, out_ids=ids, out_dists=dist)
@@ -900,6 +901,8 @@ def main():
                     help="forms to measure (the default measures all; one form alone is for profiling it)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="per offered rate; 0 skips serving")
     ap.add_argument("--no-fp8", dest="fp8", action="store_false", help="skip the scaled-FP8 configuration")
+    ap.add_argument("--fp8-rows", type=int, default=4_000_000, help="rows of the scaled-FP8 configuration")
+    ap.add_argument("--fp8-batch", type=int, default=20_000, help="queries per batch of the scaled-FP8 configuration")
     ap.add_argument("--no-lsh", dest="lsh", action="store_false", help="skip the LSH bucket-table settings")
     ap.add_argument("--no-dropin", dest="dropin", action="store_false",
                     help="skip the one-query-per-call drop-in measurement (100k x 384, backend linear)")
