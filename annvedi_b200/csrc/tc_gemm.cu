@@ -7,8 +7,8 @@
 //
 // Structure (one CTA per SM, persistent over 128 x 256 output tiles, query tiles fastest so a base
 // tile is fetched from HBM once and reused from L2 by the query tiles that follow it):
-//   warp 0    TMA producer: 128x64 A and 256x64 B boxes (128-byte swizzle) into a 4-stage ring
-//             (3 stages in the filter form), mbarrier expect-tx completion; no multicast;
+//   warp 0    TMA producer: 128x64 A and 256x64 B boxes (128-byte swizzle) into a 4-stage ring,
+//             mbarrier expect-tx completion; no multicast;
 //   warp 1    allocates 512 TMEM columns (two 128 x 256 FP32 accumulators) and, from one thread,
 //             issues tcgen05.mma (kind::f16, BF16 in, FP32 out, M = 128, N = 256, K = 16 per
 //             instruction, 4 per stage); tcgen05.commit frees each stage and publishes each tile;
@@ -195,13 +195,15 @@ __device__ __forceinline__ GroupTile group_tile(const TcGemmArgs& a, int64_t t) 
     return gt;
 }
 
-// Epilogue warps of the key-matrix and grouped forms, and of the filter form; threads, pipeline stages
-// and shared memory (stages, 1 KB alignment slack, barriers, a 32 x 33 transpose area per warp) follow.
+// Epilogue warps of the key-matrix and grouped forms, and of the filter form; threads and shared memory
+// (4 stages, 1 KB alignment slack, barriers, a per-warp area: a 32 x 33 transpose area, or in the filter
+// form only its column factors, x and y) follow.
+constexpr int kStages = 4;
 constexpr int kKeyEpi = 8, kFilterEpi = 16;
 constexpr int epi_threads(int epi) { return 64 + 32 * epi; }
-constexpr int epi_stages(int epi) { return epi == kFilterEpi ? 3 : 4; }
+constexpr int epi_area_floats(int epi) { return epi == kFilterEpi ? 2 * (kBN / (epi / 4)) : 32 * 33; }
 constexpr size_t epi_smem(int epi) {
-    return (size_t)epi_stages(epi) * (kABytes + kBBytes) + 1024 + 256 + (size_t)epi * 32 * 33 * 4;
+    return (size_t)kStages * (kABytes + kBBytes) + 1024 + 256 + (size_t)epi * epi_area_floats(epi) * 4;
 }
 static_assert(epi_smem(kKeyEpi) <= 232448 && epi_smem(kFilterEpi) <= 232448, "shared memory per CTA");
 
@@ -209,7 +211,6 @@ template <int KIND, int EPI>
 __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
                                                                      const __grid_constant__ CUtensorMap tmB,
                                                                      TcGemmArgs a) {
-    constexpr int kStages = epi_stages(EPI);
     constexpr int kCols = kBN / (EPI / 4);  // columns of a tile per epilogue warp
     constexpr bool kFilterOnly = EPI == kFilterEpi;
     extern __shared__ unsigned char smem_raw[];
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
     uint64_t* tempty = tfull + 2;
     uint64_t* done = tempty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
-    float* sT = reinterpret_cast<float*>(smem + kStages * (kABytes + kBBytes) + 256);  // [EPI warps][32][33]
+    float* sT = reinterpret_cast<float*>(smem + kStages * (kABytes + kBBytes) + 256);  // [EPI warps][area]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int kBlockK = KindOf<KIND>::kBlockK, kMmaK = KindOf<KIND>::kMmaK;
@@ -313,7 +314,7 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
         const int lane_base = 32 * (warp & 3);
         const int ew = warp - 2;
         const int col0 = kCols * (ew >> 2);  // this warp's share of the tile's columns
-        float* tw = sT + ew * 32 * 33;
+        float* tw = sT + ew * epi_area_floats(EPI);
         const int64_t wbase = ((int64_t)blockIdx.x * EPI + ew) * a.wcap;
         int wcount = 0;  // survivors met by this warp (uniform across the warp)
         int64_t acc = 0;
