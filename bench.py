@@ -553,6 +553,8 @@ def run_ours(args, rank, world, local):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and ivf is not None:
         line["cpu_baseline"] = cpu_baseline_ivf(ivf, queries, npc if npc is not None else npc_tc, args)
+    if rank == 0 and world == 1 and args.ref_gpu:
+        line["reference_gpu_kernel"] = reference_gpu_filter_c3(args, base, queries, kth)
     if rank == 0 and world == 1 and args.fp8:
         line["scaled_fp8_4m_256"] = scaled_fp8_c4(args, local)
     if rank == 0 and world == 1 and args.serve_seconds > 0 and npc is not None:
@@ -801,6 +803,64 @@ def _reference_ivf_from(ivf):
     return ix, st
 
 
+def reference_gpu_filter_c3(args, base, queries, kth):
+    """The reference's own GPU contestant (competitors/gpu_filter/src/gpu_filter.cu), built from its
+    source for sm_100a into oracle/_ref/gpu/ (oracle/Makefile), driven through its C ABI the way its
+    algorithm.py drives it: gf_create over the headline rows, then gf_query one query per call -- a
+    full-N SQ8 scan (one thread per row, dim-major codes), a CUB radix sort of all N keys, the best R
+    ids copied back and re-ranked in FP32 on the host. A baseline leg, like cpu_baseline: measured
+    beside this build's forms, never part of them. The ABI is synchronous, so the figure is wall time
+    over a bounded sample of queries (after 3 warm-up calls), with R = the headline re-rank depth."""
+    import ctypes
+    path = os.path.join(ROOT, "oracle", "_ref", "gpu", "libgpufilter.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/gpu/libgpufilter.so not built (needs the reference sources)"}
+    lib = ctypes.CDLL(path)
+    lib.gf_create.restype = ctypes.c_void_p
+    lib.gf_create.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_long, ctypes.c_long]
+    lib.gf_query.restype = ctypes.c_int
+    lib.gf_query.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int,
+                             ctypes.POINTER(ctypes.c_longlong)]
+    lib.gf_ndist.restype = ctypes.c_longlong
+    lib.gf_ndist.argtypes = [ctypes.c_void_p]
+    lib.gf_free.argtypes = [ctypes.c_void_p]
+    lib.gf_last_error.restype = ctypes.c_char_p
+    import torch
+    train = np.ascontiguousarray(base.cpu().numpy(), dtype=np.float32)  # borrowed by the handle
+    n, d = train.shape
+    t0 = time.perf_counter()
+    h = lib.gf_create(train.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n, d)
+    fit_s = time.perf_counter() - t0
+    if not h:
+        return {"unavailable": "gf_create: " + lib.gf_last_error().decode()}
+    try:
+        ns = min(args.ref_gpu_sample, queries.shape[0])
+        qs = np.ascontiguousarray(queries[:ns].cpu().numpy(), dtype=np.float32)
+        out = np.empty((ns, K_NN), np.int64)
+        r = args.refine
+
+        def one(i):
+            got = lib.gf_query(h, qs[i].ctypes.data_as(ctypes.POINTER(ctypes.c_float)), K_NN, r,
+                               out[i].ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)))
+            if got != K_NN:
+                raise RuntimeError("gf_query: " + lib.gf_last_error().decode())
+
+        for i in range(min(3, ns)):
+            one(i)
+        t0 = time.perf_counter()
+        for i in range(ns):
+            one(i)
+        dt = time.perf_counter() - t0
+        ids = torch.from_numpy(out).to(queries.device)
+        rec = recall_evaluator(base, queries[:ns], ids, kth[:ns])
+        return {"impl": "reference gpu_filter (competitors/gpu_filter/src/gpu_filter.cu, nvcc sm_100a)",
+                "qps": round(ns / dt, 1), "ms_per_query": round(dt / ns * 1e3, 4), "recall_at_100": round(rec, 4),
+                "refine_r": r, "sample": f"{ns} queries of the headline batch, one per call, wall clock",
+                "fit_s": round(fit_s, 2), "distances_per_query": int(lib.gf_ndist(h)) // (ns + min(3, ns))}
+    finally:
+        lib.gf_free(h)
+
+
 def cpu_baseline_ivf(ivf, queries, npc, args):
     """Reference IVF query on the host cores over a bounded sample. refine_r is raised until the
     reference's candidate cap (max(2000, 4 * refine_r)) no longer truncates the probed lists, so it
@@ -902,6 +962,9 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="per offered rate; 0 skips serving")
     ap.add_argument("--no-fp8", dest="fp8", action="store_false", help="skip the scaled-FP8 configuration")
     ap.add_argument("--fp8-rows", type=int, default=4_000_000, help="rows of the scaled-FP8 configuration")
+    ap.add_argument("--no-ref-gpu", dest="ref_gpu", action="store_false",
+                    help="skip timing the reference's own GPU kernel (gpu_filter) on the headline data")
+    ap.add_argument("--ref-gpu-sample", type=int, default=200, help="queries of the reference GPU kernel's sample")
     ap.add_argument("--fp8-batch", type=int, default=20_000, help="queries per batch of the scaled-FP8 configuration")
     ap.add_argument("--no-lsh", dest="lsh", action="store_false", help="skip the LSH bucket-table settings")
     ap.add_argument("--no-dropin", dest="dropin", action="store_false",
