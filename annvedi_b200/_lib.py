@@ -103,6 +103,13 @@ SIGNATURES = [
     ("ann_ivf_set_profiling", ctypes.c_int, [_vp, _i32]),
     ("ann_ivf_profile", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
     ("ann_ivf_reset_profile", ctypes.c_int, [_vp]),
+    # the reference GPU contestant's ABI (include/annvedi_gpu_filter.h)
+    ("gf_last_error", ctypes.c_char_p, []),
+    ("gf_create", _vp, [ctypes.POINTER(ctypes.c_float), ctypes.c_long, ctypes.c_long]),
+    ("gf_query", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int,
+                                ctypes.POINTER(ctypes.c_longlong)]),
+    ("gf_ndist", ctypes.c_longlong, [_vp]),
+    ("gf_free", None, [_vp]),
 ]
 
 

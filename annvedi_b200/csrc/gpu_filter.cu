@@ -1,0 +1,496 @@
+// The reference's GPU quantized-filter contestant (competitors/gpu_filter/src/gpu_filter.cu) served by B200
+// kernels behind its own C ABI (include/annvedi_gpu_filter.h).
+//
+// The reference, per query: one thread per row sums (code * scale - qshift)^2 over dim-major SQ8 codes
+// (:52-63), a CUB radix sort orders all N (key, row) pairs, the first R row ids come back to the host,
+// and the host re-ranks them in FP32 from the borrowed train array and partial-sorts (distance, id)
+// pairs (:135-176). Here, per query:
+//   gf_scan_kernel     the same key with the same FMA chain per row (4 rows per thread, one 32-bit load
+//                      of 4 codes per dimension, scale and q - offset staged in shared memory) -- HBM-
+//                      bound, N * dim code bytes per query;
+//   selection          the R rows with the smallest (key, row) -- the rows the reference's stable
+//                      ascending sort puts first -- in two stages: radix selection (radix_select.cu)
+//                      of each of up to 64 row segments' R smallest as a set (ties to the lower row),
+//                      in parallel, then the R smallest of their union as 64-bit keys (key bits << 32 |
+//                      row, exact for the non-negative keys) in gf_topk_kernel; one segment when the
+//                      base is small or R is above the top-k kernel's bound;
+//   gf_rerank_kernel   each candidate's FP32 squared distance from a device copy of train, with the
+//                      reference's host arithmetic (v = p - q, acc = acc + v * v, no fused multiply-add);
+//   gf_topk_kernel     the best k (distance, id) pairs in ascending order, as 64-bit keys
+//                      (distance bits << 32 | id) bitonic-sorted in shared memory, chunk by chunk with
+//                      the running best k kept in front.
+// Only the query (dim floats) goes in and the k ids come out.
+//
+// Build (gf_create): exact per-dimension min / max (ivf_build.cu), the scale and offset formed on the host
+// with the reference's expressions (:103-117), then gf_encode_kernel quantises with a true division and
+// round-half-even (lrintf, :119-127) into the dim-major layout the scan reads.
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "../../include/annvedi_gpu_filter.h"
+#include "common.cuh"
+#include "ivf.cuh"
+#include "radix_select.cuh"
+#include "runtime.cuh"
+
+namespace annb {
+namespace {
+
+constexpr int kGfMaxDim = 4096;  // the reference's __constant__ arrays bound dim (:49-50, :80-83)
+constexpr int kGfMaxK = 4096;
+constexpr int kGfSortCap = 8192;  // 64-bit keys in the top-k kernel's shared buffer (64 KB)
+constexpr int kGfMaxSeg = 64;     // row segments of the first selection stage
+constexpr int64_t kGfSegRows = 32768;  // rows per segment, at least
+
+__global__ void gf_encode_kernel(const float* __restrict__ x, int64_t n, int dim, int64_t npad,
+                                 const float* __restrict__ scale, const float* __restrict__ offset,
+                                 uint8_t* __restrict__ codes) {
+    // one thread per (dimension d, row i), rows fastest: the stores of a warp are 32 consecutive bytes
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= npad * dim) return;
+    const int d = (int)(t / npad);
+    const int64_t i = t - (int64_t)d * npad;
+    int c = 0;
+    if (i < n) {
+        const int v = __float2int_rn(__fdiv_rn(__fsub_rn(x[i * dim + d], offset[d]), scale[d]));
+        c = max(0, min(255, v));
+    }
+    codes[t] = (uint8_t)c;
+}
+
+// dist[i] = sum_d fma(code[d][i], scale[d], -(q[d] - offset[d]))^2, accumulated with fma in dimension
+// order; thread t takes rows 4t .. 4t + 3 (npad a multiple of 4; rows past n get keys nobody reads).
+__global__ void __launch_bounds__(256) gf_scan_kernel(const uint8_t* __restrict__ codes, int64_t npad, int dim,
+                                                      const float* __restrict__ scale,
+                                                      const float* __restrict__ offset,
+                                                      const float* __restrict__ q, float* __restrict__ dist) {
+    extern __shared__ float gf_sm[];
+    float* ssc = gf_sm;         // [dim]
+    float* snq = gf_sm + dim;   // [dim] -(q - offset)
+    for (int d = threadIdx.x; d < dim; d += blockDim.x) {
+        ssc[d] = scale[d];
+        snq[d] = -__fsub_rn(q[d], offset[d]);
+    }
+    __syncthreads();
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t quads = npad >> 2;
+    if (t >= quads) return;
+    const uchar4* col = reinterpret_cast<const uchar4*>(codes) + t;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll 16
+    for (int d = 0; d < dim; ++d) {
+        const uchar4 c = __ldcs(col + (int64_t)d * quads);
+        const float s = ssc[d], nq = snq[d];
+        const float v0 = fmaf((float)c.x, s, nq);
+        const float v1 = fmaf((float)c.y, s, nq);
+        const float v2 = fmaf((float)c.z, s, nq);
+        const float v3 = fmaf((float)c.w, s, nq);
+        a0 = fmaf(v0, v0, a0);
+        a1 = fmaf(v1, v1, a1);
+        a2 = fmaf(v2, v2, a2);
+        a3 = fmaf(v3, v3, a3);
+    }
+    reinterpret_cast<float4*>(dist)[t] = make_float4(a0, a1, a2, a3);
+}
+
+// One warp per candidate (two per CTA): the warp brings the candidate's row into shared memory with
+// coalesced loads, then one lane applies the reference's host re-rank arithmetic (a rounded product,
+// then a rounded sum, in dimension order); the distance and the row id go out as one ordered 64-bit key.
+constexpr int kGfRerankWarps = 2;
+__global__ void __launch_bounds__(32 * kGfRerankWarps) gf_rerank_kernel(const float* __restrict__ base, int64_t n,
+                                                                        int dim, const float* __restrict__ q,
+                                                                        const int* __restrict__ cand, int r,
+                                                                        unsigned long long* __restrict__ keys) {
+    extern __shared__ float gf_rs[];  // [dim] query, then [kGfRerankWarps][dim] rows
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int d = threadIdx.x; d < dim; d += blockDim.x) gf_rs[d] = q[d];
+    const int j = blockIdx.x * kGfRerankWarps + warp;
+    const int id = j < r ? cand[j] : -1;
+    const bool ok = j < r && id >= 0 && (int64_t)id < n;
+    float* row = gf_rs + dim + warp * dim;
+    if (ok) {
+        const float* p = base + (int64_t)id * dim;
+        for (int d = lane; d < dim; d += 32) row[d] = p[d];
+    }
+    __syncthreads();
+    if (j >= r || lane != 0) return;
+    if (!ok) {
+        keys[j] = ~0ull;
+        return;
+    }
+    float acc = 0.f;
+#pragma unroll 8
+    for (int d = 0; d < dim; ++d) {
+        const float v = __fsub_rn(row[d], gf_rs[d]);
+        acc = __fadd_rn(acc, __fmul_rn(v, v));
+    }
+    keys[j] = ((unsigned long long)__float_as_uint(acc) << 32) | (unsigned)id;
+}
+
+// kth[s] = segment s's R-th smallest key: the largest key of its selected set (the set is its R
+// smallest), or +inf when the set is padded (a segment shorter than R bounds nothing). One CTA per segment.
+__global__ void __launch_bounds__(256) gf_kth_kernel(const float* __restrict__ selk, const int* __restrict__ selp,
+                                                     int R, float* __restrict__ kth) {
+    __shared__ float sMax[8];
+    __shared__ int sPad[8];
+    const int64_t base = (int64_t)blockIdx.x * R;
+    float m = -kInf;
+    bool pad = false;
+    for (int j = threadIdx.x; j < R; j += blockDim.x) {
+        const int p = selp[base + j];
+        const float kv = selk[base + j];
+        if (p < 0 || p == kNoId || !(kv < kInf))
+            pad = true;
+        else
+            m = fmaxf(m, kv);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const bool wpad = __any_sync(0xffffffffu, pad);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        sMax[warp] = m;
+        sPad[warp] = wpad ? 1 : 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float mm = -kInf;
+        int pp = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            mm = fmaxf(mm, sMax[w]);
+            pp |= sPad[w];
+        }
+        kth[blockIdx.x] = pp ? kInf : mm;
+    }
+}
+
+// Segment s's selected set (keys and in-segment positions, R per segment, +inf / kNoId padding) as
+// 64-bit keys: key bits << 32 | (segment start + position), padding as the largest key, all of them
+// into keys[j]; and those at or below the bar -- the smallest segment R-th key, which the union's R-th
+// smallest key cannot exceed (a segment alone holds R keys at or below its own) -- appended to near[]
+// at slots from an atomic counter (their order does not matter: the next step sorts them).
+__global__ void gf_pack_kernel(const float* __restrict__ selk, const int* __restrict__ selp,
+                               const int64_t* __restrict__ offs, const float* __restrict__ kth, int nseg, int R,
+                               unsigned long long* __restrict__ keys, unsigned long long* __restrict__ near,
+                               int cap, int* __restrict__ count) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= (int64_t)nseg * R) return;
+    float bar = kInf;
+    for (int s2 = 0; s2 < nseg; ++s2) bar = fminf(bar, kth[s2]);
+    const int p = selp[j];
+    const float kv = selk[j];
+    const bool real = p >= 0 && p != kNoId && kv < kInf;
+    const unsigned long long key =
+        real ? ((unsigned long long)__float_as_uint(kv) << 32) | (unsigned)(offs[j / R] + p) : ~0ull;
+    keys[j] = key;
+    if (real && kv <= bar) {
+        const int slot = atomicAdd(count, 1);
+        if (slot < cap) near[slot] = key;
+    }
+}
+
+// The k smallest of r 64-bit keys, ascending, into out (the low 32 bits: row ids). P (a power of two,
+// <= kGfSortCap) keys sit in shared memory: the running best k in front, then the next P - k keys;
+// each round bitonic-sorts all P.
+// With count set: when the near set fits (*count <= cap) it replaces keys (r = *count). P is the
+// smallest power of two >= min(r + k, Pmax), Pmax the keys the launch's shared memory holds.
+template <typename OutT>
+__global__ void __launch_bounds__(512) gf_topk_kernel(const unsigned long long* __restrict__ keys, int r,
+                                                      const unsigned long long* __restrict__ near,
+                                                      const int* __restrict__ count, int cap, int k, int Pmax,
+                                                      OutT* __restrict__ out) {
+    extern __shared__ unsigned long long gf_buf[];
+    if (count != nullptr) {
+        const int c = *count;
+        if (c <= cap) {
+            keys = near;
+            r = c;
+        }
+    }
+    int P = 64;
+    while (P < min(r + k, Pmax)) P <<= 1;
+    const int C = P - k;
+    for (int i = threadIdx.x; i < k; i += blockDim.x) gf_buf[i] = ~0ull;
+    for (int b0 = 0; b0 < r; b0 += C) {
+        for (int i = threadIdx.x; i < C; i += blockDim.x) gf_buf[k + i] = b0 + i < r ? keys[b0 + i] : ~0ull;
+        __syncthreads();
+        for (int size = 2; size <= P; size <<= 1) {
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                for (int t = threadIdx.x; t < (P >> 1); t += blockDim.x) {
+                    const int i = 2 * t - (t & (stride - 1));
+                    const int j = i + stride;
+                    const unsigned long long a = gf_buf[i], b = gf_buf[j];
+                    if ((a > b) == ((i & size) == 0)) {
+                        gf_buf[i] = b;
+                        gf_buf[j] = a;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+    }
+    for (int i = threadIdx.x; i < k; i += blockDim.x) out[i] = (OutT)(unsigned)(gf_buf[i] & 0xffffffffull);
+}
+
+}  // namespace
+}  // namespace annb
+
+using namespace annb;
+
+struct gf_handle {
+    int64_t n = 0, npad = 0;
+    int dim = 0, device = 0;
+    cudaStream_t st = nullptr;
+    uint8_t* codes = nullptr;  // [dim][npad], dim-major
+    float* base = nullptr;     // [n][dim] FP32 copy of train (the re-rank's rows)
+    float* scale = nullptr;    // [dim]
+    float* offset = nullptr;   // [dim]
+    float* q = nullptr;        // [dim]
+    float* dist = nullptr;     // [npad]
+    float* selk = nullptr;     // [rcap]
+    int* seli = nullptr;       // [rcap]
+    unsigned long long* keys = nullptr;  // [rcap]
+    long long* out = nullptr;  // [kGfMaxK]
+    int64_t* segs = nullptr;   // [2][kGfMaxSeg] segment starts and lengths (fixed by n)
+    float* kth = nullptr;      // [kGfMaxSeg] each segment's R-th smallest key
+    int* count = nullptr;      // the near set's size
+    unsigned long long* near = nullptr;  // [kGfSortCap] keys at or below the bar
+    int nseg = 1;              // first-stage segments when R <= kGfMaxK
+    float* hq = nullptr;       // pinned staging: the query
+    long long* hout = nullptr; // pinned staging: the ids
+    int64_t rcap = 0;
+    std::atomic<long long> ndist{0};
+    std::mutex mu;
+};
+
+namespace {
+
+void gf_release(gf_handle* h) {
+    DeviceGuard g(h->device);
+    for (void* p : {(void*)h->codes, (void*)h->base, (void*)h->scale, (void*)h->offset, (void*)h->q, (void*)h->dist,
+                    (void*)h->selk, (void*)h->seli, (void*)h->keys, (void*)h->out, (void*)h->segs, (void*)h->kth,
+                    (void*)h->count, (void*)h->near})
+        if (p) cudaFree(p);
+    if (h->hq) cudaFreeHost(h->hq);
+    if (h->hout) cudaFreeHost(h->hout);
+    if (h->st) cudaStreamDestroy(h->st);
+}
+
+int gf_build(gf_handle* h, const float* train) {
+    const int64_t n = h->n;
+    const int dim = h->dim;
+    ANN_CUDA_TRY(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    ANN_CUDA_TRY(cudaMalloc(&h->base, sizeof(float) * (size_t)n * dim));
+    ANN_CUDA_TRY(cudaMalloc(&h->codes, (size_t)h->npad * dim));
+    ANN_CUDA_TRY(cudaMalloc(&h->scale, sizeof(float) * dim));
+    ANN_CUDA_TRY(cudaMalloc(&h->offset, sizeof(float) * dim));
+    ANN_CUDA_TRY(cudaMalloc(&h->q, sizeof(float) * dim));
+    ANN_CUDA_TRY(cudaMalloc(&h->dist, sizeof(float) * (size_t)h->npad));
+    ANN_CUDA_TRY(cudaMalloc(&h->out, sizeof(long long) * kGfMaxK));
+    ANN_CUDA_TRY(cudaMalloc(&h->segs, sizeof(int64_t) * 2 * kGfMaxSeg));
+    ANN_CUDA_TRY(cudaMalloc(&h->kth, sizeof(float) * kGfMaxSeg));
+    ANN_CUDA_TRY(cudaMalloc(&h->count, sizeof(int)));
+    ANN_CUDA_TRY(cudaMalloc(&h->near, sizeof(unsigned long long) * kGfSortCap));
+    ANN_CUDA_TRY(cudaHostAlloc(&h->hq, sizeof(float) * dim, cudaHostAllocDefault));
+    ANN_CUDA_TRY(cudaHostAlloc(&h->hout, sizeof(long long) * kGfMaxK, cudaHostAllocDefault));
+    // first-stage segments: about kGfSegRows rows each, at most kGfMaxSeg
+    h->nseg = (int)std::clamp<int64_t>(n / kGfSegRows, 1, kGfMaxSeg);
+    std::vector<int64_t> seg(2 * kGfMaxSeg, 0);
+    const int64_t L = ceil_div(n, h->nseg);
+    for (int s2 = 0; s2 < h->nseg; ++s2) {
+        seg[s2] = s2 * L;
+        seg[kGfMaxSeg + s2] = std::max<int64_t>(0, std::min(n, (s2 + 1) * L) - s2 * L);
+    }
+    ANN_CUDA_TRY(cudaMemcpyAsync(h->segs, seg.data(), sizeof(int64_t) * 2 * kGfMaxSeg, cudaMemcpyHostToDevice, h->st));
+    ANN_CUDA_TRY(cudaMemcpyAsync(h->base, train, sizeof(float) * (size_t)n * dim, cudaMemcpyHostToDevice, h->st));
+    // exact per-dimension minimum and maximum, then the reference's scale and offset (host FP32)
+    float *mn = nullptr, *mx = nullptr;
+    ANN_CUDA_TRY(cudaMalloc(&mn, sizeof(float) * dim * 2));
+    mx = mn + dim;
+    int rc = launch_sq8_minmax(h->base, n, dim, dim, mn, mx, h->st);
+    std::vector<float> hmn(dim), hmx(dim), sc(dim), off(dim);
+    if (rc == ANN_OK) {
+        cudaError_t e = cudaMemcpyAsync(hmn.data(), mn, sizeof(float) * dim, cudaMemcpyDeviceToHost, h->st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hmx.data(), mx, sizeof(float) * dim, cudaMemcpyDeviceToHost, h->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+        if (e != cudaSuccess) {
+            set_error("CUDA error %s (%s) at %s:%d", cudaGetErrorName(e), cudaGetErrorString(e), __FILE__, __LINE__);
+            rc = ANN_ERR_CUDA;
+        }
+    }
+    cudaFree(mn);
+    if (rc) return rc;
+    for (int d = 0; d < dim; ++d) {
+        const float range = hmx[d] - hmn[d];
+        sc[d] = range > 1e-8f ? range / 255.0f : 1.0f;
+        off[d] = hmn[d];
+    }
+    ANN_CUDA_TRY(cudaMemcpyAsync(h->scale, sc.data(), sizeof(float) * dim, cudaMemcpyHostToDevice, h->st));
+    ANN_CUDA_TRY(cudaMemcpyAsync(h->offset, off.data(), sizeof(float) * dim, cudaMemcpyHostToDevice, h->st));
+    const int64_t total = h->npad * dim;
+    gf_encode_kernel<<<(unsigned)ceil_div(total, 256), 256, 0, h->st>>>(h->base, n, dim, h->npad, h->scale,
+                                                                         h->offset, h->codes);
+    ANN_LAUNCH_CHECK();
+    ANN_CUDA_TRY(cudaStreamSynchronize(h->st));  // sc / off (host) feed the copies above
+    return ANN_OK;
+}
+
+int gf_reserve(gf_handle* h, int64_t r) {
+    if (r <= h->rcap) return ANN_OK;
+    if (h->selk) cudaFree(h->selk);
+    if (h->seli) cudaFree(h->seli);
+    if (h->keys) cudaFree(h->keys);
+    h->selk = nullptr;
+    h->seli = nullptr;
+    h->keys = nullptr;
+    h->rcap = 0;
+    ANN_CUDA_TRY(cudaMalloc(&h->selk, sizeof(float) * (size_t)r));
+    ANN_CUDA_TRY(cudaMalloc(&h->seli, sizeof(int) * (size_t)r));
+    ANN_CUDA_TRY(cudaMalloc(&h->keys, sizeof(unsigned long long) * (size_t)r));
+    h->rcap = r;
+    return ANN_OK;
+}
+
+// keys [r] (or the near set, see gf_topk_kernel) -> the k smallest, ascending; shared memory for
+// min(r + k, kGfSortCap) keys rounded up to a power of two.
+template <typename OutT>
+int launch_gf_topk(const unsigned long long* keys, int64_t r, const unsigned long long* near, const int* count,
+                   int cap, int k, OutT* out, cudaStream_t st) {
+    int Pmax = 64;
+    while (Pmax < std::min<int64_t>(r + k, kGfSortCap)) Pmax <<= 1;
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(gf_topk_kernel<OutT>)));
+    gf_topk_kernel<OutT><<<1, 512, sizeof(unsigned long long) * Pmax, st>>>(keys, (int)r, near, count, cap, k, Pmax,
+                                                                            out);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int gf_search(gf_handle* h, const float* q, int k, int r, long long* out_ids) {
+    const int64_t n = h->n;
+    const int dim = h->dim;
+    cudaStream_t st = h->st;
+    // one segment when R exceeds the top-k kernel's bound (the second stage keeps R keys in front of each
+    // sorted round)
+    const int nseg = r <= kGfMaxK ? h->nseg : 1;
+    int rc = gf_reserve(h, (int64_t)nseg * r);
+    if (rc) return rc;
+    std::memcpy(h->hq, q, sizeof(float) * dim);
+    ANN_CUDA_TRY(cudaMemcpyAsync(h->q, h->hq, sizeof(float) * dim, cudaMemcpyHostToDevice, st));
+    const int64_t quads = h->npad >> 2;
+    gf_scan_kernel<<<(unsigned)ceil_div(quads, 256), 256, sizeof(float) * 2 * dim, st>>>(
+        h->codes, h->npad, dim, h->scale, h->offset, h->q, h->dist);
+    ANN_LAUNCH_CHECK();
+    RadixSelectArgs sa{};
+    sa.keys = h->dist;
+    sa.ld = n;
+    sa.R = r;
+    sa.out_key = h->selk;
+    sa.out_id = h->seli;
+    if (nseg > 1) {
+        sa.offs = h->segs;
+        sa.lens = h->segs + kGfMaxSeg;
+        ANN_CUDA_TRY(cudaMemsetAsync(h->count, 0, sizeof(int), st));
+    }
+    if ((rc = launch_radix_select(sa, nseg, st))) return rc;
+    if (nseg > 1) {  // the union's R smallest (key, row), as row ids over the first R entries of seli
+        const int64_t tot = (int64_t)nseg * r;
+        const int cap = kGfSortCap - r;  // the near set sorts in one round
+        gf_kth_kernel<<<nseg, 256, 0, st>>>(h->selk, h->seli, r, h->kth);
+        ANN_LAUNCH_CHECK();
+        gf_pack_kernel<<<(unsigned)ceil_div(tot, 256), 256, 0, st>>>(h->selk, h->seli, h->segs, h->kth, nseg, r,
+                                                                     h->keys, h->near, cap, h->count);
+        ANN_LAUNCH_CHECK();
+        if ((rc = launch_gf_topk<int>(h->keys, tot, h->near, h->count, cap, r, h->seli, st))) return rc;
+    }
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(gf_rerank_kernel)));
+    gf_rerank_kernel<<<(unsigned)ceil_div(r, kGfRerankWarps), 32 * kGfRerankWarps,
+                       sizeof(float) * dim * (1 + kGfRerankWarps), st>>>(h->base, n, dim, h->q, h->seli, r, h->keys);
+    ANN_LAUNCH_CHECK();
+    if ((rc = launch_gf_topk<long long>(h->keys, r, nullptr, nullptr, 0, k, h->out, st))) return rc;
+    ANN_CUDA_TRY(cudaMemcpyAsync(h->hout, h->out, sizeof(long long) * k, cudaMemcpyDeviceToHost, st));
+    ANN_CUDA_TRY(cudaStreamSynchronize(st));
+    std::memcpy(out_ids, h->hout, sizeof(long long) * k);
+    return ANN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gf_last_error(void) { return ann_last_error(); }
+
+void* gf_create(const float* train, long n, long dim) {
+    clear_error();
+    if (dim > kGfMaxDim) {
+        set_error("dim %ld > 4096 unsupported", dim);
+        return nullptr;
+    }
+    if (!train || n <= 0 || n >= INT32_MAX || dim <= 0) {
+        set_error("gf_create: train=%p n=%ld dim=%ld", (const void*)train, n, dim);
+        return nullptr;
+    }
+    int ndev = 0;
+    const cudaError_t derr = cudaGetDeviceCount(&ndev);
+    if (derr != cudaSuccess || ndev == 0) {
+        set_error("no CUDA device visible (%s)", derr == cudaSuccess ? "0 devices" : cudaGetErrorString(derr));
+        return nullptr;
+    }
+    gf_handle* h = new (std::nothrow) gf_handle();
+    if (!h) {
+        set_error("gf_create: out of host memory");
+        return nullptr;
+    }
+    if (cudaGetDevice(&h->device) != cudaSuccess) h->device = 0;
+    h->n = n;
+    h->dim = (int)dim;
+    h->npad = ceil_div((int64_t)n, 16) * 16;
+    if (gf_build(h, train) != ANN_OK) {
+        gf_release(h);
+        delete h;
+        return nullptr;
+    }
+    return h;
+}
+
+int gf_query(void* handle, const float* q, int k, int r, long long* out_ids) {
+    clear_error();
+    gf_handle* h = static_cast<gf_handle*>(handle);
+    if (!h || !q || (k > 0 && !out_ids) || k < 0) {
+        set_error("gf_query: handle=%p q=%p k=%d out_ids=%p", handle, (const void*)q, k, (void*)out_ids);
+        return -1;
+    }
+    if (k > kGfMaxK) {
+        set_error("gf_query: k=%d > %d unsupported", k, kGfMaxK);
+        return -1;
+    }
+    if (r < k) r = k;
+    if (r > h->n) r = (int)h->n;
+    const int out_k = std::min(k, r);
+    if (out_k <= 0) {  // nothing to return; the reference still counts its r distances
+        h->ndist += r;
+        return out_k;
+    }
+    std::lock_guard<std::mutex> lk(h->mu);
+    DeviceGuard g(h->device);
+    if (!g.ok) {
+        set_error("gf_query: cannot select device %d", h->device);
+        return -1;
+    }
+    if (gf_search(h, q, out_k, r, out_ids) != ANN_OK) return -1;
+    h->ndist += r;
+    return out_k;
+}
+
+long long gf_ndist(void* handle) { return handle ? static_cast<gf_handle*>(handle)->ndist.load() : 0; }
+
+void gf_free(void* handle) {
+    gf_handle* h = static_cast<gf_handle*>(handle);
+    if (!h) return;
+    gf_release(h);
+    delete h;
+}
+
+}  // extern "C"

@@ -856,10 +856,47 @@ def reference_gpu_filter_c3(args, base, queries, kth):
         dt = time.perf_counter() - t0
         ids = torch.from_numpy(out).to(queries.device)
         rec = recall_evaluator(base, queries[:ns], ids, kth[:ns])
-        return {"impl": "reference gpu_filter (competitors/gpu_filter/src/gpu_filter.cu, nvcc sm_100a)",
+        line = {"impl": "reference gpu_filter (competitors/gpu_filter/src/gpu_filter.cu, nvcc sm_100a)",
                 "qps": round(ns / dt, 1), "ms_per_query": round(dt / ns * 1e3, 4), "recall_at_100": round(rec, 4),
                 "refine_r": r, "sample": f"{ns} queries of the headline batch, one per call, wall clock",
                 "fit_s": round(fit_s, 2), "distances_per_query": int(lib.gf_ndist(h)) // (ns + min(3, ns))}
+    finally:
+        lib.gf_free(h)
+    line["dropin"] = _gf_dropin_timing(train, qs, out, r)
+    return line
+
+
+def _gf_dropin_timing(train, qs, ref_ids, r):
+    """This library's gf_* entry points (include/annvedi_gpu_filter.h) on the same rows and queries, called
+    the same way: queries per second, and whether every id matches the reference's."""
+    import ctypes
+    from annvedi_b200 import _lib
+    lib = _lib.load()
+    n, d = train.shape
+    t0 = time.perf_counter()
+    h = lib.gf_create(train.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n, d)
+    fit_s = time.perf_counter() - t0
+    if not h:
+        return {"unavailable": "gf_create: " + lib.gf_last_error().decode()}
+    try:
+        ns = qs.shape[0]
+        out = np.empty((ns, K_NN), np.int64)
+
+        def one(i):
+            got = lib.gf_query(h, qs[i].ctypes.data_as(ctypes.POINTER(ctypes.c_float)), K_NN, r,
+                               out[i].ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)))
+            if got != K_NN:
+                raise RuntimeError("gf_query: " + lib.gf_last_error().decode())
+
+        for i in range(min(3, ns)):
+            one(i)
+        t0 = time.perf_counter()
+        for i in range(ns):
+            one(i)
+        dt = time.perf_counter() - t0
+        return {"impl": "annvedi_b200 gf_* (GPU scan, radix selection, GPU FP32 re-rank)",
+                "qps": round(ns / dt, 1), "ms_per_query": round(dt / ns * 1e3, 4), "fit_s": round(fit_s, 2),
+                "ids_identical_to_reference": bool(np.array_equal(out, ref_ids))}
     finally:
         lib.gf_free(h)
 
