@@ -553,11 +553,11 @@ def run_ours(args, rank, world, local):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and ivf is not None:
         line["cpu_baseline"] = cpu_baseline_ivf(ivf, queries, npc if npc is not None else npc_tc, args)
-    if rank == 0 and world == 1 and args.ref_gpu:
+    if rank == 0 and world == 1 and args.gf:
         try:
-            line["reference_gpu_kernel"] = reference_gpu_filter_c3(args, base, queries, kth)
-        except (OSError, RuntimeError) as e:  # a baseline leg: its failure does not void the bench line
-            line["reference_gpu_kernel"] = {"unavailable": f"{type(e).__name__}: {e}"}
+            line["gpu_filter_dropin"] = gf_dropin_c3(args, base, queries, kth)
+        except Exception as e:  # noqa: BLE001 -- a side leg: its failure does not void the bench line
+            line["gpu_filter_dropin"] = {"unavailable": f"{type(e).__name__}: {e}"}
     if rank == 0 and world == 1 and args.fp8:
         line["scaled_fp8_4m_256"] = scaled_fp8_c4(args, local)
     if rank == 0 and world == 1 and args.serve_seconds > 0 and npc is not None:
@@ -811,9 +811,9 @@ def reference_gpu_filter_c3(args, base, queries, kth):
     source for sm_100a into oracle/_ref/gpu/ (oracle/Makefile), driven through its C ABI the way its
     algorithm.py drives it: gf_create over the headline rows, then gf_query one query per call -- a
     full-N SQ8 scan (one thread per row, dim-major codes), a CUB radix sort of all N keys, the best R
-    ids copied back and re-ranked in FP32 on the host. A baseline leg, like cpu_baseline: measured
-    beside this build's forms, never part of them. The ABI is synchronous, so the figure is wall time
-    over a bounded sample of queries (after 3 warm-up calls), with R = the headline re-rank depth."""
+    ids copied back and re-ranked in FP32 on the host. Part of the reference arm. The ABI is synchronous,
+    so the figure is wall time over a bounded sample of queries (after 3 warm-up calls), with R = the
+    headline re-rank depth."""
     import ctypes
     path = os.path.join(ROOT, "oracle", "_ref", "gpu", "libgpufilter.so")
     if not os.path.exists(path):
@@ -837,7 +837,7 @@ def reference_gpu_filter_c3(args, base, queries, kth):
     if not h:
         return {"unavailable": "gf_create: " + lib.gf_last_error().decode()}
     try:
-        ns = min(args.ref_gpu_sample, queries.shape[0])
+        ns = min(args.gf_sample, queries.shape[0])
         qs = np.ascontiguousarray(queries[:ns].cpu().numpy(), dtype=np.float32)
         out = np.empty((ns, K_NN), np.int64)
         r = args.refine
@@ -862,24 +862,30 @@ def reference_gpu_filter_c3(args, base, queries, kth):
                 "fit_s": round(fit_s, 2), "distances_per_query": int(lib.gf_ndist(h)) // (ns + min(3, ns))}
     finally:
         lib.gf_free(h)
-    line["dropin"] = _gf_dropin_timing(train, qs, out, r)
     return line
 
 
-def _gf_dropin_timing(train, qs, ref_ids, r):
-    """This library's gf_* entry points (include/annvedi_gpu_filter.h) on the same rows and queries, called
-    the same way: queries per second, and whether every id matches the reference's."""
+def gf_dropin_c3(args, base, queries, kth):
+    """The GPU quantized-filter contestant through this library's gf_* entry points
+    (include/annvedi_gpu_filter.h), driven as the contestant's algorithm.py drives its own library:
+    gf_create over the headline rows, gf_query one query per call with R = the headline re-rank depth.
+    Wall time over a bounded sample (after 3 warm-up calls; the ABI is synchronous) and recall@100. The
+    ids equal the reference library's (tests/test_gpu_filter_gpu.py); the reference arm times that library."""
     import ctypes
+    import torch
     from annvedi_b200 import _lib
     lib = _lib.load()
+    train = np.ascontiguousarray(base.cpu().numpy(), dtype=np.float32)
     n, d = train.shape
     t0 = time.perf_counter()
     h = lib.gf_create(train.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n, d)
     fit_s = time.perf_counter() - t0
     if not h:
         return {"unavailable": "gf_create: " + lib.gf_last_error().decode()}
+    r = args.refine
     try:
-        ns = qs.shape[0]
+        ns = min(args.gf_sample, queries.shape[0])
+        qs = np.ascontiguousarray(queries[:ns].cpu().numpy(), dtype=np.float32)
         out = np.empty((ns, K_NN), np.int64)
 
         def one(i):
@@ -894,9 +900,11 @@ def _gf_dropin_timing(train, qs, ref_ids, r):
         for i in range(ns):
             one(i)
         dt = time.perf_counter() - t0
-        return {"impl": "annvedi_b200 gf_* (GPU scan, radix selection, GPU FP32 re-rank)",
-                "qps": round(ns / dt, 1), "ms_per_query": round(dt / ns * 1e3, 4), "fit_s": round(fit_s, 2),
-                "ids_identical_to_reference": bool(np.array_equal(out, ref_ids))}
+        rec = recall_evaluator(base, queries[:ns], torch.from_numpy(out).to(queries.device), kth[:ns])
+        return {"impl": "annvedi_b200 gf_* (GPU SQ8 scan, two-stage selection, GPU FP32 re-rank)",
+                "qps": round(ns / dt, 1), "ms_per_query": round(dt / ns * 1e3, 4), "recall_at_100": round(rec, 4),
+                "refine_r": r, "sample": f"{ns} queries of the headline batch, one per call, wall clock",
+                "fit_s": round(fit_s, 2), "distances_per_query": int(lib.gf_ndist(h)) // (ns + min(3, ns))}
     finally:
         lib.gf_free(h)
 
@@ -985,7 +993,18 @@ def run_reference(args, rank, world):
             "impl": "reference",
             "cpu_baseline": {"value": round(qps, 2), "unit": "queries/s", "cores": cores, "kind": "reference",
                              "sample": sample},
-            "e2e": {"value": round(qps, 2), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": round(qps, 2), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            **({"reference_gpu_kernel": _reference_gpu_leg(args, w.base, queries)} if args.gf else {})}
+
+
+def _reference_gpu_leg(args, base, queries):
+    """The reference's GPU contestant (its own library, oracle/_ref/gpu/) on the same data, or why not."""
+    try:
+        ns = min(args.gf_sample, queries.shape[0])
+        kth = ground_truth(base, queries[:ns], K_NN)
+        return reference_gpu_filter_c3(args, base, queries, kth)
+    except Exception as e:  # noqa: BLE001 -- a side leg: its failure does not void the arm's line
+        return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
 def main():
@@ -1002,9 +1021,10 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="per offered rate; 0 skips serving")
     ap.add_argument("--no-fp8", dest="fp8", action="store_false", help="skip the scaled-FP8 configuration")
     ap.add_argument("--fp8-rows", type=int, default=4_000_000, help="rows of the scaled-FP8 configuration")
-    ap.add_argument("--no-ref-gpu", dest="ref_gpu", action="store_false",
-                    help="skip timing the reference's own GPU kernel (gpu_filter) on the headline data")
-    ap.add_argument("--ref-gpu-sample", type=int, default=200, help="queries of the reference GPU kernel's sample")
+    ap.add_argument("--no-gpu-filter", dest="gf", action="store_false",
+                    help="skip the GPU quantized-filter contestant on the headline data (this arm: the gf_* drop-in; "
+                         "the reference arm: the reference's own libgpufilter.so)")
+    ap.add_argument("--gf-sample", type=int, default=200, help="queries of the GPU quantized-filter sample")
     ap.add_argument("--fp8-batch", type=int, default=20_000, help="queries per batch of the scaled-FP8 configuration")
     ap.add_argument("--no-lsh", dest="lsh", action="store_false", help="skip the LSH bucket-table settings")
     ap.add_argument("--no-dropin", dest="dropin", action="store_false",
