@@ -17,9 +17,10 @@
 //             per quarter taking 64 columns each, for the filter form, whose per-key test and
 //             survivor compaction are bound by issue latency at two warps per scheduler.
 //             tcgen05.ld 2 x 32 columns per wait, then either store the keys (transposed through
-//             shared memory into coalesced rows) or, in filter mode, one predicate test per key
-//             against the row's bar; survivors go to the warp's own region at slots from a warp
-//             prefix sum (no atomics, nothing waits on memory).
+//             shared memory into coalesced rows) or, in filter mode, one test per key against the
+//             row's bar (the sign bit of a packed FP32 difference, gathered by funnel shifts);
+//             survivors go to the warp's own region at slots from a warp prefix sum (no atomics,
+//             nothing waits on memory).
 // Every mbarrier wait is bounded (about 2 s); a timeout raises a device flag and the CTA winds down.
 #include <cuda.h>
 #include <cuda_fp8.h>

@@ -60,3 +60,10 @@ def test_create_without_a_device():
     from annvedi_b200.gpu_filter import Algorithm
     with pytest.raises(RuntimeError, match="no CUDA device"):
         Algorithm().fit(np.ones((16, 8), np.float32))
+
+
+def test_query_before_fit():
+    from annvedi_b200.gpu_filter import Algorithm
+    with pytest.raises(RuntimeError, match="not fitted"):
+        Algorithm().query(np.zeros(8, np.float32), 5)
+    assert Algorithm().get_n_distances() == 0
