@@ -101,6 +101,11 @@ def restate():
                                   ctypes.c_int, ctypes.c_int64, _I64, _F]
     lib.orc_sq8_train.argtypes = [_F, ctypes.c_int64, ctypes.c_int, _F, _F]
     lib.orc_sq8_encode.argtypes = [_F, ctypes.c_int64, ctypes.c_int, _F, _F, _U8]
+    lib.orc_gf_train.argtypes = [_F, ctypes.c_int64, ctypes.c_int, _F, _F]
+    lib.orc_gf_encode.argtypes = [_F, ctypes.c_int64, ctypes.c_int, _F, _F, _U8]
+    lib.orc_gf_query.restype = ctypes.c_int
+    lib.orc_gf_query.argtypes = [_F, _U8, ctypes.c_int64, ctypes.c_int, _F, _F, _F, ctypes.c_int, ctypes.c_int,
+                                 _I64, _I64]
     _lib = lib
     return lib
 
@@ -218,3 +223,28 @@ def exact_topk_f64(data, queries, k, metric="l2", chunk=256):
         sk = np.take_along_axis(pk, order, 1)
         dist[s:s + chunk] = -sk if metric == "ip" else sk
     return ids, dist
+
+
+def gf_search(x, queries, k, r):
+    """The GPU quantized-filter contestant (competitors/gpu_filter/src/gpu_filter.cu) restated on the CPU:
+    its SQ8 state from x, then gf_query per query. Returns (counts int32 [nq], ids int64 [nq, k] padded
+    with -1, the distance count after the queries)."""
+    lib = restate()
+    x = np.ascontiguousarray(x, np.float32)
+    queries = np.ascontiguousarray(np.atleast_2d(queries), np.float32)
+    n, d = x.shape
+    scale = np.empty(d, np.float32)
+    offset = np.empty(d, np.float32)
+    codes = np.empty((n, d), np.uint8)
+    lib.orc_gf_train(_p(x, _F), n, d, _p(scale, _F), _p(offset, _F))
+    lib.orc_gf_encode(_p(x, _F), n, d, _p(scale, _F), _p(offset, _F), _p(codes, _U8))
+    got = np.zeros(queries.shape[0], np.int32)
+    ids = np.full((queries.shape[0], k), -1, np.int64)
+    ndist = np.zeros(1, np.int64)
+    for i, q in enumerate(queries):
+        o = np.full(max(k, 1), -1, np.int64)
+        got[i] = lib.orc_gf_query(_p(x, _F), _p(codes, _U8), n, d, _p(scale, _F), _p(offset, _F), _p(q, _F), k, r,
+                                  _p(o, _I64), _p(ndist, _I64))
+        ids[i, :got[i]] = o[:got[i]]
+    return got, ids, int(ndist[0])
+

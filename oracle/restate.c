@@ -481,3 +481,89 @@ void orc_sq8_encode(const float *x, int64_t n, int dim, const float *scale, cons
             codes[i * dim + d] = (uint8_t)(qv < 0 ? 0 : (qv > 255 ? 255 : qv));
         }
 }
+
+/* ---------------------------------------------------------------------------------------------
+ * The GPU quantized-filter contestant (competitors/gpu_filter/src/gpu_filter.cu), restated.
+ * Its host code is compiled by nvcc with -O3 and no -ffast-math (Dockerfile:17-19), so divisions
+ * stay true divisions and the host re-rank's `acc += v * v` is an unfused multiply and add; its
+ * device key is an explicit fmaf chain (:57-60).
+ * --------------------------------------------------------------------------------------------- */
+
+/* Per-dimension SQ8 (gpu_filter.cu:100-117): min / max as std::min / std::max keep them, scale =
+ * (max - min) / 255 (a true division) when the range is > 1e-8, else 1; offset = min either way. */
+void orc_gf_train(const float *x, int64_t n, int dim, float *scale, float *offset) {
+    for (int d = 0; d < dim; ++d) {
+        float mn = 3.4e38f, mx = -3.4e38f;
+        for (int64_t i = 0; i < n; ++i) {
+            const float v = x[i * dim + d];
+            mn = (v < mn) ? v : mn;
+            mx = (mx < v) ? v : mx;
+        }
+        scale[d] = (mx - mn > 1e-8f) ? (mx - mn) / 255.0f : 1.0f;
+        offset[d] = mn;
+    }
+}
+
+/* code = clamp(lrintf((x - offset) / scale), 0, 255) (gpu_filter.cu:119-127), row-major [n, dim]. */
+void orc_gf_encode(const float *x, int64_t n, int dim, const float *scale, const float *offset, uint8_t *codes) {
+    for (int64_t i = 0; i < n; ++i)
+        for (int d = 0; d < dim; ++d) {
+            const int qv = (int)lrintf((x[i * dim + d] - offset[d]) / scale[d]);
+            codes[i * dim + d] = (uint8_t)(qv < 0 ? 0 : (qv > 255 ? 255 : qv));
+        }
+}
+
+typedef struct {
+    float key;
+    int32_t id;
+} gf_pair_t;
+
+static int cmp_gf_pair(const void *x, const void *y) {
+    const gf_pair_t *a = (const gf_pair_t *)x, *b = (const gf_pair_t *)y;
+    if (a->key < b->key) return -1;
+    if (b->key < a->key) return 1;
+    return (a->id > b->id) - (a->id < b->id);
+}
+
+/* gf_query (gpu_filter.cu:135-176): r raised to k and capped at n; every row's key
+ * sum_d fmaf(code, scale, -(q - offset))^2 by an fmaf chain in dimension order (:52-63); the first r
+ * rows of the stable ascending sort by key (:155-157), i.e. by (key, row); their FP32 squared
+ * distances v = x - q, acc += v * v (:163-171); the best min(k, r) by (distance, id) (:173-175).
+ * Returns min(k, r); adds r to *ndist. */
+int orc_gf_query(const float *x, const uint8_t *codes, int64_t n, int dim, const float *scale,
+                 const float *offset, const float *q, int k, int r, int64_t *out_ids, int64_t *ndist) {
+    if (r < k) r = k;
+    if (r > n) r = (int)n;
+    float *qshift = (float *)malloc(sizeof(float) * (size_t)dim);
+    gf_pair_t *keys = (gf_pair_t *)malloc(sizeof(gf_pair_t) * (size_t)(n > 0 ? n : 1));
+    gf_pair_t *exact = (gf_pair_t *)malloc(sizeof(gf_pair_t) * (size_t)(r > 0 ? r : 1));
+    for (int d = 0; d < dim; ++d) qshift[d] = q[d] - offset[d];
+    for (int64_t i = 0; i < n; ++i) {
+        float acc = 0.0f;
+        for (int d = 0; d < dim; ++d) {
+            const float v = fmaf((float)codes[i * dim + d], scale[d], -qshift[d]);
+            acc = fmaf(v, v, acc);
+        }
+        keys[i].key = acc;
+        keys[i].id = (int32_t)i;
+    }
+    qsort(keys, (size_t)n, sizeof(gf_pair_t), cmp_gf_pair);
+    for (int j = 0; j < r; ++j) {
+        const float *p = x + (int64_t)keys[j].id * dim;
+        float acc = 0.0f;
+        for (int d = 0; d < dim; ++d) {
+            const float v = p[d] - q[d];
+            acc += v * v;
+        }
+        exact[j].key = acc;
+        exact[j].id = keys[j].id;
+    }
+    qsort(exact, (size_t)r, sizeof(gf_pair_t), cmp_gf_pair);
+    const int out_k = k < r ? k : r;
+    for (int j = 0; j < out_k; ++j) out_ids[j] = exact[j].id;
+    if (ndist) *ndist += r;
+    free(qshift);
+    free(keys);
+    free(exact);
+    return out_k;
+}

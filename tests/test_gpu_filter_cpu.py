@@ -67,3 +67,16 @@ def test_query_before_fit():
     with pytest.raises(RuntimeError, match="not fitted"):
         Algorithm().query(np.zeros(8, np.float32), 5)
     assert Algorithm().get_n_distances() == 0
+
+
+def test_restatement_matches_the_reference_goldens(golden_dir):
+    """oracle/restate.c's gf restatement against the reference library's own outputs
+    (tests/golden/gf_ref.npz, made by tests/golden/make_gf_golden.py on a GPU)."""
+    from oracle import refmod
+    from tests.golden.make_gf_golden import cases
+    g = np.load(os.path.join(golden_dir, "gf_ref.npz"))
+    for name, x, qs, k, r in cases():
+        got, ids, ndist = refmod.gf_search(x, qs, k, r)
+        np.testing.assert_array_equal(got, g[f"{name}_got"], err_msg=name)
+        np.testing.assert_array_equal(ids, g[f"{name}_ids"], err_msg=name)
+        assert ndist == int(g[f"{name}_ndist"]), name
