@@ -142,3 +142,20 @@ def test_algorithm_class(ours):
         assert np.array_equal(ours.query(h, q, 10, 40)[1], ids)
     finally:
         ours.lib.gf_free(h)
+
+
+def test_golden_outputs_of_the_reference(ours, golden_dir):
+    """The drop-in against tests/golden/gf_ref.npz: the reference library's own outputs on six seeded
+    cases (tests/golden/make_gf_golden.py), so this check needs no reference build on the machine."""
+    from tests.golden.make_gf_golden import cases
+    g = np.load(os.path.join(golden_dir, "gf_ref.npz"))
+    for name, x, qs, k, r in cases():
+        h = ours.create(x)
+        try:
+            for i, q in enumerate(qs):
+                got, ids = ours.query(h, q, k, r)
+                assert got == g[f"{name}_got"][i], (name, i)
+                np.testing.assert_array_equal(ids, g[f"{name}_ids"][i, :got], err_msg=f"{name} query {i}")
+            assert ours.lib.gf_ndist(h) == int(g[f"{name}_ndist"]), name
+        finally:
+            ours.lib.gf_free(h)
