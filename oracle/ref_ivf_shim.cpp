@@ -12,6 +12,11 @@
 //   * set_num_threads, which replaces the reference's ThreadPool (sized from
 //     hardware_concurrency() at lsh_index_optimized.cpp:140) so the SQ8 pass's per-chunk
 //     64-entry heaps (:86-122, :465-469) are reproducible on any host.
+//   * set_fit_threads, which pins the thread count fit() reads from hardware_concurrency()
+//     (:140): its k-means sums per ThreadPool chunk (:61-73, :594-601), so a fit is reproducible
+//     only with the count fixed. The reference asks std::thread for it on one line (:140); within
+//     the reference include the token `thread` names a stand-in whose hardware_concurrency()
+//     returns the pinned count (0 = the real one). No other `thread` token appears in code there.
 // Member access uses a preprocessor override of `private`, confined to the reference include.
 #include <pybind11/pybind11.h>
 #include <pybind11/numpy.h>
@@ -37,11 +42,25 @@
 #include <immintrin.h>
 #endif
 
+namespace annvedi_shim {
+static int g_fit_threads = 0;
+struct pinned_thread {
+    static unsigned hardware_concurrency() noexcept {
+        return g_fit_threads > 0 ? (unsigned)g_fit_threads : std::thread::hardware_concurrency();
+    }
+};
+}  // namespace annvedi_shim
+namespace std {
+using annvedi_pinned_thread = ::annvedi_shim::pinned_thread;
+}
+
 #pragma push_macro("PYBIND11_MODULE")
 #undef PYBIND11_MODULE
 #define PYBIND11_MODULE(name, variable) static void annvedi_ref_register_##name(pybind11::module_ &variable)
 #define private public
+#define thread annvedi_pinned_thread
 #include "lsh_index_optimized.cpp"
+#undef thread
 #undef private
 #pragma pop_macro("PYBIND11_MODULE")
 
@@ -141,6 +160,7 @@ PYBIND11_MODULE(ref_ivf_shim, m) {
     m.def("export_state", &export_state);
     m.def("import_state", &import_state, py::arg("index"), py::arg("state"), py::arg("num_threads"));
     m.def("set_num_threads", [](IVFLSHIndex &ix, int t) { ix.pool_ = std::make_unique<ThreadPool>(t > 0 ? t : 1); });
+    m.def("set_fit_threads", [](int t) { annvedi_shim::g_fit_threads = t > 0 ? t : 0; });
     m.def("get_num_threads", [](const IVFLSHIndex &ix) { return ix.pool_ ? ix.pool_->get_num_threads() : 0; });
     m.def("l2_distance",
           [](f32arr a, f32arr b, float threshold) {

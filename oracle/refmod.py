@@ -101,6 +101,10 @@ def restate():
                                   ctypes.c_int, ctypes.c_int64, _I64, _F]
     lib.orc_sq8_train.argtypes = [_F, ctypes.c_int64, ctypes.c_int, _F, _F]
     lib.orc_sq8_encode.argtypes = [_F, ctypes.c_int64, ctypes.c_int, _F, _F, _U8]
+    lib.orc_kmeans_order.argtypes = [ctypes.c_int64, _I32]
+    lib.orc_kmeans.restype = ctypes.c_int
+    lib.orc_kmeans.argtypes = [_F, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                               ctypes.c_int, ctypes.c_int, _F, _I32]
     lib.orc_gf_train.argtypes = [_F, ctypes.c_int64, ctypes.c_int, _F, _F]
     lib.orc_gf_encode.argtypes = [_F, ctypes.c_int64, ctypes.c_int, _F, _F, _U8]
     lib.orc_gf_query.restype = ctypes.c_int
@@ -178,6 +182,41 @@ def ivf_query(state: dict, q, k, n_probes=0, n_probe_clusters=8, refine_r=-1, nu
     if nc < 0:
         raise MemoryError("orc_ivf_query failed")
     return ids, dists, int(nc)
+
+
+def kmeans_order(n: int) -> np.ndarray:
+    """rand_indices of the reference's k-means: std::shuffle(iota(n), std::mt19937(1337))."""
+    out = np.empty(n, np.int32)
+    restate().orc_kmeans_order(n, _p(out, _I32))
+    return out
+
+
+def kmeans(x, n_clusters: int, num_threads: int, iters: int = 15, lanes: int = 16, workers: int | None = None):
+    """The reference's k-means restated (oracle/restate_kmeans.cpp) with a ThreadPool of `num_threads`:
+    (centroids float32 [C, dim], last assignment int32 [n]). C = min(n_clusters, n) as the reference's fit."""
+    x = np.ascontiguousarray(x, np.float32)
+    n, d = x.shape
+    c = min(int(n_clusters), n)
+    cent = np.empty((c, d), np.float32)
+    assign = np.empty(n, np.int32)
+    rc = restate().orc_kmeans(_p(x, _F), n, d, c, iters, num_threads, lanes, workers or os.cpu_count() or 1,
+                              _p(cent, _F), _p(assign, _I32))
+    if rc != 0:
+        raise ValueError("orc_kmeans: bad arguments")
+    return cent, assign
+
+
+def ref_fit(x, n_tables: int, n_bits: int, n_clusters: int, num_threads: int, isa: str | None = None):
+    """The reference's own LSHIndex.fit with its thread count pinned to `num_threads` (the shim's
+    set_fit_threads); returns the fitted index, whose query pool has the same size."""
+    m = load_ref("ref_ivf_shim", isa)
+    ix = m.LSHIndex()
+    m.set_fit_threads(num_threads)
+    try:
+        ix.fit(np.ascontiguousarray(x, np.float32), n_tables, n_bits, n_clusters)
+    finally:
+        m.set_fit_threads(0)
+    return ix
 
 
 def sq8_train(x):

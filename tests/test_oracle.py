@@ -136,3 +136,46 @@ def test_state_builder_matches_reference_fit():
         for key in ("original_data", "quantized_data", "scale", "offset", "mean", "reordered_to_original",
                     "table_offsets", "table_ids"):
             np.testing.assert_array_equal(mine[key], st[key], err_msg=key)
+
+
+# ---- k-means (IVFLSHIndex::run_kmeans) --------------------------------------------------------
+
+def test_kmeans_restatement_matches_reference_golden(golden_dir):
+    from tests.golden import make_kmeans_golden as mk
+    fx = np.load(os.path.join(golden_dir, "kmeans_ref.npz"))
+    for name, n, dim, c, t, dup, seed, _ in mk.kmeans_cases():
+        x, _ = mk.make_rows(n, dim, dup, seed)
+        cent, assign = refmod.kmeans(x, c, t, lanes=LANES)
+        np.testing.assert_array_equal(cent, fx[f"{name}/centroids"], err_msg=name)
+        np.testing.assert_array_equal(np.argsort(assign, kind="stable"), fx[f"{name}/reordered_to_original"],
+                                      err_msg=name)
+        np.testing.assert_array_equal(np.bincount(assign, minlength=min(c, n)), fx[f"{name}/list_sizes"],
+                                      err_msg=name)
+
+
+def test_kmeans_restatement_depends_on_thread_count():
+    # the reason the thread count is pinned: per-chunk float sums change the centroids' last bits
+    from tests.golden import make_kmeans_golden as mk
+    x, _ = mk.make_rows(3000, 64, 0, 0)
+    a, _ = refmod.kmeans(x, 16, 3, lanes=LANES)
+    b, _ = refmod.kmeans(x, 16, 4, lanes=LANES)
+    assert not np.array_equal(a, b)
+    np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-6)
+
+
+def test_kmeans_order_is_a_permutation():
+    o = refmod.kmeans_order(1000)
+    np.testing.assert_array_equal(np.sort(o), np.arange(1000))
+    np.testing.assert_array_equal(o, refmod.kmeans_order(1000))
+
+
+@needs_ref
+def test_kmeans_restatement_matches_reference_fit_directly():
+    ivfm = refmod.load_ref("ref_ivf_shim", "avx512")
+    w = synth.zipf_mixture(6000, 48, 4, c=24, lo=20, hi=1500, seed=11)
+    for t in (1, 6, 13):
+        ix = refmod.ref_fit(w.base, 1, 0, 24, t, "avx512")
+        st = ivfm.export_state(ix)
+        cent, assign = refmod.kmeans(w.base, 24, t, lanes=LANES)
+        np.testing.assert_array_equal(cent, st["centroids"])
+        np.testing.assert_array_equal(np.argsort(assign, kind="stable"), st["reordered_to_original"])
