@@ -88,7 +88,7 @@ SIGNATURES = [
     ("ann_flat_size", _i64, [_vp]),
     ("ann_ivf_create", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int]),
     ("ann_ivf_destroy", ctypes.c_int, [_vp]),
-    ("ann_ivf_fit", ctypes.c_int, [_vp, _vp, _i64, _i32, _i64, _i32, _vp, _vp, _i32, _i32, _vp]),
+    ("ann_ivf_fit", ctypes.c_int, [_vp, _vp, _i64, _i32, _i64, _i32, _vp, _vp, _i32, _i32, _i32, _vp]),
     ("ann_ivf_import", ctypes.c_int, [_vp, _i64, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("ann_ivf_export", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("ann_ivf_info", ctypes.c_int, [_vp, ctypes.POINTER(_i64)]),

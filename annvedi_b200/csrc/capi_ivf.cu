@@ -8,6 +8,7 @@
 #include <cstring>
 #include <cmath>
 #include <mutex>
+#include <numeric>
 #include <random>
 #include <thread>
 #include <vector>
@@ -132,27 +133,53 @@ static int ivf_finish_lists(ann_ivf* h, cudaStream_t st) {
 }
 
 // Nearest centroid of every row (exact FP32 scan, k = 1): assign[i] in [0, C).
-static int assign_rows(const float* x, int64_t n, int dpad, const float* cent, int C, int32_t* assign,
+// Nearest centroid of every row, as the reference's kmeans_assign_worker picks it (first minimum of
+// compute_l2_distance, lsh_index_optimized.cpp:32-47): the exact FP32 scan's two nearest per row,
+// certified by the rounding bound of both arithmetics, the near-ties redone in the reference's.
+static int assign_rows(const float* x, int64_t n, int dim, int dpad, const float* cent, int C, int32_t* assign,
                        ann_workspace* ws, cudaStream_t st) {
     const int bq = 32;
     const int nq_chunk = 1 << 20;
+    // relative error of a computed squared distance: the scan's FMA chain over dpad terms, and the
+    // reference's 16 lane sums of dim/16 terms, folds and remainder; margin covers both with room
+    const double u = 1.0 / 16777216.0;
+    const double e_fast = (dpad + 4) * u, e_ref = (dim / 16 + 24) * u;
+    const float margin = (float)(1.0 + 4.0 * (e_fast + e_ref));
+    const int k = C >= 2 ? 2 : 1;
     for (int64_t r0 = 0; r0 < n; r0 += nq_chunk) {
         const int nq = (int)std::min<int64_t>(nq_chunk, n - r0);
         Sizer sz;
-        sz.take<float>((size_t)nq);
-        sz.take<int>((size_t)nq);
-        sz.take<int64_t>((size_t)nq);
+        sz.take<float>((size_t)nq * k);
+        sz.take<int>((size_t)nq * k);
+        sz.take<float>((size_t)nq * 2);
+        sz.take<int>((size_t)nq * 2);
+        sz.take<int32_t>((size_t)nq);
+        sz.take<int>(1);
         int rc = ws_reserve_device(ws, sz.bytes());
         if (rc) return rc;
         Carver cv(ws->dev);
-        float* sk = cv.take<float>((size_t)nq);
-        int* si = cv.take<int>((size_t)nq);
-        FlatScanArgs a{cent, C, dpad, x + r0 * dpad, nq, ANN_METRIC_L2, 1, (int64_t)C, 1, sk, si};
+        float* sk = cv.take<float>((size_t)nq * k);
+        int* si = cv.take<int>((size_t)nq * k);
+        float* k2 = cv.take<float>((size_t)nq * 2);
+        int* i2 = cv.take<int>((size_t)nq * 2);
+        int32_t* amb = cv.take<int32_t>((size_t)nq);
+        int* amb_count = cv.take<int>(1);
+        if (k == 1) {  // one centroid: every row is in list 0
+            ANN_CUDA_TRY(cudaMemsetAsync(assign + r0, 0, sizeof(int32_t) * nq, st));
+            continue;
+        }
+        FlatScanArgs a{cent, C, dpad, x + r0 * dpad, nq, ANN_METRIC_L2, k, (int64_t)C, 1, sk, si};
         rc = launch_flat_scan(a, bq, st);
         if (rc) return rc;
-        MergeArgs m{sk, si, nq, 1, 1, 1, 0, nullptr, nullptr};
-        m.out_id32 = assign + r0;
+        MergeArgs m{sk, si, nq, 1, k, 2, 0, nullptr, nullptr};
+        m.out_id32 = i2;
+        m.out_key32 = k2;
         rc = launch_merge_splits(m, st);
+        if (rc) return rc;
+        ANN_CUDA_TRY(cudaMemsetAsync(amb_count, 0, sizeof(int), st));
+        rc = launch_kmeans_certify(k2, i2, nq, margin, assign + r0, amb, amb_count, st);
+        if (rc) return rc;
+        rc = launch_kmeans_ref_assign(x + r0 * dpad, dpad, dim, cent, dpad, C, amb, amb_count, assign + r0, st);
         if (rc) return rc;
     }
     return ANN_OK;
@@ -199,7 +226,8 @@ int ann_ivf_destroy(ann_ivf* h) {
 }
 
 int ann_ivf_fit(ann_ivf* h, const float* data, int64_t n, int32_t dim, int64_t ld, int32_t n_clusters,
-                const float* centroids, const int32_t* assign, int32_t kmeans_iters, int32_t mem, void* stream) {
+                const float* centroids, const int32_t* assign, int32_t kmeans_iters, int32_t num_threads, int32_t mem,
+                void* stream) {
     clear_error();
     ANN_CHECK_ARG(h != nullptr, "ann_ivf_fit: null index");
     ANN_CHECK_ARG(n >= 1 && dim >= 1 && data, "ann_ivf_fit: need a non-empty 2-D array");
@@ -208,6 +236,8 @@ int ann_ivf_fit(ann_ivf* h, const float* data, int64_t n, int32_t dim, int64_t l
     ANN_CHECK_ARG(n_clusters >= 1, "ann_ivf_fit: n_clusters=%d < 1", n_clusters);
     ANN_CHECK_ARG(kmeans_iters >= 0, "ann_ivf_fit: kmeans_iters < 0");
     DeviceGuard g(h->device);
+    // the reference sizes its ThreadPool, and with it the k-means chunks, from hardware_concurrency() (:140)
+    const int fit_threads = num_threads > 0 ? num_threads : (int)std::max(1u, std::thread::hardware_concurrency());
     cudaStream_t st = as_stream(stream);
     const int C = (int)std::min<int64_t>(n_clusters, n);  // the reference clamps too (:137)
     const int dpad = (int)ceil_div(dim, 32) * 32;
@@ -225,7 +255,7 @@ int ann_ivf_fit(ann_ivf* h, const float* data, int64_t n, int32_t dim, int64_t l
     size_t tmp_bytes = 0;
     float* mn = nullptr;
     float* mx = nullptr;
-    float* fallback = nullptr;
+    int32_t* seed_rows = nullptr;
     int rc = ANN_OK;
 #define FIT_TRY(x)          \
     do {                    \
@@ -252,16 +282,27 @@ int ann_ivf_fit(ann_ivf* h, const float* data, int64_t n, int32_t dim, int64_t l
         FIT_CUDA(cudaMemsetAsync(X, 0, sizeof(float) * (size_t)n * dpad, st));
         FIT_CUDA(cudaMemcpy2DAsync(X, sizeof(float) * dpad, data, sizeof(float) * ld, sizeof(float) * dim, n, kind, st));
         FIT_CUDA(cudaMemsetAsync(h->centroids, 0, sizeof(float) * (size_t)C * dpad, st));
+        // rand_indices of run_kmeans: std::shuffle(iota(n), std::mt19937(1337)) (:553-555), the same
+        // libstdc++ algorithm the reference runs. Row rand_indices[c] seeds list c (:557-561); row
+        // rand_indices[(c * 37) % n] reseeds it whenever it ends an update empty (:608-613).
+        {
+            std::vector<int32_t> perm((size_t)n);
+            std::iota(perm.begin(), perm.end(), 0);
+            std::shuffle(perm.begin(), perm.end(), std::mt19937(1337));
+            std::vector<int32_t> seeds(2 * (size_t)C);
+            for (int c = 0; c < C; ++c) {
+                seeds[c] = perm[(size_t)(c % n)];
+                seeds[(size_t)C + c] = perm[(size_t)(((int64_t)c * 37) % n)];
+            }
+            FIT_TRY(dmalloc(&seed_rows, 2 * (size_t)C));
+            FIT_CUDA(cudaMemcpyAsync(seed_rows, seeds.data(), sizeof(int32_t) * 2 * C, cudaMemcpyHostToDevice, st));
+            FIT_CUDA(cudaStreamSynchronize(st));
+        }
         if (centroids) {
             FIT_CUDA(cudaMemcpy2DAsync(h->centroids, sizeof(float) * dpad, centroids, sizeof(float) * dim,
                                        sizeof(float) * dim, C, kind, st));
         } else {
-            // deterministic initial centroids: rows floor(c * n / C)
-            for (int c = 0; c < C; ++c) {
-                const int64_t r = (int64_t)c * n / C;
-                FIT_CUDA(cudaMemcpyAsync(h->centroids + (size_t)c * dpad, X + (size_t)r * dpad, sizeof(float) * dpad,
-                                         cudaMemcpyDeviceToDevice, st));
-            }
+            FIT_TRY(launch_gather_rows(X, C, dpad, seed_rows, h->centroids, dpad, st));
         }
         // iota for the sort values
         {
@@ -272,27 +313,21 @@ int ann_ivf_fit(ann_ivf* h, const float* data, int64_t n, int32_t dim, int64_t l
         }
         FIT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, a_raw, a_sorted, idx, order, (int)n, 0, 32, st));
         FIT_CUDA(cudaMalloc(&tmp, tmp_bytes));
-        FIT_TRY(dmalloc(&fallback, (size_t)C * dpad));
-        // reseed rows for empty lists: rows ((c * 37) % n) as the reference does (:611)
-        for (int c = 0; c < C; ++c) {
-            const int64_t r = ((int64_t)c * 37) % n;
-            FIT_CUDA(cudaMemcpyAsync(fallback + (size_t)c * dpad, X + (size_t)r * dpad, sizeof(float) * dpad,
-                                     cudaMemcpyDeviceToDevice, st));
-        }
         const bool given_assign = assign != nullptr;
         const int iters = (centroids || given_assign) ? 0 : kmeans_iters;
         for (int it = 0; it < iters; ++it) {
-            FIT_TRY(assign_rows(X, n, dpad, h->centroids, C, a_raw, &h->ws, st));
+            FIT_TRY(assign_rows(X, n, dim, dpad, h->centroids, C, a_raw, &h->ws, st));
             FIT_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, a_raw, a_sorted, idx, order, (int)n, 0, 32, st));
             FIT_TRY(launch_list_offsets(a_sorted, n, C, h->list_off, st));
-            FIT_TRY(launch_centroid_update(X, dpad, dim, order, h->list_off, C, h->centroids, dpad, fallback, st));
+            FIT_TRY(launch_kmeans_update(X, dpad, dim, order, h->list_off, C, h->centroids, dpad, seed_rows + C, n,
+                                         fit_threads, st));
         }
         // the lists: given assignment, else nearest to the current centroids (the last k-means
         // assignment when iterating, as the reference's lists come from its last assign step)
         if (given_assign) {
             FIT_CUDA(cudaMemcpyAsync(a_raw, assign, sizeof(int32_t) * n, kind, st));
         } else if (iters == 0) {
-            FIT_TRY(assign_rows(X, n, dpad, h->centroids, C, a_raw, &h->ws, st));
+            FIT_TRY(assign_rows(X, n, dim, dpad, h->centroids, C, a_raw, &h->ws, st));
         }
         FIT_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, a_raw, a_sorted, idx, order, (int)n, 0, 32, st));
         FIT_TRY(launch_list_offsets(a_sorted, n, C, h->list_off, st));
@@ -319,7 +354,7 @@ int ann_ivf_fit(ann_ivf* h, const float* data, int64_t n, int32_t dim, int64_t l
     }
 fail:
     for (void* p : {(void*)X, (void*)a_raw, (void*)a_sorted, (void*)idx, (void*)order, tmp, (void*)mn, (void*)mx,
-                    (void*)fallback})
+                    (void*)seed_rows})
         if (p) cudaFree(p);
     if (rc) ivf_free_state(h);
     return rc;

@@ -107,7 +107,14 @@ int launch_clear_every_row(const IvfPlan& plan, cudaStream_t st);
 constexpr int kQueryOrderMaxLists = 32768;
 int launch_query_order(const int32_t* probes, int npc, int nq, int C, int32_t* order, cudaStream_t st);
 int launch_add_offset(int64_t* v, int64_t n, int64_t add, cudaStream_t st);  // v[i] += add
-int launch_centroid_update(const float* x, int ld, int dim, const int32_t* order, const int64_t* off, int C,
-                           float* centroids, int ldc, const float* fallback_rows, cudaStream_t st);
+// k-means of the reference (ivf_build.cu): certification of the fast two nearest centroids, the
+// reference arithmetic for the queued near-ties, and the ThreadPool-chunk-ordered update.
+int launch_kmeans_certify(const float* key2, const int* id2, int64_t n, float margin, int32_t* assign, int32_t* amb,
+                          int* amb_count, cudaStream_t st);
+int launch_kmeans_ref_assign(const float* x, int ldx, int dim, const float* cent, int ldc, int C, const int32_t* amb,
+                             const int* amb_count, int32_t* assign, cudaStream_t st);
+int launch_kmeans_update(const float* x, int ldx, int dim, const int32_t* order, const int64_t* off, int C,
+                         float* centroids, int ldc, const int32_t* reseed_rows, int64_t n, int num_threads,
+                         cudaStream_t st);
 
 }  // namespace annb

@@ -74,7 +74,7 @@ class IVFIndex:
                 raise RuntimeError("assign must have one entry per row")
         st = _lib.stream_ptr(x) if mem == _lib.MEM_DEVICE else None
         _lib.check(self._lib.ann_ivf_fit(self._h, _lib.ptr(x), n, d, ld, int(n_clusters), _lib.ptr(cen),
-                                         _lib.ptr(asg), int(kmeans_iters), mem, st))
+                                         _lib.ptr(asg), int(kmeans_iters), int(self.num_threads), mem, st))
         self._n, self._dim = n, d
         self._C = min(int(n_clusters), n)
         if int(n_tables) != 1 or int(n_bits) != 0:  # LSH bucket tables over the lists

@@ -169,13 +169,17 @@ int ann_ivf_create(ann_ivf** out, int device);
 int ann_ivf_destroy(ann_ivf* h);
 
 /* LSHIndex::fit (lsh_index_optimized.cpp:128-292) on the GPU: `n_clusters` lists (clamped to n).
- * Centroids: `centroids` [n_clusters, dim] if not NULL, else `kmeans_iters` k-means iterations
- * from deterministic seeds. Lists: `assign` [n] if not NULL, else the nearest centroid (the last
- * k-means assignment when iterating). Rows are reordered list by list and SQ8-encoded with
- * per-dimension scale/offset exactly as the reference computes them. `data`, `centroids` and
- * `assign` live where `mem` says. */
+ * Centroids: `centroids` [n_clusters, dim] if not NULL, else the reference's k-means (run_kmeans,
+ * :551-616) for `kmeans_iters` rounds (the reference runs 15): seeds from std::shuffle with
+ * std::mt19937(1337), assignment by the reference's distance arithmetic, sums per ThreadPool chunk
+ * of `num_threads` (<= 0: this host's hardware concurrency, as the reference sizes its pool, :140).
+ * With the same thread count the centroids and lists are bit-identical to the reference's fit.
+ * Lists: `assign` [n] if not NULL, else the nearest centroid (the last k-means assignment when
+ * iterating). Rows are reordered list by list and SQ8-encoded with per-dimension scale/offset
+ * exactly as the reference computes them. `data`, `centroids` and `assign` live where `mem` says. */
 int ann_ivf_fit(ann_ivf* h, const float* data, int64_t n, int32_t dim, int64_t ld, int32_t n_clusters,
-                const float* centroids, const int32_t* assign, int32_t kmeans_iters, int32_t mem, void* stream);
+                const float* centroids, const int32_t* assign, int32_t kmeans_iters, int32_t num_threads,
+                int32_t mem, void* stream);
 
 /* Imports an index state in the reference's layout (all host pointers, rows in list order):
  * centroids [C, dim], original [n, dim] FP32, codes [n, dim] uint8, scale / offset [dim],

@@ -48,3 +48,21 @@ def check_exact_topk(base, queries, ids, dists, k, metric="l2", rtol=1e-5, atol=
 def recall_at_k(true_d_kth, got_d, k):
     """Evaluator recall: mean(pred_d[:k] <= true_d[k-1]) (orthogonal-competition/evaluator.py:149-157)."""
     return float(np.mean(got_d[:, :k] <= true_d_kth[:, None]))
+
+
+def assert_ids_equal_up_to_ties(base, queries, got, want, rtol=1e-6, err_msg=""):
+    """Per query: the same ids, or -- where they differ -- ids whose FP64 distances, sorted, equal the
+    wanted ids' within rtol (the two lists differ only by which of equally distant rows they keep).
+    Returns the number of queries that needed the tie rule."""
+    got, want = np.asarray(got), np.asarray(want)
+    assert got.shape == want.shape, err_msg
+    nties = 0
+    for i in range(got.shape[0]):
+        if np.array_equal(got[i], want[i]):
+            continue
+        nties += 1
+        assert ((got[i] >= 0) == (want[i] >= 0)).all(), f"{err_msg}: query {i} returns a different count"
+        dg = np.sort(fp64_dists(base, queries[i:i + 1], got[i:i + 1])[0])
+        dw = np.sort(fp64_dists(base, queries[i:i + 1], want[i:i + 1])[0])
+        np.testing.assert_allclose(dg, dw, rtol=rtol, atol=1e-12, err_msg=f"{err_msg}: query {i}")
+    return nties
