@@ -83,7 +83,7 @@ def flat_normal(n: int, d: int, q: int, seed: int = 0, backend: str = "numpy", d
     return Workload(base, qs, None, None, "l2", f"flat_normal_{n}x{d}")
 
 
-def _mixture(n, d, q, c, sigma, sizes, seed, backend, device, scale_norms, metric, name):
+def _mixture(n, d, q, c, sigma, sizes, seed, backend, device, scale_norms, metric, name, query_seed=None):
     if backend == "numpy":
         rng = np.random.default_rng(seed)
         centres = rng.standard_normal((c, d), dtype=np.float32)
@@ -95,6 +95,8 @@ def _mixture(n, d, q, c, sigma, sizes, seed, backend, device, scale_norms, metri
             rng.shuffle(assign)
             p = sizes / sizes.sum()
         base = centres[assign] + sigma * rng.standard_normal((n, d), dtype=np.float32)
+        if query_seed is not None:  # the same base, queries from their own stream
+            rng = np.random.default_rng(query_seed)
         qc = rng.choice(c, size=q, p=p) if p is not None else rng.integers(0, c, q)
         qs = centres[qc] + sigma * rng.standard_normal((q, d), dtype=np.float32)
         base = _normalise_np(base)
@@ -132,9 +134,11 @@ def mixture(n, d, q, c=1024, sigma=0.35, seed=0, backend="numpy", device="cpu", 
 
 
 def zipf_mixture(n, d, q, c=2048, sigma=0.3, s=1.1, lo=20, hi=40000, seed=0, backend="numpy",
-                 device="cpu") -> Workload:
+                 device="cpu", query_seed=None) -> Workload:
+    """query_seed (numpy backend): draw the queries from their own seeded stream (same base)."""
     sizes = zipf_sizes(n, c, s, lo, hi)
-    return _mixture(n, d, q, c, sigma, sizes, seed, backend, device, False, "l2", f"zipf_mixture_{n}x{d}_c{c}")
+    return _mixture(n, d, q, c, sigma, sizes, seed, backend, device, False, "l2", f"zipf_mixture_{n}x{d}_c{c}",
+                    query_seed)
 
 
 def scaled_mixture(n, d, q, c=4096, sigma=0.4, seed=0, backend="numpy", device="cpu") -> Workload:
