@@ -199,295 +199,12 @@ __global__ void __launch_bounds__(256) ivf_sq8_scan_kernel(IvfQueryArgs a) {
     }
 }
 
-// ---- 3a'. exact-mode SQ8 stream kernel (bulk-copy staged, warp-specialised) ----------------------
-// One CTA per (query, split) of its candidate stream. Warp 8 (one thread) is the producer: it walks the
-// query's probed lists (segment table in shared memory) and streams each tile of consecutive list rows
-// into a 4-stage shared-memory ring with one cp.async.bulk per tile, completion tracked by an mbarrier
-// (expect-tx bytes). Warps 0-7 consume: 16 threads per row, each owning W code bytes whose scale and
-// shifted query are held in registers; codes are decoded in registers (byte -> 2^23 + byte -> exact
-// integer) and the squared differences summed with packed f32x2 FMAs; each warp keeps its own best R.
-// Every wait is bounded (about 2 s); a timeout sets a device flag and the CTA winds down.
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ uint64_t global_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-// Waits for the phase of `bar` with the given parity to complete; gives up after ~2 s and flags it.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = global_ns();
-    while (!mbar_try_wait(bar, parity)) {
-        if (global_ns() - t0 > 2000000000ull) {
-            if (err) atomicExch(err, 1);
-            return false;
-        }
-    }
-    return true;
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ uint64_t pk2(float lo, float hi) {
-    uint64_t r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-__device__ __forceinline__ float2 upk2(uint64_t v) {
-    float2 f;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(f.x), "=f"(f.y) : "l"(v));
-    return f;
-}
-__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
-    uint64_t d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
-    uint64_t d;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-// codes b0 and b0+1 of `w` as two exact floats
-__device__ __forceinline__ uint64_t codes2(uint32_t w, int b0, uint64_t minus_2p23) {
-    const uint32_t lo = __byte_perm(w, 0x4B000000u, 0x7540u | b0);
-    const uint32_t hi = __byte_perm(w, 0x4B000000u, 0x7540u | (b0 + 1));
-    uint64_t r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(lo), "r"(hi));
-    return add2(r, minus_2p23);
-}
-
-constexpr int kStreamStages = 4;
-
-template <int W>
-__global__ void __launch_bounds__(288) ivf_sq8_stream_kernel(IvfQueryArgs a, int tile_rows) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    constexpr int DPAD8 = 16 * W;
-    const int cap = topk_cap(a.R);
-    const int npc = a.plan.npc;
-    unsigned char* sTiles = smem_raw;
-    size_t off = (size_t)kStreamStages * tile_rows * DPAD8;
-    float* wKey = reinterpret_cast<float*>(smem_raw + off);
-    off += (size_t)8 * cap * 4;
-    int* wId = reinterpret_cast<int*>(smem_raw + off);
-    off += (size_t)8 * cap * 4;
-    int64_t* sPref = reinterpret_cast<int64_t*>(smem_raw + off);
-    off += (size_t)(npc + 1) * 8;
-    int64_t* sStart = reinterpret_cast<int64_t*>(smem_raw + off);
-    off += (size_t)npc * 8;
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + off);
-    uint64_t* empty = full + kStreamStages;
-    int* sMeta = reinterpret_cast<int*>(empty + kStreamStages);  // [stage][n rows, first row]
-
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int q = blockIdx.x, split = blockIdx.y;
-    const int ns = a.plan.n_seg[q];
-    if (tid == 0) {
-        for (int s = 0; s < kStreamStages; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 8);
-        }
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    for (int j = tid; j < ns; j += blockDim.x) sStart[j] = a.plan.seg_start[(int64_t)q * npc + j];
-    for (int j = tid; j <= ns; j += blockDim.x) sPref[j] = a.plan.seg_pref[(int64_t)q * (npc + 1) + j];
-    __syncthreads();
-    const int64_t L = a.plan.n_cands[q];
-    const int64_t ps = L * split / a.nsplit, pe = L * (split + 1) / a.nsplit;
-
-    if (warp == 8) {
-        // ---- producer ----
-        if (lane == 0) {
-            int j = 0;
-            if (ns > 0) {
-                while (j + 1 < ns && sPref[j + 1] <= ps) ++j;
-            }
-            int64_t pos = ps, t = 0;
-            int last_phase[kStreamStages];
-            for (int s = 0; s < kStreamStages; ++s) last_phase[s] = -1;
-            while (true) {
-                int n = 0;
-                int64_t row0 = 0;
-                if (pos < pe) {
-                    int64_t seg_end;
-                    if (ns < 0) {
-                        seg_end = a.ix.n;
-                        row0 = pos;
-                    } else {
-                        while (sPref[j + 1] <= pos) ++j;
-                        seg_end = sPref[j + 1];
-                        row0 = sStart[j] + (pos - sPref[j]);
-                    }
-                    n = (int)min((int64_t)tile_rows, min(seg_end, pe) - pos);
-                }
-                const int s = (int)(t % kStreamStages);
-                const uint32_t ph = (uint32_t)((t / kStreamStages) & 1);
-                if (!mbar_wait(&empty[s], ph ^ 1u, a.err)) break;
-                last_phase[s] = -1;  // the stage's previous copy has been consumed
-                sMeta[2 * s] = n;
-                sMeta[2 * s + 1] = (int)row0;
-                if (n > 0) {
-                    mbar_expect_tx(&full[s], (uint32_t)(n * DPAD8));
-                    bulk_g2s(sTiles + (size_t)s * tile_rows * DPAD8, a.ix.codes + row0 * DPAD8, (uint32_t)(n * DPAD8),
-                             &full[s]);
-                    last_phase[s] = (int)ph;
-                } else {
-                    mbar_arrive(&full[s]);
-                }
-                ++t;
-                pos += n;
-                if (n == 0) break;
-            }
-            // no copy may still be landing when the CTA exits (matters only after a timeout)
-            for (int s = 0; s < kStreamStages; ++s)
-                if (last_phase[s] >= 0) mbar_wait(&full[s], (uint32_t)last_phase[s], nullptr);
-        }
-        return;
-    }
-
-    // ---- consumers ----
-    const int j16 = lane & 15;
-    const uint64_t minus_2p23 = pk2(-8388608.f, -8388608.f);
-    uint64_t sc2[W / 2], nq2[W / 2];
-    {
-        const float* qv = a.q + (int64_t)q * a.ldq;
-#pragma unroll
-        for (int u = 0; u < W / 2; ++u) {
-            const int d0 = j16 * W + 2 * u, d1 = d0 + 1;
-            const float s0 = d0 < a.ix.dim ? a.ix.scale[d0] : 0.f;
-            const float s1 = d1 < a.ix.dim ? a.ix.scale[d1] : 0.f;
-            const float q0 = d0 < a.ix.dim ? __fsub_rn(qv[d0], a.ix.offset[d0]) : 0.f;
-            const float q1 = d1 < a.ix.dim ? __fsub_rn(qv[d1], a.ix.offset[d1]) : 0.f;
-            sc2[u] = pk2(s0, s1);
-            nq2[u] = pk2(-q0, -q1);
-        }
-    }
-    WarpTopK top;
-    top.init(wKey + warp * cap, wId + warp * cap, a.R);
-    for (int64_t t = 0;; ++t) {
-        const int s = (int)(t % kStreamStages);
-        if (!mbar_wait(&full[s], (uint32_t)((t / kStreamStages) & 1), a.err)) break;
-        const int n = sMeta[2 * s];
-        const int row0 = sMeta[2 * s + 1];
-        if (n == 0) break;
-        const unsigned char* tile = sTiles + (size_t)s * tile_rows * DPAD8;
-        for (int r0 = warp * 2; r0 < n; r0 += 16) {
-            const int r = r0 + (lane >> 4);
-            const bool valid = r < n;
-            const unsigned char* rowp = tile + (size_t)(valid ? r : r0) * DPAD8 + j16 * W;
-            uint64_t acc0 = 0, acc1 = 0;
-#pragma unroll
-            for (int u = 0; u < W / 8; ++u) {
-                const uint2 c = *reinterpret_cast<const uint2*>(rowp + 8 * u);
-                const uint64_t c01 = codes2(c.x, 0, minus_2p23), c23 = codes2(c.x, 2, minus_2p23);
-                const uint64_t c45 = codes2(c.y, 0, minus_2p23), c67 = codes2(c.y, 2, minus_2p23);
-                const uint64_t d01 = fma2(c01, sc2[4 * u], nq2[4 * u]);
-                const uint64_t d23 = fma2(c23, sc2[4 * u + 1], nq2[4 * u + 1]);
-                const uint64_t d45 = fma2(c45, sc2[4 * u + 2], nq2[4 * u + 2]);
-                const uint64_t d67 = fma2(c67, sc2[4 * u + 3], nq2[4 * u + 3]);
-                acc0 = fma2(d01, d01, acc0);
-                acc1 = fma2(d23, d23, acc1);
-                acc0 = fma2(d45, d45, acc0);
-                acc1 = fma2(d67, d67, acc1);
-            }
-            const float2 f = upk2(add2(acc0, acc1));
-            float dist = f.x + f.y;
-            dist += __shfl_xor_sync(0xffffffffu, dist, 8);
-            dist += __shfl_xor_sync(0xffffffffu, dist, 4);
-            dist += __shfl_xor_sync(0xffffffffu, dist, 2);
-            dist += __shfl_xor_sync(0xffffffffu, dist, 1);
-            top.offer(dist, row0 + r, valid && j16 == 0);
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);
-    }
-    top.compact();
-    asm volatile("bar.sync 1, 256;" ::: "memory");
-    if (warp == 0) {
-        for (int w = 1; w < 8; ++w)
-            for (int e0 = 0; e0 < a.R; e0 += 32) {
-                const int e = e0 + lane;
-                const bool ok = e < a.R && wId[w * cap + e] != kNoId;
-                top.offer(ok ? wKey[w * cap + e] : kInf, ok ? wId[w * cap + e] : kNoId, ok);
-            }
-        top.compact();
-        float* okey = a.keyR + ((int64_t)q * a.nsplit + split) * a.R;
-        int* oid = a.idR + ((int64_t)q * a.nsplit + split) * a.R;
-        for (int e = lane; e < a.R; e += 32) {
-            const bool ok = e < top.count;
-            okey[e] = ok ? wKey[e] : kInf;
-            oid[e] = ok ? wId[e] : kNoId;
-        }
-    }
-}
-
-static int stream_tile_rows(int dpad8) { return std::max(16, (24576 / dpad8) / 16 * 16); }
-
-static size_t stream_smem(int dpad8, int R, int npc) {
-    return (size_t)kStreamStages * stream_tile_rows(dpad8) * dpad8 + (size_t)8 * topk_cap(R) * 8 +
-           (size_t)(2 * npc + 1) * 8 + (size_t)kStreamStages * 16 + (size_t)kStreamStages * 8 + 64;
-}
-
-template <int W>
-static int launch_stream_t(const IvfQueryArgs& a, cudaStream_t st) {
-    const int dpad8 = 16 * W;
-    const size_t smem = stream_smem(dpad8, a.R, a.plan.npc);
-    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(ivf_sq8_stream_kernel<W>)));
-    dim3 grid(a.plan.nq, a.nsplit);
-    ivf_sq8_stream_kernel<W><<<grid, 288, smem, st>>>(a, stream_tile_rows(dpad8));
-    ANN_LAUNCH_CHECK();
-    return ANN_OK;
-}
-
-// Whether the stream kernel serves this shape (else the cp.async kernel below does).
-static bool stream_ok(const IvfQueryArgs& a) {
-    const int W = a.ix.dpad8 / 16;
-    const bool w_ok = a.ix.dpad8 % 128 == 0 && (W == 8 || W == 16 || W == 24 || W == 32 || W == 48 || W == 64);
-    return w_ok && a.err != nullptr && a.plan.npc <= 1024 && stream_smem(a.ix.dpad8, a.R, a.plan.npc) <= 227 * 1024;
-}
-
-static int launch_stream(const IvfQueryArgs& a, cudaStream_t st) {
-    switch (a.ix.dpad8 / 16) {
-    case 8: return launch_stream_t<8>(a, st);
-    case 16: return launch_stream_t<16>(a, st);
-    case 24: return launch_stream_t<24>(a, st);
-    case 32: return launch_stream_t<32>(a, st);
-    case 48: return launch_stream_t<48>(a, st);
-    default: return launch_stream_t<64>(a, st);
-    }
-}
-
 static size_t sq8_scan_smem(int dpad8, int R) {
     return (size_t)2 * kSq8Tile * (dpad8 + 16) + (size_t)2 * dpad8 * 4 + (size_t)topk_cap(R) * 8 + 16;
 }
 
 int launch_ivf_sq8_scan(const IvfQueryArgs& a, cudaStream_t st) {
     if (a.plan.nq == 0) return ANN_OK;
-    if (a.use_stream && stream_ok(a)) return launch_stream(a, st);
     ANN_CHECK_ARG(a.ix.dpad8 % 32 == 0, "sq8 scan: code stride %d not a multiple of 32", a.ix.dpad8);
     const size_t smem = sq8_scan_smem(a.ix.dpad8, a.R);
     if (smem > 227 * 1024) {

@@ -72,7 +72,6 @@ struct IvfQueryArgs {
     float* V;                  // reference mode [nq, L]
     unsigned long long* ndist; // device counter of candidates scanned (get_n_distances)
     int* err;                  // device flag: a bounded wait gave up
-    int use_stream;            // exact mode: use the bulk-copy stream kernel where it applies
     int metric;                // re-rank metric: ANN_METRIC_L2 (default) or ANN_METRIC_IP
     int64_t* out_ids;          // [nq, k]
     float* out_dists;          // [nq, k]
