@@ -631,18 +631,10 @@ int ann_ivf_build_tables(ann_ivf* h, int32_t n_tables, int32_t n_bits, void* str
 namespace {
 
 // Exact-mode SQ8 pass: batches of at least kBatchedMinQueries queries run list-major (ivf_batched.cu),
-// smaller ones query by query (ivf.cu). ANNB_IVF_SCAN=cpasync or =stream forces a per-query kernel
-// (for comparisons).
+// smaller ones query by query (ivf.cu).
 constexpr int kBatchedMinQueries = 32;
 constexpr int kQueryOrderMinBatch = 256;  // smaller batches have no shared candidates worth grouping
 constexpr int kEveryRowMinSplit = 8;      // exact batches split fewer ways redo every-row queries apart
-enum { kScanBatched = 0, kScanCpAsync = 1, kScanStream = 2 };
-const int g_scan_kind = [] {
-    const char* v = getenv("ANNB_IVF_SCAN");
-    if (v && std::strcmp(v, "stream") == 0) return (int)kScanStream;
-    if (v && std::strcmp(v, "cpasync") == 0) return (int)kScanCpAsync;
-    return (int)kScanBatched;
-}();
 
 struct IvfQueryCfg {
     int k, npc, R, nsplit, num_threads, bqc, nsplit_c, ncp;
@@ -707,7 +699,12 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
         sz.take<float>((size_t)nq * h->dpad);
         sz.take<char>(c.bscratch);
     }
-    if (c.lsh) sz.take<int32_t>((size_t)nq * c.ub_cand);
+    const int lsh_p = c.lsh ? lsh_flips_kept(h->B, c.n_probes) : 0;
+    if (c.lsh) {
+        sz.take<int32_t>((size_t)nq * c.ub_cand);
+        sz.take<uint32_t>((size_t)nq * h->T);
+        sz.take<int>((size_t)nq * h->T * std::max(1, lsh_p));
+    }
     if (c.lsh_keys) sz.take<float>((size_t)nq * c.ub_cand);
     if (c.tc) {
         sz.take<float>((size_t)nq * h->C);  // BF16 coarse keys
@@ -748,7 +745,10 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     float* DP = c.ref ? cv.take<float>((size_t)nq * c.ub * (c.ncp + 2)) : nullptr;
     float* qs = c.batched ? cv.take<float>((size_t)nq * h->dpad) : nullptr;
     void* bscratch = c.batched ? cv.take<char>(c.bscratch) : nullptr;
+    const int lsh_p = c.lsh ? lsh_flips_kept(h->B, c.n_probes) : 0;
     int32_t* cand = c.lsh ? cv.take<int32_t>((size_t)nq * c.ub_cand) : nullptr;
+    uint32_t* lsig = c.lsh ? cv.take<uint32_t>((size_t)nq * h->T) : nullptr;
+    int* lpert = c.lsh ? cv.take<int>((size_t)nq * h->T * std::max(1, lsh_p)) : nullptr;
     float* lkeys = c.lsh_keys ? cv.take<float>((size_t)nq * c.ub_cand) : nullptr;
     float* ckeys = c.tc ? cv.take<float>((size_t)nq * h->C) : nullptr;
     __nv_bfloat16* qb = c.tc ? cv.take<__nv_bfloat16>((size_t)nq * h->kpad) : nullptr;
@@ -779,7 +779,6 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     a.num_threads = c.num_threads;
     a.ndist = h->d_ndist;
     a.err = h->d_err;
-    a.use_stream = g_scan_kind == kScanStream;
     a.out_ids = ids_dev;
     a.out_dists = dists_dev;
 
@@ -804,18 +803,24 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         if ((rc = launch_select_topk(Dc, h->C, nullptr, nq, c.npc, nullptr, pkey, probes, st))) return rc;
     }
     h->prof.mark(prec, st);
-    // 2. plan: whole lists, or the LSH buckets' explicit streams
+    // 2. plan: whole lists, or the LSH buckets' explicit streams (signatures first, their own stage)
+    LshCandArgs la{};
     if (c.lsh) {
-        LshCandArgs la{};
         la.ix = a.ix;
         la.lsh = h->lsh_view();
-        la.probes = probes;
-        la.npc = c.npc;
         la.q = qdev;
         la.ldq = h->dpad;
         la.nq = nq;
-        la.k = c.k;
         la.n_probes = c.n_probes;
+        la.sig = lsig;
+        la.pert = lpert;
+        if ((rc = launch_lsh_signatures(la, st))) return rc;
+    }
+    h->prof.mark(prec, st);
+    if (c.lsh) {
+        la.probes = probes;
+        la.npc = c.npc;
+        la.k = c.k;
         la.max_c = c.max_c;
         la.ld = c.ub_cand;
         la.largest_list = h->sizes_desc.empty() ? 1 : h->sizes_desc[0];
@@ -826,7 +831,6 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         if ((rc = launch_lsh_candidates(la, st))) return rc;
         a.plan.cand_ids = cand;
         a.plan.cand_ld = c.ub_cand;
-        a.use_stream = false;
     } else if ((rc = launch_ivf_plan(a, st))) {
         return rc;
     }
@@ -879,6 +883,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                 g.g_lists = h->C;
                 g.g_item_list = titem_list;
                 if ((rc = launch_tc_gemm(Apk, h->base_bf16, g, st))) return rc;
+                h->prof.mark(prec, st);
                 RadixSelectArgs rs{};
                 rs.keys = D;
                 rs.offs = b.cand_off;
@@ -891,6 +896,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                 if ((rc = launch_radix_select(rs, nq, st))) return rc;
             } else {
                 if ((rc = launch_batched(b, qdev, qs, D, st))) return rc;
+                h->prof.mark(prec, st);
                 // the best R of each stream as a set (ties by stream position); the re-rank orders them
                 RadixSelectArgs rs{};
                 rs.keys = D;
@@ -908,6 +914,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     }
     if (!done && c.lsh_keys) {
         if ((rc = launch_ivf_sq8_dists(a, lkeys, c.ub_cand, st))) return rc;
+        h->prof.mark(prec, st);
         if ((rc = launch_select_topk(lkeys, c.ub_cand, n_cands, nq, c.R, &a.plan, keyR, idR, st, nullptr, true))) return rc;
         done = true;
     }
@@ -915,7 +922,8 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     } else if (!c.ref) {
         a.keyR = keyS;
         a.idR = idS;
-        if ((rc = launch_ivf_sq8_scan(a, st))) return rc;
+        if ((rc = launch_ivf_sq8_scan(a, st))) return rc;  // keys and each split's best R in one kernel
+        h->prof.mark(prec, st);
         if (c.nsplit > 1) {
             MergeArgs m{keyS, idS, nq, c.nsplit, c.R, c.R, 0, nullptr, nullptr};
             m.out_id32 = idR;
@@ -932,6 +940,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         a.V = DP + (size_t)nq * c.ub;
         a.P = DP + (size_t)2 * nq * c.ub;
         if ((rc = launch_ivf_ref_sq8(a, c.ub, st))) return rc;
+        h->prof.mark(prec, st);
         if ((rc = launch_select_topk(a.V, c.ub, n_cands, nq, c.R, &a.plan, keyR, idR, st, nullptr, true))) return rc;
     }
     h->prof.mark(prec, st);
@@ -971,7 +980,6 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                 if ((rc = launch_ivf_ref_sq8(b, L, st))) return rc;
                 if ((rc = launch_select_topk(b.V, L, b.plan.n_cands, 1, c.R, &b.plan, kq, iq, st, nullptr, true))) return rc;
             } else {
-                b.use_stream = false;
                 b.nsplit = nsp;
                 b.keyR = big;
                 b.idR = reinterpret_cast<int*>(big + (size_t)nsp * c.R);
@@ -1052,7 +1060,7 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     }
     c.ncp = ref_num_checkpoints(h->dim);
     c.coarse_flat = !c.ref && c.npc <= 512;
-    c.batched = !c.ref && !c.lsh && (c.tc || (g_scan_kind == kScanBatched && nq >= kBatchedMinQueries));
+    c.batched = !c.ref && !c.lsh && (c.tc || nq >= kBatchedMinQueries);
     if (c.tc && (rc0 = ivf_ensure_bf16(h, st))) return rc0;
     const int dpad = h->dpad;
     const bool host = mem == ANN_MEM_HOST;
@@ -1156,13 +1164,13 @@ int ann_ivf_set_profiling(ann_ivf* h, int32_t enable) {
     return ANN_OK;
 }
 
-int ann_ivf_profile(ann_ivf* h, double* out6) {
-    ANN_CHECK_ARG(h != nullptr && out6 != nullptr, "null argument");
+int ann_ivf_profile(ann_ivf* h, double* out8) {
+    ANN_CHECK_ARG(h != nullptr && out8 != nullptr, "null argument");
     DeviceGuard g(h->device);
     h->prof.collect();
-    for (int i = 0; i < 4; ++i) out6[i] = h->prof.total_ms[i];
-    out6[4] = (double)h->prof.calls;
-    out6[5] = (double)h->query_count;
+    for (int i = 0; i < 6; ++i) out8[i] = h->prof.total_ms[i];
+    out8[6] = (double)h->prof.calls;
+    out8[7] = (double)h->query_count;
     return ANN_OK;
 }
 

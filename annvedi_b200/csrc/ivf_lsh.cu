@@ -9,8 +9,9 @@
 // and each probed bucket, never inside a bucket; fewer than k candidates fall back to every row
 // (:453-457).
 //
-// One warp per query, no block barriers. The signatures and flip orders are computed once. Per probed
-// list the warp walks the list's T * (1 + flips) buckets 32 at a time: each lane loads one bucket's
+// Two kernels, one warp per query each, no block barriers. lsh_signatures_kernel computes the query's
+// signature in every table and its flip masks in probe order once (global scratch); lsh_candidates_kernel
+// walks the buckets. Per probed list the walk warp walks the list's T * (1 + flips) buckets 32 at a time: each lane loads one bucket's
 // bounds, a warp scan lays the 32 buckets' members out in walk order, and the members are read 32 at a
 // time. A member is new if the list's visited bitmap (shared memory) does not hold it and no earlier lane
 // of the same 32 holds the same row (__match_any_sync): the first occurrence in walk order wins, as in
@@ -35,34 +36,39 @@ __device__ __forceinline__ bool flip_before(float sa, int ga, float sb, int gb) 
     return sa < sb || (sa == sb && ga < gb);
 }
 
-// Per-warp shared memory (32-bit words): q - mean [dim], dots [T * B], signatures [T], flip masks
-// [T * P], visited bitmap of one list [nwords].
-struct LshWarpSmem {
-    int qm, dots, sig, pert, vis, total;
-    __host__ __device__ LshWarpSmem(int dim, int T, int B, int P, int nwords) {
+// Per-warp shared memory (32-bit words) of the signatures kernel: q - mean [dim], dots [T * B].
+struct LshSigSmem {
+    int qm, dots, total;
+    __host__ __device__ LshSigSmem(int dim, int T, int B) {
         qm = 0;
         dots = qm + dim;
-        sig = dots + T * B;
+        total = (dots + T * B + 3) & ~3;  // 16-byte aligned per warp
+    }
+};
+// ... and of the walk: signatures [T], flip masks [T * P], visited bitmap of one list [nwords].
+struct LshWarpSmem {
+    int sig, pert, vis, total;
+    __host__ __device__ LshWarpSmem(int T, int P, int nwords) {
+        sig = 0;
         pert = sig + T;
         vis = pert + T * P;
-        total = (vis + nwords + 3) & ~3;  // 16-byte aligned per warp
+        total = (vis + nwords + 3) & ~3;
     }
 };
 
-__global__ void __launch_bounds__(32 * kMaxWarps) lsh_candidates_kernel(LshCandArgs a, int P, int nwords) {
+__global__ void __launch_bounds__(32 * kMaxWarps) lsh_signatures_kernel(LshCandArgs a, int P) {
     extern __shared__ __align__(16) uint32_t smem_w[];
     const int T = a.lsh.T, B = a.lsh.B, TB = T * B;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
     if (qi >= a.nq) return;  // the whole warp; no block barrier follows
     const int dim = a.ix.dim;
-    const LshWarpSmem L(dim, T, B, P, nwords);
+    const LshSigSmem L(dim, T, B);
     uint32_t* ws = smem_w + (size_t)warp * L.total;
     float* sQm = reinterpret_cast<float*>(ws + L.qm);
     float* sDot = reinterpret_cast<float*>(ws + L.dots);
-    uint32_t* sSig = ws + L.sig;
-    int* sPert = reinterpret_cast<int*>(ws + L.pert);
-    uint32_t* sVis = ws + L.vis;
+    uint32_t* sSig = a.sig + (int64_t)qi * T;
+    int* sPert = a.pert + (int64_t)qi * T * P;
     const float* q = a.q + (int64_t)qi * a.ldq;
     // 1. the query's dot with every projection: sum over d ascending of (q[d] - mean[d]) * p[d], each
     // product rounded, no fused multiply-add (the restatement's order). Lane l runs four independent sums,
@@ -137,6 +143,21 @@ __global__ void __launch_bounds__(32 * kMaxWarps) lsh_candidates_kernel(LshCandA
             }
         }
     }
+}
+
+__global__ void __launch_bounds__(32 * kMaxWarps) lsh_candidates_kernel(LshCandArgs a, int P, int nwords) {
+    extern __shared__ __align__(16) uint32_t smem_w[];
+    const int T = a.lsh.T, B = a.lsh.B;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (qi >= a.nq) return;  // the whole warp; no block barrier follows
+    const LshWarpSmem L(T, P, nwords);
+    uint32_t* ws = smem_w + (size_t)warp * L.total;
+    uint32_t* sSig = ws + L.sig;
+    int* sPert = reinterpret_cast<int*>(ws + L.pert);
+    uint32_t* sVis = ws + L.vis;
+    for (int i = lane; i < T; i += 32) sSig[i] = a.sig[(int64_t)qi * T + i];
+    for (int i = lane; i < T * P; i += 32) sPert[i] = a.pert[(int64_t)qi * T * P + i];
     __syncwarp();
     // 3. the walk
     const int64_t nb = (int64_t)1 << B;
@@ -288,15 +309,34 @@ int launch_lsh_candidates(const LshCandArgs& a, cudaStream_t st) {
     ANN_CHECK_ARG(a.lsh.T >= 1 && a.lsh.T <= 64 && a.lsh.B >= 0 && a.lsh.B <= 16 && a.lsh.T * a.lsh.B <= kMaxSigDots,
                   "LSH candidates: %d tables of %d bits", a.lsh.T, a.lsh.B);
     ANN_CHECK_ARG(a.lsh.B == 0 || a.lsh.projT != nullptr, "LSH candidates: no projections");
+    ANN_CHECK_ARG(a.sig != nullptr && a.pert != nullptr, "LSH candidates: no signature scratch");
     const int P = lsh_flips_kept(a.lsh.B, a.n_probes);
     const int nwords = (int)std::max<int64_t>(1, (a.largest_list + 31) / 32);
-    const LshWarpSmem L(a.ix.dim, a.lsh.T, a.lsh.B, P, nwords);
+    const LshWarpSmem L(a.lsh.T, P, nwords);
     const size_t per_warp = sizeof(uint32_t) * (size_t)L.total;
     const int warps = (int)std::min<size_t>(kMaxWarps, (227 * 1024) / per_warp);
     ANN_CHECK_ARG(warps >= 1, "LSH candidates: lists of %lld rows with %d tables x %d flips need too much shared memory",
                   (long long)a.largest_list, a.lsh.T, P);
     ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(lsh_candidates_kernel)));
     lsh_candidates_kernel<<<(unsigned)ceil_div(a.nq, warps), 32 * warps, per_warp * warps, st>>>(a, P, nwords);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int launch_lsh_signatures(const LshCandArgs& a, cudaStream_t st) {
+    if (a.nq == 0) return ANN_OK;
+    ANN_CHECK_ARG(a.lsh.T >= 1 && a.lsh.T <= 64 && a.lsh.B >= 0 && a.lsh.B <= 16 && a.lsh.T * a.lsh.B <= kMaxSigDots,
+                  "LSH signatures: %d tables of %d bits", a.lsh.T, a.lsh.B);
+    ANN_CHECK_ARG(a.lsh.B == 0 || a.lsh.projT != nullptr, "LSH signatures: no projections");
+    ANN_CHECK_ARG(a.sig != nullptr && a.pert != nullptr, "LSH signatures: no scratch");
+    const int P = lsh_flips_kept(a.lsh.B, a.n_probes);
+    const LshSigSmem L(a.ix.dim, a.lsh.T, a.lsh.B);
+    const size_t per_warp = sizeof(uint32_t) * (size_t)L.total;
+    const int warps = (int)std::min<size_t>(kMaxWarps, (227 * 1024) / per_warp);
+    ANN_CHECK_ARG(warps >= 1, "LSH signatures: dim %d with %d projections needs too much shared memory", a.ix.dim,
+                  a.lsh.T * a.lsh.B);
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(lsh_signatures_kernel)));
+    lsh_signatures_kernel<<<(unsigned)ceil_div(a.nq, warps), 32 * warps, per_warp * warps, st>>>(a, P);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

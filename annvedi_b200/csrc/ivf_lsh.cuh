@@ -32,10 +32,15 @@ struct LshCandArgs {
     int64_t* n_cands;       // [nq]
     int32_t* n_seg;         // [nq] 0, or -1 when the query falls back to every row
     unsigned long long* ndist;  // distance counter (+= n_cands)
+    uint32_t* sig;          // [nq, T] the query's signature per table (written by launch_lsh_signatures)
+    int* pert;              // [nq, T, P] its flip masks in probe order, P = lsh_flips_kept(B, n_probes)
 };
 
-// LSHIndex::query's candidate stream (competitors/ivf_lsh/src/lsh_index_optimized.cpp:352-457), one warp
-// per query.
+// The query's signatures and multiprobe flips (lsh_index_optimized.cpp:376-394, 407-426), one warp per
+// query, into a.sig / a.pert.
+int launch_lsh_signatures(const LshCandArgs& a, cudaStream_t st);
+// LSHIndex::query's candidate stream (competitors/ivf_lsh/src/lsh_index_optimized.cpp:352-457) from the
+// signatures above, one warp per query.
 int launch_lsh_candidates(const LshCandArgs& a, cudaStream_t st);
 // Flips probed per table: min(n_probes, m + m(m-1)/2), m = min(B, n_probes) (:407-426).
 int lsh_flips_kept(int B, int n_probes);

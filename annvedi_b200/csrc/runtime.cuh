@@ -44,6 +44,7 @@ int ws_reserve_big(ann_workspace* ws, size_t bytes);
 // chosen at begin(), so different call kinds report into different slots of one table.
 struct StageProfiler {
     static constexpr int kStages = 6;
+    static constexpr size_t kMaxPending = 1024;
     bool enabled = false;
     struct Rec {
         cudaEvent_t ev[kStages + 1];
@@ -73,6 +74,7 @@ struct StageProfiler {
     int begin(cudaStream_t st, int first_stage = 0) {
         if (!enabled) return -1;
         std::lock_guard<std::mutex> lk(mu);
+        if (pending.size() >= kMaxPending) collect_locked();  // bounded record list for long runs
         Rec r{};
         r.first = first_stage;
         r.nstage = 0;
@@ -91,6 +93,9 @@ struct StageProfiler {
     }
     void collect() {
         std::lock_guard<std::mutex> lk(mu);
+        collect_locked();
+    }
+    void collect_locked() {
         for (Rec& r : pending) {
             for (int s = 0; s < r.nstage; ++s) {
                 cudaEventSynchronize(r.ev[s + 1]);

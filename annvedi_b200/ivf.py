@@ -39,6 +39,8 @@ class IVFIndex:
         self.device = device
         self.mode = mode
         self.num_threads = int(num_threads) if num_threads else (os.cpu_count() or 1)
+        if mode == "reference":  # the reference times every query's stages (lsh_index_optimized.cpp:305-515)
+            _lib.check(self._lib.ann_ivf_set_profiling(self._h, 1))
         self._n = 0
         self._dim = 0
         self._C = 0
@@ -171,18 +173,25 @@ class IVFIndex:
         _lib.check(self._lib.ann_ivf_set_profiling(self._h, int(enable)))
 
     def get_profile_results(self) -> dict:
-        """The reference's keys (lsh_index_optimized.cpp:535-548), from CUDA events: averages per
-        query of the batched stages (a batch's stage time divided by its queries)."""
-        out = (ctypes.c_double * 6)()
+        """The reference's keys (lsh_index_optimized.cpp:535-548): with queries answered, the six
+        averages per query, else {"query_count": 0}, as the reference returns them. The stage times come
+        from CUDA events on the query stream while profiling is on (the default in reference mode; a
+        batch's stage time is divided by its queries): centroid search = the coarse ranking, signature
+        calc = the LSH signatures and flips, bucket lookup = the candidate plan / bucket walk, distance
+        calc = the SQ8 (or BF16) keys plus the exact FP32 re-rank and its top-k, candidate sort = the
+        selection of the best R candidates (the reference's partial sort before its re-rank)."""
+        out = (ctypes.c_double * 8)()
         _lib.check(self._lib.ann_ivf_profile(self._h, out))
-        nq = int(out[5])
-        if nq == 0 or out[4] == 0:
-            return {"query_count": nq}
-        return {"avg_centroid_search_ms": out[0] / nq, "avg_signature_calc_ms": 0.0,
-                "avg_bucket_lookup_ms": out[1] / nq, "avg_distance_calc_ms": (out[2] + out[3]) / nq,
-                "avg_candidate_sort_ms": 0.0, "query_count": nq,
-                "stage_ms": {"coarse": out[0], "plan": out[1], "sq8": out[2], "rerank": out[3]},
-                "profiled_calls": int(out[4])}
+        nq = int(out[7])
+        if nq == 0:
+            return {"query_count": 0}
+        coarse, sig, plan, keys, select, rerank = (float(out[i]) for i in range(6))
+        return {"avg_centroid_search_ms": coarse / nq, "avg_signature_calc_ms": sig / nq,
+                "avg_bucket_lookup_ms": plan / nq, "avg_distance_calc_ms": (keys + rerank) / nq,
+                "avg_candidate_sort_ms": select / nq, "query_count": nq,
+                "stage_ms": {"coarse": coarse, "signatures": sig, "plan": plan, "keys": keys, "select": select,
+                             "rerank": rerank},
+                "profiled_calls": int(out[6])}
 
     def reset_profile_results(self) -> None:
         _lib.check(self._lib.ann_ivf_reset_profile(self._h))

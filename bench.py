@@ -518,7 +518,7 @@ def run_ours(args, rank, world, local):
         prof = ivf.get_profile_results()
         stage = prof.get("stage_ms", {})
         calls = max(1, prof.get("profiled_calls", 1))
-        sq8_ms = stage.get("sq8", 0.0) / calls
+        sq8_ms = stage.get("keys", 0.0) / calls
         cands = cands_timed
         bytes_per_launch = (cands / max(1, args.steps)) * d
         achieved = bytes_per_launch / (sq8_ms / 1e3) / 1e9 if sq8_ms > 0 else 0.0
