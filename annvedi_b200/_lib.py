@@ -63,6 +63,8 @@ _lib = None
 # (name, restype, argtypes) of every exported function the bindings use.
 SIGNATURES = [
     ("ann_version", ctypes.c_char_p, []),
+    ("ann_kernel_arch", ctypes.c_int, [_i32, _vp]),
+    ("ann_tc_wait_selftest", ctypes.c_int, [_i32, _i64, _vp]),
     ("ann_last_error", ctypes.c_char_p, []),
     ("ann_kernel_launches", _i64, []),
     ("ann_workspace_create", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int]),

@@ -101,9 +101,45 @@ int ws_reserve_big(ann_workspace* ws, size_t bytes) {
 using namespace annb;
 
 
+// An empty kernel compiled with the library's flags: its attributes are the library's code form.
+__global__ void arch_probe_kernel() {}
+
 extern "C" {
 
 const char* ann_version(void) { return "annvedi_b200 0.1 sm_100a"; }
+
+int ann_tc_wait_selftest(int device, int64_t wait_ns, int32_t* flag_out) {
+    clear_error();
+    ANN_CHECK_ARG(flag_out != nullptr, "ann_tc_wait_selftest: flag_out is NULL");
+    ANN_CHECK_ARG(wait_ns >= 1000 && wait_ns <= 2000000000LL, "ann_tc_wait_selftest: wait_ns=%lld outside [1e3, 2e9]",
+                  (long long)wait_ns);
+    DeviceGuard g(device);
+    if (!g.ok) {
+        cudaGetLastError();
+        set_error("ann_tc_wait_selftest: device %d not usable", device);
+        return ANN_ERR_CUDA;
+    }
+    int flag = -1;
+    const int rc = tc_wait_selftest((uint64_t)wait_ns, &flag);
+    *flag_out = flag;
+    return rc;
+}
+
+int ann_kernel_arch(int device, int32_t* out2) {
+    clear_error();
+    ANN_CHECK_ARG(out2 != nullptr, "ann_kernel_arch: out2 is NULL");
+    DeviceGuard g(device);
+    if (!g.ok) {
+        cudaGetLastError();
+        set_error("ann_kernel_arch: device %d not usable", device);
+        return ANN_ERR_CUDA;
+    }
+    cudaFuncAttributes fa{};
+    ANN_CUDA_TRY(cudaFuncGetAttributes(&fa, arch_probe_kernel));
+    out2[0] = fa.binaryVersion;
+    out2[1] = fa.ptxVersion;
+    return ANN_OK;
+}
 const char* ann_last_error(void) { return g_err; }
 int64_t ann_kernel_launches(void) { return g_launches.load(); }
 

@@ -72,11 +72,13 @@ __device__ __forceinline__ bool bar_try_sleep(uint64_t* b, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, int* err) {
+// Waits for the phase; gives up after `limit_ns` (2 s when 0), sets *err = 2 and returns false.
+__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, int* err, uint64_t limit_ns = 0) {
     if (bar_try(b, parity)) return true;
+    const uint64_t limit = limit_ns ? limit_ns : 2000000000ull;
     const uint64_t t0 = gtimer();
     while (!bar_try_sleep(b, parity))
-        if (gtimer() - t0 > 2000000000ull) {
+        if (gtimer() - t0 > limit) {
             if (err) atomicExch(err, 2);
             return false;
         }
@@ -258,7 +260,9 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 0) {
-        if (lane == 0) {  // TMA producer
+        // TMA producer (with test_no_loads it issues nothing, so that the other roles' bounded waits
+        // run out with no copy in flight: the self-test of the timeout path)
+        if (lane == 0 && !a.test_no_loads) {
             int64_t it = 0;
             bool ok = true;
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
@@ -274,7 +278,7 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                 for (int kb = 0; kb < kt; ++kb, ++it) {
                     const int s = (int)(it % kStages);
                     const uint32_t ph = (uint32_t)((it / kStages) & 1);
-                    if (!(ok = bar_wait(&empty[s], ph ^ 1u, a.err))) break;
+                    if (!(ok = bar_wait(&empty[s], ph ^ 1u, a.err, a.wait_ns))) break;
                     bar_expect(&full[s], kABytes + kBBytes);
                     tma_load_2d(sA + s * kABytes, &tmA, kb * kBlockK, (int)arow, &full[s]);
                     tma_load_2d(sB + s * kBBytes, &tmB, kb * kBlockK, (int)brow, &full[s]);
@@ -288,13 +292,13 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++acc) {
                 const int b = (int)(acc & 1);
                 const uint32_t aph = (uint32_t)((acc >> 1) & 1);
-                if (!(ok = bar_wait(&tempty[b], aph ^ 1u, a.err))) break;
+                if (!(ok = bar_wait(&tempty[b], aph ^ 1u, a.err, a.wait_ns))) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t d = tmem + (uint32_t)(b * kBN);
                 for (int kb = 0; kb < kt; ++kb, ++it) {
                     const int s = (int)(it % kStages);
                     const uint32_t ph = (uint32_t)((it / kStages) & 1);
-                    if (!(ok = bar_wait(&full[s], ph, a.err))) break;
+                    if (!(ok = bar_wait(&full[s], ph, a.err, a.wait_ns))) break;
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     // the last k-block's box runs past K (zero fill); its zero columns are not multiplied
                     const int n16 = kb == kt - 1 ? k16_last : kBlockK / kMmaK;
@@ -321,7 +325,7 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
         int64_t acc = 0;
         for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x, ++acc) {
             const int b = (int)(acc & 1);
-            if (!bar_wait(&tfull[b], (uint32_t)((acc >> 1) & 1), a.err)) break;
+            if (!bar_wait(&tfull[b], (uint32_t)((acc >> 1) & 1), a.err, a.wait_ns)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int m0 = (int)(t % mt) * kBM, n0 = (int)(t / mt) * kBN;
             const int m = m0 + lane_base + lane;
@@ -595,6 +599,31 @@ int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream
                    : run_tc_gemm<kTcE4M3, kKeyEpi>(tmA, tmB, a, grid, st);
     ANN_CUDA_TRY(e);
     ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int tc_wait_selftest(uint64_t wait_ns, int* flag_out) {
+    // A [128, 64] and B [256, 64] BF16 (zeros), keys [128, 256], the flag
+    const size_t a_bytes = (size_t)kBM * 64 * 2, b_bytes = (size_t)kBN * 64 * 2, o_bytes = (size_t)kBM * kBN * 4;
+    char* buf = nullptr;
+    ANN_CUDA_TRY(cudaMalloc(&buf, a_bytes + b_bytes + o_bytes + 256));
+    int rc = ANN_OK;
+    cudaStream_t st = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMemsetAsync(buf, 0, a_bytes + b_bytes + o_bytes + 256, st);
+    if (e == cudaSuccess) {
+        int* flag = reinterpret_cast<int*>(buf + a_bytes + b_bytes + o_bytes);
+        TcGemmArgs a{kBM, kBN, 64, nullptr, reinterpret_cast<float*>(buf + a_bytes + b_bytes), kBN, flag};
+        a.wait_ns = wait_ns;
+        a.test_no_loads = 1;
+        rc = launch_tc_gemm(buf, buf + a_bytes, a, st);
+        if (rc == ANN_OK) e = cudaMemcpyAsync(flag_out, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (rc == ANN_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (st) cudaStreamDestroy(st);
+    cudaFree(buf);
+    if (rc) return rc;
+    ANN_CUDA_TRY(e);
     return ANN_OK;
 }
 

@@ -18,7 +18,7 @@ struct TcGemmArgs {
     const float* normA;    // [M] optional per-row addend (|a|^2 turns the L2 key into the squared distance)
     float* out;            // [M, ldo] keys; null in filter mode
     int64_t ldo;
-    int* err;              // device flag set if a bounded wait gives up
+    int* err;              // device flag set (to 2) if a bounded wait gives up
     int b_tile_stride = 1; // B rows of output tile j start at row j * 256 * b_tile_stride (a strided sample)
     int64_t b_rows = 0;    // rows of the B matrix when sampling (0: N)
     // Filter mode (out == null): keys <= tau[m] are appended, as (key, column, row m), to the region of
@@ -47,6 +47,11 @@ struct TcGemmArgs {
     int kind = kTcBF16;
     const float2* col_fac = nullptr;  // per B row, indexed like B's rows
     const float* row_fac = nullptr;   // per A row
+    // Bounded waits: every mbarrier wait gives up after wait_ns (0: 2 s), sets *err = 2 and the CTA
+    // winds down (remaining copies and MMAs drained, TMEM released). test_no_loads (self-test only):
+    // the producer issues no copies, so the waits run out with nothing in flight.
+    uint64_t wait_ns = 0;
+    int test_no_loads = 0;
 };
 
 enum TcRole { kTcBase = 0, kTcQuery = 1 };
@@ -58,6 +63,9 @@ int tc_kpad(int dim, int metric);
 int tc_filter_warps(int M, int N);
 size_t tc_gemm_smem();
 int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream_t st);
+// Runs one small GEMM whose producer issues no copies, with every wait limited to wait_ns, and returns the
+// device flag it left (2: a bounded wait gave up, as it must); the flag is cleared afterwards.
+int tc_wait_selftest(uint64_t wait_ns, int* flag_out);
 // FP32 rows -> E4M3 [rows, kpad] (kpad >= cols, a multiple of 32) with a per-row scale: a query row's
 // scale into qfac[row]; a base row's key factors into bfac[row] (row_mult as for launch_tc_operand).
 int launch_tc_operand_e4m3(const float* x, int64_t rows, int cols, int64_t ld, uint8_t* out, int kpad, int role,

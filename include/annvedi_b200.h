@@ -53,6 +53,18 @@ typedef struct ann_workspace ann_workspace;
 /* Library version string ("annvedi_b200 <major>.<minor> sm_100a"). */
 const char* ann_version(void);
 
+/* The code the loaded library runs on `device` (no counterpart in the reference): out2 = {binary
+ * version, PTX version} of its kernels as cudaFuncGetAttributes reports them (100 = sm_100a machine
+ * code). Needs a visible device. */
+int ann_kernel_arch(int device, int32_t* out2);
+
+/* Self-test of the tensor-core GEMM's bounded waits (no counterpart in the reference; the failure
+ * path of its error status, gf_last_error at competitors/gpu_filter/src/gpu_filter.cu:27-47): one small
+ * GEMM on `device` whose producer issues no copies and whose waits give up after `wait_ns`
+ * (1e3..2e9). Every waiting warp gives up, sets the device flag and leaves; TMEM is released and the
+ * context stays usable. flag_out = the flag the kernel left (2: a wait gave up). */
+int ann_tc_wait_selftest(int device, int64_t wait_ns, int32_t* flag_out);
+
 /* Message for the last failing call on this host thread ("" if none). Mirrors gf_last_error
  * (competitors/gpu_filter/src/gpu_filter.cu:77). */
 const char* ann_last_error(void);
@@ -237,10 +249,11 @@ int64_t ann_ivf_total_distances(ann_ivf* h);
 int ann_ivf_reset_distances(ann_ivf* h);
 
 /* LSHIndex::get_profile_results / reset_profile_results (lsh_index_optimized.cpp:526-548), timed
- * with CUDA events on the query stream: out6 = {coarse ranking ms, plan ms, SQ8 pass ms,
- * re-rank ms, profiled calls, queries}. Totals, not averages. */
+ * with CUDA events on the query stream while profiling is on: out8 = {coarse ranking ms, LSH
+ * signature ms, candidate plan / bucket walk ms, SQ8 (or BF16) key ms, best-R selection ms, FP32
+ * re-rank + top-k ms, profiled calls, queries}. Totals, not averages. */
 int ann_ivf_set_profiling(ann_ivf* h, int32_t enable);
-int ann_ivf_profile(ann_ivf* h, double* out6);
+int ann_ivf_profile(ann_ivf* h, double* out8);
 int ann_ivf_reset_profile(ann_ivf* h);
 
 #ifdef __cplusplus

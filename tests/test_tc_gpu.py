@@ -185,3 +185,28 @@ def test_tc_e4m3_search_recovers_exact(cuda, metric):
         np.testing.assert_allclose(d, fp64_dists(w.base, w.queries, ids), rtol=1e-5, atol=1e-5)
     gt, _ = exact_topk_f64(w.base, w.queries, 50, metric)
     assert np.mean([len(set(a) & set(b)) / 50 for a, b in zip(ids, gt)]) > 0.99
+
+
+def test_bounded_wait_runs_out_and_the_context_stays_usable(cuda):
+    """The GEMM's mbarrier waits are bounded: with no copies issued (self-test), the waits give up after
+    1 ms, the kernel sets its device flag (2) and returns; afterwards the same process searches normally."""
+    import ctypes
+    import time
+    from annvedi_b200 import _lib
+    from annvedi_b200.linear import LinearIndex
+    from tests.helpers import check_exact_topk
+    lib = _lib.load()
+    for _ in range(2):
+        flag = ctypes.c_int32(-1)
+        t0 = time.perf_counter()
+        _lib.check(lib.ann_tc_wait_selftest(0, 1_000_000, ctypes.byref(flag)))
+        assert flag.value == 2, f"device flag {flag.value}"
+        assert time.perf_counter() - t0 < 5.0
+    w = synth.flat_normal(20000, 128, 32, seed=3)
+    ix = LinearIndex(device=0, metric="l2", mode="exact")
+    ix.fit(w.base)
+    ids, d = ix.search_tc(w.queries, 10, refine_r=400)
+    check_exact_topk(w.base, w.queries, ids, d, 10)
+    assert lib.ann_flat_device_status(ix._h) == _lib.ANN_OK  # the index's own flag was never set
+    bad = ctypes.c_int32(0)
+    assert lib.ann_tc_wait_selftest(0, 10, ctypes.byref(bad)) == _lib.ANN_ERR_INVALID
