@@ -5,15 +5,17 @@
 // size, so the big lists are shared by hundreds of queries). Scanning query by query decodes every
 // code once per query; here a work item is (list, up to 32 of the queries probing it, a range of up to
 // kItemRows of its rows): the rows stream through shared memory in tiles of 256 rows x 32 dimensions,
-// are decoded once (code * scale, FP32) and scored against the item's queries with a register-tiled
-// micro-kernel (8 queries x 4 rows per thread, one subtract and one fused multiply-add per element
+// are decoded once (the exact integer of each code, FP32) and scored against the item's queries with a
+// register-tiled micro-kernel (8 queries x 4 rows per thread, two fused multiply-adds per element
 // pair). Each distance lands at its position in its query's candidate stream (the positions the plan
 // assigns, lsh_index_optimized.cpp:372-405 order), so a per-query selection and the FP32 re-rank
 // follow unchanged. Items are taken from a global counter by a persistent grid (uneven list lengths and
 // query counts balance dynamically).
 //
-// The SQ8 distance here is sum_d (code_d * scale_d - (q_d - offset_d))^2 with code*scale rounded to
-// FP32 before the subtraction; the FP32 re-rank that follows decides the final order.
+// The SQ8 distance is the per-query scan kernel's arithmetic (ivf.cu), so a query's keys do not depend
+// on the batch it came in: diff_d = fma(code_d, scale_d, -(q_d - offset_d)), the squares summed by fused
+// multiply-adds in dimension order separately over the two halves of the padded code row, then
+// low + high. The FP32 re-rank that follows decides the final order.
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -88,6 +90,7 @@ __global__ void __launch_bounds__(kThreads, 2) ivf_batched_kernel(IvfBatchArgs a
     const int tq = tid / kWR, tr = tid % kWR;
     for (int d = tid; d < dpad; d += kThreads) sScale[d] = a.ix.scale[d];
     const int nkc = dpad8 / kKC;  // code chunks (>= dpad / kKC; extra chunks hold zero codes and scale)
+    const int half_kc = nkc / 2;  // first chunk of the high half of the padded code row (dpad8 / 2)
 
     while (true) {
         __syncthreads();
@@ -148,11 +151,11 @@ __global__ void __launch_bounds__(kThreads, 2) ivf_batched_kernel(IvfBatchArgs a
             cp_commit();
         };
         issue(0);
-        float acc[kTQ][kTR];
+        float acc[kTQ][kTR], lowh[kTQ][kTR];
 #pragma unroll
         for (int j = 0; j < kTQ; ++j)
 #pragma unroll
-            for (int i = 0; i < kTR; ++i) acc[j][i] = 0.f;
+            for (int i = 0; i < kTR; ++i) acc[j][i] = lowh[j][i] = 0.f;
         for (int64_t step = 0; step < nsteps; ++step) {
             cp_wait0();
             __syncthreads();  // raw codes of this step (and the queries) landed; last step's reads are done
@@ -166,23 +169,30 @@ __global__ void __launch_bounds__(kThreads, 2) ivf_batched_kernel(IvfBatchArgs a
                     const uint32_t w = *reinterpret_cast<const uint32_t*>(raw + r * kKC + w4 * 4);
                     const int d0 = kc * kKC + w4 * 4;
                     float4 v;
-                    v.x = __fmul_rn(__fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u)), 8388608.f),
-                                    d0 < dpad ? sScale[d0] : 0.f);
-                    v.y = __fmul_rn(__fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7541u)), 8388608.f),
-                                    d0 + 1 < dpad ? sScale[d0 + 1] : 0.f);
-                    v.z = __fmul_rn(__fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7542u)), 8388608.f),
-                                    d0 + 2 < dpad ? sScale[d0 + 2] : 0.f);
-                    v.w = __fmul_rn(__fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7543u)), 8388608.f),
-                                    d0 + 3 < dpad ? sScale[d0 + 3] : 0.f);
+                    (void)d0;
+                    v.x = __fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u)), 8388608.f);
+                    v.y = __fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7541u)), 8388608.f);
+                    v.z = __fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7542u)), 8388608.f);
+                    v.w = __fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7543u)), 8388608.f);
                     *reinterpret_cast<float4*>(sX + r * kPitch + w4 * 4) = v;
                 }
             }
             __syncthreads();
+            if (kc == half_kc) {  // the high half starts: keep the low half's sums apart
+#pragma unroll
+                for (int j = 0; j < kTQ; ++j)
+#pragma unroll
+                    for (int i = 0; i < kTR; ++i) {
+                        lowh[j][i] = acc[j][i];
+                        acc[j][i] = 0.f;
+                    }
+            }
             if (kc * kKC < dpad) {
                 const float* qbase = sQ + kc * kKC;
 #pragma unroll
                 for (int kk = 0; kk < kKC; kk += 4) {
                     float4 xv[kTR], qv[kTQ];
+                    const float4 sc = *reinterpret_cast<const float4*>(sScale + kc * kKC + kk);
 #pragma unroll
                     for (int i = 0; i < kTR; ++i) xv[i] = *reinterpret_cast<const float4*>(sX + (tr + i * kWR) * kPitch + kk);
 #pragma unroll
@@ -192,12 +202,14 @@ __global__ void __launch_bounds__(kThreads, 2) ivf_batched_kernel(IvfBatchArgs a
                     for (int j = 0; j < kTQ; ++j)
 #pragma unroll
                         for (int i = 0; i < kTR; ++i) {
-                            const float d0 = xv[i].x - qv[j].x, d1 = xv[i].y - qv[j].y;
-                            const float d2 = xv[i].z - qv[j].z, d3 = xv[i].w - qv[j].w;
-                            acc[j][i] = fmaf(d0, d0, acc[j][i]);
-                            acc[j][i] = fmaf(d1, d1, acc[j][i]);
-                            acc[j][i] = fmaf(d2, d2, acc[j][i]);
-                            acc[j][i] = fmaf(d3, d3, acc[j][i]);
+                            const float d0 = __fmaf_rn(xv[i].x, sc.x, -qv[j].x);
+                            const float d1 = __fmaf_rn(xv[i].y, sc.y, -qv[j].y);
+                            const float d2 = __fmaf_rn(xv[i].z, sc.z, -qv[j].z);
+                            const float d3 = __fmaf_rn(xv[i].w, sc.w, -qv[j].w);
+                            acc[j][i] = __fmaf_rn(d0, d0, acc[j][i]);
+                            acc[j][i] = __fmaf_rn(d1, d1, acc[j][i]);
+                            acc[j][i] = __fmaf_rn(d2, d2, acc[j][i]);
+                            acc[j][i] = __fmaf_rn(d3, d3, acc[j][i]);
                         }
                 }
             }
@@ -209,8 +221,9 @@ __global__ void __launch_bounds__(kThreads, 2) ivf_batched_kernel(IvfBatchArgs a
 #pragma unroll
                     for (int i = 0; i < kTR; ++i) {
                         const int64_t row = r_begin + t * kBR + tr + i * kWR;
-                        if (qq < nqi && row < r_end) a.D[sBase[qq] + row] = acc[j][i];
+                        if (qq < nqi && row < r_end) a.D[sBase[qq] + row] = __fadd_rn(lowh[j][i], acc[j][i]);
                         acc[j][i] = 0.f;
+                        lowh[j][i] = 0.f;
                     }
                 }
             }

@@ -564,8 +564,11 @@ def run_ours(args, rank, world, local):
             line["gpu_filter_dropin"] = {"unavailable": f"{type(e).__name__}: {e}"}
     if rank == 0 and world == 1 and args.fp8:
         line["scaled_fp8_4m_256"] = scaled_fp8_c4(args, local)
-    if rank == 0 and world == 1 and args.serve_seconds > 0 and npc is not None:
-        line["serving"] = serving_c5(args, local, ivf, npc, w)
+    if rank == 0 and world == 1 and args.serve_seconds > 0 and (npc is not None or "ivf_tc" in forms):
+        if "ivf_tc" in forms:
+            line["serving"] = serving_c5(args, local, ivf, forms["ivf_tc"]["config"]["nprobe"], w, "tc")
+        else:
+            line["serving"] = serving_c5(args, local, ivf, npc, w, "exact")
     if rank == 0 and world == 1 and args.lsh and ivf is not None:
         line["ivf_lsh_tables"] = lsh_tables_c3(args, ivf, w)
     if rank == 0 and world == 1 and args.dropin:
@@ -573,9 +576,10 @@ def run_ours(args, rank, world, local):
     return line
 
 
-def serving_c5(args, local, ivf, npc, w3):
-    """The serving configuration: two device-resident indexes -- the IVF-SQ8 index over the 1M x 384
-    zipf mixture (the headline data set) and an exact 1M x 768 inner-product index (1,024-centre
+def serving_c5(args, local, ivf, npc, w3, ivf_mode="tc"):
+    """The serving configuration: two device-resident indexes -- the IVF index over the 1M x 384
+    zipf mixture (the headline data set; its lists scored on the tensor cores, ivf_mode "tc", or by SQ8
+    keys, "exact"; exact FP32 re-rank either way) and an exact 1M x 768 inner-product index (1,024-centre
     mixture, sigma 0.35, normalised; tensor-core form, re-rank depth 400) -- behind the continuous-
     batching server. Poisson arrivals of queries at each rate, request sizes geometric(0.1) capped at
     256, 70% of requests to the IVF index and 30% to the exact one, k = 100. Reports p50 / p99 latency,
@@ -616,8 +620,9 @@ def serving_c5(args, local, ivf, npc, w3):
                       "10k-query batches", "form": "tensor-core exact search, R = 400",
           "qps": round(10_000 / (c2_ms / 1e3), 1), "ms_per_batch": round(c2_ms, 3),
           "recall_at_100": round(float(np.mean(hit)), 4)}
-    pools = {"ivf_sq8_384": w3.queries.cpu().numpy(), "exact_ip_768": w2.queries.cpu().numpy()}
-    routes = [serving.ivf_route("ivf_sq8_384", ivf, npc, args.refine),
+    ivf_name = "ivf_tc_384" if ivf_mode == "tc" else "ivf_sq8_384"
+    pools = {ivf_name: w3.queries.cpu().numpy(), "exact_ip_768": w2.queries.cpu().numpy()}
+    routes = [serving.ivf_route(ivf_name, ivf, npc, args.refine, mode=ivf_mode),
               serving.tc_route("exact_ip_768", exact, refine_r=400)]
     srv = serving.Server(routes, device=local, workers=3, max_batch=4096).start()
     out = []
@@ -627,7 +632,7 @@ def serving_c5(args, local, ivf, npc, w3):
             arrivals = synth.poisson_arrivals(rate, args.serve_seconds, p_geom=0.1, cap=256, seed=int(rate))
             traffic, picks = [], []
             for at, b in arrivals:
-                route = "ivf_sq8_384" if rng.random() < 0.7 else "exact_ip_768"
+                route = ivf_name if rng.random() < 0.7 else "exact_ip_768"
                 rows = rng.integers(0, pools[route].shape[0], b)
                 traffic.append((at, route, pools[route][rows]))
                 picks.append(rows)
@@ -645,7 +650,7 @@ def serving_c5(args, local, ivf, npc, w3):
                     continue
                 ids = torch.from_numpy(np.concatenate([r.ids for r, _ in sel])).to(dev)
                 rows = torch.from_numpy(np.concatenate([rw for _, rw in sel])).to(dev)
-                if route == "ivf_sq8_384":
+                if route == ivf_name:
                     rec[route] = round(recall_evaluator(w3.base, w3.queries[rows], ids, kth_l2[rows]), 4)
                 else:
                     ok = ids >= 0
@@ -661,7 +666,8 @@ def serving_c5(args, local, ivf, npc, w3):
         srv.stop()
     del exact
     torch.cuda.empty_cache()
-    return {"config": "IVF-SQ8 1M x 384 (70%) + exact IP 1M x 768 tensor-core form (30%); Poisson arrivals, "
+    return {"config": f"IVF 1M x 384 ({ivf_mode} keys, nprobe {npc}, R {args.refine}; 70%) + exact IP 1M x 768 "
+                      "tensor-core form (30%); Poisson arrivals, "
                       "request sizes geometric(0.1) capped at 256, k=100, 3 workers, admission by free HBM",
             "runs": out, "exact_ip_768_batch": c2}
 
