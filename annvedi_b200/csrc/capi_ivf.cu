@@ -1,6 +1,7 @@
 // C ABI of the IVF-SQ8 index: the B200 form of ivf_lsh_cpp.LSHIndex
 // (competitors/ivf_lsh/src/lsh_index_optimized.cpp:124-667) for n_tables = 1, n_bits = 0.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <atomic>
@@ -720,6 +721,188 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
     return sz.off;
 }
 
+// IVF on the tensor cores with sampled bars (large batches). Every probed list's head -- its first
+// ceil(size / kSampleDiv) rows, an even sample since rows are in ascending original id inside a list --
+// is scored by a first grouped GEMM into each query's sample stream. Per query, the fast bar is the
+// rF-th smallest sampled key (rF = ceil(3 R / kSampleDiv): about 3 R keys of the whole stream pass it)
+// and the safe bar the R-th (at or above the stream's R-th key). The grouped GEMM over all rows then
+// keeps only keys at or below the fast bar, recorded per query; a query left with fewer than
+// min(R, its candidates) survivors is redone under its safe bar. Each query ends with the exact best R
+// keys of its stream, as the key-stream path below selects them, without writing the stream.
+// Returns with *done = false (and no output) when a warp's survivor region overflowed.
+constexpr int kTcSampledMinQueries = 256;
+constexpr int kSampleDiv = 8;
+
+static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, const IvfQueryArgs& a,
+                          const IvfBatchArgs& b, const __nv_bfloat16* qb, __nv_bfloat16* Apk, int64_t* titem,
+                          int32_t* titem_list, int64_t items_cap, float* keyR, int* idR, int prec, bool* done,
+                          cudaStream_t st) {
+    *done = false;
+    const int nq = a.plan.nq, npc = c.npc, C = (int)h->C, R = c.R;
+    const int kpad = h->kpad;
+    const int64_t max_pairs = (int64_t)nq * npc;
+    const int64_t largest = h->sizes_desc.empty() ? 1 : h->sizes_desc[0];
+    const int64_t head_max = ceil_div(largest, kSampleDiv);
+    const int64_t s_bound = (int64_t)nq * npc * head_max;  // sample keys at most
+    const int64_t scap = tc_items_bound(max_pairs, C, head_max);
+    const int rF = (int)std::min<int64_t>(R, std::max<int64_t>(1, ceil_div(3 * (int64_t)R, kSampleDiv)));
+    const int nwarps = tc_grouped_filter_warps();
+    const int64_t expect = 3 * (int64_t)R * nq;
+    const int wcap = (int)std::min<int64_t>(4 * ceil_div(expect, nwarps) + 1024, INT32_MAX / nwarps);
+    const size_t ent = (size_t)nwarps * wcap;
+    size_t scan_tmp = 0;
+    ANN_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, (int64_t*)nullptr, (int64_t*)nullptr, nq + 1, st));
+    Sizer sz;
+    sz.take<int64_t>((size_t)C);                 // list heads
+    sz.take<int64_t>((size_t)max_pairs);         // sseg
+    sz.take<int64_t>((size_t)nq + 1);            // slen
+    sz.take<int64_t>((size_t)nq + 1);            // soff
+    sz.take<char>(scan_tmp);
+    sz.take<int64_t>((size_t)C + 1);             // sample items
+    sz.take<int32_t>((size_t)scap);
+    sz.take<int64_t>((size_t)max_pairs);         // sdbase
+    sz.take<int32_t>((size_t)max_pairs);         // row -> query
+    sz.take<float>((size_t)s_bound);             // sample keys
+    for (int i = 0; i < 3; ++i) sz.take<float>((size_t)nq);  // fast, safe, re-run bars
+    sz.take<float>(ent);                         // survivors: key, column, query
+    sz.take<int>(ent);
+    sz.take<int>(ent);
+    sz.take<float>(ent);                         // grouped: key, id
+    sz.take<int>(ent);
+    sz.take<int>((size_t)nwarps);
+    for (int i = 0; i < 5; ++i) sz.take<int>((size_t)nq);    // counts, cursors, re-run list, marks, lens2
+    sz.take<int64_t>((size_t)nq);                // offs
+    sz.take<int64_t>((size_t)nq);                // offs2
+    sz.take<int>(4);                             // flags
+    int rc = ws_reserve_big(ws, sz.bytes());
+    if (rc) return rc;
+    Carver cv(ws->big);
+    int64_t* lcap = cv.take<int64_t>((size_t)C);
+    int64_t* sseg = cv.take<int64_t>((size_t)max_pairs);
+    int64_t* slen = cv.take<int64_t>((size_t)nq + 1);
+    int64_t* soff = cv.take<int64_t>((size_t)nq + 1);
+    void* stmp = cv.take<char>(scan_tmp);
+    int64_t* sitem = cv.take<int64_t>((size_t)C + 1);
+    int32_t* sitem_list = cv.take<int32_t>((size_t)scap);
+    int64_t* sdbase = cv.take<int64_t>((size_t)max_pairs);
+    int32_t* rowq = cv.take<int32_t>((size_t)max_pairs);
+    float* SK = cv.take<float>((size_t)s_bound);
+    float* tauF = cv.take<float>((size_t)nq);
+    float* tauS = cv.take<float>((size_t)nq);
+    float* tauR = cv.take<float>((size_t)nq);
+    float* fkey = cv.take<float>(ent);
+    int* fcol = cv.take<int>(ent);
+    int* frow = cv.take<int>(ent);
+    float* gkey = cv.take<float>(ent);
+    int* gid = cv.take<int>(ent);
+    int* wcnt = cv.take<int>((size_t)nwarps);
+    int* rowcnt = cv.take<int>((size_t)nq);
+    int* cursor = cv.take<int>((size_t)nq);
+    int* list = cv.take<int>((size_t)nq);
+    int* mark = cv.take<int>((size_t)nq);
+    int* lens2 = cv.take<int>((size_t)nq);
+    int64_t* offs = cv.take<int64_t>((size_t)nq);
+    int64_t* offs2 = cv.take<int64_t>((size_t)nq);
+    int* flags = cv.take<int>(4);
+
+    // sample streams: heads of the probed lists, each query's stream offsets
+    if ((rc = launch_tc_ivf_sample_plan(a.plan, h->list_off, C, kSampleDiv, lcap, sseg, slen, st))) return rc;
+    ANN_CUDA_TRY(cudaMemsetAsync(slen + nq, 0, sizeof(int64_t), st));
+    size_t tb = scan_tmp;
+    ANN_CUDA_TRY(cub::DeviceScan::ExclusiveSum(stmp, tb, slen, soff, nq + 1, st));
+    TcIvfSampleMaps maps;
+    maps.row_query = rowq;
+    maps.soff = soff;
+    maps.sseg = sseg;
+    maps.sdbase = sdbase;
+    if ((rc = launch_tc_ivf_pairs(qb, kpad, b.pair_vals, b.pair_lists, b.lq_off + C, max_pairs, npc, b.cand_off,
+                                  a.plan.seg_pref, h->list_off, Apk, nullptr, st, maps)))
+        return rc;
+    // 1. sample pass: keys of the list heads into the sample streams; the two bars per query
+    if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, C, sitem, st, lcap))) return rc;
+    if ((rc = launch_tc_item_lists(sitem, C, sitem_list, scap, st))) return rc;
+    TcGemmArgs gs{(int)max_pairs, (int)h->n, kpad, nullptr, SK, 0, h->d_err};
+    gs.g_item_off = sitem;
+    gs.g_a_off = b.lq_off;
+    gs.g_b_off = h->list_off;
+    gs.g_b_len = lcap;
+    gs.g_dbase = sdbase;
+    gs.g_total = sitem + C;
+    gs.g_lists = C;
+    gs.g_item_list = sitem_list;
+    if ((rc = launch_tc_gemm(Apk, h->base_bf16, gs, st))) return rc;
+    RadixSelectArgs bar{};
+    bar.keys = SK;
+    bar.ld = npc * head_max;
+    bar.offs = soff;
+    bar.lens = slen;
+    bar.R = rF;
+    bar.out_kth = tauF;
+    bar.R2 = R;
+    bar.out_kth2 = tauS;
+    bar.kth_upper = 1;
+    if ((rc = launch_radix_select(bar, nq, st))) return rc;
+    // 2. filter pass over every row of the probed lists, survivors grouped per query
+    if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, C, titem, st))) return rc;
+    if ((rc = launch_tc_item_lists(titem, C, titem_list, items_cap, st))) return rc;
+    auto filter = [&](const float* tau) -> int {
+        TcGemmArgs g{(int)max_pairs, (int)h->n, kpad, nullptr, nullptr, 0, h->d_err};
+        g.g_item_off = titem;
+        g.g_a_off = b.lq_off;
+        g.g_b_off = h->list_off;
+        g.g_total = titem + C;
+        g.g_lists = C;
+        g.g_item_list = titem_list;
+        g.g_row_query = rowq;
+        g.tau = tau;
+        g.fkey = fkey;
+        g.fcol = fcol;
+        g.frow = frow;
+        g.wcount = wcnt;
+        g.wcap = wcap;
+        int r = launch_tc_gemm(Apk, h->base_bf16, g, st);
+        if (r) return r;
+        TcGroupArgs ga{fkey, fcol, frow, wcnt, nwarps, wcap, nq, h->n, 1, rowcnt, offs, cursor, gkey, gid, flags + 1};
+        return launch_tc_group(ga, st);
+    };
+    if ((rc = filter(tauF))) return rc;
+    h->prof.mark(prec, st);
+    ANN_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int), st));
+    if ((rc = launch_tc_bar_check(rowcnt, nq, R, list, flags, st, a.plan.n_cands, mark))) return rc;
+    int hf[2] = {0, 0};  // re-runs, largest warp count
+    ANN_CUDA_TRY(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
+    ANN_CUDA_TRY(cudaStreamSynchronize(st));
+    if (hf[1] > wcap) return ANN_OK;  // a region overflowed: the caller takes the key-stream path
+    RadixSelectArgs sv{};
+    sv.keys = gkey;
+    sv.ld = (int64_t)ent;
+    sv.offs = offs;
+    sv.lens32 = rowcnt;
+    sv.ids = gid;
+    sv.R = R;
+    sv.out_key = keyR;
+    sv.out_id = idR;
+    if ((rc = launch_radix_select(sv, nq, st))) return rc;
+    if (hf[0] > 0) {  // queries short of survivors: again under their safe bars, the others under -inf
+        if ((rc = launch_tc_rerun_bars(mark, tauS, nq, tauR, st))) return rc;
+        if ((rc = filter(tauR))) return rc;
+        int hmax = 0;
+        ANN_CUDA_TRY(cudaMemcpyAsync(&hmax, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        ANN_CUDA_TRY(cudaStreamSynchronize(st));
+        if (hmax > wcap) return ANN_OK;
+        if ((rc = launch_tc_compact_rows(list, flags, hf[0], offs, rowcnt, offs2, lens2, st))) return rc;
+        RadixSelectArgs sv2 = sv;
+        sv2.offs = offs2;
+        sv2.lens32 = lens2;
+        sv2.out_rows = list;
+        if ((rc = launch_radix_select(sv2, hf[0], st))) return rc;
+        if (prec >= 0) h->prof.tc_launches += 1;
+    }
+    if (prec >= 0) h->prof.tc_launches += 2;
+    *done = true;
+    return ANN_OK;
+}
+
 // All stages for nq device-resident padded queries; scratch carved from `base`.
 static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, char* base, const float* qdev,
                             int nq, int64_t* ids_dev, float* dists_dev, cudaStream_t st) {
@@ -861,7 +1044,14 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         IvfBatchArgs b{};
         int64_t tot[3] = {0, 0, 0};
         if ((rc = batched_prepare(a, bscratch, c.sort_tmp, c.scan_tmp, &b, tot, st))) return rc;
-        if (tot[2] == 0) {  // no query fell back to scanning every row
+        bool sampled_done = false;
+        if (tot[2] == 0 && c.tc && nq >= kTcSampledMinQueries) {
+            if ((rc = ivf_tc_sampled(h, ws, c, a, b, qb, Apk, titem, titem_list, items_cap, keyR, idR, prec,
+                                     &sampled_done, st)))
+                return rc;
+            done = sampled_done;
+        }
+        if (tot[2] == 0 && !sampled_done) {  // no query fell back to scanning every row
             if ((rc = ws_reserve_big(ws, sizeof(float) * (size_t)std::max<int64_t>(tot[1], 1)))) return rc;
             float* D = reinterpret_cast<float*>(ws->big);
             if (c.tc) {

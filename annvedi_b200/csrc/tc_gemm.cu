@@ -186,7 +186,7 @@ __device__ __forceinline__ GroupTile group_tile(const TcGemmArgs& a, int64_t t) 
         }
     }
     const int64_t np = a.g_a_off[lo + 1] - a.g_a_off[lo];
-    const int64_t nr = a.g_b_off[lo + 1] - a.g_b_off[lo];
+    const int64_t nr = a.g_b_len ? a.g_b_len[lo] : a.g_b_off[lo + 1] - a.g_b_off[lo];
     const int64_t npt = (np + kBM - 1) / kBM;
     const int64_t local = t - a.g_item_off[lo];
     const int64_t g = local % npt, rt = local / npt;
@@ -363,10 +363,24 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                 bar_arrive(&tempty[b]);
                 continue;
             }
-            const float an = (a.normA && m < a.M) ? a.normA[m] : 0.f;
-            const float rfac = (a.row_fac && m < a.M) ? a.row_fac[m] : 1.f;
+            // the tile's rows and columns: a dense tile, or a grouped one (a list's pairs and rows; rows and
+            // columns past them belong to the next list and are masked like rows past M)
+            int rq = m;                         // the row recorded for a survivor (grouped: its query)
+            bool mvalid = m < a.M;
+            int64_t cbase = n0;                 // recorded column of the tile's first column
+            int ncols = a.N - n0;               // valid columns of the tile from its first
+            if (grouped) {
+                const GroupTile gt = group_tile(a, t);
+                const int ml = lane_base + lane;
+                mvalid = ml < gt.am;
+                rq = mvalid ? (a.g_row_query ? a.g_row_query[gt.a0 + ml] : (int)(gt.a0 + ml)) : 0;
+                cbase = gt.b0;
+                ncols = gt.bn;
+            }
+            const float an = (a.normA && mvalid) ? a.normA[m] : 0.f;
+            const float rfac = (a.row_fac && mvalid) ? a.row_fac[m] : 1.f;
             // rows past M (TMA zero fill) get a bar no key passes
-            const float tau = (a.tau && m < a.M) ? a.tau[m] : -kInf;
+            const float tau = (a.tau && mvalid) ? a.tau[rq] : -kInf;
             const float tau_up = nextafterf(tau, kInf);
             const float2 ntau2 = make_float2(-tau_up, -tau_up);
             const uint32_t tbase = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kBN + col0);
@@ -407,6 +421,7 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                         for (int u = 0; u < 32; ++u) v[u] = __uint_as_float(h ? r1[u] : r0[u]);
                     }
                     const int nb = n0 + col0 + c + 32 * h;  // output column of v[0]
+                    const int lb = col0 + c + 32 * h;       // its column within the tile
                     if (staged) {  // scaled operands: key = f.y + f.x * (row scale * accumulator), two at a time
                         const float2 r2 = make_float2(rfac, rfac);
 #pragma unroll
@@ -430,10 +445,10 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                         for (int u = 0; u < 32; ++u)
                             v[u] = fmaf(__shfl_sync(0xffffffffu, f.x, u), rfac * v[u], __shfl_sync(0xffffffffu, f.y, u));
                     }
-                    if (nb + 32 > a.N) {  // ragged last tile: columns past N pass no bar (NaN) and are not stored
+                    if (lb + 32 > ncols) {  // ragged last tile: columns past it pass no bar (NaN) and are not stored
 #pragma unroll
                         for (int u = 0; u < 32; ++u)
-                            if (nb + u >= a.N) v[u] = __int_as_float(0x7fffffff);
+                            if (lb + u >= ncols) v[u] = __int_as_float(0x7fffffff);
                     }
                     if (!kFilterOnly && a.out) {
                         // transpose through shared memory so each store covers 32 consecutive columns
@@ -487,8 +502,8 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                                     for (int z = 0; z < 2; ++z) s2[z] = (u & 2) ? s4[z + 2] : s4[z];
                                     const float kv = (u & 1) ? s2[1] : s2[0];
                                     a.fkey[wbase + slot] = kv;
-                                    a.fcol[wbase + slot] = nb + u;
-                                    a.frow[wbase + slot] = m;
+                                    a.fcol[wbase + slot] = (int)(cbase + lb + u);
+                                    a.frow[wbase + slot] = rq;
                                 }
                                 ++slot;
                             }
@@ -554,6 +569,7 @@ int tc_kpad(int dim, int metric) { return (int)ceil_div(dim + (metric == ANN_MET
 
 static int tc_grid(int M, int N) { return (int)std::min<int64_t>(ceil_div(M, kBM) * ceil_div(N, kBN), kNumSMs); }
 int tc_filter_warps(int M, int N) { return tc_grid(M, N) * kFilterEpi; }
+int tc_grouped_filter_warps() { return kNumSMs * kFilterEpi; }
 
 template <int KIND, int EPI>
 static cudaError_t run_tc_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcGemmArgs& a, int grid,
@@ -575,7 +591,8 @@ int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream
     ANN_CHECK_ARG(a.out != nullptr || (a.tau && a.fkey && a.fcol && a.frow && a.wcount && a.wcap > 0),
                   "tensor-core scan: neither an output matrix nor a filter");
     ANN_CHECK_ARG(a.g_item_off == nullptr ||
-                      (a.out && a.g_a_off && a.g_b_off && a.g_dbase && a.g_total && a.g_lists > 0 && a.tau == nullptr),
+                      (a.g_a_off && a.g_b_off && a.g_total && a.g_lists > 0 &&
+                       ((a.out && a.g_dbase && a.tau == nullptr) || (a.out == nullptr && a.tau && a.g_row_query))),
                   "tensor-core scan: incomplete grouping");
     ANN_CHECK_ARG(a.b_tile_stride >= 1, "tensor-core scan: bad sample stride");
     if (a.M == 0 || a.N == 0) return ANN_OK;

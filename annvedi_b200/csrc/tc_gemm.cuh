@@ -42,6 +42,10 @@ struct TcGemmArgs {
     const int64_t* g_total = nullptr;
     int g_lists = 0;
     const int32_t* g_item_list = nullptr;  // optional: the list of each item (else a search of g_item_off)
+    const int64_t* g_b_len = nullptr;      // optional: rows of list l taken (else g_b_off[l+1] - g_b_off[l])
+    // Grouped filter mode (grouped, out == null): A row i belongs to query g_row_query[i]; its bar is
+    // tau[g_row_query[i]], and a survivor is recorded as (key, list row g_b_off[l] + r, that query).
+    const int32_t* g_row_query = nullptr;
     // Element kind of A and B. E4M3 operands carry a scale per row (launch_tc_operand_e4m3): the key is
     // col_fac[n].y + col_fac[n].x * row_fac[m] * accumulator (key-matrix and filter modes).
     int kind = kTcBF16;
@@ -61,6 +65,8 @@ enum TcRole { kTcBase = 0, kTcQuery = 1 };
 int tc_kpad(int dim, int metric);
 // Epilogue warps of a filter launch over M x N keys (the size of the wcount array).
 int tc_filter_warps(int M, int N);
+// ... and of a grouped filter launch (persistent over the work items).
+int tc_grouped_filter_warps();
 size_t tc_gemm_smem();
 int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream_t st);
 // Runs one small GEMM whose producer issues no copies, with every wait limited to wait_ns, and returns the

@@ -78,9 +78,14 @@ __global__ void tc_scatter_kernel(TcGroupArgs g) {
     }
 }
 
-__global__ void tc_bar_check_kernel(const int* rowcnt, int M, int R, int* list, int* flags) {
+__global__ void tc_bar_check_kernel(const int* rowcnt, int M, int R, int* list, int* flags, const int64_t* lens,
+                                    int* mark) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q < M && rowcnt[q] < R) list[atomicAdd(&flags[0], 1)] = q;
+    if (q >= M) return;
+    const int64_t need = lens ? min((int64_t)R, lens[q]) : (int64_t)R;
+    const bool rerun = rowcnt[q] < need;
+    if (rerun) list[atomicAdd(&flags[0], 1)] = q;
+    if (mark) mark[q] = rerun;
 }
 
 __global__ void tc_gather_kernel(const unsigned char* A, int row_bytes, const int* list, int nb, const float* tau,
@@ -111,12 +116,13 @@ __global__ void tc_unpermute_kernel(const float* keys, int64_t n, int64_t mult, 
 }
 
 __global__ void __launch_bounds__(1024) tc_ivf_items_kernel(const int64_t* lq_off, const int64_t* list_off, int C,
-                                                            int64_t* item_off) {
+                                                            int64_t* item_off, const int64_t* list_len) {
     __shared__ int64_t sPart[1024];
     const int per = (C + 1023) / 1024;
     const int l0 = threadIdx.x * per;
     auto items = [&](int l) -> int64_t {
-        const int64_t np = lq_off[l + 1] - lq_off[l], nr = list_off[l + 1] - list_off[l];
+        const int64_t np = lq_off[l + 1] - lq_off[l];
+        const int64_t nr = list_len ? list_len[l] : list_off[l + 1] - list_off[l];
         return (np == 0 || nr == 0) ? 0 : ((np + 127) / 128) * ((nr + 255) / 256);
     };
     int64_t local = 0;
@@ -145,7 +151,7 @@ __global__ void __launch_bounds__(1024) tc_ivf_items_kernel(const int64_t* lq_of
 __global__ void tc_ivf_pairs_kernel(const __nv_bfloat16* qb, int kpad, const int32_t* pair_vals,
                                     const int32_t* pair_lists, const int64_t* n_pairs, int64_t max_pairs, int npc,
                                     const int64_t* cand_off, const int64_t* seg_pref, const int64_t* list_off,
-                                    __nv_bfloat16* A, int64_t* dbase) {
+                                    __nv_bfloat16* A, int64_t* dbase, TcIvfSampleMaps sm) {
     const int64_t np = min(*n_pairs, max_pairs);
     const int lane = threadIdx.x & 31;
     for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < np;
@@ -155,7 +161,52 @@ __global__ void tc_ivf_pairs_kernel(const __nv_bfloat16* qb, int kpad, const int
         const uint4* src = reinterpret_cast<const uint4*>(qb + (size_t)q * kpad);
         uint4* dst = reinterpret_cast<uint4*>(A + (size_t)i * kpad);
         for (int c = lane; c < kpad / 8; c += 32) dst[c] = src[c];
-        if (lane == 0) dbase[i] = cand_off[q] + seg_pref[(int64_t)q * (npc + 1) + j] - list_off[pair_lists[i]];
+        if (lane == 0) {
+            if (dbase) dbase[i] = cand_off[q] + seg_pref[(int64_t)q * (npc + 1) + j] - list_off[pair_lists[i]];
+            if (sm.row_query) sm.row_query[i] = q;
+            // the grouped epilogue adds the tile's absolute list row, as for dbase
+            if (sm.sdbase) sm.sdbase[i] = sm.soff[q] + sm.sseg[(int64_t)q * npc + j] - list_off[pair_lists[i]];
+        }
+    }
+}
+
+// One thread per query: the sample stream of its probed lists (the first lcap[l] rows of each), the
+// segment starts sseg[q][j] and its length slen[q]; the candidates' count comes from the plan.
+__global__ void tc_ivf_sample_plan_kernel(IvfPlan p, const int64_t* __restrict__ lcap, int64_t* __restrict__ sseg,
+                                          int64_t* __restrict__ slen) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= p.nq) return;
+    const int ns = p.n_seg[q];
+    int64_t run = 0;
+    for (int j = 0; j < p.npc; ++j) {
+        sseg[(int64_t)q * p.npc + j] = run;
+        const int l = p.probes[(int64_t)q * p.npc + j];
+        if (j < ns && l >= 0) run += lcap[l];
+    }
+    slen[q] = run;
+}
+
+// lcap[l] = ceil(size_l / div): the sampled head of list l
+__global__ void tc_ivf_list_caps_kernel(const int64_t* __restrict__ list_off, int C, int div, int64_t* __restrict__ lcap) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l < C) lcap[l] = (list_off[l + 1] - list_off[l] + div - 1) / div;
+}
+
+// tauR[q] = tauS[q] for the queries marked for a re-run, else -inf (no key passes)
+__global__ void tc_rerun_bars_kernel(const int* __restrict__ mark, const float* __restrict__ tauS, int nq,
+                                     float* __restrict__ tauR) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < nq) tauR[q] = mark[q] ? tauS[q] : -kInf;
+}
+
+// offs2[j] = offs[list[j]], lens2[j] = rowcnt[list[j]] for the j < count listed rows
+__global__ void tc_compact_rows_kernel(const int* __restrict__ list, const int* __restrict__ count,
+                                       const int64_t* __restrict__ offs, const int* __restrict__ rowcnt,
+                                       int64_t* __restrict__ offs2, int* __restrict__ lens2) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < *count) {
+        offs2[j] = offs[list[j]];
+        lens2[j] = rowcnt[list[j]];
     }
 }
 
@@ -291,9 +342,10 @@ int launch_tc_coarse(const float* keys, int64_t ldk, int nq, int C, int npc, int
     return ANN_OK;
 }
 
-int launch_tc_ivf_items(const int64_t* lq_off, const int64_t* list_off, int C, int64_t* item_off, cudaStream_t st) {
+int launch_tc_ivf_items(const int64_t* lq_off, const int64_t* list_off, int C, int64_t* item_off, cudaStream_t st,
+                        const int64_t* list_len) {
     ANN_CHECK_ARG(C >= 1, "tensor-core IVF: no lists");
-    tc_ivf_items_kernel<<<1, 1024, 0, st>>>(lq_off, list_off, C, item_off);
+    tc_ivf_items_kernel<<<1, 1024, 0, st>>>(lq_off, list_off, C, item_off, list_len);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }
@@ -317,12 +369,12 @@ int launch_tc_item_lists(const int64_t* item_off, int C, int32_t* item_list, int
 int launch_tc_ivf_pairs(const __nv_bfloat16* qb, int kpad, const int32_t* pair_vals, const int32_t* pair_lists,
                         const int64_t* n_pairs, int64_t max_pairs, int npc, const int64_t* cand_off,
                         const int64_t* seg_pref, const int64_t* list_off, __nv_bfloat16* A, int64_t* dbase,
-                        cudaStream_t st) {
+                        cudaStream_t st, const TcIvfSampleMaps& sm) {
     if (max_pairs == 0) return ANN_OK;
     ANN_CHECK_ARG(kpad % 8 == 0, "tensor-core IVF: kpad %d", kpad);
     const int grid = (int)std::min<int64_t>(ceil_div(max_pairs * 32, 256), 16 * kNumSMs);
     tc_ivf_pairs_kernel<<<grid, 256, 0, st>>>(qb, kpad, pair_vals, pair_lists, n_pairs, max_pairs, npc, cand_off,
-                                              seg_pref, list_off, A, dbase);
+                                              seg_pref, list_off, A, dbase, sm);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }
@@ -340,9 +392,36 @@ int launch_tc_group(const TcGroupArgs& g, cudaStream_t st) {
     return ANN_OK;
 }
 
-int launch_tc_bar_check(const int* rowcnt, int M, int R, int* list, int* flags, cudaStream_t st) {
+int launch_tc_bar_check(const int* rowcnt, int M, int R, int* list, int* flags, cudaStream_t st, const int64_t* lens,
+                        int* mark) {
     if (M == 0) return ANN_OK;
-    tc_bar_check_kernel<<<(unsigned)ceil_div(M, 256), 256, 0, st>>>(rowcnt, M, R, list, flags);
+    tc_bar_check_kernel<<<(unsigned)ceil_div(M, 256), 256, 0, st>>>(rowcnt, M, R, list, flags, lens, mark);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int launch_tc_ivf_sample_plan(const IvfPlan& p, const int64_t* list_off, int C, int div, int64_t* lcap, int64_t* sseg,
+                              int64_t* slen, cudaStream_t st) {
+    ANN_CHECK_ARG(C >= 1 && div >= 1, "IVF sample plan: %d lists, 1/%d", C, div);
+    tc_ivf_list_caps_kernel<<<(unsigned)ceil_div(C, 256), 256, 0, st>>>(list_off, C, div, lcap);
+    ANN_LAUNCH_CHECK();
+    if (p.nq == 0) return ANN_OK;
+    tc_ivf_sample_plan_kernel<<<(unsigned)ceil_div(p.nq, 128), 128, 0, st>>>(p, lcap, sseg, slen);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int launch_tc_rerun_bars(const int* mark, const float* tauS, int nq, float* tauR, cudaStream_t st) {
+    if (nq == 0) return ANN_OK;
+    tc_rerun_bars_kernel<<<(unsigned)ceil_div(nq, 256), 256, 0, st>>>(mark, tauS, nq, tauR);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int launch_tc_compact_rows(const int* list, const int* count, int max_count, const int64_t* offs, const int* rowcnt,
+                           int64_t* offs2, int* lens2, cudaStream_t st) {
+    if (max_count == 0) return ANN_OK;
+    tc_compact_rows_kernel<<<(unsigned)ceil_div(max_count, 256), 256, 0, st>>>(list, count, offs, rowcnt, offs2, lens2);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

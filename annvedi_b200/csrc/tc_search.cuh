@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "ivf.cuh"
+
 namespace annb {
 
 // The BF16 base copy stores row (p * mult) mod n at position p (a Weyl sequence with mult ~ 0.618 n,
@@ -33,8 +35,10 @@ struct TcGroupArgs {
 };
 int launch_tc_group(const TcGroupArgs& g, cudaStream_t st);
 
-// Rows with fewer than R survivors go to list (count in flags[0]).
-int launch_tc_bar_check(const int* rowcnt, int M, int R, int* list, int* flags, cudaStream_t st);
+// Rows with fewer than R survivors -- fewer than min(R, lens[row]) where lens is given -- go to list (count in
+// flags[0]); mark[row], if given, is 1 for them and 0 for the others.
+int launch_tc_bar_check(const int* rowcnt, int M, int R, int* list, int* flags, cudaStream_t st,
+                        const int64_t* lens = nullptr, int* mark = nullptr);
 // A2[j] = A[list[j]] (rows of row_bytes), tau2[j] = tau[list[j]] and, if given, rfac2[j] = rfac[list[j]].
 int launch_tc_gather(const void* A, int row_bytes, const int* list, int nb, const float* tau, void* A2, float* tau2,
                      const float* rfac, float* rfac2, cudaStream_t st);
@@ -46,7 +50,9 @@ int launch_tc_unpermute(const float* keys, int nq, int64_t n, int64_t mult, floa
 // IVF batches on the tensor cores (a list-major grouping of (query, list) pairs, ivf_batched.cu):
 // items per list = ceil(pairs / 128) x ceil(rows / 256), exclusively scanned into item_off[0..C]
 // (item_off[C] = all items). One block.
-int launch_tc_ivf_items(const int64_t* lq_off, const int64_t* list_off, int C, int64_t* item_off, cudaStream_t st);
+// With list_len, list l counts list_len[l] rows (a capped head of each list) instead of its size.
+int launch_tc_ivf_items(const int64_t* lq_off, const int64_t* list_off, int C, int64_t* item_off, cudaStream_t st,
+                        const int64_t* list_len = nullptr);
 // item_list[t] = the list of work item t (item_off [C + 1] from launch_tc_ivf_items), for t < cap.
 int launch_tc_item_lists(const int64_t* item_off, int C, int32_t* item_list, int64_t cap, cudaStream_t st);
 // Work items of a grouped batch at most: (pairs / 128 + C) x (largest list / 256 + 1).
@@ -54,10 +60,27 @@ inline int64_t tc_items_bound(int64_t pairs, int C, int64_t largest) { return (p
 // For each valid pair i (< lq_off[C]; pairs grouped by list, pair_vals = q * npc + j, pair_lists = the
 // list): A[i] = qb[q] (kpad BF16 columns) and dbase[i] = cand_off[q] + seg_pref[q][j] - list_off[list],
 // the stream position of the list's row 0 in the candidate array.
+// Optional maps of the sampled form: row_query[i] = q; sdbase[i] = soff[q] + sseg[q][j] - list_off[list]
+// (the sample-stream position of the list's row 0, as dbase is for the candidate stream).
+struct TcIvfSampleMaps {
+    int32_t* row_query = nullptr;
+    const int64_t* soff = nullptr;
+    const int64_t* sseg = nullptr;  // [nq, npc]
+    int64_t* sdbase = nullptr;
+};
 int launch_tc_ivf_pairs(const __nv_bfloat16* qb, int kpad, const int32_t* pair_vals, const int32_t* pair_lists,
                         const int64_t* n_pairs, int64_t max_pairs, int npc, const int64_t* cand_off,
                         const int64_t* seg_pref, const int64_t* list_off, __nv_bfloat16* A, int64_t* dbase,
-                        cudaStream_t st);
+                        cudaStream_t st, const TcIvfSampleMaps& sm = TcIvfSampleMaps{});
+// The sampled heads of the lists, lcap[l] = ceil(size_l / div), and each query's sample stream over its
+// probed lists: segment starts sseg [nq, npc] and length slen [nq].
+int launch_tc_ivf_sample_plan(const IvfPlan& p, const int64_t* list_off, int C, int div, int64_t* lcap, int64_t* sseg,
+                              int64_t* slen, cudaStream_t st);
+// tauR[q] = mark[q] ? tauS[q] : -inf.
+int launch_tc_rerun_bars(const int* mark, const float* tauS, int nq, float* tauR, cudaStream_t st);
+// offs2[j] = offs[list[j]], lens2[j] = rowcnt[list[j]] for j < *count (<= max_count).
+int launch_tc_compact_rows(const int* list, const int* count, int max_count, const int64_t* offs, const int* rowcnt,
+                           int64_t* offs2, int* lens2, cudaStream_t st);
 
 // Coarse ranking of the tensor-core IVF form from BF16 keys [nq, C] (ldk per row): per query, the best
 // m = min(C, npc + margin) centroids by key, their exact FP32 squared distances (FP32 queries and

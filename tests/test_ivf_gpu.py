@@ -236,6 +236,48 @@ def test_tc_mode_ranks_the_same_streams(cuda, nq):
     assert ix.total_distances_count() == ex.total_distances_count()
 
 
+@pytest.mark.parametrize("nq,npc,R", [(1200, 12, 300), (600, 40, 100), (256, 3, 500)])
+def test_tc_sampled_bars_select_what_the_key_stream_selects(cuda, nq, npc, R):
+    """Batches of 256+ queries on the tensor cores keep only keys under sampled per-query bars (a pass over
+    the heads of the probed lists, re-runs under a safe bar where a query falls short); smaller batches
+    select from the whole key stream. Both take each query's exact best R BF16 keys, so the same queries
+    return the same ids and distances in one batch and in batches of 200."""
+    from tests.helpers import assert_ids_equal_up_to_ties
+    w = synth.zipf_mixture(80000, 128, nq, c=128, lo=20, hi=6000, seed=nq + npc)
+    st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
+    ix = _ivf(mode="tc")
+    ix.import_state(st)
+    ids, d = ix.search(w.queries, 100, 0, npc, R)
+    parts = [ix.search(w.queries[s:s + 200], 100, 0, npc, R) for s in range(0, nq, 200)]
+    ids2 = np.concatenate([p[0] for p in parts])
+    d2 = np.concatenate([p[1] for p in parts])
+    assert_ids_equal_up_to_ties(w.base, w.queries, ids, ids2, rtol=1e-6)
+    same = ids == ids2
+    np.testing.assert_array_equal(d[same], d2[same])
+    from tests.helpers import fp64_dists
+    np.testing.assert_allclose(d, fp64_dists(w.base, w.queries, ids), rtol=1e-5, atol=1e-6)
+
+
+def test_tc_sampled_bars_rerun_path(cuda):
+    """Lists of two rows: a query's sample is half its candidates, so about 2.3 R/3 keys pass the fast bar
+    and most queries are redone under their safe bars; the result still equals the key-stream path's."""
+    from tests.helpers import assert_ids_equal_up_to_ties
+    rng = np.random.default_rng(5)
+    base = rng.standard_normal((8192, 64)).astype(np.float32)
+    base /= np.linalg.norm(base, axis=1, keepdims=True)
+    q = base[rng.integers(0, 8192, 300)] + 0.05 * rng.standard_normal((300, 64)).astype(np.float32)
+    q = np.ascontiguousarray(q / np.linalg.norm(q, axis=1, keepdims=True), np.float32)
+    st = ivf_state.build_state(base, np.ascontiguousarray(base[::2]), np.arange(8192) // 2, 1, 0)
+    ix = _ivf(mode="tc")
+    ix.import_state(st)
+    ids, d = ix.search(q, 100, 0, 400, 300)
+    parts = [ix.search(q[s:s + 150], 100, 0, 400, 300) for s in range(0, 300, 150)]
+    ids2 = np.concatenate([p[0] for p in parts])
+    assert_ids_equal_up_to_ties(base, q, ids, ids2, rtol=1e-6)
+    from tests.helpers import fp64_dists
+    np.testing.assert_allclose(d, fp64_dists(base, q, ids), rtol=1e-5, atol=1e-6)
+
+
 def test_tc_mode_over_all_lists_is_exact(cuda):
     """Probing every list makes each candidate stream the whole base: the result is the exact top-k."""
     import torch
