@@ -32,7 +32,8 @@ MEM_DEVICE = 1
 METRICS = {"l2": METRIC_L2, "sqeuclidean": METRIC_L2, "euclidean": METRIC_L2, "ip": METRIC_IP,
            "inner_product": METRIC_IP, "dot": METRIC_IP}
 MODE_TC = 2
-MODES = {"exact": MODE_EXACT, "reference": MODE_REFERENCE, "tc": MODE_TC}
+MODE_TC_SQ8 = 3
+MODES = {"exact": MODE_EXACT, "reference": MODE_REFERENCE, "tc": MODE_TC, "tc_sq8": MODE_TC_SQ8}
 
 
 class AnnError(RuntimeError):

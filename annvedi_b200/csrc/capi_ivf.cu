@@ -55,6 +55,7 @@ struct ann_ivf {
     LshView lsh_view() const { return LshView{T, B, proj, projT, lsh_mean, tab_off, tab_ids}; }
     __nv_bfloat16* base_bf16 = nullptr;  // [n, kpad] BF16 operand form of the list-ordered rows (tensor-core form)
     __nv_bfloat16* cent_bf16 = nullptr;  // [C, kpad] BF16 operand form of the centroids
+    float2* sq8_fac = nullptr;           // [n] (1, reconstructed |x|^2) of the SQ8 rows (codes on the tensor cores)
     int kpad = 0;
     std::mutex tc_mu;
     int64_t query_count = 0;
@@ -80,10 +81,11 @@ struct ann_ivf {
 static void ivf_free_state(ann_ivf* h) {
     for (void* p : {(void*)h->centroids, (void*)h->original, (void*)h->codes, (void*)h->scale, (void*)h->offset,
                     (void*)h->r2o, (void*)h->list_off, (void*)h->base_bf16, (void*)h->cent_bf16, (void*)h->proj,
-                    (void*)h->projT, (void*)h->lsh_mean, (void*)h->tab_off, (void*)h->tab_ids})
+                    (void*)h->projT, (void*)h->lsh_mean, (void*)h->tab_off, (void*)h->tab_ids, (void*)h->sq8_fac})
         if (p) cudaFree(p);
     h->base_bf16 = nullptr;
     h->cent_bf16 = nullptr;
+    h->sq8_fac = nullptr;
     h->proj = h->projT = h->lsh_mean = nullptr;
     h->tab_off = nullptr;
     h->tab_ids = nullptr;
@@ -641,6 +643,7 @@ struct IvfQueryCfg {
     int k, npc, R, nsplit, num_threads, bqc, nsplit_c, ncp;
     int64_t max_c, ub, rps_c;
     bool ref, coarse_flat, batched, tc, lsh;
+    bool i8;          // the tensor-core form over the SQ8 codes (int8 x uint8 MMA) instead of BF16 rows
     bool fallback;    // a query's stream can fall short of k points and become every row
     bool lsh_keys;    // exact LSH batch: SQ8 keys of the whole streams, then selection
     int64_t ub_cand;  // longest explicit candidate stream (LSH buckets; a fallback to every row needs none)
@@ -648,32 +651,63 @@ struct IvfQueryCfg {
     size_t sort_tmp, scan_tmp, bscratch;
 };
 
-// BF16 operand form of the list-ordered rows for the tensor-core form, built once.
-static int ivf_ensure_bf16(ann_ivf* h, cudaStream_t st) {
+// Operand forms of the tensor-core forms, built once: BF16 centroids (the coarse ranking of both), and the BF16
+// list-ordered rows (ANN_MODE_TC) or the SQ8 rows' reconstructed norms (ANN_MODE_TC_SQ8, whose B operand is the
+// codes themselves).
+static int ivf_ensure_tc(ann_ivf* h, bool i8, cudaStream_t st) {
     std::lock_guard<std::mutex> lk(h->tc_mu);
-    if (h->base_bf16) return ANN_OK;
     const int kpad = tc_kpad(h->dim, ANN_METRIC_L2);
-    __nv_bfloat16 *b = nullptr, *cb = nullptr;
-    cudaError_t e = cudaMalloc(&b, sizeof(__nv_bfloat16) * (size_t)h->n * kpad);
-    if (e == cudaSuccess) e = cudaMalloc(&cb, sizeof(__nv_bfloat16) * (size_t)h->C * kpad);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        if (b) cudaFree(b);
-        set_error("tensor-core IVF: cannot allocate the BF16 copy of the lists (%s)", cudaGetErrorString(e));
-        return ANN_ERR_NOMEM;
+    int rc = ANN_OK;
+    if (!h->cent_bf16) {
+        __nv_bfloat16* cb = nullptr;
+        if (cudaMalloc(&cb, sizeof(__nv_bfloat16) * (size_t)h->C * kpad) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("tensor-core IVF: cannot allocate the BF16 centroids");
+            return ANN_ERR_NOMEM;
+        }
+        if ((rc = launch_tc_operand(h->centroids, h->C, h->dim, h->dpad, cb, kpad, kTcBase, ANN_METRIC_L2, 0, st))) {
+            cudaFree(cb);
+            return rc;
+        }
+        ANN_CUDA_TRY(cudaStreamSynchronize(st));
+        h->cent_bf16 = cb;
+        h->kpad = kpad;
     }
-    int rc = launch_tc_operand(h->original, h->n, h->dim, h->dpad, b, kpad, kTcBase, ANN_METRIC_L2, 0, st);
-    if (!rc) rc = launch_tc_operand(h->centroids, h->C, h->dim, h->dpad, cb, kpad, kTcBase, ANN_METRIC_L2, 0, st);
-    if (rc) {
-        cudaFree(b);
-        cudaFree(cb);
-        return rc;
+    if (!i8 && !h->base_bf16) {
+        __nv_bfloat16* b = nullptr;
+        const cudaError_t e = cudaMalloc(&b, sizeof(__nv_bfloat16) * (size_t)h->n * kpad);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error("tensor-core IVF: cannot allocate the BF16 copy of the lists (%s)", cudaGetErrorString(e));
+            return ANN_ERR_NOMEM;
+        }
+        if ((rc = launch_tc_operand(h->original, h->n, h->dim, h->dpad, b, kpad, kTcBase, ANN_METRIC_L2, 0, st))) {
+            cudaFree(b);
+            return rc;
+        }
+        ANN_CUDA_TRY(cudaStreamSynchronize(st));
+        h->base_bf16 = b;
     }
-    ANN_CUDA_TRY(cudaStreamSynchronize(st));
-    h->kpad = kpad;
-    h->cent_bf16 = cb;
-    h->base_bf16 = b;
+    if (i8 && !h->sq8_fac) {
+        float2* f = nullptr;
+        if (cudaMalloc(&f, sizeof(float2) * (size_t)h->n) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("tensor-core IVF: cannot allocate the SQ8 row norms");
+            return ANN_ERR_NOMEM;
+        }
+        if ((rc = launch_tc_sq8_norms(h->codes, h->n, h->dim, h->dpad8, h->scale, f, st))) {
+            cudaFree(f);
+            return rc;
+        }
+        ANN_CUDA_TRY(cudaStreamSynchronize(st));
+        h->sq8_fac = f;
+    }
     return ANN_OK;
+}
+
+// Operand rows of the pairs: BF16 (kpad columns) or int8 weights (dpad8 bytes).
+static int64_t tc_pair_row_bytes(const ann_ivf* h) {
+    return std::max<int64_t>(2 * (int64_t)tc_kpad(h->dim, ANN_METRIC_L2), h->dpad8);
 }
 
 // Bytes of scratch one device-side query call of nq queries needs (mirrors the carving below).
@@ -710,7 +744,10 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
     if (c.tc) {
         sz.take<float>((size_t)nq * h->C);  // BF16 coarse keys
         sz.take<__nv_bfloat16>((size_t)nq * h->kpad);
-        sz.take<__nv_bfloat16>((size_t)nq * c.npc * h->kpad);
+        sz.take<unsigned char>((size_t)nq * c.npc * tc_pair_row_bytes(h));
+        sz.take<int8_t>((size_t)nq * h->dpad8);  // int8 query weights and factors (ANN_MODE_TC_SQ8)
+        sz.take<float>((size_t)nq);
+        sz.take<float>((size_t)nq * c.npc);
         sz.take<int64_t>((size_t)nq * c.npc);
         sz.take<int64_t>((size_t)h->C + 1);
         sz.take<int32_t>((size_t)tc_items_bound((int64_t)nq * c.npc, (int)h->C, h->sizes_desc[0]));
@@ -730,16 +767,31 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
 // min(R, its candidates) survivors is redone under its safe bar. Each query ends with the exact best R
 // keys of its stream, as the key-stream path below selects them, without writing the stream.
 // Returns with *done = false (and no output) when a warp's survivor region overflowed.
+struct TcOperands {
+    const void* qrows;     // the queries' operand rows
+    int row_bytes;
+    const void* B;         // the list-ordered base operand
+    int K;                 // operand columns (elements)
+    int kind;
+    const float2* col_fac;  // per base row (int8 form)
+    const float* qfac;      // per query (int8 form)
+    float* pfac;            // per pair, filled with the pairs (int8 form)
+};
+static TcOperands tc_operands(const ann_ivf* h, const IvfQueryCfg& c, const __nv_bfloat16* qb, const int8_t* q8,
+                              const float* qfac, float* pfac) {
+    if (c.i8) return TcOperands{q8, h->dpad8, h->codes, h->dpad8, kTcI8, h->sq8_fac, qfac, pfac};
+    return TcOperands{qb, 2 * h->kpad, h->base_bf16, h->kpad, kTcBF16, nullptr, nullptr, nullptr};
+}
+
 constexpr int kTcSampledMinQueries = 256;
 constexpr int kSampleDiv = 8;
 
 static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, const IvfQueryArgs& a,
-                          const IvfBatchArgs& b, const __nv_bfloat16* qb, __nv_bfloat16* Apk, int64_t* titem,
+                          const IvfBatchArgs& b, const TcOperands& op, unsigned char* Apk, int64_t* titem,
                           int32_t* titem_list, int64_t items_cap, float* keyR, int* idR, int prec, bool* done,
                           cudaStream_t st) {
     *done = false;
     const int nq = a.plan.nq, npc = c.npc, C = (int)h->C, R = c.R;
-    const int kpad = h->kpad;
     const int64_t max_pairs = (int64_t)nq * npc;
     const int64_t largest = h->sizes_desc.empty() ? 1 : h->sizes_desc[0];
     const int64_t head_max = ceil_div(largest, kSampleDiv);
@@ -815,13 +867,18 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     maps.soff = soff;
     maps.sseg = sseg;
     maps.sdbase = sdbase;
-    if ((rc = launch_tc_ivf_pairs(qb, kpad, b.pair_vals, b.pair_lists, b.lq_off + C, max_pairs, npc, b.cand_off,
-                                  a.plan.seg_pref, h->list_off, Apk, nullptr, st, maps)))
+    maps.qfac = op.qfac;
+    maps.pfac = op.pfac;
+    if ((rc = launch_tc_ivf_pairs(op.qrows, op.row_bytes, b.pair_vals, b.pair_lists, b.lq_off + C, max_pairs, npc,
+                                  b.cand_off, a.plan.seg_pref, h->list_off, Apk, nullptr, st, maps)))
         return rc;
     // 1. sample pass: keys of the list heads into the sample streams; the two bars per query
     if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, C, sitem, st, lcap))) return rc;
     if ((rc = launch_tc_item_lists(sitem, C, sitem_list, scap, st))) return rc;
-    TcGemmArgs gs{(int)max_pairs, (int)h->n, kpad, nullptr, SK, 0, h->d_err};
+    TcGemmArgs gs{(int)max_pairs, (int)h->n, op.K, nullptr, SK, 0, h->d_err};
+    gs.kind = op.kind;
+    gs.col_fac = op.col_fac;
+    gs.row_fac = op.pfac;
     gs.g_item_off = sitem;
     gs.g_a_off = b.lq_off;
     gs.g_b_off = h->list_off;
@@ -830,7 +887,7 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     gs.g_total = sitem + C;
     gs.g_lists = C;
     gs.g_item_list = sitem_list;
-    if ((rc = launch_tc_gemm(Apk, h->base_bf16, gs, st))) return rc;
+    if ((rc = launch_tc_gemm(Apk, op.B, gs, st))) return rc;
     RadixSelectArgs bar{};
     bar.keys = SK;
     bar.ld = npc * head_max;
@@ -846,7 +903,10 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, C, titem, st))) return rc;
     if ((rc = launch_tc_item_lists(titem, C, titem_list, items_cap, st))) return rc;
     auto filter = [&](const float* tau) -> int {
-        TcGemmArgs g{(int)max_pairs, (int)h->n, kpad, nullptr, nullptr, 0, h->d_err};
+        TcGemmArgs g{(int)max_pairs, (int)h->n, op.K, nullptr, nullptr, 0, h->d_err};
+        g.kind = op.kind;
+        g.col_fac = op.col_fac;
+        g.row_fac = op.pfac;
         g.g_item_off = titem;
         g.g_a_off = b.lq_off;
         g.g_b_off = h->list_off;
@@ -860,7 +920,7 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
         g.frow = frow;
         g.wcount = wcnt;
         g.wcap = wcap;
-        int r = launch_tc_gemm(Apk, h->base_bf16, g, st);
+        int r = launch_tc_gemm(Apk, op.B, g, st);
         if (r) return r;
         TcGroupArgs ga{fkey, fcol, frow, wcnt, nwarps, wcap, nq, h->n, 1, rowcnt, offs, cursor, gkey, gid, flags + 1};
         return launch_tc_group(ga, st);
@@ -935,7 +995,10 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     float* lkeys = c.lsh_keys ? cv.take<float>((size_t)nq * c.ub_cand) : nullptr;
     float* ckeys = c.tc ? cv.take<float>((size_t)nq * h->C) : nullptr;
     __nv_bfloat16* qb = c.tc ? cv.take<__nv_bfloat16>((size_t)nq * h->kpad) : nullptr;
-    __nv_bfloat16* Apk = c.tc ? cv.take<__nv_bfloat16>((size_t)nq * c.npc * h->kpad) : nullptr;
+    unsigned char* Apk = c.tc ? cv.take<unsigned char>((size_t)nq * c.npc * tc_pair_row_bytes(h)) : nullptr;
+    int8_t* q8 = c.tc ? cv.take<int8_t>((size_t)nq * h->dpad8) : nullptr;
+    float* qfac = c.tc ? cv.take<float>((size_t)nq) : nullptr;
+    float* pfac = c.tc ? cv.take<float>((size_t)nq * c.npc) : nullptr;
     int64_t* dbase = c.tc ? cv.take<int64_t>((size_t)nq * c.npc) : nullptr;
     int64_t* titem = c.tc ? cv.take<int64_t>((size_t)h->C + 1) : nullptr;
     const int64_t items_cap = c.tc ? tc_items_bound((int64_t)nq * c.npc, (int)h->C, h->sizes_desc[0]) : 0;
@@ -974,6 +1037,8 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         TcGemmArgs ca{nq, h->C, h->kpad, nullptr, ckeys, h->C, h->d_err};
         if ((rc = launch_tc_gemm(qb, h->cent_bf16, ca, st))) return rc;
         if ((rc = launch_tc_coarse(ckeys, h->C, nq, h->C, c.npc, 16, qdev, h->centroids, h->dpad, probes, st)))
+            return rc;
+        if (c.i8 && (rc = launch_tc_sq8_query(qdev, nq, h->dim, h->dpad, h->scale, h->offset, q8, h->dpad8, qfac, st)))
             return rc;
     } else if (c.coarse_flat) {
         FlatScanArgs fa{h->centroids, h->C, h->dpad, qdev, nq, ANN_METRIC_L2, c.npc, c.rps_c, c.nsplit_c, ckey, cid};
@@ -1046,8 +1111,8 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         if ((rc = batched_prepare(a, bscratch, c.sort_tmp, c.scan_tmp, &b, tot, st))) return rc;
         bool sampled_done = false;
         if (tot[2] == 0 && c.tc && nq >= kTcSampledMinQueries) {
-            if ((rc = ivf_tc_sampled(h, ws, c, a, b, qb, Apk, titem, titem_list, items_cap, keyR, idR, prec,
-                                     &sampled_done, st)))
+            if ((rc = ivf_tc_sampled(h, ws, c, a, b, tc_operands(h, c, qb, q8, qfac, pfac), Apk, titem, titem_list,
+                                     items_cap, keyR, idR, prec, &sampled_done, st)))
                 return rc;
             done = sampled_done;
         }
@@ -1057,14 +1122,21 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
             if (c.tc) {
                 // BF16 keys of every (pair, list row) from grouped tcgen05 GEMMs, the best R of each
                 // query's stream by radix selection
-                const int kpad = h->kpad;
+                const TcOperands op = tc_operands(h, c, qb, q8, qfac, pfac);
                 const int64_t max_pairs = (int64_t)nq * c.npc;
-                if ((rc = launch_tc_ivf_pairs(qb, kpad, b.pair_vals, b.pair_lists, b.lq_off + h->C, max_pairs, c.npc,
-                                              b.cand_off, a.plan.seg_pref, h->list_off, Apk, dbase, st)))
+                TcIvfSampleMaps maps;
+                maps.qfac = op.qfac;
+                maps.pfac = op.pfac;
+                if ((rc = launch_tc_ivf_pairs(op.qrows, op.row_bytes, b.pair_vals, b.pair_lists, b.lq_off + h->C,
+                                              max_pairs, c.npc, b.cand_off, a.plan.seg_pref, h->list_off, Apk, dbase,
+                                              st, maps)))
                     return rc;
                 if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, h->C, titem, st))) return rc;
                 if ((rc = launch_tc_item_lists(titem, (int)h->C, titem_list, items_cap, st))) return rc;
-                TcGemmArgs g{(int)max_pairs, (int)h->n, kpad, nullptr, D, 0, h->d_err};
+                TcGemmArgs g{(int)max_pairs, (int)h->n, op.K, nullptr, D, 0, h->d_err};
+                g.kind = op.kind;
+                g.col_fac = op.col_fac;
+                g.row_fac = op.pfac;
                 g.g_item_off = titem;
                 g.g_a_off = b.lq_off;
                 g.g_b_off = h->list_off;
@@ -1072,7 +1144,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                 g.g_total = titem + h->C;
                 g.g_lists = h->C;
                 g.g_item_list = titem_list;
-                if ((rc = launch_tc_gemm(Apk, h->base_bf16, g, st))) return rc;
+                if ((rc = launch_tc_gemm(Apk, op.B, g, st))) return rc;
                 h->prof.mark(prec, st);
                 RadixSelectArgs rs{};
                 rs.keys = D;
@@ -1201,7 +1273,7 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     }
     ANN_CHECK_ARG(nq >= 0 && k >= 1, "ann_ivf_query: nq=%d, k=%d", nq, k);
     ANN_CHECK_ARG(ldq >= h->dim, "ann_ivf_query: query stride < dim");
-    ANN_CHECK_ARG(mode == ANN_MODE_EXACT || mode == ANN_MODE_REFERENCE || mode == ANN_MODE_TC,
+    ANN_CHECK_ARG(mode == ANN_MODE_EXACT || mode == ANN_MODE_REFERENCE || mode == ANN_MODE_TC || mode == ANN_MODE_TC_SQ8,
                   "ann_ivf_query: unknown mode %d", mode);
     ANN_CHECK_ARG(nq == 0 || (queries && out_ids), "ann_ivf_query: null pointer");
     ANN_CHECK_ARG(k <= 1024, "ann_ivf_query: k=%d > 1024", k);
@@ -1214,7 +1286,8 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     IvfQueryCfg c{};
     int rc0 = ANN_OK;
     c.ref = mode == ANN_MODE_REFERENCE;
-    c.tc = mode == ANN_MODE_TC;
+    c.tc = mode == ANN_MODE_TC || mode == ANN_MODE_TC_SQ8;
+    c.i8 = mode == ANN_MODE_TC_SQ8;
     c.k = k;
     c.npc = std::max(1, std::min(n_probe_clusters, h->C));  // active_clusters (:332)
     // R = max(k, refine_r > 0 ? refine_r : 4k) (:472-474); cap max(2000, 4 * target) (:357-358)
@@ -1244,14 +1317,14 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     c.fallback = c.lsh || smallest < k;
     c.ub_cand = std::max<int64_t>(ub, 1);
     c.ub = c.ub_cand;
-    if (c.lsh && mode == ANN_MODE_TC) {
+    if (c.lsh && c.tc) {
         set_error("ann_ivf_query: the tensor-core form scores whole lists; LSH bucket tables use the SQ8 forms");
         return ANN_ERR_UNSUPPORTED;
     }
     c.ncp = ref_num_checkpoints(h->dim);
     c.coarse_flat = !c.ref && c.npc <= 512;
     c.batched = !c.ref && !c.lsh && (c.tc || nq >= kBatchedMinQueries);
-    if (c.tc && (rc0 = ivf_ensure_bf16(h, st))) return rc0;
+    if (c.tc && (rc0 = ivf_ensure_tc(h, c.i8, st))) return rc0;
     const int dpad = h->dpad;
     const bool host = mem == ANN_MEM_HOST;
 

@@ -112,6 +112,8 @@ __device__ __forceinline__ uint64_t sw128_desc(const void* p) {
 constexpr uint32_t kIdescShape = (1u << 4) | ((uint32_t)(kBN >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24);
 constexpr uint32_t kIdescBF16 = kIdescShape | (1u << 7) | (1u << 10);
 constexpr uint32_t kIdescE4M3 = kIdescShape;
+// kind::i8: S32 accumulator (bits 4-5 = 2), A signed (bits 7-9 = 1), B unsigned (bits 10-12 = 0)
+constexpr uint32_t kIdescI8 = (2u << 4) | ((uint32_t)(kBN >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24) | (1u << 7);
 
 // One MMA of the 32 bytes of K that follow each descriptor's start: 16 BF16 or 32 E4M3 elements.
 template <int KIND>
@@ -122,12 +124,23 @@ __device__ __forceinline__ void mma_issue(uint32_t tmem_d, uint64_t ad, uint64_t
             " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
             "l"(ad), "l"(bd), "r"(kIdescBF16), "r"(accumulate)
             : "memory");
-    else
+    else if (KIND == kTcE4M3)
         asm volatile(
             "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
             " tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
             "l"(ad), "l"(bd), "r"(kIdescE4M3), "r"(accumulate)
             : "memory");
+    else
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
+            "l"(ad), "l"(bd), "r"(kIdescI8), "r"(accumulate)
+            : "memory");
+}
+// An accumulator read from TMEM as a float: FP32 bits, or (kind::i8) an int32 converted (exact below 2^24).
+template <int KIND>
+__device__ __forceinline__ float acc_value(uint32_t r) {
+    return KIND == kTcI8 ? __int2float_rn((int)r) : __uint_as_float(r);
 }
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
@@ -335,6 +348,7 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                 // the stream position of list row b0 for each of the warp's 32 pairs (lane r holds row r's)
                 const int64_t dst_lane = (ml < gt.am ? a.g_dbase[gt.a0 + ml] : 0) + gt.b0;
                 const int rows = min(32, gt.am - lane_base);  // valid pairs of this warp
+                const float grf = (a.row_fac && ml < gt.am) ? a.row_fac[gt.a0 + ml] : 1.f;
                 const uint32_t tb = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kBN + col0);
 #pragma unroll 1
                 for (int c = 0; c < kCols; c += 64) {
@@ -347,11 +361,20 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                     for (int h = 0; h < 2; ++h) {
                         const int cb = col0 + c + 32 * h;
                         if (rows <= 0 || cb >= gt.bn) continue;  // uniform across the warp
-                        // transpose through shared memory: each store writes 32 consecutive keys of one pair
-#pragma unroll
-                        for (int u = 0; u < 32; ++u) tw[lane * 33 + u] = __uint_as_float(h ? r1[u] : r0[u]);
-                        __syncwarp();
                         const bool cok = cb + lane < gt.bn;
+                        // transpose through shared memory: each store writes 32 consecutive keys of one pair
+                        if (a.col_fac) {  // scaled operands: the column factors of the 32 columns by shuffles
+                            const float2 f = cok ? a.col_fac[gt.b0 + cb + lane] : make_float2(0.f, 0.f);
+#pragma unroll
+                            for (int u = 0; u < 32; ++u)
+                                tw[lane * 33 + u] = fmaf(__shfl_sync(0xffffffffu, f.x, u),
+                                                         grf * acc_value<KIND>(h ? r1[u] : r0[u]),
+                                                         __shfl_sync(0xffffffffu, f.y, u));
+                        } else {
+#pragma unroll
+                            for (int u = 0; u < 32; ++u) tw[lane * 33 + u] = acc_value<KIND>(h ? r1[u] : r0[u]);
+                        }
+                        __syncwarp();
                         for (int r = 0; r < rows; ++r) {
                             const int64_t dr = __shfl_sync(0xffffffffu, dst_lane, r);
                             if (cok) a.out[dr + cb + lane] = tw[r * 33 + lane];
@@ -366,6 +389,7 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
             // the tile's rows and columns: a dense tile, or a grouped one (a list's pairs and rows; rows and
             // columns past them belong to the next list and are masked like rows past M)
             int rq = m;                         // the row recorded for a survivor (grouped: its query)
+            int64_t arow = m;                   // the A row (per-row factors)
             bool mvalid = m < a.M;
             int64_t cbase = n0;                 // recorded column of the tile's first column
             int ncols = a.N - n0;               // valid columns of the tile from its first
@@ -373,12 +397,13 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                 const GroupTile gt = group_tile(a, t);
                 const int ml = lane_base + lane;
                 mvalid = ml < gt.am;
+                arow = gt.a0 + ml;
                 rq = mvalid ? (a.g_row_query ? a.g_row_query[gt.a0 + ml] : (int)(gt.a0 + ml)) : 0;
                 cbase = gt.b0;
                 ncols = gt.bn;
             }
-            const float an = (a.normA && mvalid) ? a.normA[m] : 0.f;
-            const float rfac = (a.row_fac && mvalid) ? a.row_fac[m] : 1.f;
+            const float an = (a.normA && mvalid) ? a.normA[arow] : 0.f;
+            const float rfac = (a.row_fac && mvalid) ? a.row_fac[arow] : 1.f;
             // rows past M (TMA zero fill) get a bar no key passes
             const float tau = (a.tau && mvalid) ? a.tau[rq] : -kInf;
             const float tau_up = nextafterf(tau, kInf);
@@ -394,9 +419,10 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                 __syncwarp();
 #pragma unroll
                 for (int i = 0; i < kCols / 32; ++i) {
-                    const int col = n0 + col0 + 32 * i + lane;
-                    const int64_t nrow = (int64_t)(col / kBN) * kBN * a.b_tile_stride + col % kBN;
-                    const float2 f = col < a.N ? a.col_fac[nrow] : make_float2(0.f, 0.f);
+                    const int lcol = col0 + 32 * i + lane;  // column within the tile
+                    const int col = n0 + lcol;
+                    const int64_t nrow = grouped ? cbase + lcol : (int64_t)(col / kBN) * kBN * a.b_tile_stride + col % kBN;
+                    const float2 f = lcol < ncols ? a.col_fac[nrow] : make_float2(0.f, 0.f);
                     sfx[32 * i + lane] = f.x;
                     sfy[32 * i + lane] = f.y;
                 }
@@ -415,10 +441,10 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                     float v[32];
                     if (has_an) {
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) v[u] = __uint_as_float(h ? r1[u] : r0[u]) + an;
+                        for (int u = 0; u < 32; ++u) v[u] = acc_value<KIND>(h ? r1[u] : r0[u]) + an;
                     } else {
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) v[u] = __uint_as_float(h ? r1[u] : r0[u]);
+                        for (int u = 0; u < 32; ++u) v[u] = acc_value<KIND>(h ? r1[u] : r0[u]);
                     }
                     const int nb = n0 + col0 + c + 32 * h;  // output column of v[0]
                     const int lb = col0 + c + 32 * h;       // its column within the tile
@@ -582,10 +608,11 @@ static cudaError_t run_tc_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, c
 
 int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream_t st) {
     const int step = a.kind == kTcBF16 ? 16 : 32;
-    ANN_CHECK_ARG(a.kind == kTcBF16 || a.kind == kTcE4M3, "tensor-core scan: element kind %d", a.kind);
+    ANN_CHECK_ARG(a.kind == kTcBF16 || a.kind == kTcE4M3 || a.kind == kTcI8, "tensor-core scan: element kind %d",
+                  a.kind);
     ANN_CHECK_ARG(a.K % step == 0 && a.K > 0, "tensor-core scan: K=%d not a positive multiple of %d", a.K, step);
-    ANN_CHECK_ARG(a.kind == kTcBF16 || (a.col_fac && a.row_fac && a.g_item_off == nullptr),
-                  "tensor-core scan: E4M3 operands need their scale factors (and no grouping)");
+    ANN_CHECK_ARG(a.kind == kTcBF16 || (a.col_fac && a.row_fac && (a.g_item_off == nullptr || a.kind == kTcI8)),
+                  "tensor-core scan: E4M3 / I8 operands need their scale factors (E4M3: no grouping)");
     ANN_CHECK_ARG((reinterpret_cast<uintptr_t>(A) & 15) == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0,
                   "tensor-core scan: operands must be 16-byte aligned");
     ANN_CHECK_ARG(a.out != nullptr || (a.tau && a.fkey && a.fcol && a.frow && a.wcount && a.wcap > 0),
@@ -611,9 +638,12 @@ int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream
     if (a.kind == kTcBF16)
         e = filter ? run_tc_gemm<kTcBF16, kFilterEpi>(tmA, tmB, a, grid, st)
                    : run_tc_gemm<kTcBF16, kKeyEpi>(tmA, tmB, a, grid, st);
-    else
+    else if (a.kind == kTcE4M3)
         e = filter ? run_tc_gemm<kTcE4M3, kFilterEpi>(tmA, tmB, a, grid, st)
                    : run_tc_gemm<kTcE4M3, kKeyEpi>(tmA, tmB, a, grid, st);
+    else
+        e = filter ? run_tc_gemm<kTcI8, kFilterEpi>(tmA, tmB, a, grid, st)
+                   : run_tc_gemm<kTcI8, kKeyEpi>(tmA, tmB, a, grid, st);
     ANN_CUDA_TRY(e);
     ANN_LAUNCH_CHECK();
     return ANN_OK;

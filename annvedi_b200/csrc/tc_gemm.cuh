@@ -11,7 +11,9 @@ namespace annb {
 //       query row [bf16(-2a), 1, 1, 1]  ->  sum = |b|^2 - 2 a.b
 //   IP: base row [bf16(b)], query row [bf16(-a)]  ->  sum = -a.b
 // Smaller keys are better in both metrics.
-enum TcKind { kTcBF16 = 0, kTcE4M3 = 1 };
+// kTcI8: A int8, B uint8 (tcgen05.mma.kind::i8, exact int32 accumulation): the SQ8 codes of an IVF index as
+// they are stored, against an int8 query weight; the key is col_fac[n].y + col_fac[n].x * row_fac[m] * acc.
+enum TcKind { kTcBF16 = 0, kTcE4M3 = 1, kTcI8 = 2 };
 
 struct TcGemmArgs {
     int M, N, K;           // A [M, K], B [N, K] BF16 row-major; K a multiple of 16
@@ -46,8 +48,9 @@ struct TcGemmArgs {
     // Grouped filter mode (grouped, out == null): A row i belongs to query g_row_query[i]; its bar is
     // tau[g_row_query[i]], and a survivor is recorded as (key, list row g_b_off[l] + r, that query).
     const int32_t* g_row_query = nullptr;
-    // Element kind of A and B. E4M3 operands carry a scale per row (launch_tc_operand_e4m3): the key is
-    // col_fac[n].y + col_fac[n].x * row_fac[m] * accumulator (key-matrix and filter modes).
+    // Element kind of A and B. E4M3 and I8 operands carry factors per row: the key is
+    // col_fac[n].y + col_fac[n].x * row_fac[m] * accumulator (key-matrix and filter modes; I8 also grouped,
+    // with n the absolute B row and m the A row).
     int kind = kTcBF16;
     const float2* col_fac = nullptr;  // per B row, indexed like B's rows
     const float* row_fac = nullptr;   // per A row

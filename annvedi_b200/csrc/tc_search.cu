@@ -148,20 +148,21 @@ __global__ void __launch_bounds__(1024) tc_ivf_items_kernel(const int64_t* lq_of
 }
 
 // one warp per pair
-__global__ void tc_ivf_pairs_kernel(const __nv_bfloat16* qb, int kpad, const int32_t* pair_vals,
+__global__ void tc_ivf_pairs_kernel(const unsigned char* qrows, int row_bytes, const int32_t* pair_vals,
                                     const int32_t* pair_lists, const int64_t* n_pairs, int64_t max_pairs, int npc,
                                     const int64_t* cand_off, const int64_t* seg_pref, const int64_t* list_off,
-                                    __nv_bfloat16* A, int64_t* dbase, TcIvfSampleMaps sm) {
+                                    unsigned char* A, int64_t* dbase, TcIvfSampleMaps sm) {
     const int64_t np = min(*n_pairs, max_pairs);
     const int lane = threadIdx.x & 31;
     for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < np;
          i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int32_t v = pair_vals[i];
         const int q = v / npc, j = v % npc;
-        const uint4* src = reinterpret_cast<const uint4*>(qb + (size_t)q * kpad);
-        uint4* dst = reinterpret_cast<uint4*>(A + (size_t)i * kpad);
-        for (int c = lane; c < kpad / 8; c += 32) dst[c] = src[c];
+        const uint4* src = reinterpret_cast<const uint4*>(qrows + (size_t)q * row_bytes);
+        uint4* dst = reinterpret_cast<uint4*>(A + (size_t)i * row_bytes);
+        for (int c = lane; c < row_bytes / 16; c += 32) dst[c] = src[c];
         if (lane == 0) {
+            if (sm.pfac) sm.pfac[i] = sm.qfac[q];
             if (dbase) dbase[i] = cand_off[q] + seg_pref[(int64_t)q * (npc + 1) + j] - list_off[pair_lists[i]];
             if (sm.row_query) sm.row_query[i] = q;
             // the grouped epilogue adds the tile's absolute list row, as for dbase
@@ -184,6 +185,45 @@ __global__ void tc_ivf_sample_plan_kernel(IvfPlan p, const int64_t* __restrict__
         if (j < ns && l >= 0) run += lcap[l];
     }
     slen[q] = run;
+}
+
+// One warp per query: the int8 weights of the SQ8 tensor-core key. w_d = -2 scale_d (q_d - offset_d), so that
+// sum_d code_d * w_d + sum_d (code_d scale_d)^2 = the SQ8 distance - |q - offset|^2 (a per-query constant).
+// a_d = rint(w_d * 127 / max|w|) as int8 (zero past dim), qfac = max|w| / 127 (1 for an all-zero w).
+__global__ void tc_sq8_query_kernel(const float* __restrict__ q, int nq, int dim, int ldq,
+                                    const float* __restrict__ scale, const float* __restrict__ offset,
+                                    int8_t* __restrict__ out, int ldo, float* __restrict__ qfac) {
+    const int qi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (qi >= nq) return;
+    const float* qr = q + (int64_t)qi * ldq;
+    float mx = 0.f;
+    for (int d = lane; d < dim; d += 32) mx = fmaxf(mx, fabsf(-2.f * scale[d] * (qr[d] - offset[d])));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const float alpha = mx > 0.f ? 127.f / mx : 1.f;
+    for (int d = lane; d < ldo; d += 32) {
+        float v = 0.f;
+        if (d < dim) v = rintf(-2.f * scale[d] * (qr[d] - offset[d]) * alpha);
+        out[(int64_t)qi * ldo + d] = (int8_t)fmaxf(-127.f, fminf(127.f, v));
+    }
+    if (lane == 0) qfac[qi] = 1.f / alpha;
+}
+
+// One warp per row: fac[i] = (1, sum_d (code_d scale_d)^2), the row's reconstructed squared norm.
+__global__ void tc_sq8_norms_kernel(const uint8_t* __restrict__ codes, int64_t n, int dim, int ldc,
+                                    const float* __restrict__ scale, float2* __restrict__ fac) {
+    const int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    float s = 0.f;
+    for (int d = lane; d < dim; d += 32) {
+        const float x = (float)codes[i * ldc + d] * scale[d];
+        s = fmaf(x, x, s);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) fac[i] = make_float2(1.f, s);
 }
 
 // lcap[l] = ceil(size_l / div): the sampled head of list l
@@ -366,15 +406,17 @@ int launch_tc_item_lists(const int64_t* item_off, int C, int32_t* item_list, int
     return ANN_OK;
 }
 
-int launch_tc_ivf_pairs(const __nv_bfloat16* qb, int kpad, const int32_t* pair_vals, const int32_t* pair_lists,
+int launch_tc_ivf_pairs(const void* qrows, int row_bytes, const int32_t* pair_vals, const int32_t* pair_lists,
                         const int64_t* n_pairs, int64_t max_pairs, int npc, const int64_t* cand_off,
-                        const int64_t* seg_pref, const int64_t* list_off, __nv_bfloat16* A, int64_t* dbase,
-                        cudaStream_t st, const TcIvfSampleMaps& sm) {
+                        const int64_t* seg_pref, const int64_t* list_off, void* A, int64_t* dbase, cudaStream_t st,
+                        const TcIvfSampleMaps& sm) {
     if (max_pairs == 0) return ANN_OK;
-    ANN_CHECK_ARG(kpad % 8 == 0, "tensor-core IVF: kpad %d", kpad);
+    ANN_CHECK_ARG(row_bytes % 16 == 0, "tensor-core IVF: operand rows of %d bytes", row_bytes);
+    ANN_CHECK_ARG((sm.pfac == nullptr) == (sm.qfac == nullptr), "tensor-core IVF: pair factors need query factors");
     const int grid = (int)std::min<int64_t>(ceil_div(max_pairs * 32, 256), 16 * kNumSMs);
-    tc_ivf_pairs_kernel<<<grid, 256, 0, st>>>(qb, kpad, pair_vals, pair_lists, n_pairs, max_pairs, npc, cand_off,
-                                              seg_pref, list_off, A, dbase, sm);
+    tc_ivf_pairs_kernel<<<grid, 256, 0, st>>>(static_cast<const unsigned char*>(qrows), row_bytes, pair_vals,
+                                              pair_lists, n_pairs, max_pairs, npc, cand_off, seg_pref, list_off,
+                                              static_cast<unsigned char*>(A), dbase, sm);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }
@@ -407,6 +449,23 @@ int launch_tc_ivf_sample_plan(const IvfPlan& p, const int64_t* list_off, int C, 
     ANN_LAUNCH_CHECK();
     if (p.nq == 0) return ANN_OK;
     tc_ivf_sample_plan_kernel<<<(unsigned)ceil_div(p.nq, 128), 128, 0, st>>>(p, lcap, sseg, slen);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int launch_tc_sq8_query(const float* q, int nq, int dim, int ldq, const float* scale, const float* offset, int8_t* out,
+                        int ldo, float* qfac, cudaStream_t st) {
+    if (nq == 0) return ANN_OK;
+    ANN_CHECK_ARG(ldo >= dim && ldo % 16 == 0, "SQ8 query weights: row of %d bytes for dim %d", ldo, dim);
+    tc_sq8_query_kernel<<<(unsigned)ceil_div(nq, 8), 256, 0, st>>>(q, nq, dim, ldq, scale, offset, out, ldo, qfac);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int launch_tc_sq8_norms(const uint8_t* codes, int64_t n, int dim, int ldc, const float* scale, float2* fac,
+                        cudaStream_t st) {
+    if (n == 0) return ANN_OK;
+    tc_sq8_norms_kernel<<<(unsigned)ceil_div(n, 8), 256, 0, st>>>(codes, n, dim, ldc, scale, fac);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

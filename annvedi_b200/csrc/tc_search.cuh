@@ -62,16 +62,27 @@ inline int64_t tc_items_bound(int64_t pairs, int C, int64_t largest) { return (p
 // the stream position of the list's row 0 in the candidate array.
 // Optional maps of the sampled form: row_query[i] = q; sdbase[i] = soff[q] + sseg[q][j] - list_off[list]
 // (the sample-stream position of the list's row 0, as dbase is for the candidate stream).
+// With qfac / pfac (the int8 form), pfac[i] = qfac[q].
 struct TcIvfSampleMaps {
     int32_t* row_query = nullptr;
     const int64_t* soff = nullptr;
     const int64_t* sseg = nullptr;  // [nq, npc]
     int64_t* sdbase = nullptr;
+    const float* qfac = nullptr;
+    float* pfac = nullptr;
 };
-int launch_tc_ivf_pairs(const __nv_bfloat16* qb, int kpad, const int32_t* pair_vals, const int32_t* pair_lists,
+// qrows: the queries' operand rows of row_bytes each (BF16 kpad columns, or int8 weights); A: the pairs' rows.
+int launch_tc_ivf_pairs(const void* qrows, int row_bytes, const int32_t* pair_vals, const int32_t* pair_lists,
                         const int64_t* n_pairs, int64_t max_pairs, int npc, const int64_t* cand_off,
-                        const int64_t* seg_pref, const int64_t* list_off, __nv_bfloat16* A, int64_t* dbase,
-                        cudaStream_t st, const TcIvfSampleMaps& sm = TcIvfSampleMaps{});
+                        const int64_t* seg_pref, const int64_t* list_off, void* A, int64_t* dbase, cudaStream_t st,
+                        const TcIvfSampleMaps& sm = TcIvfSampleMaps{});
+// SQ8 codes on the tensor cores (kind::i8): the int8 query weights rint(-2 scale_d (q_d - offset_d) * 127 / max)
+// [nq, ldo] (zero past dim) with their factor qfac = max / 127, and per row fac = (1, sum_d (code_d scale_d)^2);
+// the key fac.y + qfac * sum_d code_d a_d is the SQ8 distance less |q - offset|^2, up to the weights' rounding.
+int launch_tc_sq8_query(const float* q, int nq, int dim, int ldq, const float* scale, const float* offset, int8_t* out,
+                        int ldo, float* qfac, cudaStream_t st);
+int launch_tc_sq8_norms(const uint8_t* codes, int64_t n, int dim, int ldc, const float* scale, float2* fac,
+                        cudaStream_t st);
 // The sampled heads of the lists, lcap[l] = ceil(size_l / div), and each query's sample stream over its
 // probed lists: segment starts sseg [nq, npc] and length slen [nq].
 int launch_tc_ivf_sample_plan(const IvfPlan& p, const int64_t* list_off, int C, int div, int64_t* lcap, int64_t* sseg,

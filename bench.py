@@ -347,7 +347,8 @@ def run_ours(args, rank, world, local):
         }
 
     # ---- IVF-SQ8: lists = the 2,048 L2-normalised generating centres ----
-    if "ivf" in sel or "ivf_tc" in sel:
+    ivf_forms = {"ivf", "ivf_tc", "ivf_tc_sq8"}
+    if sel & ivf_forms:
         ivf = IVFIndex(device=local, mode="exact")
         t0 = time.perf_counter()
         ivf.fit(base, 1, 0, 2048, centroids=w.centres, assign=w.assign)
@@ -358,9 +359,9 @@ def run_ours(args, rank, world, local):
     # nprobe for each IVF form: the autotuner's cheapest probe count with recall@100 >= 0.95 (re-rank
     # depth fixed at the configuration's R)
     sweep, sweep_tc = [], []
-    if "ivf" in sel or "ivf_tc" in sel:
+    if sel & ivf_forms:
         from annvedi_b200 import autotune
-        modes = [m for m, f in (("exact", "ivf"), ("tc", "ivf_tc")) if f in sel]
+        modes = [m for m, f in (("exact", "ivf"), ("tc", "ivf_tc"), ("tc_sq8", "ivf_tc_sq8")) if f in sel]
         tuned = autotune.tune_ivf(ivf, base, queries, kth, K_NN, 0.95, modes=modes, nprobes=(8, 16, 32, 64, 128),
                                   refines=(args.refine,), reps=2)
 
@@ -406,11 +407,33 @@ def run_ours(args, rank, world, local):
                        "candidate_cap": "none"},
         }
 
+    # ---- IVF on the tensor cores over the SQ8 codes themselves: int8 query weights x uint8 codes ----
+    sweep_sq8 = []
+    if "ivf_tc_sq8" in sel:
+        npc_q, q_rec, q_qps, sweep_sq8 = pick("tc_sq8")
+
+        def ivf_q_step():
+            ivf.search(queries, K_NN, 0, npc_q, args.refine, max_candidates=0, mode="tc_sq8", out_ids=o_ids,
+                       out_dists=o_d)
+
+        forms["ivf_tc_sq8"] = {
+            "qps": q_qps, "recall": q_rec, "step": ivf_q_step,
+            "host": lambda: ivf.search(qh, K_NN, 0, npc_q, args.refine, max_candidates=0, mode="tc_sq8",
+                                       with_dists=False),
+            "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc_q, args.refine, max_candidates=0, mode="tc_sq8",
+                                            out_ids=o_ids[:1], with_dists=False),
+            "lat_host": lambda x: ivf.search(x, K_NN, 0, npc_q, args.refine, max_candidates=0, mode="tc_sq8",
+                                             with_dists=False),
+            "dtype": "u8 x s8 (tcgen05 kind::i8 over the SQ8 codes, int32 accumulate, exact fp32 re-rank)",
+            "config": {"form": "ivf-sq8 codes on tensor cores", "n_lists": 2048, "nprobe": npc_q,
+                       "refine_r": args.refine, "candidate_cap": "none"},
+        }
+
     # ---- the headline: the fastest form at recall@100 >= 0.95 (or the one asked for) ----
     ok = {k2: v for k2, v in forms.items() if v["recall"] >= 0.95} or forms
-    if args.form in ("tc", "ivf", "ivf_tc") and {"tc": "tensor_core_exact", "ivf": "ivf_sq8",
-                                                  "ivf_tc": "ivf_tc"}[args.form] in forms:
-        head = {"tc": "tensor_core_exact", "ivf": "ivf_sq8", "ivf_tc": "ivf_tc"}[args.form]
+    form_names = {"tc": "tensor_core_exact", "ivf": "ivf_sq8", "ivf_tc": "ivf_tc", "ivf_tc_sq8": "ivf_tc_sq8"}
+    if args.form in form_names and form_names[args.form] in forms:
+        head = form_names[args.form]
     else:
         head = max(ok, key=lambda k2: ok[k2]["qps"])
     hf = forms[head]
@@ -491,7 +514,7 @@ def run_ours(args, rank, world, local):
                   "select": stt["tc_select_ms"], "rerank": stt["rerank_ms"]}
         stage_ms = {k2: round(v / args.steps, 4) for k2, v in stages.items()}
         extra = {"gemm_launches_per_batch": round(stt["tc_gemm_launches"] / args.steps, 2)}
-    elif head == "ivf_tc":
+    elif head in ("ivf_tc", "ivf_tc_sq8"):
         prof = ivf.get_profile_results()
         stage = prof.get("stage_ms", {})
         calls = max(1, prof.get("profiled_calls", 1))
@@ -543,7 +566,7 @@ def run_ours(args, rank, world, local):
         "speedup_vs_plain_fp32_scan": round(qps / (flat_qps * world), 2) if flat_qps else None,
         "forms": summary,
         "plain_fp32_scan": flat_line,
-        "nprobe_sweep": {"ivf_sq8": sweep, "ivf_tc": sweep_tc,
+        "nprobe_sweep": {"ivf_sq8": sweep, "ivf_tc": sweep_tc, "ivf_tc_sq8": sweep_sq8,
                          "chosen_by": "annvedi_b200.autotune.tune_ivf (cheapest nprobe with recall@100 >= 0.95)"},
         "latency_ms_batch1": latency,
         "ivf_build_s": round(build_s, 3) if build_s is not None else None,
@@ -1108,8 +1131,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--refine", type=int, default=300)
     ap.add_argument("--tc-refine", type=int, default=400)
-    ap.add_argument("--form", choices=["auto", "tc", "ivf", "ivf_tc"], default="auto")
-    ap.add_argument("--forms", default="plain,tc,ivf,ivf_tc",
+    ap.add_argument("--form", choices=["auto", "tc", "ivf", "ivf_tc", "ivf_tc_sq8"], default="auto")
+    ap.add_argument("--forms", default="plain,tc,ivf,ivf_tc,ivf_tc_sq8",
                     help="forms to measure (the default measures all; one form alone is for profiling it)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="per offered rate; 0 skips serving")
     ap.add_argument("--no-fp8", dest="fp8", action="store_false", help="skip the scaled-FP8 configuration")

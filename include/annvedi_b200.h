@@ -41,6 +41,8 @@ extern "C" {
 #define ANN_MODE_EXACT 0     /* the true top-k by (distance, id) */
 #define ANN_MODE_REFERENCE 1 /* the reference's ranking, incl. its 64-entry early-abandon heap */
 #define ANN_MODE_TC 2        /* IVF: candidates ranked by BF16 tensor-core keys, then the exact FP32 re-rank */
+#define ANN_MODE_TC_SQ8 3    /* IVF: candidates ranked by tensor-core keys over the SQ8 codes themselves (int8
+                                query weights x uint8 codes, int32 accumulation), then the exact FP32 re-rank */
 
 /* where caller pointers live */
 #define ANN_MEM_HOST 0

@@ -213,14 +213,16 @@ def test_reference_ivf_unit_test_shape(cuda):
     assert len(a.query(data[0], 5)) == 5
 
 
+@pytest.mark.parametrize("mode", ["tc", "tc_sq8"])
 @pytest.mark.parametrize("nq", [1, 7, 64, 300])
-def test_tc_mode_ranks_the_same_streams(cuda, nq):
-    """The tensor-core form ranks each query's candidate stream (the same probed lists) by BF16 keys
-    before the exact FP32 re-rank: distances are exact for the ids returned, the result agrees with
-    the exact-selection pipeline, and the distance counter counts the same candidates."""
+def test_tc_mode_ranks_the_same_streams(cuda, nq, mode):
+    """The tensor-core forms rank each query's candidate stream (the same probed lists) by tensor-core keys
+    -- BF16 rows ("tc"), or the SQ8 codes themselves against int8 query weights ("tc_sq8") -- before the
+    exact FP32 re-rank: distances are exact for the ids returned, the result agrees with the
+    exact-selection pipeline, and the distance counter counts the same candidates."""
     w = synth.zipf_mixture(40000, 128, nq, c=96, lo=20, hi=4000, seed=nq)
     st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
-    ix = _ivf(mode="tc")
+    ix = _ivf(mode=mode)
     ix.import_state(st)
     k, npc, R = 100, 12, 300
     ids, d = ix.search(w.queries, k, 0, npc, R)
@@ -236,8 +238,9 @@ def test_tc_mode_ranks_the_same_streams(cuda, nq):
     assert ix.total_distances_count() == ex.total_distances_count()
 
 
-@pytest.mark.parametrize("nq,npc,R", [(1200, 12, 300), (600, 40, 100), (256, 3, 500)])
-def test_tc_sampled_bars_select_what_the_key_stream_selects(cuda, nq, npc, R):
+@pytest.mark.parametrize("nq,npc,R,mode", [(1200, 12, 300, "tc"), (600, 40, 100, "tc"), (256, 3, 500, "tc"),
+                                           (1200, 12, 300, "tc_sq8"), (300, 20, 200, "tc_sq8")])
+def test_tc_sampled_bars_select_what_the_key_stream_selects(cuda, nq, npc, R, mode):
     """Batches of 256+ queries on the tensor cores keep only keys under sampled per-query bars (a pass over
     the heads of the probed lists, re-runs under a safe bar where a query falls short); smaller batches
     select from the whole key stream. Both take each query's exact best R BF16 keys, so the same queries
@@ -245,7 +248,7 @@ def test_tc_sampled_bars_select_what_the_key_stream_selects(cuda, nq, npc, R):
     from tests.helpers import assert_ids_equal_up_to_ties
     w = synth.zipf_mixture(80000, 128, nq, c=128, lo=20, hi=6000, seed=nq + npc)
     st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
-    ix = _ivf(mode="tc")
+    ix = _ivf(mode=mode)
     ix.import_state(st)
     ids, d = ix.search(w.queries, 100, 0, npc, R)
     parts = [ix.search(w.queries[s:s + 200], 100, 0, npc, R) for s in range(0, nq, 200)]
@@ -258,7 +261,8 @@ def test_tc_sampled_bars_select_what_the_key_stream_selects(cuda, nq, npc, R):
     np.testing.assert_allclose(d, fp64_dists(w.base, w.queries, ids), rtol=1e-5, atol=1e-6)
 
 
-def test_tc_sampled_bars_rerun_path(cuda):
+@pytest.mark.parametrize("mode", ["tc", "tc_sq8"])
+def test_tc_sampled_bars_rerun_path(cuda, mode):
     """Lists of two rows: a query's sample is half its candidates, so about 2.3 R/3 keys pass the fast bar
     and most queries are redone under their safe bars; the result still equals the key-stream path's."""
     from tests.helpers import assert_ids_equal_up_to_ties
@@ -268,7 +272,7 @@ def test_tc_sampled_bars_rerun_path(cuda):
     q = base[rng.integers(0, 8192, 300)] + 0.05 * rng.standard_normal((300, 64)).astype(np.float32)
     q = np.ascontiguousarray(q / np.linalg.norm(q, axis=1, keepdims=True), np.float32)
     st = ivf_state.build_state(base, np.ascontiguousarray(base[::2]), np.arange(8192) // 2, 1, 0)
-    ix = _ivf(mode="tc")
+    ix = _ivf(mode=mode)
     ix.import_state(st)
     ids, d = ix.search(q, 100, 0, 400, 300)
     parts = [ix.search(q[s:s + 150], 100, 0, 400, 300) for s in range(0, 300, 150)]
@@ -278,13 +282,14 @@ def test_tc_sampled_bars_rerun_path(cuda):
     np.testing.assert_allclose(d, fp64_dists(base, q, ids), rtol=1e-5, atol=1e-6)
 
 
-def test_tc_mode_over_all_lists_is_exact(cuda):
+@pytest.mark.parametrize("mode", ["tc", "tc_sq8"])
+def test_tc_mode_over_all_lists_is_exact(cuda, mode):
     """Probing every list makes each candidate stream the whole base: the result is the exact top-k."""
     import torch
     from tests.helpers import check_exact_topk
     w = synth.zipf_mixture(60000, 96, 80, c=64, lo=20, hi=6000, seed=9)
     st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
-    ix = _ivf(mode="tc")
+    ix = _ivf(mode=mode)
     ix.import_state(st)
     ids, d = ix.search(torch.from_numpy(w.queries).cuda(), 50, 0, 64, 400)
     torch.cuda.synchronize()
