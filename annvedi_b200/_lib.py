@@ -33,6 +33,7 @@ METRICS = {"l2": METRIC_L2, "sqeuclidean": METRIC_L2, "euclidean": METRIC_L2, "i
            "inner_product": METRIC_IP, "dot": METRIC_IP}
 MODE_TC = 2
 MODE_TC_SQ8 = 3
+QUERY_SHARD = 0x100
 MODES = {"exact": MODE_EXACT, "reference": MODE_REFERENCE, "tc": MODE_TC, "tc_sq8": MODE_TC_SQ8}
 
 

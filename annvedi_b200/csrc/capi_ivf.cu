@@ -242,7 +242,8 @@ int ann_ivf_fit(ann_ivf* h, const float* data, int64_t n, int32_t dim, int64_t l
     // the reference sizes its ThreadPool, and with it the k-means chunks, from hardware_concurrency() (:140)
     const int fit_threads = num_threads > 0 ? num_threads : (int)std::max(1u, std::thread::hardware_concurrency());
     cudaStream_t st = as_stream(stream);
-    const int C = (int)std::min<int64_t>(n_clusters, n);  // the reference clamps too (:137)
+    // the reference clamps too (:137); given centroids are kept as they are (lists may be empty)
+    const int C = centroids ? n_clusters : (int)std::min<int64_t>(n_clusters, n);
     const int dpad = (int)ceil_div(dim, 32) * 32;
     const int dpad8 = (int)ceil_div(dim, 128) * 128;  // 16 threads x (multiple of 8) code bytes per row
     ANN_CUDA_TRY(cudaDeviceSynchronize());
@@ -644,6 +645,7 @@ struct IvfQueryCfg {
     int64_t max_c, ub, rps_c;
     bool ref, coarse_flat, batched, tc, lsh;
     bool i8;          // the tensor-core form over the SQ8 codes (int8 x uint8 MMA) instead of BF16 rows
+    bool shard;       // ANN_QUERY_SHARD: streams short of k are not widened to every row
     bool fallback;    // a query's stream can fall short of k points and become every row
     bool lsh_keys;    // exact LSH batch: SQ8 keys of the whole streams, then selection
     int64_t ub_cand;  // longest explicit candidate stream (LSH buckets; a fallback to every row needs none)
@@ -1021,6 +1023,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     a.k = c.k;
     a.R = c.R;
     a.max_cands = c.max_c;
+    a.no_fallback = c.shard ? 1 : 0;
     a.nsplit = c.nsplit;
     a.num_threads = c.num_threads;
     a.ndist = h->d_ndist;
@@ -1273,6 +1276,9 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     }
     ANN_CHECK_ARG(nq >= 0 && k >= 1, "ann_ivf_query: nq=%d, k=%d", nq, k);
     ANN_CHECK_ARG(ldq >= h->dim, "ann_ivf_query: query stride < dim");
+    const bool shard = (mode & ANN_QUERY_SHARD) != 0;
+    mode &= ~ANN_QUERY_SHARD;
+    ANN_CHECK_ARG(!shard || mode != ANN_MODE_REFERENCE, "ann_ivf_query: a shard of the lists has no reference semantics");
     ANN_CHECK_ARG(mode == ANN_MODE_EXACT || mode == ANN_MODE_REFERENCE || mode == ANN_MODE_TC || mode == ANN_MODE_TC_SQ8,
                   "ann_ivf_query: unknown mode %d", mode);
     ANN_CHECK_ARG(nq == 0 || (queries && out_ids), "ann_ivf_query: null pointer");
@@ -1288,6 +1294,7 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     c.ref = mode == ANN_MODE_REFERENCE;
     c.tc = mode == ANN_MODE_TC || mode == ANN_MODE_TC_SQ8;
     c.i8 = mode == ANN_MODE_TC_SQ8;
+    c.shard = shard;
     c.k = k;
     c.npc = std::max(1, std::min(n_probe_clusters, h->C));  // active_clusters (:332)
     // R = max(k, refine_r > 0 ? refine_r : 4k) (:472-474); cap max(2000, 4 * target) (:357-358)
@@ -1314,7 +1321,11 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
     c.n_probes = c.lsh ? n_probes : 0;
     // an LSH stream can fall short of k however large its lists; reference-mode scratch is sized for the
     // capped streams and a query that scans every row is redone on its own (ivf_query_device)
-    c.fallback = c.lsh || smallest < k;
+    c.fallback = !c.shard && (c.lsh || smallest < k);
+    if (c.shard && c.lsh) {
+        set_error("ann_ivf_query: a shard of the lists is searched without LSH bucket tables");
+        return ANN_ERR_UNSUPPORTED;
+    }
     c.ub_cand = std::max<int64_t>(ub, 1);
     c.ub = c.ub_cand;
     if (c.lsh && c.tc) {

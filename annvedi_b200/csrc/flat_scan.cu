@@ -596,12 +596,12 @@ __global__ void __launch_bounds__(128) merge_parts_kernel(const float* __restric
         const int64_t e = e0 + lane;
         const bool ok = e < total && iq[e] >= 0;
         const float kv = ok ? (ip ? -dq[e] : dq[e]) : kInf;
-        top.offer(kv, ok ? (int)e : kNoId, ok);
+        top.offer(kv, ok ? (int)iq[e] : kNoId, ok);  // ties by the lower id, whatever part holds it
     }
     top.compact();
     for (int e = lane; e < k; e += 32) {
         const bool ok = e < top.count;
-        out_ids[(int64_t)q * k + e] = ok ? iq[slot[e]] : -1;
+        out_ids[(int64_t)q * k + e] = ok ? slot[e] : -1;
         if (out_d) out_d[(int64_t)q * k + e] = ok ? (ip ? -key[e] : key[e]) : (ip ? -kInf : kInf);
     }
 }

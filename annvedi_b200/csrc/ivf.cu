@@ -53,7 +53,7 @@ __global__ void ivf_plan_kernel(IvfQueryArgs a) {
         cands += e - s;
     }
     pref[j] = cands;
-    if (cands < a.k) {
+    if (cands < a.k && !a.no_fallback) {
         p.n_seg[q] = -1;
         cands = a.ix.n;
     } else {

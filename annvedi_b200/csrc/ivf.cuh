@@ -61,6 +61,7 @@ struct IvfQueryArgs {
     int k;
     int R;                     // candidates kept for the FP32 re-rank
     int64_t max_cands;         // cap on the candidate stream (INT64_MAX = none)
+    int no_fallback;           // a shard of the lists: a stream short of k stays as it is (no every-row scan)
     int nsplit;                // CTAs per query in the exact SQ8 scan
     int num_threads;           // reference mode: the reference ThreadPool size
     int ncp;                   // reference mode: SQ8 checkpoints

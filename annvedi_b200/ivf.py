@@ -207,10 +207,11 @@ class IVFIndex:
 
     def search(self, queries, k: int, n_probes: int = 0, n_probe_clusters: int = 8, refine_r: int = -1,
                max_candidates: int | None = None, mode: str | None = None, workspace=None, out_ids=None,
-               out_dists=None, stream=None, with_dists: bool = True):
+               out_dists=None, stream=None, with_dists: bool = True, shard: bool = False):
         """Top-k per query row: (ids int64 [nq, k], squared distances float32 [nq, k]).
         max_candidates: None = the mode's default (reference: the reference's cap; exact: none),
-        -1 = the reference's cap, 0 = none, > 0 = that cap."""
+        -1 = the reference's cap, 0 = none, > 0 = that cap. shard: this index holds one rank's share of the
+        lists (ShardedIVFIndex); a query short of k candidates returns what it has (-1 padded)."""
         if self._n == 0:
             raise RuntimeError("index not fitted")
         k = int(k)
@@ -220,7 +221,8 @@ class IVFIndex:
         if max_candidates is None:
             max_candidates = -1 if mode == "reference" else 0
         ws = workspace.handle if workspace is not None else None
-        args = (int(n_probes), int(n_probe_clusters), int(refine_r), int(max_candidates), _lib.MODES[mode],
+        mode_v = _lib.MODES[mode] | (_lib.QUERY_SHARD if shard else 0)
+        args = (int(n_probes), int(n_probe_clusters), int(refine_r), int(max_candidates), mode_v,
                 int(self.num_threads))
         if _lib.is_torch(queries) and queries.is_cuda:
             import torch

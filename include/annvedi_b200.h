@@ -43,6 +43,10 @@ extern "C" {
 #define ANN_MODE_TC 2        /* IVF: candidates ranked by BF16 tensor-core keys, then the exact FP32 re-rank */
 #define ANN_MODE_TC_SQ8 3    /* IVF: candidates ranked by tensor-core keys over the SQ8 codes themselves (int8
                                 query weights x uint8 codes, int32 accumulation), then the exact FP32 re-rank */
+/* IVF query flag, or'ed into the mode (no counterpart in the reference): the index holds one rank's share of
+ * the lists (list sharding), so a query whose probed lists hold fewer than k of its rows returns what they
+ * hold instead of scanning every row; the caller applies the every-row rule to the whole index. */
+#define ANN_QUERY_SHARD 0x100
 
 /* where caller pointers live */
 #define ANN_MEM_HOST 0
@@ -140,12 +144,13 @@ int ann_flat_scores_tc(ann_flat* h, const float* queries, int32_t nq, int64_t ld
 /* Reads and clears the index's device error flag (ANN_ERR_TIMEOUT if a bounded device wait gave up). */
 int ann_flat_device_status(ann_flat* h);
 
-/* Merge of per-shard results (row sharding over ranks: each rank searches its rows, adds its first
- * row to the ids, and the ranks' lists are all-gathered): dists / ids [nq, parts, k] device arrays,
- * each part as ann_flat_query returns it (sorted, ids < 0 empty; squared L2 distances, or inner-product
- * scores when metric = ANN_METRIC_IP), parts in increasing id ranges; out_ids / out_dists [nq, k]
- * (out_dists may be NULL) get the best k by (distance, id). Asynchronous on `stream`. No counterpart in
- * the reference, whose indexes live in one process (the exchange step of a sharded linear_index). */
+/* Merge of per-shard results (row or list sharding over ranks: each rank searches its share, maps its
+ * ids to global ids, and the ranks' lists are all-gathered): dists / ids [nq, parts, k] device arrays,
+ * each part as the search returns it (ids < 0 empty, global ids below 2^31; squared L2 distances, or
+ * inner-product scores when metric = ANN_METRIC_IP); out_ids / out_dists [nq, k] (out_dists may be NULL)
+ * get the best k by (distance, id), ties by the lower id whatever part holds it. Asynchronous on
+ * `stream`. No counterpart in the reference, whose indexes live in one process (the exchange step of a
+ * sharded linear_index or IVF index). */
 int ann_merge_topk(const float* dists, const int64_t* ids, int32_t nq, int32_t parts, int32_t k, int32_t metric,
                    int64_t* out_ids, float* out_dists, void* stream);
 
