@@ -77,3 +77,63 @@ def test_sharded_index_over_nccl_one_rank(cuda):
         torch.cuda.synchronize()
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("mode,parts", [("exact", 2), ("tc", 3), ("tc_sq8", 2)])
+def test_merged_list_shards_equal_the_full_ivf_index(cuda, mode, parts):
+    """List sharding: each shard holds its lists' rows (and every centroid), searches with ANN_QUERY_SHARD;
+    the merged lists equal the single IVF index when the re-rank covers every candidate."""
+    import torch
+    from annvedi_b200.ivf import IVFIndex
+    from annvedi_b200.sharded import assign_lists, merge_topk
+    from tests.helpers import assert_ids_equal_up_to_ties
+    w = synth.zipf_mixture(6000, 64, 64, c=48, lo=20, hi=250, seed=17)
+    k, npc, R = 50, 4, 1000
+    full = IVFIndex(device=0, mode="exact")
+    full.fit(w.base, 1, 0, 48, centroids=w.centres, assign=w.assign)
+    fi, fd = full.search(w.queries, k, 0, npc, R, max_candidates=0, mode=mode)
+    owner = assign_lists(np.bincount(w.assign, minlength=48), parts)
+    ds, is_ = [], []
+    for r in range(parts):
+        rows = np.nonzero(owner[w.assign] == r)[0]
+        ix = IVFIndex(device=0, mode="exact")
+        ix.fit(w.base[rows], 1, 0, 48, centroids=w.centres, assign=w.assign[rows])
+        i, d = ix.search(w.queries, k, 0, npc, R, max_candidates=0, mode=mode, shard=True)
+        i = torch.from_numpy(i)
+        g = torch.from_numpy(rows)
+        is_.append(torch.where(i >= 0, g[i.clamp(min=0)], i).cuda())
+        ds.append(torch.from_numpy(np.where(i.numpy() >= 0, d, np.inf).astype(np.float32)).cuda())
+    mi, md = merge_topk(torch.stack(ds, 1), torch.stack(is_, 1), k)
+    assert_ids_equal_up_to_ties(w.base, w.queries, mi.cpu().numpy(), fi, rtol=1e-6)
+    np.testing.assert_allclose(md.cpu().numpy(), fd, rtol=1e-6, atol=1e-7)
+
+
+def test_sharded_ivf_index_over_nccl_one_rank(cuda):
+    """ShardedIVFIndex over a one-rank NCCL group, with queries whose probed list holds fewer than k rows:
+    the every-row rule applied to the merged result gives the single index's answer."""
+    import torch
+    import torch.distributed as dist
+    from annvedi_b200.ivf import IVFIndex
+    from annvedi_b200.sharded import ShardedIVFIndex
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        w = synth.zipf_mixture(6000, 64, 40, c=48, lo=20, hi=250, seed=5)
+        ix = ShardedIVFIndex(device=0, mode="exact")
+        ix.fit(w.base, w.centres, w.assign)
+        q = torch.from_numpy(w.queries).cuda()
+        ids, d = ix.search(q, 50, n_probe_clusters=1, refine_r=1000)
+        full = IVFIndex(device=0, mode="exact")
+        full.fit(w.base, 1, 0, 48, centroids=w.centres, assign=w.assign)
+        fi, fd = full.search(w.queries, 50, 0, 1, 1000, max_candidates=0)
+        sizes = np.bincount(w.assign, minlength=48)
+        assert (sizes < 50).any()
+        np.testing.assert_array_equal(ids.cpu().numpy(), fi)
+        np.testing.assert_allclose(d.cpu().numpy(), fd, rtol=1e-6, atol=1e-7)
+        assert ix.total_distances_count() > 0
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
