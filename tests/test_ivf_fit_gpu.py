@@ -27,6 +27,24 @@ needs_ref = pytest.mark.skipif(not (refmod.ref_available("avx512") and refmod.ho
                                reason="reference AVX-512 build not available on this host")
 
 
+def assert_same_up_to_exact_ties(base, queries, got, want, err_msg=""):
+    """The same ids per query; where positions differ, the ids there are rows at exactly equal distances
+    (the reference's own arithmetic, restated bit for bit): the reference orders its candidates by
+    distance alone with std::partial_sort (lsh_index_optimized.cpp:476-479, 498-501), whose order among
+    equal distances is its sort's internal one. Returns the number of queries with such swaps."""
+    swaps = 0
+    for i in range(got.shape[0]):
+        if np.array_equal(got[i], want[i]):
+            continue
+        swaps += 1
+        assert sorted(got[i].tolist()) == sorted(want[i].tolist()), f"{err_msg}: query {i} returns other ids"
+        for p in np.nonzero(got[i] != want[i])[0]:
+            dg = refmod.l2(base[got[i][p]], queries[i]) if got[i][p] >= 0 else None
+            dw = refmod.l2(base[want[i][p]], queries[i]) if want[i][p] >= 0 else None
+            assert dg == dw, f"{err_msg}: query {i} position {p}: {got[i][p]} ({dg}) vs {want[i][p]} ({dw})"
+    return swaps
+
+
 def test_fit_reproduces_reference_kmeans_goldens(cuda, golden_dir):
     fx = np.load(os.path.join(golden_dir, "kmeans_ref.npz"))
     for name, n, dim, c, t, dup, seed, (k, npc, rr) in mk.kmeans_cases():
@@ -89,7 +107,8 @@ def test_algorithm_fit_query_equals_reference_fit_query_50k(cuda):
         n0 = algo.get_n_distances()
         want = np.stack([ref.query(q, 100, 0, npc, rr) for q in w.queries])
         got = np.stack([algo.query(q, 100, n_probe_clusters=npc, refine_r=rr) for q in w.queries])
-        np.testing.assert_array_equal(got, want, err_msg=f"npc={npc} refine_r={rr}")
+        swaps = assert_same_up_to_exact_ties(w.base, w.queries, got, want, err_msg=f"npc={npc} refine_r={rr}")
+        assert swaps <= 3, swaps  # exact FP32 ties among a query's top 100: about one query in a hundred
         assert algo.get_n_distances() - n0 == ref.total_distances_count()
 
 
@@ -130,5 +149,5 @@ def test_ivf_c3_shape_reference_mode_equals_compiled_reference(cuda):
         ix.reset_distances_count()
         want = np.stack([ref.query(q, 100, 0, npc, rr) for q in z.queries])
         got, _ = ix.search(z.queries, 100, 0, npc, rr)
-        np.testing.assert_array_equal(got, want, err_msg=f"npc={npc} refine_r={rr}")
+        assert_same_up_to_exact_ties(z.base, z.queries, got, want, err_msg=f"npc={npc} refine_r={rr}")
         assert ix.total_distances_count() == ref.total_distances_count()
