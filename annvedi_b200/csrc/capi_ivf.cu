@@ -764,11 +764,12 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
 // ceil(size / kSampleDiv) rows, an even sample since rows are in ascending original id inside a list --
 // is scored by a first grouped GEMM into each query's sample stream. Per query, the fast bar is the
 // rF-th smallest sampled key (rF = ceil(3 R / kSampleDiv): about 3 R keys of the whole stream pass it)
-// and the safe bar the R-th (at or above the stream's R-th key). The grouped GEMM over all rows then
-// keeps only keys at or below the fast bar, recorded per query; a query left with fewer than
-// min(R, its candidates) survivors is redone under its safe bar. Each query ends with the exact best R
-// keys of its stream, as the key-stream path below selects them, without writing the stream.
-// Returns with *done = false (and no output) when a warp's survivor region overflowed.
+// and the safe bar the R-th (at or above the stream's R-th key), both exact (warp_bars_kernel). The
+// grouped GEMM over all rows then appends only the keys at or below the fast bar to the query's own
+// buffer (kRowCapFactor R slots); a query left with fewer than min(R, its candidates) survivors is redone
+// under its safe bar. Each query ends with the exact best R keys of its stream (warp_select_kernel: the
+// keys below the R-th, then equal ones by increasing row), as the key-stream path selects them, without
+// writing the stream. Returns with *done = false (and no output) when a query's buffer overflowed.
 struct TcOperands {
     const void* qrows;     // the queries' operand rows
     int row_bytes;
@@ -787,6 +788,7 @@ static TcOperands tc_operands(const ann_ivf* h, const IvfQueryCfg& c, const __nv
 
 constexpr int kTcSampledMinQueries = 256;
 constexpr int kSampleDiv = 8;
+constexpr int kRowCapFactor = 16;
 
 static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, const IvfQueryArgs& a,
                           const IvfBatchArgs& b, const TcOperands& op, unsigned char* Apk, int64_t* titem,
@@ -800,10 +802,7 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     const int64_t s_bound = (int64_t)nq * npc * head_max;  // sample keys at most
     const int64_t scap = tc_items_bound(max_pairs, C, head_max);
     const int rF = (int)std::min<int64_t>(R, std::max<int64_t>(1, ceil_div(3 * (int64_t)R, kSampleDiv)));
-    const int nwarps = tc_grouped_filter_warps();
-    const int64_t expect = 3 * (int64_t)R * nq;
-    const int wcap = (int)std::min<int64_t>(4 * ceil_div(expect, nwarps) + 1024, INT32_MAX / nwarps);
-    const size_t ent = (size_t)nwarps * wcap;
+    const int cap = kRowCapFactor * R;
     size_t scan_tmp = 0;
     ANN_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, (int64_t*)nullptr, (int64_t*)nullptr, nq + 1, st));
     Sizer sz;
@@ -818,15 +817,9 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     sz.take<int32_t>((size_t)max_pairs);         // row -> query
     sz.take<float>((size_t)s_bound);             // sample keys
     for (int i = 0; i < 3; ++i) sz.take<float>((size_t)nq);  // fast, safe, re-run bars
-    sz.take<float>(ent);                         // survivors: key, column, query
-    sz.take<int>(ent);
-    sz.take<int>(ent);
-    sz.take<float>(ent);                         // grouped: key, id
-    sz.take<int>(ent);
-    sz.take<int>((size_t)nwarps);
-    for (int i = 0; i < 5; ++i) sz.take<int>((size_t)nq);    // counts, cursors, re-run list, marks, lens2
-    sz.take<int64_t>((size_t)nq);                // offs
-    sz.take<int64_t>((size_t)nq);                // offs2
+    sz.take<float>((size_t)nq * cap);            // survivors per query: key, list row
+    sz.take<int>((size_t)nq * cap);
+    for (int i = 0; i < 3; ++i) sz.take<int>((size_t)nq);    // counts, re-run list, marks
     sz.take<int>(4);                             // flags
     int rc = ws_reserve_big(ws, sz.bytes());
     if (rc) return rc;
@@ -844,19 +837,11 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     float* tauF = cv.take<float>((size_t)nq);
     float* tauS = cv.take<float>((size_t)nq);
     float* tauR = cv.take<float>((size_t)nq);
-    float* fkey = cv.take<float>(ent);
-    int* fcol = cv.take<int>(ent);
-    int* frow = cv.take<int>(ent);
-    float* gkey = cv.take<float>(ent);
-    int* gid = cv.take<int>(ent);
-    int* wcnt = cv.take<int>((size_t)nwarps);
-    int* rowcnt = cv.take<int>((size_t)nq);
-    int* cursor = cv.take<int>((size_t)nq);
+    float* skey = cv.take<float>((size_t)nq * cap);
+    int* srow = cv.take<int>((size_t)nq * cap);
+    int* scount = cv.take<int>((size_t)nq);
     int* list = cv.take<int>((size_t)nq);
     int* mark = cv.take<int>((size_t)nq);
-    int* lens2 = cv.take<int>((size_t)nq);
-    int64_t* offs = cv.take<int64_t>((size_t)nq);
-    int64_t* offs2 = cv.take<int64_t>((size_t)nq);
     int* flags = cv.take<int>(4);
 
     // sample streams: heads of the probed lists, each query's stream offsets
@@ -890,18 +875,8 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     gs.g_lists = C;
     gs.g_item_list = sitem_list;
     if ((rc = launch_tc_gemm(Apk, op.B, gs, st))) return rc;
-    RadixSelectArgs bar{};
-    bar.keys = SK;
-    bar.ld = npc * head_max;
-    bar.offs = soff;
-    bar.lens = slen;
-    bar.R = rF;
-    bar.out_kth = tauF;
-    bar.R2 = R;
-    bar.out_kth2 = tauS;
-    bar.kth_upper = 1;
-    if ((rc = launch_radix_select(bar, nq, st))) return rc;
-    // 2. filter pass over every row of the probed lists, survivors grouped per query
+    if ((rc = launch_warp_bars(SK, soff, slen, nq, rF, R, tauF, tauS, st))) return rc;
+    // 2. filter pass over every row of the probed lists into the queries' buffers
     if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, C, titem, st))) return rc;
     if ((rc = launch_tc_item_lists(titem, C, titem_list, items_cap, st))) return rc;
     auto filter = [&](const float* tau) -> int {
@@ -917,49 +892,32 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
         g.g_item_list = titem_list;
         g.g_row_query = rowq;
         g.tau = tau;
-        g.fkey = fkey;
-        g.fcol = fcol;
-        g.frow = frow;
-        g.wcount = wcnt;
-        g.wcap = wcap;
-        int r = launch_tc_gemm(Apk, op.B, g, st);
-        if (r) return r;
-        TcGroupArgs ga{fkey, fcol, frow, wcnt, nwarps, wcap, nq, h->n, 1, rowcnt, offs, cursor, gkey, gid, flags + 1};
-        return launch_tc_group(ga, st);
+        g.fkey = skey;
+        g.fcol = srow;
+        g.row_cap = cap;
+        g.rcount = scount;
+        return launch_tc_gemm(Apk, op.B, g, st);
     };
+    ANN_CUDA_TRY(cudaMemsetAsync(scount, 0, sizeof(int) * (size_t)nq, st));
     if ((rc = filter(tauF))) return rc;
     h->prof.mark(prec, st);
     ANN_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int), st));
-    if ((rc = launch_tc_bar_check(rowcnt, nq, R, list, flags, st, a.plan.n_cands, mark))) return rc;
-    int hf[2] = {0, 0};  // re-runs, largest warp count
-    ANN_CUDA_TRY(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
+    if ((rc = launch_tc_bar_check(scount, nq, R, list, flags, st, a.plan.n_cands, mark))) return rc;
+    int nre = 0;
+    ANN_CUDA_TRY(cudaMemcpyAsync(&nre, flags, sizeof(int), cudaMemcpyDeviceToHost, st));
     ANN_CUDA_TRY(cudaStreamSynchronize(st));
-    if (hf[1] > wcap) return ANN_OK;  // a region overflowed: the caller takes the key-stream path
-    RadixSelectArgs sv{};
-    sv.keys = gkey;
-    sv.ld = (int64_t)ent;
-    sv.offs = offs;
-    sv.lens32 = rowcnt;
-    sv.ids = gid;
-    sv.R = R;
-    sv.out_key = keyR;
-    sv.out_id = idR;
-    if ((rc = launch_radix_select(sv, nq, st))) return rc;
-    if (hf[0] > 0) {  // queries short of survivors: again under their safe bars, the others under -inf
-        if ((rc = launch_tc_rerun_bars(mark, tauS, nq, tauR, st))) return rc;
+    if (nre > 0) {  // queries short of survivors: again under their safe bars (their buffers refilled), the rest under -inf
+        if ((rc = launch_tc_rerun_bars(mark, tauS, nq, tauR, st, scount))) return rc;
         if ((rc = filter(tauR))) return rc;
-        int hmax = 0;
-        ANN_CUDA_TRY(cudaMemcpyAsync(&hmax, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-        ANN_CUDA_TRY(cudaStreamSynchronize(st));
-        if (hmax > wcap) return ANN_OK;
-        if ((rc = launch_tc_compact_rows(list, flags, hf[0], offs, rowcnt, offs2, lens2, st))) return rc;
-        RadixSelectArgs sv2 = sv;
-        sv2.offs = offs2;
-        sv2.lens32 = lens2;
-        sv2.out_rows = list;
-        if ((rc = launch_radix_select(sv2, hf[0], st))) return rc;
         if (prec >= 0) h->prof.tc_launches += 1;
     }
+    // a query with more survivors than its buffer holds: the caller takes the key-stream path
+    if ((rc = launch_max_int(scount, nq, flags + 1, st))) return rc;
+    int most = 0;
+    ANN_CUDA_TRY(cudaMemcpyAsync(&most, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ANN_CUDA_TRY(cudaStreamSynchronize(st));
+    if (most > cap) return ANN_OK;
+    if ((rc = launch_warp_select(skey, srow, scount, cap, nq, R, keyR, idR, st))) return rc;
     if (prec >= 0) h->prof.tc_launches += 2;
     *done = true;
     return ANN_OK;

@@ -502,7 +502,30 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                             }
                         }
                         uint32_t msk = (mq[0] | (mq[1] << 8)) | ((mq[2] << 16) | (mq[3] << 24));
-                        if (__any_sync(0xffffffffu, msk != 0)) {
+                        if (a.row_cap > 0) {  // per-row buffers: this lane's survivors, one atomic
+                            if (msk) {
+                                int slot = atomicAdd(&a.rcount[rq], __popc(msk));
+                                const int64_t rbase = (int64_t)rq * a.row_cap;
+                                while (msk) {
+                                    const int u = __ffs(msk) - 1;
+                                    msk &= msk - 1;
+                                    if (slot < a.row_cap) {
+                                        float s16[16], s8[8], s4[4], s2[2];
+#pragma unroll
+                                        for (int z = 0; z < 16; ++z) s16[z] = (u & 16) ? v[z + 16] : v[z];
+#pragma unroll
+                                        for (int z = 0; z < 8; ++z) s8[z] = (u & 8) ? s16[z + 8] : s16[z];
+#pragma unroll
+                                        for (int z = 0; z < 4; ++z) s4[z] = (u & 4) ? s8[z + 4] : s8[z];
+#pragma unroll
+                                        for (int z = 0; z < 2; ++z) s2[z] = (u & 2) ? s4[z + 2] : s4[z];
+                                        a.fkey[rbase + slot] = (u & 1) ? s2[1] : s2[0];
+                                        a.fcol[rbase + slot] = (int)(cbase + lb + u);
+                                    }
+                                    ++slot;
+                                }
+                            }
+                        } else if (__any_sync(0xffffffffu, msk != 0)) {
                             const int cnt = __popc(msk);
                             int incl = cnt;
 #pragma unroll
@@ -615,7 +638,8 @@ int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream
                   "tensor-core scan: E4M3 / I8 operands need their scale factors (E4M3: no grouping)");
     ANN_CHECK_ARG((reinterpret_cast<uintptr_t>(A) & 15) == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0,
                   "tensor-core scan: operands must be 16-byte aligned");
-    ANN_CHECK_ARG(a.out != nullptr || (a.tau && a.fkey && a.fcol && a.frow && a.wcount && a.wcap > 0),
+    ANN_CHECK_ARG(a.out != nullptr || (a.tau && a.fkey && a.fcol &&
+                                       ((a.frow && a.wcount && a.wcap > 0) || (a.row_cap > 0 && a.rcount))),
                   "tensor-core scan: neither an output matrix nor a filter");
     ANN_CHECK_ARG(a.g_item_off == nullptr ||
                       (a.g_a_off && a.g_b_off && a.g_total && a.g_lists > 0 &&

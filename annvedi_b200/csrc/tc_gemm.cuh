@@ -32,6 +32,12 @@ struct TcGemmArgs {
     int* frow = nullptr;
     int* wcount = nullptr;
     int wcap = 0;
+    // Filter mode, per-row buffers (row_cap > 0; the grouped form, rows = queries): a survivor of row r goes
+    // to fkey / fcol [r * row_cap + slot] at slot = atomicAdd(&rcount[r], n) -- one atomic per lane per 32
+    // columns, n its survivors there -- and nothing is written at slots past row_cap (rcount[r] may exceed
+    // it: the caller checks).
+    int row_cap = 0;
+    int* rcount = nullptr;
     // Grouped mode (g_item_off != null; out receives the keys): tile t is work item t of a list-major
     // grouping (an IVF batch). List l owns A rows [g_a_off[l], g_a_off[l+1]) (its (query, list) pairs)
     // and B rows [g_b_off[l], g_b_off[l+1]) (its rows); its items are ceil(pairs/128) x ceil(rows/256)

@@ -226,6 +226,136 @@ __global__ void tc_sq8_norms_kernel(const uint8_t* __restrict__ codes, int64_t n
     if (lane == 0) fac[i] = make_float2(1.f, s);
 }
 
+// ---- warp-level exact selection (one warp per query) -----------------------------------------------
+__device__ __forceinline__ uint32_t ord_key(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float from_ord(uint32_t o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+
+// The r-th smallest (1 <= r <= n) of keys[0..n) as an ordered key, by one warp: four passes of 8-bit digits
+// from the top, each counting the keys that match the digits found so far into the warp's 256-bin
+// histogram `hist` (shared memory). Exact; every lane returns it.
+__device__ uint32_t warp_kth_ord(const float* __restrict__ keys, int64_t n, int64_t r, int* hist) {
+    const int lane = threadIdx.x & 31;
+    uint32_t prefix = 0, pmask = 0;
+    int64_t rem = r;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int i = lane; i < 256; i += 32) hist[i] = 0;
+        __syncwarp();
+        for (int64_t p = lane; p < n; p += 32) {
+            const uint32_t o = ord_key(keys[p]);
+            if ((o & pmask) == prefix) atomicAdd(&hist[(o >> shift) & 255u], 1);
+        }
+        __syncwarp();
+        int c[8];
+        int sum = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            c[j] = hist[lane * 8 + j];
+            sum += c[j];
+        }
+        int incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int excl = incl - sum;
+        const unsigned hit = __ballot_sync(0xffffffffu, excl < rem && rem <= incl);
+        const int src = __ffs(hit) - 1;
+        int d = 0, before = 0;
+        if (lane == src) {
+            int acc = excl;
+            for (int j = 0; j < 8; ++j) {
+                if (acc + c[j] >= rem) {
+                    d = lane * 8 + j;
+                    before = acc;
+                    break;
+                }
+                acc += c[j];
+            }
+        }
+        d = __shfl_sync(0xffffffffu, d, src);
+        before = __shfl_sync(0xffffffffu, before, src);
+        rem -= before;
+        prefix |= (uint32_t)d << shift;
+        pmask |= 255u << shift;
+        __syncwarp();
+    }
+    return prefix;
+}
+
+// One warp per query: bar1 / bar2 = the r1-th / r2-th smallest of the query's keys[offs[q] .. + lens[q])
+// (+inf where the stream is shorter).
+__global__ void __launch_bounds__(256) warp_bars_kernel(const float* __restrict__ keys, const int64_t* __restrict__ offs,
+                                                        const int64_t* __restrict__ lens, int nq, int r1, int r2,
+                                                        float* __restrict__ bar1, float* __restrict__ bar2) {
+    __shared__ int sHist[8][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q = blockIdx.x * 8 + warp;
+    if (q >= nq) return;  // the whole warp
+    const float* kq = keys + offs[q];
+    const int64_t n = lens[q];
+    const float b1 = r1 <= n ? from_ord(warp_kth_ord(kq, n, r1, sHist[warp])) : kInf;
+    const float b2 = r2 <= n ? from_ord(warp_kth_ord(kq, n, r2, sHist[warp])) : kInf;
+    if (lane == 0) {
+        bar1[q] = b1;
+        bar2[q] = b2;
+    }
+}
+
+// One warp per query: the R smallest of the query's (key, id) buffer [q * cap, + min(count[q], cap)) as a set:
+// every key below the R-th smallest, then the keys equal to it with the lowest ids; padded with
+// (+inf, kNoId) when fewer. Written unordered to out_key / out_id [q * R ..].
+__global__ void __launch_bounds__(256) warp_select_kernel(const float* __restrict__ keys, const int* __restrict__ ids,
+                                                          const int* __restrict__ count, int cap, int nq, int R,
+                                                          float* __restrict__ out_key, int* __restrict__ out_id) {
+    __shared__ int sHist[8][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q = blockIdx.x * 8 + warp;
+    if (q >= nq) return;
+    const int64_t n = min(count[q], cap);
+    const float* kq = keys + (int64_t)q * cap;
+    const int* iq = ids + (int64_t)q * cap;
+    float* ok = out_key + (int64_t)q * R;
+    int* oi = out_id + (int64_t)q * R;
+    const uint32_t T = n > R ? warp_kth_ord(kq, n, R, sHist[warp]) : 0xffffffffu;
+    int w = 0;  // written so far (uniform)
+    for (int64_t p0 = 0; p0 < n; p0 += 32) {  // every key below T (all of them when n <= R)
+        const int64_t p = p0 + lane;
+        const bool take = p < n && (n <= R || ord_key(kq[p]) < T);
+        const unsigned b = __ballot_sync(0xffffffffu, take);
+        if (take) {
+            const int at = w + __popc(b & ((1u << lane) - 1u));
+            ok[at] = kq[p];
+            oi[at] = iq[p];
+        }
+        w += __popc(b);
+    }
+    int last = -1;  // then keys equal to T by increasing id
+    while (n > R && w < R) {
+        int best = INT_MAX;
+        for (int64_t p = lane; p < n; p += 32)
+            if (ord_key(kq[p]) == T && iq[p] > last) best = min(best, iq[p]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+        if (best == INT_MAX) break;
+        if (lane == 0) {
+            ok[w] = from_ord(T);
+            oi[w] = best;
+        }
+        last = best;
+        ++w;
+    }
+    for (int e = w + lane; e < R; e += 32) {
+        ok[e] = kInf;
+        oi[e] = kNoId;
+    }
+}
+
 // lcap[l] = ceil(size_l / div): the sampled head of list l
 __global__ void tc_ivf_list_caps_kernel(const int64_t* __restrict__ list_off, int C, int div, int64_t* __restrict__ lcap) {
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
@@ -234,9 +364,11 @@ __global__ void tc_ivf_list_caps_kernel(const int64_t* __restrict__ list_off, in
 
 // tauR[q] = tauS[q] for the queries marked for a re-run, else -inf (no key passes)
 __global__ void tc_rerun_bars_kernel(const int* __restrict__ mark, const float* __restrict__ tauS, int nq,
-                                     float* __restrict__ tauR) {
+                                     float* __restrict__ tauR, int* __restrict__ rcount) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q < nq) tauR[q] = mark[q] ? tauS[q] : -kInf;
+    if (q >= nq) return;
+    tauR[q] = mark[q] ? tauS[q] : -kInf;
+    if (rcount && mark[q]) rcount[q] = 0;  // the re-run refills the query's buffer from its start
 }
 
 // offs2[j] = offs[list[j]], lens2[j] = rowcnt[list[j]] for the j < count listed rows
@@ -470,9 +602,45 @@ int launch_tc_sq8_norms(const uint8_t* codes, int64_t n, int dim, int ldc, const
     return ANN_OK;
 }
 
-int launch_tc_rerun_bars(const int* mark, const float* tauS, int nq, float* tauR, cudaStream_t st) {
+namespace {
+__global__ void max_int_kernel(const int* __restrict__ v, int n, int* __restrict__ out) {
+    int m = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = max(m, v[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, m);
+}
+}  // namespace
+
+int launch_max_int(const int* v, int n, int* out, cudaStream_t st) {
+    ANN_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(int), st));
+    if (n == 0) return ANN_OK;
+    max_int_kernel<<<(unsigned)std::min<int64_t>(ceil_div(n, 256), 4 * kNumSMs), 256, 0, st>>>(v, n, out);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int launch_warp_bars(const float* keys, const int64_t* offs, const int64_t* lens, int nq, int r1, int r2, float* bar1,
+                     float* bar2, cudaStream_t st) {
     if (nq == 0) return ANN_OK;
-    tc_rerun_bars_kernel<<<(unsigned)ceil_div(nq, 256), 256, 0, st>>>(mark, tauS, nq, tauR);
+    ANN_CHECK_ARG(r1 >= 1 && r2 >= 1, "bars: ranks %d, %d", r1, r2);
+    warp_bars_kernel<<<(unsigned)ceil_div(nq, 8), 256, 0, st>>>(keys, offs, lens, nq, r1, r2, bar1, bar2);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int launch_warp_select(const float* keys, const int* ids, const int* count, int cap, int nq, int R, float* out_key,
+                       int* out_id, cudaStream_t st) {
+    if (nq == 0) return ANN_OK;
+    ANN_CHECK_ARG(R >= 1 && cap >= 1, "warp select: R=%d, cap=%d", R, cap);
+    warp_select_kernel<<<(unsigned)ceil_div(nq, 8), 256, 0, st>>>(keys, ids, count, cap, nq, R, out_key, out_id);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+int launch_tc_rerun_bars(const int* mark, const float* tauS, int nq, float* tauR, cudaStream_t st, int* rcount) {
+    if (nq == 0) return ANN_OK;
+    tc_rerun_bars_kernel<<<(unsigned)ceil_div(nq, 256), 256, 0, st>>>(mark, tauS, nq, tauR, rcount);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

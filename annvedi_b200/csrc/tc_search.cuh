@@ -87,8 +87,19 @@ int launch_tc_sq8_norms(const uint8_t* codes, int64_t n, int dim, int ldc, const
 // probed lists: segment starts sseg [nq, npc] and length slen [nq].
 int launch_tc_ivf_sample_plan(const IvfPlan& p, const int64_t* list_off, int C, int div, int64_t* lcap, int64_t* sseg,
                               int64_t* slen, cudaStream_t st);
-// tauR[q] = mark[q] ? tauS[q] : -inf.
-int launch_tc_rerun_bars(const int* mark, const float* tauS, int nq, float* tauR, cudaStream_t st);
+// tauR[q] = mark[q] ? tauS[q] : -inf; with rcount, the marked queries' counts are reset to 0.
+int launch_tc_rerun_bars(const int* mark, const float* tauS, int nq, float* tauR, cudaStream_t st,
+                         int* rcount = nullptr);
+// *out = max(0, v[0..n)) (out zeroed first).
+int launch_max_int(const int* v, int n, int* out, cudaStream_t st);
+// One warp per query: bar1 / bar2 = the r1-th / r2-th smallest key of keys[offs[q] .. + lens[q]) (exact; +inf
+// where the stream is shorter).
+int launch_warp_bars(const float* keys, const int64_t* offs, const int64_t* lens, int nq, int r1, int r2, float* bar1,
+                     float* bar2, cudaStream_t st);
+// One warp per query: the R smallest (key, id) of the buffer [q * cap, + min(count[q], cap)) as a set (the keys
+// below the R-th smallest, then those equal to it by increasing id), padded with (+inf, kNoId), unordered.
+int launch_warp_select(const float* keys, const int* ids, const int* count, int cap, int nq, int R, float* out_key,
+                       int* out_id, cudaStream_t st);
 // offs2[j] = offs[list[j]], lens2[j] = rowcnt[list[j]] for j < *count (<= max_count).
 int launch_tc_compact_rows(const int* list, const int* count, int max_count, const int64_t* offs, const int* rowcnt,
                            int64_t* offs2, int* lens2, cudaStream_t st);
