@@ -448,7 +448,7 @@ def run_ours(args, rank, world, local):
     if ivf is not None:
         ivf.reset_profile_results()
         ivf.reset_distances_count()
-        ivf.set_profiling(head in ("ivf_sq8", "ivf_tc"))
+        ivf.set_profiling(head in ("ivf_sq8", "ivf_tc", "ivf_tc_sq8"))
     launches0 = _lib.kernel_launches()
     barrier(world)
     torch.cuda.synchronize()
