@@ -862,31 +862,31 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     // 1. sample pass: keys of the list heads into the sample streams; the two bars per query
     if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, C, sitem, st, lcap))) return rc;
     if ((rc = launch_tc_item_lists(sitem, C, sitem_list, scap, st))) return rc;
-    TcGemmArgs gs{(int)h->n, (int)max_pairs, op.K, nullptr, SK, 0, h->d_err};
+    TcGemmArgs gs{(int)max_pairs, (int)h->n, op.K, nullptr, SK, 0, h->d_err};
     gs.kind = op.kind;
     gs.col_fac = op.col_fac;
     gs.row_fac = op.pfac;
     gs.g_item_off = sitem;
-    gs.g_pair_off = b.lq_off;
-    gs.g_row_off = h->list_off;
-    gs.g_row_len = lcap;
+    gs.g_a_off = b.lq_off;
+    gs.g_b_off = h->list_off;
+    gs.g_b_len = lcap;
     gs.g_dbase = sdbase;
     gs.g_total = sitem + C;
     gs.g_lists = C;
     gs.g_item_list = sitem_list;
-    if ((rc = launch_tc_gemm(op.B, Apk, gs, st))) return rc;
+    if ((rc = launch_tc_gemm(Apk, op.B, gs, st))) return rc;
     if ((rc = launch_warp_bars(SK, soff, slen, nq, rF, R, tauF, tauS, st))) return rc;
     // 2. filter pass over every row of the probed lists into the queries' buffers
     if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, C, titem, st))) return rc;
     if ((rc = launch_tc_item_lists(titem, C, titem_list, items_cap, st))) return rc;
     auto filter = [&](const float* tau) -> int {
-        TcGemmArgs g{(int)h->n, (int)max_pairs, op.K, nullptr, nullptr, 0, h->d_err};
+        TcGemmArgs g{(int)max_pairs, (int)h->n, op.K, nullptr, nullptr, 0, h->d_err};
         g.kind = op.kind;
         g.col_fac = op.col_fac;
         g.row_fac = op.pfac;
         g.g_item_off = titem;
-        g.g_pair_off = b.lq_off;
-        g.g_row_off = h->list_off;
+        g.g_a_off = b.lq_off;
+        g.g_b_off = h->list_off;
         g.g_total = titem + C;
         g.g_lists = C;
         g.g_item_list = titem_list;
@@ -896,7 +896,7 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
         g.fcol = srow;
         g.row_cap = cap;
         g.rcount = scount;
-        return launch_tc_gemm(op.B, Apk, g, st);
+        return launch_tc_gemm(Apk, op.B, g, st);
     };
     ANN_CUDA_TRY(cudaMemsetAsync(scount, 0, sizeof(int) * (size_t)nq, st));
     if ((rc = filter(tauF))) return rc;
@@ -1094,18 +1094,18 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                     return rc;
                 if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, h->C, titem, st))) return rc;
                 if ((rc = launch_tc_item_lists(titem, (int)h->C, titem_list, items_cap, st))) return rc;
-                TcGemmArgs g{(int)h->n, (int)max_pairs, op.K, nullptr, D, 0, h->d_err};
+                TcGemmArgs g{(int)max_pairs, (int)h->n, op.K, nullptr, D, 0, h->d_err};
                 g.kind = op.kind;
                 g.col_fac = op.col_fac;
                 g.row_fac = op.pfac;
                 g.g_item_off = titem;
-                g.g_pair_off = b.lq_off;
-                g.g_row_off = h->list_off;
+                g.g_a_off = b.lq_off;
+                g.g_b_off = h->list_off;
                 g.g_dbase = dbase;
                 g.g_total = titem + h->C;
                 g.g_lists = h->C;
                 g.g_item_list = titem_list;
-                if ((rc = launch_tc_gemm(op.B, Apk, g, st))) return rc;
+                if ((rc = launch_tc_gemm(Apk, op.B, g, st))) return rc;
                 h->prof.mark(prec, st);
                 RadixSelectArgs rs{};
                 rs.keys = D;

@@ -137,34 +137,6 @@ __device__ __forceinline__ void mma_issue(uint32_t tmem_d, uint64_t ad, uint64_t
             "l"(ad), "l"(bd), "r"(kIdescI8), "r"(accumulate)
             : "memory");
 }
-// The instruction descriptor of KIND with N = n (a multiple of 16 in [16, 256]) in place of 256.
-template <int KIND>
-__device__ __forceinline__ uint32_t idesc_n(int n) {
-    const uint32_t base = KIND == kTcBF16 ? kIdescBF16 : (KIND == kTcE4M3 ? kIdescE4M3 : kIdescI8);
-    return (base & ~(0x3Fu << 17)) | ((uint32_t)(n >> 3) << 17);
-}
-template <int KIND>
-__device__ __forceinline__ void mma_issue_d(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t idesc,
-                                            uint32_t accumulate) {
-    if (KIND == kTcBF16)
-        asm volatile(
-            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
-            "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate)
-            : "memory");
-    else if (KIND == kTcE4M3)
-        asm volatile(
-            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-            " tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
-            "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate)
-            : "memory");
-    else
-        asm volatile(
-            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-            " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
-            "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate)
-            : "memory");
-}
 // An accumulator read from TMEM as a float: FP32 bits, or (kind::i8) an int32 converted (exact below 2^24).
 template <int KIND>
 __device__ __forceinline__ float acc_value(uint32_t r) {
@@ -208,12 +180,10 @@ __device__ __forceinline__ void tmem_after_wait(uint32_t (&r)[32]) {
                  : "memory");
 }
 
-// A grouped-mode work item of list l: its rows [r0, r0 + rows) on the M side (A, at most 128) and its pairs
-// [p0, p0 + np) on the N side (B, at most 256); the MMA runs N = nt, np rounded up to 16. Items of a list:
-// ceil(pairs / 256) x ceil(rows / 128), pair tiles fastest.
+// A grouped-mode work item: A rows [a0, a0 + am), B rows [b0, b0 + bn).
 struct GroupTile {
-    int64_t r0, p0;
-    int rows, np, nt;
+    int64_t a0, b0;
+    int am, bn;
 };
 __device__ __forceinline__ GroupTile group_tile(const TcGemmArgs& a, int64_t t) {
     int lo = 0, hi = a.g_lists - 1;
@@ -228,17 +198,16 @@ __device__ __forceinline__ GroupTile group_tile(const TcGemmArgs& a, int64_t t) 
                 hi = mid - 1;
         }
     }
-    const int64_t npairs = a.g_pair_off[lo + 1] - a.g_pair_off[lo];
-    const int64_t nrows = a.g_row_len ? a.g_row_len[lo] : a.g_row_off[lo + 1] - a.g_row_off[lo];
-    const int64_t npt = (npairs + kBN - 1) / kBN;
+    const int64_t np = a.g_a_off[lo + 1] - a.g_a_off[lo];
+    const int64_t nr = a.g_b_len ? a.g_b_len[lo] : a.g_b_off[lo + 1] - a.g_b_off[lo];
+    const int64_t npt = (np + kBM - 1) / kBM;
     const int64_t local = t - a.g_item_off[lo];
-    const int64_t pt = local % npt, rt = local / npt;
+    const int64_t g = local % npt, rt = local / npt;
     GroupTile gt;
-    gt.r0 = a.g_row_off[lo] + rt * kBM;
-    gt.p0 = a.g_pair_off[lo] + pt * kBN;
-    gt.rows = (int)min((int64_t)kBM, nrows - rt * kBM);
-    gt.np = (int)min((int64_t)kBN, npairs - pt * kBN);
-    gt.nt = max(16, (gt.np + 15) & ~15);
+    gt.a0 = a.g_a_off[lo] + g * kBM;
+    gt.b0 = a.g_b_off[lo] + rt * kBN;
+    gt.am = (int)min((int64_t)kBM, np - g * kBM);
+    gt.bn = (int)min((int64_t)kBN, nr - rt * kBN);
     return gt;
 }
 
@@ -313,8 +282,8 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                 int64_t arow, brow;
                 if (grouped) {
                     const GroupTile gt = group_tile(a, t);
-                    arow = gt.r0;
-                    brow = gt.p0;
+                    arow = gt.a0;
+                    brow = gt.b0;
                 } else {
                     arow = (t % mt) * kBM;
                     brow = (t / mt) * kBN * a.b_tile_stride;
@@ -339,7 +308,6 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                 if (!(ok = bar_wait(&tempty[b], aph ^ 1u, a.err, a.wait_ns))) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t d = tmem + (uint32_t)(b * kBN);
-                const uint32_t idesc = idesc_n<KIND>(grouped ? group_tile(a, t).nt : kBN);
                 for (int kb = 0; kb < kt; ++kb, ++it) {
                     const int s = (int)(it % kStages);
                     const uint32_t ph = (uint32_t)((it / kStages) & 1);
@@ -350,8 +318,8 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
 #pragma unroll
                     for (int k16 = 0; k16 < kBlockK / kMmaK; ++k16)
                         if (k16 < n16)
-                            mma_issue_d<KIND>(d, sw128_desc(sA + s * kABytes + k16 * 32),
-                                              sw128_desc(sB + s * kBBytes + k16 * 32), idesc, (kb | k16) ? 1u : 0u);
+                            mma_issue<KIND>(d, sw128_desc(sA + s * kABytes + k16 * 32),
+                                            sw128_desc(sB + s * kBBytes + k16 * 32), (kb | k16) ? 1u : 0u);
                     mma_commit(&empty[s]);
                 }
                 mma_commit(&tfull[b]);
@@ -370,80 +338,78 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
         int64_t acc = 0;
         for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x, ++acc) {
             const int b = (int)(acc & 1);
-            if (!bar_wait(&tfull[b], (uint32_t)((acc >> 1) & 1), a.err, a.wait_ns)) break;
+            // every lane waits; the warp leaves together if any lane gave up, so that no lane is left
+            // behind at a warp-wide instruction
+            const bool got = bar_wait(&tfull[b], (uint32_t)((acc >> 1) & 1), a.err, a.wait_ns);
+            if (!__all_sync(0xffffffffu, got)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int m0 = (int)(t % mt) * kBM, n0 = (int)(t / mt) * kBN;
             const int m = m0 + lane_base + lane;
-            if (grouped) {
-                // a list's rows (TMEM lanes) x its pairs (columns): column j is pair p0 + j, lane r list row
-                // r0 + r. Keys go to the pair's stream positions (32 consecutive rows per store), or, in filter
-                // mode, those at or below the pair's query's bar to the query's buffer (a ballot per column,
-                // one atomic per warp and column).
+            if (!kFilterOnly && grouped) {  // keys of pair a0 + row, list rows b0 + column, to their stream positions
                 const GroupTile gt = group_tile(a, t);
                 const int ml = lane_base + lane;
-                const bool rvalid = ml < gt.rows;
-                const int64_t grow = gt.r0 + ml;
-                float cfx = 1.f, cfy = 0.f;  // per-row factors of scaled operands
-                if (a.col_fac && rvalid) {
-                    const float2 f = a.col_fac[grow];
-                    cfx = f.x;
-                    cfy = f.y;
-                }
-                constexpr int kGroups = EPI / 4;
-                const uint32_t tb = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kBN);
+                // the stream position of list row b0 for each of the warp's 32 pairs (lane r holds row r's)
+                const int64_t dst_lane = (ml < gt.am ? a.g_dbase[gt.a0 + ml] : 0) + gt.b0;
+                const int rows = min(32, gt.am - lane_base);  // valid pairs of this warp
+                const float grf = (a.row_fac && ml < gt.am) ? a.row_fac[gt.a0 + ml] : 1.f;
+                const uint32_t tb = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kBN + col0);
 #pragma unroll 1
-                for (int c = (ew >> 2) * 32; c < gt.np; c += kGroups * 32) {
-                    uint32_t r[32];
-                    tmem_ld32(tb + (uint32_t)c, r);
-                    tmem_wait(r);
-                    const int j = c + lane;
-                    const bool jv = j < gt.np;
-                    const int64_t pj = gt.p0 + j;
-                    const float rf = (a.row_fac && jv) ? a.row_fac[pj] : 1.f;
-                    if (!kFilterOnly) {
-                        const int64_t db = jv ? a.g_dbase[pj] : 0;
-#pragma unroll 4
-                        for (int u = 0; u < 32; ++u) {
-                            if (c + u >= gt.np) break;  // uniform across the warp
-                            const int64_t dbu = __shfl_sync(0xffffffffu, db, u);
-                            float val = acc_value<KIND>(r[u]);
-                            if (a.col_fac) val = fmaf(cfx, __shfl_sync(0xffffffffu, rf, u) * val, cfy);
-                            if (rvalid) a.out[dbu + grow] = val;
+                for (int c = 0; c < kCols; c += 64) {
+                    uint32_t r0[32], r1[32];
+                    __syncwarp();  // tcgen05.ld is .sync.aligned: the whole warp, converged
+                    tmem_ld32(tb + (uint32_t)c, r0);
+                    tmem_ld32(tb + (uint32_t)(c + 32), r1);
+                    tmem_wait(r0);
+                    tmem_after_wait(r1);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int cb = col0 + c + 32 * h;
+                        if (rows <= 0 || cb >= gt.bn) continue;  // uniform across the warp
+                        const bool cok = cb + lane < gt.bn;
+                        // transpose through shared memory: each store writes 32 consecutive keys of one pair
+                        if (a.col_fac) {  // scaled operands: the column factors of the 32 columns by shuffles
+                            const float2 f = cok ? a.col_fac[gt.b0 + cb + lane] : make_float2(0.f, 0.f);
+#pragma unroll
+                            for (int u = 0; u < 32; ++u)
+                                tw[lane * 33 + u] = fmaf(__shfl_sync(0xffffffffu, f.x, u),
+                                                         grf * acc_value<KIND>(h ? r1[u] : r0[u]),
+                                                         __shfl_sync(0xffffffffu, f.y, u));
+                        } else {
+#pragma unroll
+                            for (int u = 0; u < 32; ++u) tw[lane * 33 + u] = acc_value<KIND>(h ? r1[u] : r0[u]);
                         }
-                    } else {
-                        const int qj = jv ? (a.g_row_query ? a.g_row_query[pj] : (int)pj) : 0;
-                        const float tj = jv ? a.tau[qj] : -kInf;
-#pragma unroll 4
-                        for (int u = 0; u < 32; ++u) {
-                            if (c + u >= gt.np) break;  // uniform across the warp
-                            const int qu = __shfl_sync(0xffffffffu, qj, u);
-                            float val = acc_value<KIND>(r[u]);
-                            if (a.col_fac) val = fmaf(cfx, __shfl_sync(0xffffffffu, rf, u) * val, cfy);
-                            const bool pass = rvalid && val <= __shfl_sync(0xffffffffu, tj, u);
-                            const unsigned m = __ballot_sync(0xffffffffu, pass);
-                            if (m) {
-                                int base = 0;
-                                if (lane == 0) base = atomicAdd(&a.rcount[qu], __popc(m));
-                                base = __shfl_sync(0xffffffffu, base, 0);
-                                const int slot = base + __popc(m & ((1u << lane) - 1u));
-                                if (pass && slot < a.row_cap) {
-                                    a.fkey[(int64_t)qu * a.row_cap + slot] = val;
-                                    a.fcol[(int64_t)qu * a.row_cap + slot] = (int)grow;
-                                }
-                            }
+                        __syncwarp();
+                        for (int r = 0; r < rows; ++r) {
+                            const int64_t dr = __shfl_sync(0xffffffffu, dst_lane, r);
+                            if (cok) a.out[dr + cb + lane] = tw[r * 33 + lane];
                         }
+                        __syncwarp();
                     }
                 }
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                 bar_arrive(&tempty[b]);
                 continue;
             }
-            const bool mvalid = m < a.M;
-            const int ncols = a.N - n0;  // valid columns of the tile from its first
-            const float an = (a.normA && mvalid) ? a.normA[m] : 0.f;
-            const float rfac = (a.row_fac && mvalid) ? a.row_fac[m] : 1.f;
+            // the tile's rows and columns: a dense tile, or a grouped one (a list's pairs and rows; rows and
+            // columns past them belong to the next list and are masked like rows past M)
+            int rq = m;                         // the row recorded for a survivor (grouped: its query)
+            int64_t arow = m;                   // the A row (per-row factors)
+            bool mvalid = m < a.M;
+            int64_t cbase = n0;                 // recorded column of the tile's first column
+            int ncols = a.N - n0;               // valid columns of the tile from its first
+            if (grouped) {
+                const GroupTile gt = group_tile(a, t);
+                const int ml = lane_base + lane;
+                mvalid = ml < gt.am;
+                arow = gt.a0 + ml;
+                rq = mvalid ? (a.g_row_query ? a.g_row_query[gt.a0 + ml] : (int)(gt.a0 + ml)) : 0;
+                cbase = gt.b0;
+                ncols = gt.bn;
+            }
+            const float an = (a.normA && mvalid) ? a.normA[arow] : 0.f;
+            const float rfac = (a.row_fac && mvalid) ? a.row_fac[arow] : 1.f;
             // rows past M (TMA zero fill) get a bar no key passes
-            const float tau = (a.tau && mvalid) ? a.tau[m] : -kInf;
+            const float tau = (a.tau && mvalid) ? a.tau[rq] : -kInf;
             const float tau_up = nextafterf(tau, kInf);
             const float2 ntau2 = make_float2(-tau_up, -tau_up);
             const uint32_t tbase = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kBN + col0);
@@ -459,7 +425,7 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                 for (int i = 0; i < kCols / 32; ++i) {
                     const int lcol = col0 + 32 * i + lane;  // column within the tile
                     const int col = n0 + lcol;
-                    const int64_t nrow = (int64_t)(col / kBN) * kBN * a.b_tile_stride + col % kBN;
+                    const int64_t nrow = grouped ? cbase + lcol : (int64_t)(col / kBN) * kBN * a.b_tile_stride + col % kBN;
                     const float2 f = lcol < ncols ? a.col_fac[nrow] : make_float2(0.f, 0.f);
                     sfx[32 * i + lane] = f.x;
                     sfy[32 * i + lane] = f.y;
@@ -470,6 +436,7 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
 #pragma unroll 1
             for (int c = 0; c < kCols; c += 64) {
                 uint32_t r0[32], r1[32];
+                __syncwarp();  // .sync.aligned loads after the divergent survivor stores of the last chunk
                 tmem_ld32(tbase + (uint32_t)c, r0);
                 tmem_ld32(tbase + (uint32_t)(c + 32), r1);
                 tmem_wait(r0);
@@ -540,7 +507,30 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                             }
                         }
                         uint32_t msk = (mq[0] | (mq[1] << 8)) | ((mq[2] << 16) | (mq[3] << 24));
-                        if (__any_sync(0xffffffffu, msk != 0)) {
+                        if (a.row_cap > 0) {  // per-row buffers: this lane's survivors, one atomic
+                            if (msk) {
+                                int slot = atomicAdd(&a.rcount[rq], __popc(msk));
+                                const int64_t rbase = (int64_t)rq * a.row_cap;
+                                while (msk) {
+                                    const int u = __ffs(msk) - 1;
+                                    msk &= msk - 1;
+                                    if (slot < a.row_cap) {
+                                        float s16[16], s8[8], s4[4], s2[2];
+#pragma unroll
+                                        for (int z = 0; z < 16; ++z) s16[z] = (u & 16) ? v[z + 16] : v[z];
+#pragma unroll
+                                        for (int z = 0; z < 8; ++z) s8[z] = (u & 8) ? s16[z + 8] : s16[z];
+#pragma unroll
+                                        for (int z = 0; z < 4; ++z) s4[z] = (u & 4) ? s8[z + 4] : s8[z];
+#pragma unroll
+                                        for (int z = 0; z < 2; ++z) s2[z] = (u & 2) ? s4[z + 2] : s4[z];
+                                        a.fkey[rbase + slot] = (u & 1) ? s2[1] : s2[0];
+                                        a.fcol[rbase + slot] = (int)(cbase + lb + u);
+                                    }
+                                    ++slot;
+                                }
+                            }
+                        } else if (__any_sync(0xffffffffu, msk != 0)) {
                             const int cnt = __popc(msk);
                             int incl = cnt;
 #pragma unroll
@@ -566,8 +556,8 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                                     for (int z = 0; z < 2; ++z) s2[z] = (u & 2) ? s4[z + 2] : s4[z];
                                     const float kv = (u & 1) ? s2[1] : s2[0];
                                     a.fkey[wbase + slot] = kv;
-                                    a.fcol[wbase + slot] = nb + u;
-                                    a.frow[wbase + slot] = m;
+                                    a.fcol[wbase + slot] = (int)(cbase + lb + u);
+                                    a.frow[wbase + slot] = rq;
                                 }
                                 ++slot;
                             }
@@ -582,6 +572,7 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
     }
     __syncthreads();
     if (warp == 1) {
+        __syncwarp();  // lane 0 issued the MMAs alone: the warp meets again before the .sync.aligned dealloc
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
     }
@@ -654,11 +645,10 @@ int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream
     ANN_CHECK_ARG((reinterpret_cast<uintptr_t>(A) & 15) == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0,
                   "tensor-core scan: operands must be 16-byte aligned");
     ANN_CHECK_ARG(a.out != nullptr || (a.tau && a.fkey && a.fcol &&
-                                       (a.g_item_off ? (a.row_cap > 0 && a.rcount != nullptr)
-                                                     : (a.frow && a.wcount && a.wcap > 0))),
+                                       ((a.frow && a.wcount && a.wcap > 0) || (a.row_cap > 0 && a.rcount))),
                   "tensor-core scan: neither an output matrix nor a filter");
     ANN_CHECK_ARG(a.g_item_off == nullptr ||
-                      (a.g_pair_off && a.g_row_off && a.g_total && a.g_lists > 0 &&
+                      (a.g_a_off && a.g_b_off && a.g_total && a.g_lists > 0 &&
                        ((a.out && a.g_dbase && a.tau == nullptr) || (a.out == nullptr && a.tau && a.g_row_query))),
                   "tensor-core scan: incomplete grouping");
     ANN_CHECK_ARG(a.b_tile_stride >= 1, "tensor-core scan: bad sample stride");

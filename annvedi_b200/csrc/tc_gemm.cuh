@@ -32,33 +32,34 @@ struct TcGemmArgs {
     int* frow = nullptr;
     int* wcount = nullptr;
     int wcap = 0;
-    // Grouped mode (g_item_off != null): work item t of a list-major grouping (an IVF batch). List l owns
-    // the A rows [g_row_off[l], + g_row_len[l] or up to g_row_off[l+1]) -- its list-ordered base rows, the
-    // M side -- and the B rows [g_pair_off[l], g_pair_off[l+1]) -- its (query, list) pairs, the N side; its
-    // items are ceil(pairs / 256) x ceil(rows / 128) tiles, pair tiles fastest, numbered from
-    // g_item_off[l]; *g_total items in all (read on the device); the MMA runs N = the tile's pairs
-    // rounded up to 16. Keys (out != null): the key of pair i and list row r goes to out[g_dbase[i] + r].
-    // Filter (out == null): pair i belongs to query g_row_query[i]; a key at or below tau[that query] goes
-    // to fkey / fcol [query * row_cap + slot] (fcol = the list row) at slot = atomicAdd(&rcount[query], ..)
-    // -- one atomic per warp and column -- and nothing is written at slots past row_cap (rcount may exceed
-    // it: the caller checks). With scaled operands, col_fac is per list row and row_fac per pair.
+    // Filter mode, per-row buffers (row_cap > 0; the grouped form, rows = queries): a survivor of row r goes
+    // to fkey / fcol [r * row_cap + slot] at slot = atomicAdd(&rcount[r], n) -- one atomic per lane per 32
+    // columns, n its survivors there -- and nothing is written at slots past row_cap (rcount[r] may exceed
+    // it: the caller checks).
+    int row_cap = 0;
+    int* rcount = nullptr;
+    // Grouped mode (g_item_off != null; out receives the keys): tile t is work item t of a list-major
+    // grouping (an IVF batch). List l owns A rows [g_a_off[l], g_a_off[l+1]) (its (query, list) pairs)
+    // and B rows [g_b_off[l], g_b_off[l+1]) (its rows); its items are ceil(pairs/128) x ceil(rows/256)
+    // tiles, pair tiles fastest, numbered from g_item_off[l]; *g_total items in all (read on the
+    // device). The key of pair i and list row r goes to out[g_dbase[i] + r].
     const int64_t* g_item_off = nullptr;
-    const int64_t* g_pair_off = nullptr;
-    const int64_t* g_row_off = nullptr;
-    const int64_t* g_row_len = nullptr;
+    const int64_t* g_a_off = nullptr;
+    const int64_t* g_b_off = nullptr;
     const int64_t* g_dbase = nullptr;
     const int64_t* g_total = nullptr;
     int g_lists = 0;
     const int32_t* g_item_list = nullptr;  // optional: the list of each item (else a search of g_item_off)
+    const int64_t* g_b_len = nullptr;      // optional: rows of list l taken (else g_b_off[l+1] - g_b_off[l])
+    // Grouped filter mode (grouped, out == null): A row i belongs to query g_row_query[i]; its bar is
+    // tau[g_row_query[i]], and a survivor is recorded as (key, list row g_b_off[l] + r, that query).
     const int32_t* g_row_query = nullptr;
-    int row_cap = 0;
-    int* rcount = nullptr;
     // Element kind of A and B. E4M3 and I8 operands carry factors per row: the key is
-    // col_fac[n].y + col_fac[n].x * row_fac[m] * accumulator for the dense key-matrix and filter modes (n the
-    // B row, m the A row); in the grouped mode (I8) col_fac is per list row and row_fac per pair.
+    // col_fac[n].y + col_fac[n].x * row_fac[m] * accumulator (key-matrix and filter modes; I8 also grouped,
+    // with n the absolute B row and m the A row).
     int kind = kTcBF16;
-    const float2* col_fac = nullptr;
-    const float* row_fac = nullptr;
+    const float2* col_fac = nullptr;  // per B row, indexed like B's rows
+    const float* row_fac = nullptr;   // per A row
     // Bounded waits: every mbarrier wait gives up after wait_ns (0: 2 s), sets *err = 2 and the CTA
     // winds down (remaining copies and MMAs drained, TMEM released). test_no_loads (self-test only):
     // the producer issues no copies, so the waits run out with nothing in flight.

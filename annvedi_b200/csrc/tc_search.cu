@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(1024) tc_ivf_items_kernel(const int64_t* lq_of
     auto items = [&](int l) -> int64_t {
         const int64_t np = lq_off[l + 1] - lq_off[l];
         const int64_t nr = list_len ? list_len[l] : list_off[l + 1] - list_off[l];
-        return (np == 0 || nr == 0) ? 0 : ((np + 255) / 256) * ((nr + 127) / 128);
+        return (np == 0 || nr == 0) ? 0 : ((np + 127) / 128) * ((nr + 255) / 256);
     };
     int64_t local = 0;
     for (int i = 0; i < per; ++i)
@@ -235,41 +235,6 @@ __device__ __forceinline__ float from_ord(uint32_t o) {
     return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
 }
 
-// The digit of rank `rem` in a 256-bin histogram, and the count of keys below that digit (every lane).
-__device__ __forceinline__ void warp_hist_pick(const int* hist, int64_t rem, int* digit, int* before) {
-    const int lane = threadIdx.x & 31;
-    int c[8];
-    int sum = 0;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        c[j] = hist[lane * 8 + j];
-        sum += c[j];
-    }
-    int incl = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-    }
-    const int excl = incl - sum;
-    const unsigned hit = __ballot_sync(0xffffffffu, excl < rem && rem <= incl);
-    const int src = __ffs(hit) - 1;
-    int d = 0, bf = 0;
-    if (lane == src) {
-        int acc = excl;
-        for (int j = 0; j < 8; ++j) {
-            if (acc + c[j] >= rem) {
-                d = lane * 8 + j;
-                bf = acc;
-                break;
-            }
-            acc += c[j];
-        }
-    }
-    *digit = __shfl_sync(0xffffffffu, d, src);
-    *before = __shfl_sync(0xffffffffu, bf, src);
-}
-
 // The r-th smallest (1 <= r <= n) of keys[0..n) as an ordered key, by one warp: four passes of 8-bit digits
 // from the top, each counting the keys that match the digits found so far into the warp's 256-bin
 // histogram `hist` (shared memory). Exact; every lane returns it.
@@ -285,8 +250,36 @@ __device__ uint32_t warp_kth_ord(const float* __restrict__ keys, int64_t n, int6
             if ((o & pmask) == prefix) atomicAdd(&hist[(o >> shift) & 255u], 1);
         }
         __syncwarp();
-        int d, before;
-        warp_hist_pick(hist, rem, &d, &before);
+        int c[8];
+        int sum = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            c[j] = hist[lane * 8 + j];
+            sum += c[j];
+        }
+        int incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int excl = incl - sum;
+        const unsigned hit = __ballot_sync(0xffffffffu, excl < rem && rem <= incl);
+        const int src = __ffs(hit) - 1;
+        int d = 0, before = 0;
+        if (lane == src) {
+            int acc = excl;
+            for (int j = 0; j < 8; ++j) {
+                if (acc + c[j] >= rem) {
+                    d = lane * 8 + j;
+                    before = acc;
+                    break;
+                }
+                acc += c[j];
+            }
+        }
+        d = __shfl_sync(0xffffffffu, d, src);
+        before = __shfl_sync(0xffffffffu, before, src);
         rem -= before;
         prefix |= (uint32_t)d << shift;
         pmask |= 255u << shift;
@@ -296,52 +289,21 @@ __device__ uint32_t warp_kth_ord(const float* __restrict__ keys, int64_t n, int6
 }
 
 // One warp per query: bar1 / bar2 = the r1-th / r2-th smallest of the query's keys[offs[q] .. + lens[q])
-// (+inf where the stream is shorter). Both ranks' digits are found in the same four passes over the keys
-// (two 256-bin histograms per warp).
+// (+inf where the stream is shorter).
 __global__ void __launch_bounds__(256) warp_bars_kernel(const float* __restrict__ keys, const int64_t* __restrict__ offs,
                                                         const int64_t* __restrict__ lens, int nq, int r1, int r2,
                                                         float* __restrict__ bar1, float* __restrict__ bar2) {
-    __shared__ int sHist[8][2][256];
+    __shared__ int sHist[8][256];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int q = blockIdx.x * 8 + warp;
     if (q >= nq) return;  // the whole warp
     const float* kq = keys + offs[q];
     const int64_t n = lens[q];
-    int* h1 = sHist[warp][0];
-    int* h2 = sHist[warp][1];
-    const bool want1 = r1 <= n, want2 = r2 <= n;
-    uint32_t p1 = 0, p2 = 0, pmask = 0;
-    int64_t rem1 = r1, rem2 = r2;
-    for (int shift = 24; shift >= 0 && (want1 || want2); shift -= 8) {
-        for (int i = lane; i < 256; i += 32) {
-            h1[i] = 0;
-            h2[i] = 0;
-        }
-        __syncwarp();
-        for (int64_t p = lane; p < n; p += 32) {
-            const uint32_t o = ord_key(kq[p]);
-            const uint32_t dgt = (o >> shift) & 255u;
-            if (want1 && (o & pmask) == p1) atomicAdd(&h1[dgt], 1);
-            if (want2 && (o & pmask) == p2) atomicAdd(&h2[dgt], 1);
-        }
-        __syncwarp();
-        int d, bf;
-        if (want1) {
-            warp_hist_pick(h1, rem1, &d, &bf);
-            rem1 -= bf;
-            p1 |= (uint32_t)d << shift;
-        }
-        if (want2) {
-            warp_hist_pick(h2, rem2, &d, &bf);
-            rem2 -= bf;
-            p2 |= (uint32_t)d << shift;
-        }
-        pmask |= 255u << shift;
-        __syncwarp();
-    }
+    const float b1 = r1 <= n ? from_ord(warp_kth_ord(kq, n, r1, sHist[warp])) : kInf;
+    const float b2 = r2 <= n ? from_ord(warp_kth_ord(kq, n, r2, sHist[warp])) : kInf;
     if (lane == 0) {
-        bar1[q] = want1 ? from_ord(p1) : kInf;
-        bar2[q] = want2 ? from_ord(p2) : kInf;
+        bar1[q] = b1;
+        bar2[q] = b2;
     }
 }
 

@@ -48,15 +48,15 @@ int launch_tc_map_ids(int* ids, int64_t count, int64_t n, int64_t mult, cudaStre
 int launch_tc_unpermute(const float* keys, int nq, int64_t n, int64_t mult, float* out, cudaStream_t st);
 
 // IVF batches on the tensor cores (a list-major grouping of (query, list) pairs, ivf_batched.cu):
-// items per list = ceil(pairs / 256) x ceil(rows / 128), exclusively scanned into item_off[0..C]
+// items per list = ceil(pairs / 128) x ceil(rows / 256), exclusively scanned into item_off[0..C]
 // (item_off[C] = all items). One block.
 // With list_len, list l counts list_len[l] rows (a capped head of each list) instead of its size.
 int launch_tc_ivf_items(const int64_t* lq_off, const int64_t* list_off, int C, int64_t* item_off, cudaStream_t st,
                         const int64_t* list_len = nullptr);
 // item_list[t] = the list of work item t (item_off [C + 1] from launch_tc_ivf_items), for t < cap.
 int launch_tc_item_lists(const int64_t* item_off, int C, int32_t* item_list, int64_t cap, cudaStream_t st);
-// Work items of a grouped batch at most: (pairs / 256 + C) x (largest list / 128 + 1).
-inline int64_t tc_items_bound(int64_t pairs, int C, int64_t largest) { return (pairs / 256 + C) * (largest / 128 + 1); }
+// Work items of a grouped batch at most: (pairs / 128 + C) x (largest list / 256 + 1).
+inline int64_t tc_items_bound(int64_t pairs, int C, int64_t largest) { return (pairs / 128 + C) * (largest / 256 + 1); }
 // For each valid pair i (< lq_off[C]; pairs grouped by list, pair_vals = q * npc + j, pair_lists = the
 // list): A[i] = qb[q] (kpad BF16 columns) and dbase[i] = cand_off[q] + seg_pref[q][j] - list_off[list],
 // the stream position of the list's row 0 in the candidate array.
