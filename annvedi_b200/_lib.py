@@ -106,6 +106,8 @@ SIGNATURES = [
     ("ann_ivf_reset_distances", ctypes.c_int, [_vp]),
     ("ann_ivf_set_profiling", ctypes.c_int, [_vp, _i32]),
     ("ann_ivf_profile", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    ("ann_ivf_kernel_profile", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    ("ann_ivf_set_option", ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int64]),
     ("ann_ivf_reset_profile", ctypes.c_int, [_vp]),
     # the reference GPU contestant's ABI (include/annvedi_gpu_filter.h)
     ("gf_last_error", ctypes.c_char_p, []),

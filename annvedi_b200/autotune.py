@@ -37,12 +37,19 @@ def _time(fn, reps, stream):
     return e0.elapsed_time(e1) / reps
 
 
+IVF_NPROBES = (2, 3, 4, 5, 6, 8, 10, 12, 16, 24, 32, 64, 128)
+IVF_REFINES = (100, 150, 200, 300)
+
+
 def tune_ivf(index, base, queries, kth, k: int = 100, target: float = 0.95, modes=("tc", "exact"),
-             nprobes=(8, 16, 32, 64, 128), refines=(300,), reps: int = 3) -> dict:
+             nprobes=IVF_NPROBES, refines=IVF_REFINES, reps: int = 3, sample_divs=(4, 8, 16)) -> dict:
     """Fastest (mode, nprobe, refine_r) of an IVFIndex whose recall@k on `queries` is >= target.
 
-    Returns {"best": {...} or None, "table": [...]}; each entry has mode, nprobe, refine_r, recall,
-    ms_per_batch and qps (queries per second at this batch size)."""
+    For every mode and re-rank depth the probe counts run in increasing order up to the first that meets
+    the target. At each tensor-core mode's best point the sampled bars' list share (sample_divs) is then
+    swept and the fastest kept on the index. Returns {"best": {...} or None, "best_by_mode": {mode: {...}},
+    "table": [...]}; each entry has mode, nprobe, refine_r, recall, ms_per_batch and qps (queries per second at
+    this batch size), and sample_div where swept. The index keeps the last mode's best sample_div."""
     import torch
     stream = torch.cuda.current_stream()
     nq = queries.shape[0]
@@ -63,7 +70,31 @@ def tune_ivf(index, base, queries, kth, k: int = 100, target: float = 0.95, mode
                     if best is None or row["qps"] > best["qps"]:
                         best = row
                     break  # a larger nprobe costs more for this (mode, refine_r)
-    return {"best": best, "table": table, "target": target}
+    by_mode = {}
+    for row in table:
+        b = by_mode.get(row["mode"])
+        if row["recall"] >= target and (b is None or row["qps"] > b["qps"]):
+            by_mode[row["mode"]] = row
+    # the tensor-core forms' sampling knob at each mode's best point: the share of every probed list the
+    # sampled bars score (results do not depend on it; time does)
+    for mode, row in list(by_mode.items()):
+        if mode not in ("tc", "tc_sq8") or not sample_divs:
+            continue
+        row["sample_div"] = 8
+        for div in sample_divs:
+            if div == 8:
+                continue
+            index.set_option("sample_div", div)
+            fn = lambda: index.search(queries, k, 0, row["nprobe"], row["refine_r"], max_candidates=0, mode=mode,
+                                      out_ids=ids, out_dists=dists)
+            ms = _time(fn, reps, stream)
+            alt = {**row, "sample_div": div, "ms_per_batch": round(ms, 4), "qps": round(nq / (ms / 1e3), 1)}
+            table.append(alt)
+            if alt["qps"] > by_mode[mode]["qps"]:
+                by_mode[mode] = alt
+        index.set_option("sample_div", by_mode[mode].get("sample_div", 8))
+    best = max(by_mode.values(), key=lambda r: r["qps"]) if by_mode else best
+    return {"best": best, "best_by_mode": by_mode, "table": table, "target": target}
 
 
 def tune_flat_tc(index, base, queries, kth, k: int = 100, target: float = 0.95, refines=(100, 200, 400),

@@ -59,6 +59,9 @@ struct ann_ivf {
     int kpad = 0;
     std::mutex tc_mu;
     int64_t query_count = 0;
+    // query options (ann_ivf_set_option)
+    int sample_div = 8;             // the sampled bars score the first ceil(size / sample_div) rows of a list
+    int sampled_min_queries = 256;  // batches from this size take the sampled tensor-core path
 
     IvfView view() const {
         IvfView v;
@@ -761,15 +764,16 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
 }
 
 // IVF on the tensor cores with sampled bars (large batches). Every probed list's head -- its first
-// ceil(size / kSampleDiv) rows, an even sample since rows are in ascending original id inside a list --
-// is scored by a first grouped GEMM into each query's sample stream. Per query, the fast bar is the
-// rF-th smallest sampled key (rF = ceil(3 R / kSampleDiv): about 3 R keys of the whole stream pass it)
-// and the safe bar the R-th (at or above the stream's R-th key), both exact (warp_bars_kernel). The
-// grouped GEMM over all rows then appends only the keys at or below the fast bar to the query's own
-// buffer (kRowCapFactor R slots); a query left with fewer than min(R, its candidates) survivors is redone
-// under its safe bar. Each query ends with the exact best R keys of its stream (warp_select_kernel: the
-// keys below the R-th, then equal ones by increasing row), as the key-stream path selects them, without
-// writing the stream. Returns with *done = false (and no output) when a query's buffer overflowed.
+// ceil(size / div) rows (div = the sample_div option, 8 by default), an even sample since rows are in
+// ascending original id inside a list -- is scored by a first grouped GEMM into each query's sample
+// stream. Per query, the fast bar is the rF-th smallest sampled key (rF = ceil(3 R / div): about 3 R keys
+// of the whole stream pass it) and the safe bar the R-th (at or above the stream's R-th key), both exact
+// (the bars kernel). The grouped GEMM over all rows then appends only the keys at or below the fast bar to
+// the query's own buffer (kRowCapFactor R slots); a query left with fewer than min(R, its candidates)
+// survivors is redone under its safe bar. Each query ends with the exact best R keys of its stream
+// (warp_select_kernel: the keys below the R-th, then equal ones by increasing row), as the key-stream path
+// selects them, without writing the stream. Returns with *done = false (and no output) when a query's
+// buffer overflowed.
 struct TcOperands {
     const void* qrows;     // the queries' operand rows
     int row_bytes;
@@ -786,8 +790,9 @@ static TcOperands tc_operands(const ann_ivf* h, const IvfQueryCfg& c, const __nv
     return TcOperands{qb, 2 * h->kpad, h->base_bf16, h->kpad, kTcBF16, nullptr, nullptr, nullptr};
 }
 
-constexpr int kTcSampledMinQueries = 256;
-constexpr int kSampleDiv = 8;
+// Kernel timer slots of the IVF query (ann_ivf_kernel_profile): the list-keys kernel (the grouped GEMM,
+// or the SQ8 batched kernel), the sampled bars, the best-R selection and the exact re-rank.
+constexpr int kKernKeys = 0, kKernBars = 1, kKernSelect = 2, kKernRerank = 3;
 constexpr int kRowCapFactor = 16;
 
 static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, const IvfQueryArgs& a,
@@ -798,10 +803,11 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     const int nq = a.plan.nq, npc = c.npc, C = (int)h->C, R = c.R;
     const int64_t max_pairs = (int64_t)nq * npc;
     const int64_t largest = h->sizes_desc.empty() ? 1 : h->sizes_desc[0];
-    const int64_t head_max = ceil_div(largest, kSampleDiv);
+    const int div = h->sample_div;
+    const int64_t head_max = ceil_div(largest, div);
     const int64_t s_bound = (int64_t)nq * npc * head_max;  // sample keys at most
     const int64_t scap = tc_items_bound(max_pairs, C, head_max);
-    const int rF = (int)std::min<int64_t>(R, std::max<int64_t>(1, ceil_div(3 * (int64_t)R, kSampleDiv)));
+    const int rF = (int)std::min<int64_t>(R, std::max<int64_t>(1, ceil_div(3 * (int64_t)R, div)));
     const int cap = kRowCapFactor * R;
     size_t scan_tmp = 0;
     ANN_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, (int64_t*)nullptr, (int64_t*)nullptr, nq + 1, st));
@@ -845,7 +851,7 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     int* flags = cv.take<int>(4);
 
     // sample streams: heads of the probed lists, each query's stream offsets
-    if ((rc = launch_tc_ivf_sample_plan(a.plan, h->list_off, C, kSampleDiv, lcap, sseg, slen, st))) return rc;
+    if ((rc = launch_tc_ivf_sample_plan(a.plan, h->list_off, C, div, lcap, sseg, slen, st))) return rc;
     ANN_CUDA_TRY(cudaMemsetAsync(slen + nq, 0, sizeof(int64_t), st));
     size_t tb = scan_tmp;
     ANN_CUDA_TRY(cub::DeviceScan::ExclusiveSum(stmp, tb, slen, soff, nq + 1, st));
@@ -875,12 +881,15 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     gs.g_lists = C;
     gs.g_item_list = sitem_list;
     if ((rc = launch_tc_gemm(Apk, op.B, gs, st))) return rc;
-    if ((rc = launch_warp_bars(SK, soff, slen, nq, rF, R, tauF, tauS, st))) return rc;
+    int kt = h->prof.kbegin(st);
+    if ((rc = launch_warp_bars(SK, soff, slen, nq, rF, R, tauF, tauS, st, (int64_t)npc * head_max))) return rc;
+    h->prof.kend(kt, kKernBars, st);
     // 2. filter pass over every row of the probed lists into the queries' buffers
     if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, C, titem, st))) return rc;
     if ((rc = launch_tc_item_lists(titem, C, titem_list, items_cap, st))) return rc;
-    auto filter = [&](const float* tau) -> int {
+    auto filter = [&](const float* tau, const int* skip_if_zero) -> int {
         TcGemmArgs g{(int)max_pairs, (int)h->n, op.K, nullptr, nullptr, 0, h->d_err};
+        g.skip_if_zero = skip_if_zero;
         g.kind = op.kind;
         g.col_fac = op.col_fac;
         g.row_fac = op.pfac;
@@ -896,28 +905,30 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
         g.fcol = srow;
         g.row_cap = cap;
         g.rcount = scount;
-        return launch_tc_gemm(Apk, op.B, g, st);
+        const int k0 = skip_if_zero ? -1 : h->prof.kbegin(st);  // the timer sees the first pass only
+        const int r = launch_tc_gemm(Apk, op.B, g, st);
+        h->prof.kend(k0, kKernKeys, st);
+        return r;
     };
     ANN_CUDA_TRY(cudaMemsetAsync(scount, 0, sizeof(int) * (size_t)nq, st));
-    if ((rc = filter(tauF))) return rc;
+    if ((rc = filter(tauF, nullptr))) return rc;
     h->prof.mark(prec, st);
     ANN_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int), st));
     if ((rc = launch_tc_bar_check(scount, nq, R, list, flags, st, a.plan.n_cands, mark))) return rc;
-    int nre = 0;
-    ANN_CUDA_TRY(cudaMemcpyAsync(&nre, flags, sizeof(int), cudaMemcpyDeviceToHost, st));
-    ANN_CUDA_TRY(cudaStreamSynchronize(st));
-    if (nre > 0) {  // queries short of survivors: again under their safe bars (their buffers refilled), the rest under -inf
-        if ((rc = launch_tc_rerun_bars(mark, tauS, nq, tauR, st, scount))) return rc;
-        if ((rc = filter(tauR))) return rc;
-        if (prec >= 0) h->prof.tc_launches += 1;
-    }
+    // queries short of survivors: again under their safe bars (their buffers refilled), the rest under -inf;
+    // the pass returns at once on the device when no query is short (flags[0] == 0), with no host round trip
+    if ((rc = launch_tc_rerun_bars(mark, tauS, nq, tauR, st, scount))) return rc;
+    if ((rc = filter(tauR, flags))) return rc;
+    if (prec >= 0) h->prof.tc_launches += 1;
     // a query with more survivors than its buffer holds: the caller takes the key-stream path
     if ((rc = launch_max_int(scount, nq, flags + 1, st))) return rc;
     int most = 0;
     ANN_CUDA_TRY(cudaMemcpyAsync(&most, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     ANN_CUDA_TRY(cudaStreamSynchronize(st));
     if (most > cap) return ANN_OK;
+    kt = h->prof.kbegin(st);
     if ((rc = launch_warp_select(skey, srow, scount, cap, nq, R, keyR, idR, st))) return rc;
+    h->prof.kend(kt, kKernSelect, st);
     if (prec >= 0) h->prof.tc_launches += 2;
     *done = true;
     return ANN_OK;
@@ -1071,7 +1082,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         int64_t tot[3] = {0, 0, 0};
         if ((rc = batched_prepare(a, bscratch, c.sort_tmp, c.scan_tmp, &b, tot, st))) return rc;
         bool sampled_done = false;
-        if (tot[2] == 0 && c.tc && nq >= kTcSampledMinQueries) {
+        if (tot[2] == 0 && c.tc && nq >= h->sampled_min_queries) {
             if ((rc = ivf_tc_sampled(h, ws, c, a, b, tc_operands(h, c, qb, q8, qfac, pfac), Apk, titem, titem_list,
                                      items_cap, keyR, idR, prec, &sampled_done, st)))
                 return rc;
@@ -1105,7 +1116,9 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                 g.g_total = titem + h->C;
                 g.g_lists = h->C;
                 g.g_item_list = titem_list;
+                const int kg = h->prof.kbegin(st);
                 if ((rc = launch_tc_gemm(Apk, op.B, g, st))) return rc;
+                h->prof.kend(kg, kKernKeys, st);
                 h->prof.mark(prec, st);
                 RadixSelectArgs rs{};
                 rs.keys = D;
@@ -1116,9 +1129,13 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                 rs.R = c.R;
                 rs.out_key = keyR;
                 rs.out_id = idR;
+                const int ks = h->prof.kbegin(st);
                 if ((rc = launch_radix_select(rs, nq, st))) return rc;
+                h->prof.kend(ks, kKernSelect, st);
             } else {
+                const int kb = h->prof.kbegin(st);
                 if ((rc = launch_batched(b, qdev, qs, D, st))) return rc;
+                h->prof.kend(kb, kKernKeys, st);
                 h->prof.mark(prec, st);
                 // the best R of each stream as a set (ties by stream position); the re-rank orders them
                 RadixSelectArgs rs{};
@@ -1130,7 +1147,9 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                 rs.R = c.R;
                 rs.out_key = keyR;
                 rs.out_id = idR;
+                const int ks = h->prof.kbegin(st);
                 if ((rc = launch_radix_select(rs, nq, st))) return rc;
+                h->prof.kend(ks, kKernSelect, st);
             }
             done = true;
         }
@@ -1173,7 +1192,9 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         if ((rc = launch_query_order(probes, c.npc, nq, (int)h->C, qorder, st))) return rc;
         a.qorder = qorder;
     }
+    const int kr = h->prof.kbegin(st);
     if ((rc = launch_ivf_rerank(a, keyR, idR, c.ref ? 1 : 0, st))) return rc;
+    h->prof.kend(kr, kKernRerank, st);
     if (!every_row.empty()) {
         const int64_t L = h->n;
         const int nsp = (int)std::min<int64_t>(2 * kNumSMs, std::max<int64_t>(1, ceil_div(L, 2048)));
@@ -1403,6 +1424,34 @@ int ann_ivf_profile(ann_ivf* h, double* out8) {
     for (int i = 0; i < 6; ++i) out8[i] = h->prof.total_ms[i];
     out8[6] = (double)h->prof.calls;
     out8[7] = (double)h->query_count;
+    return ANN_OK;
+}
+
+int ann_ivf_set_option(ann_ivf* h, int32_t option, int64_t value) {
+    ANN_CHECK_ARG(h != nullptr, "null index");
+    switch (option) {
+        case ANN_IVF_OPT_SAMPLE_DIV:
+            ANN_CHECK_ARG(value >= 2 && value <= 64, "sample divisor %lld (2..64)", (long long)value);
+            h->sample_div = (int)value;
+            return ANN_OK;
+        case ANN_IVF_OPT_SAMPLED_MIN:
+            ANN_CHECK_ARG(value >= 1 && value <= INT32_MAX, "sampled-path batch size %lld", (long long)value);
+            h->sampled_min_queries = (int)value;
+            return ANN_OK;
+        default:
+            set_error("ann_ivf_set_option: unknown option %d", option);
+            return ANN_ERR_INVALID;
+    }
+}
+
+int ann_ivf_kernel_profile(ann_ivf* h, double* out8) {
+    ANN_CHECK_ARG(h != nullptr && out8 != nullptr, "null argument");
+    DeviceGuard g(h->device);
+    h->prof.collect();
+    for (int i = 0; i < StageProfiler::kKernels; ++i) {
+        out8[i] = h->prof.kern_ms[i];
+        out8[4 + i] = (double)h->prof.kern_launches[i];
+    }
     return ANN_OK;
 }
 

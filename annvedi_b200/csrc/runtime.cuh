@@ -54,6 +54,15 @@ struct StageProfiler {
     std::vector<Rec> pending;
     std::vector<cudaEvent_t> pool;
     double total_ms[kStages] = {0, 0, 0, 0, 0, 0};
+    // Kernel timers: events around single launches (the largest kernels of a call), by slot.
+    static constexpr int kKernels = 4;
+    struct KRec {
+        cudaEvent_t a, b;
+        int slot;
+    };
+    std::vector<KRec> kpending;
+    double kern_ms[kKernels] = {0, 0, 0, 0};
+    int64_t kern_launches[kKernels] = {0, 0, 0, 0};
     int64_t launches = 0;     // exact-scan launches
     int64_t tc_launches = 0;  // tensor-core GEMM launches
     int64_t filter_launches = 0;  // tensor-core filter passes timed alone
@@ -86,16 +95,54 @@ struct StageProfiler {
     void mark(int rec, cudaStream_t st) {
         if (rec < 0) return;
         std::lock_guard<std::mutex> lk(mu);
+        if (rec >= (int)pending.size()) return;
         Rec& r = pending[rec];
         if (r.first + r.nstage >= kStages) return;
         r.ev[++r.nstage] = get_event();
         cudaEventRecord(r.ev[r.nstage], st);
+    }
+    // kbegin() before a launch, kend(rec, slot) after it: the launch's time goes to kern_ms[slot].
+    int kbegin(cudaStream_t st) {
+        if (!enabled) return -1;
+        std::lock_guard<std::mutex> lk(mu);
+        if (kpending.size() >= kMaxPending) collect_kernels_locked();  // the stage records stay open
+        KRec r{get_event(), nullptr, -1};
+        cudaEventRecord(r.a, st);
+        kpending.push_back(r);
+        return (int)kpending.size() - 1;
+    }
+    void kend(int rec, int slot, cudaStream_t st) {
+        if (rec < 0 || slot < 0 || slot >= kKernels) return;
+        std::lock_guard<std::mutex> lk(mu);
+        if (rec >= (int)kpending.size() || kpending[rec].b != nullptr) return;
+        KRec& r = kpending[rec];
+        r.b = get_event();
+        r.slot = slot;
+        cudaEventRecord(r.b, st);
     }
     void collect() {
         std::lock_guard<std::mutex> lk(mu);
         collect_locked();
     }
     void collect_locked() {
+        collect_kernels_locked();
+        collect_stages_locked();
+    }
+    void collect_kernels_locked() {
+        for (KRec& r : kpending) {
+            if (r.b != nullptr) {
+                cudaEventSynchronize(r.b);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, r.a, r.b);
+                kern_ms[r.slot] += ms;
+                kern_launches[r.slot] += 1;
+                pool.push_back(r.b);
+            }
+            pool.push_back(r.a);
+        }
+        kpending.clear();
+    }
+    void collect_stages_locked() {
         for (Rec& r : pending) {
             for (int s = 0; s < r.nstage; ++s) {
                 cudaEventSynchronize(r.ev[s + 1]);
@@ -112,6 +159,10 @@ struct StageProfiler {
         collect();
         std::lock_guard<std::mutex> lk(mu);
         for (double& t : total_ms) t = 0;
+        for (int i = 0; i < kKernels; ++i) {
+            kern_ms[i] = 0;
+            kern_launches[i] = 0;
+        }
         launches = 0;
         tc_launches = 0;
         filter_launches = 0;
@@ -121,6 +172,10 @@ struct StageProfiler {
         for (cudaEvent_t e : pool) cudaEventDestroy(e);
         for (Rec& r : pending)
             for (int s = 0; s <= r.nstage; ++s) cudaEventDestroy(r.ev[s]);
+        for (KRec& r : kpending) {
+            cudaEventDestroy(r.a);
+            if (r.b) cudaEventDestroy(r.b);
+        }
     }
 };
 

@@ -229,6 +229,7 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                                                                      TcGemmArgs a) {
     constexpr int kCols = kBN / (EPI / 4);  // columns of a tile per epilogue warp
     constexpr bool kFilterOnly = EPI == kFilterEpi;
+    if (a.skip_if_zero && *a.skip_if_zero == 0) return;  // every thread reads the same flag
     extern __shared__ unsigned char smem_raw[];
     // 1024-byte alignment for the swizzled tiles
     unsigned char* smem = smem_raw + ((1024 - (su32(smem_raw) & 1023)) & 1023);

@@ -65,6 +65,9 @@ struct TcGemmArgs {
     // the producer issues no copies, so the waits run out with nothing in flight.
     uint64_t wait_ns = 0;
     int test_no_loads = 0;
+    // If given and *skip_if_zero == 0 (read on the device), the launch does nothing: a pass whose need is
+    // known only on the device, without a host round trip.
+    const int* skip_if_zero = nullptr;
 };
 
 enum TcRole { kTcBase = 0, kTcQuery = 1 };

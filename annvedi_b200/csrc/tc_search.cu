@@ -307,6 +307,111 @@ __global__ void __launch_bounds__(256) warp_bars_kernel(const float* __restrict_
     }
 }
 
+// The digit of rank `rem` (1-based) in a 256-bin histogram and the count of keys below that digit, on
+// every lane of the warp.
+__device__ __forceinline__ void warp_hist_pick(const int* hist, int64_t rem, int* digit, int* before) {
+    const int lane = threadIdx.x & 31;
+    int c[8];
+    int sum = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        c[j] = hist[lane * 8 + j];
+        sum += c[j];
+    }
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int excl = incl - sum;
+    const unsigned hit = __ballot_sync(0xffffffffu, excl < rem && rem <= incl);
+    const int src = hit ? __ffs(hit) - 1 : 31;
+    int d = 255, bf = 0;
+    if (lane == src && hit) {
+        int acc = excl;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if (acc + c[j] >= rem) {
+                d = lane * 8 + j;
+                bf = acc;
+                break;
+            }
+            acc += c[j];
+        }
+    }
+    *digit = __shfl_sync(0xffffffffu, d, src);
+    *before = __shfl_sync(0xffffffffu, bf, src);
+}
+
+// Adds one to hist[digit] for every lane whose key is valid, one atomic per distinct digit of the warp.
+__device__ __forceinline__ void warp_hist_add(int* hist, bool valid, uint32_t digit) {
+    const uint32_t key = valid ? digit : 0xffffffffu;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (valid && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[digit], __popc(peers));
+}
+
+// One 128-thread block per query: bar1 / bar2 = the r1-th / r2-th smallest of keys[offs[q] .. + lens[q]) (+inf
+// where the stream is shorter), both ranks' digits found in the same four 8-bit radix passes. A stream of at most
+// `staged` keys is read once into shared memory (as ordered keys) and the passes run there; a longer one is read
+// from global memory by every pass.
+constexpr int kBarThreads = 128;
+__global__ void __launch_bounds__(kBarThreads) block_bars_kernel(const float* __restrict__ keys,
+                                                                 const int64_t* __restrict__ offs,
+                                                                 const int64_t* __restrict__ lens, int nq, int r1,
+                                                                 int r2, int staged, float* __restrict__ bar1,
+                                                                 float* __restrict__ bar2) {
+    extern __shared__ uint32_t smem_bars[];
+    __shared__ int sHist[2][256];
+    __shared__ int sPick[4];  // digit and count below it, per rank
+    const int q = blockIdx.x;
+    if (q >= nq) return;  // the whole block
+    const int warp = threadIdx.x >> 5;
+    const int64_t n = lens[q];
+    const float* kq = keys + offs[q];
+    const bool in_smem = n <= staged;
+    if (in_smem)
+        for (int64_t p = threadIdx.x; p < n; p += kBarThreads) smem_bars[p] = ord_key(kq[p]);
+    const bool want1 = r1 <= n, want2 = r2 <= n;  // uniform across the block
+    uint32_t p1 = 0, p2 = 0, pmask = 0;
+    int64_t rem1 = r1, rem2 = r2;
+    for (int shift = 24; shift >= 0 && (want1 || want2); shift -= 8) {
+        for (int i = threadIdx.x; i < 512; i += kBarThreads) (&sHist[0][0])[i] = 0;
+        __syncthreads();  // also orders the staging above before the first pass
+        for (int64_t p0 = 0; p0 < n; p0 += kBarThreads) {  // uniform trip count: all lanes take part in the match
+            const int64_t p = p0 + threadIdx.x;
+            const bool ok = p < n;
+            const uint32_t o = ok ? (in_smem ? smem_bars[p] : ord_key(kq[p])) : 0u;
+            const uint32_t dgt = (o >> shift) & 255u;
+            if (want1) warp_hist_add(sHist[0], ok && (o & pmask) == p1, dgt);
+            if (want2) warp_hist_add(sHist[1], ok && (o & pmask) == p2, dgt);
+        }
+        __syncthreads();
+        if (warp < 2 && (warp == 0 ? want1 : want2)) {
+            int d, bf;
+            warp_hist_pick(sHist[warp], warp == 0 ? rem1 : rem2, &d, &bf);
+            if ((threadIdx.x & 31) == 0) {
+                sPick[2 * warp] = d;
+                sPick[2 * warp + 1] = bf;
+            }
+        }
+        __syncthreads();
+        if (want1) {
+            rem1 -= sPick[1];
+            p1 |= (uint32_t)sPick[0] << shift;
+        }
+        if (want2) {
+            rem2 -= sPick[3];
+            p2 |= (uint32_t)sPick[2] << shift;
+        }
+        pmask |= 255u << shift;
+    }
+    if (threadIdx.x == 0) {
+        bar1[q] = want1 ? from_ord(p1) : kInf;
+        bar2[q] = want2 ? from_ord(p2) : kInf;
+    }
+}
+
 // One warp per query: the R smallest of the query's (key, id) buffer [q * cap, + min(count[q], cap)) as a set:
 // every key below the R-th smallest, then the keys equal to it with the lowest ids; padded with
 // (+inf, kNoId) when fewer. Written unordered to out_key / out_id [q * R ..].
@@ -621,10 +726,16 @@ int launch_max_int(const int* v, int n, int* out, cudaStream_t st) {
 }
 
 int launch_warp_bars(const float* keys, const int64_t* offs, const int64_t* lens, int nq, int r1, int r2, float* bar1,
-                     float* bar2, cudaStream_t st) {
+                     float* bar2, cudaStream_t st, int64_t max_len) {
     if (nq == 0) return ANN_OK;
     ANN_CHECK_ARG(r1 >= 1 && r2 >= 1, "bars: ranks %d, %d", r1, r2);
-    warp_bars_kernel<<<(unsigned)ceil_div(nq, 8), 256, 0, st>>>(keys, offs, lens, nq, r1, r2, bar1, bar2);
+    if (max_len > 0) {  // one block per query; streams of up to 6,144 keys (24 KB) staged in shared memory
+        const int staged = (int)std::min<int64_t>(max_len, 6144);
+        block_bars_kernel<<<(unsigned)nq, kBarThreads, (size_t)staged * 4, st>>>(keys, offs, lens, nq, r1, r2, staged,
+                                                                                bar1, bar2);
+    } else {
+        warp_bars_kernel<<<(unsigned)ceil_div(nq, 8), 256, 0, st>>>(keys, offs, lens, nq, r1, r2, bar1, bar2);
+    }
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

@@ -94,8 +94,10 @@ int launch_tc_rerun_bars(const int* mark, const float* tauS, int nq, float* tauR
 int launch_max_int(const int* v, int n, int* out, cudaStream_t st);
 // One warp per query: bar1 / bar2 = the r1-th / r2-th smallest key of keys[offs[q] .. + lens[q]) (exact; +inf
 // where the stream is shorter).
+// With max_len > 0 (a bound of the lens[q]) one block works on each query and streams of up to
+// min(max_len, 6144) keys are staged in shared memory.
 int launch_warp_bars(const float* keys, const int64_t* offs, const int64_t* lens, int nq, int r1, int r2, float* bar1,
-                     float* bar2, cudaStream_t st);
+                     float* bar2, cudaStream_t st, int64_t max_len = 0);
 // One warp per query: the R smallest (key, id) of the buffer [q * cap, + min(count[q], cap)) as a set (the keys
 // below the R-th smallest, then those equal to it by increasing id), padded with (+inf, kNoId), unordered.
 int launch_warp_select(const float* keys, const int* ids, const int* count, int cap, int nq, int R, float* out_key,

@@ -193,6 +193,25 @@ class IVFIndex:
                              "rerank": rerank},
                 "profiled_calls": int(out[6])}
 
+    OPTIONS = {"sample_div": 2, "sampled_min_queries": 3}
+
+    def set_option(self, name: str, value: int) -> None:
+        """Query options (ann_ivf_set_option): "sample_div" (the sampled bars score the first
+        ceil(size / div) rows of each list), "sampled_min_queries" (batch size from which the tensor-core
+        forms take the sampled path). Neither changes results."""
+        if name not in self.OPTIONS:
+            raise RuntimeError(f"unknown option {name!r}")
+        _lib.check(self._lib.ann_ivf_set_option(self._h, self.OPTIONS[name], int(value)))
+
+    def get_kernel_times(self) -> dict:
+        """Single-kernel CUDA-event times of the profiled calls (totals): {slot: {"ms", "launches"}} for
+        the list-keys kernel ("keys"), the sampled bars ("bars"), the best-R selection ("select") and the
+        exact re-rank ("rerank")."""
+        out = (ctypes.c_double * 8)()
+        _lib.check(self._lib.ann_ivf_kernel_profile(self._h, out))
+        return {name: {"ms": float(out[i]), "launches": int(out[4 + i])}
+                for i, name in enumerate(("keys", "bars", "select", "rerank"))}
+
     def reset_profile_results(self) -> None:
         _lib.check(self._lib.ann_ivf_reset_profile(self._h))
 

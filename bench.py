@@ -203,11 +203,10 @@ def _time_steps(fn, steps, stream):
     return e0.elapsed_time(e1)
 
 
-# DRAM traffic per query of the dominant kernels, measured once with ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum, one launch) on this workload at its default sizes: the exact re-rank of the IVF
-# tensor-core form (4.00 GB per 10,000-query launch, R = 300) and the filter pass of the tensor-core exact
-# search (0.878 GB per 5,000-query launch). Other sizes report traffic as null.
-MEASURED_TRAFFIC_PER_QUERY = {"ivf_rerank": 1.40e9 / 10_000, "tc_filter": 0.878e9 / 5_000}
+# DRAM traffic per query of the tensor-core exact search's filter pass, measured once with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum, one launch: 0.878 GB per 5,000-query launch) at the default
+# sizes; other sizes report traffic as null.
+MEASURED_TRAFFIC_PER_QUERY = {"tc_filter": 0.878e9 / 5_000}
 
 WORKLOAD = "1M x 384 zipf mixture (2,048 centres, sigma 0.3, L2-normalised), 10k-query batches, k=100, squared L2"
 DATA = "synthetic (seeded zipf mixture, 2,048 centres, sigma 0.3, L2-normalised)"
@@ -356,54 +355,65 @@ def run_ours(args, rank, world, local):
         build_s = time.perf_counter() - t0
         o_ids = torch.empty(q, K_NN, dtype=torch.int64, device=dev)
         o_d = torch.empty(q, K_NN, dtype=torch.float32, device=dev)
-    # nprobe for each IVF form: the autotuner's cheapest probe count with recall@100 >= 0.95 (re-rank
-    # depth fixed at the configuration's R)
+    # (nprobe, refine_r) of each IVF form: the autotuner's fastest point with recall@100 >= 0.95, and the
+    # tensor-core forms' sampling share
     sweep, sweep_tc = [], []
+    rr_of, div_of = {}, {}
     if sel & ivf_forms:
         from annvedi_b200 import autotune
         modes = [m for m, f in (("exact", "ivf"), ("tc", "ivf_tc"), ("tc_sq8", "ivf_tc_sq8")) if f in sel]
-        tuned = autotune.tune_ivf(ivf, base, queries, kth, K_NN, 0.95, modes=modes, nprobes=(8, 16, 32, 64, 128),
-                                  refines=(args.refine,), reps=2)
+        refines = autotune.IVF_REFINES if args.refine_sweep and not args.nprobe else (args.refine,)
+        nprobes = (args.nprobe,) if args.nprobe else autotune.IVF_NPROBES
+        tuned = autotune.tune_ivf(ivf, base, queries, kth, K_NN, 0.95, modes=modes, nprobes=nprobes,
+                                  refines=refines, reps=2)
 
         def pick(mode):
             rows = [r for r in tuned["table"] if r["mode"] == mode]
-            ok = [r for r in rows if r["recall"] >= 0.95]
-            r = ok[0] if ok else rows[-1]
-            return r["nprobe"], r["recall"], r["qps"], [{"nprobe": x["nprobe"], "recall_at_100": x["recall"],
-                                                         "qps": x["qps"]} for x in rows]
+            r = tuned["best_by_mode"].get(mode) or rows[-1]
+            rr_of[mode] = r["refine_r"]
+            div_of[mode] = r.get("sample_div", 8)
+            return r["nprobe"], r["recall"], r["qps"], [{"nprobe": x["nprobe"], "refine_r": x["refine_r"],
+                                                         "sample_div": x.get("sample_div"),
+                                                         "recall_at_100": x["recall"], "qps": x["qps"]}
+                                                        for x in rows]
     if "ivf" in sel:
         npc, ivf_rec, ivf_qps, sweep = pick("exact")
+        rr_x = rr_of["exact"]
 
         def ivf_step():
-            ivf.search(queries, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids, out_dists=o_d)
+            ivf.search(queries, K_NN, 0, npc, rr_x, max_candidates=0, out_ids=o_ids, out_dists=o_d)
 
         forms["ivf_sq8"] = {
             "qps": ivf_qps, "recall": ivf_rec, "step": ivf_step,
-            "host": lambda: ivf.search(qh, K_NN, 0, npc, args.refine, max_candidates=0, with_dists=False),
-            "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc, args.refine, max_candidates=0, out_ids=o_ids[:1],
+            "host": lambda: ivf.search(qh, K_NN, 0, npc, rr_x, max_candidates=0, with_dists=False),
+            "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc, rr_x, max_candidates=0, out_ids=o_ids[:1],
                                             with_dists=False),
-            "lat_host": lambda x: ivf.search(x, K_NN, 0, npc, args.refine, max_candidates=0, with_dists=False),
+            "lat_host": lambda x: ivf.search(x, K_NN, 0, npc, rr_x, max_candidates=0, with_dists=False),
             "dtype": "f32 (sq8 codes, fp32 re-rank)",
-            "config": {"form": "ivf-sq8 exact selection", "n_lists": 2048, "nprobe": npc, "refine_r": args.refine,
+            "config": {"form": "ivf-sq8 exact selection", "n_lists": 2048, "nprobe": npc, "refine_r": rr_x,
                        "candidate_cap": "none"},
         }
 
     # ---- IVF on the tensor cores: the same lists scored by grouped BF16 tcgen05 GEMMs ----
     if "ivf_tc" in sel:
         npc_tc, tc_rec, tc_qps, sweep_tc = pick("tc")
+        rr_t = rr_of["tc"]
 
         def ivf_tc_step():
-            ivf.search(queries, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc", out_ids=o_ids, out_dists=o_d)
+            ivf.set_option("sample_div", div_of["tc"])
+            ivf.search(queries, K_NN, 0, npc_tc, rr_t, max_candidates=0, mode="tc", out_ids=o_ids, out_dists=o_d)
 
         forms["ivf_tc"] = {
             "qps": tc_qps, "recall": tc_rec, "step": ivf_tc_step,
-            "host": lambda: ivf.search(qh, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc", with_dists=False),
-            "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc",
+            "host": lambda: (ivf.set_option("sample_div", div_of["tc"]),
+                             ivf.search(qh, K_NN, 0, npc_tc, rr_t, max_candidates=0, mode="tc", with_dists=False)),
+            "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc_tc, rr_t, max_candidates=0, mode="tc",
                                             out_ids=o_ids[:1], with_dists=False),
-            "lat_host": lambda x: ivf.search(x, K_NN, 0, npc_tc, args.refine, max_candidates=0, mode="tc",
+            "lat_host": lambda x: ivf.search(x, K_NN, 0, npc_tc, rr_t, max_candidates=0, mode="tc",
                                              with_dists=False),
             "dtype": "bf16 (tcgen05 list keys, fp32 accumulate, exact fp32 re-rank)",
-            "config": {"form": "ivf on tensor cores", "n_lists": 2048, "nprobe": npc_tc, "refine_r": args.refine,
+            "config": {"form": "ivf on tensor cores", "n_lists": 2048, "nprobe": npc_tc, "refine_r": rr_t,
+                       "sample_div": div_of["tc"],
                        "candidate_cap": "none"},
         }
 
@@ -411,22 +421,25 @@ def run_ours(args, rank, world, local):
     sweep_sq8 = []
     if "ivf_tc_sq8" in sel:
         npc_q, q_rec, q_qps, sweep_sq8 = pick("tc_sq8")
+        rr_q = rr_of["tc_sq8"]
 
         def ivf_q_step():
-            ivf.search(queries, K_NN, 0, npc_q, args.refine, max_candidates=0, mode="tc_sq8", out_ids=o_ids,
+            ivf.set_option("sample_div", div_of["tc_sq8"])
+            ivf.search(queries, K_NN, 0, npc_q, rr_q, max_candidates=0, mode="tc_sq8", out_ids=o_ids,
                        out_dists=o_d)
 
         forms["ivf_tc_sq8"] = {
             "qps": q_qps, "recall": q_rec, "step": ivf_q_step,
-            "host": lambda: ivf.search(qh, K_NN, 0, npc_q, args.refine, max_candidates=0, mode="tc_sq8",
-                                       with_dists=False),
-            "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc_q, args.refine, max_candidates=0, mode="tc_sq8",
+            "host": lambda: (ivf.set_option("sample_div", div_of["tc_sq8"]),
+                             ivf.search(qh, K_NN, 0, npc_q, rr_q, max_candidates=0, mode="tc_sq8", with_dists=False)),
+            "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc_q, rr_q, max_candidates=0, mode="tc_sq8",
                                             out_ids=o_ids[:1], with_dists=False),
-            "lat_host": lambda x: ivf.search(x, K_NN, 0, npc_q, args.refine, max_candidates=0, mode="tc_sq8",
+            "lat_host": lambda x: ivf.search(x, K_NN, 0, npc_q, rr_q, max_candidates=0, mode="tc_sq8",
                                              with_dists=False),
             "dtype": "u8 x s8 (tcgen05 kind::i8 over the SQ8 codes, int32 accumulate, exact fp32 re-rank)",
             "config": {"form": "ivf-sq8 codes on tensor cores", "n_lists": 2048, "nprobe": npc_q,
-                       "refine_r": args.refine, "candidate_cap": "none"},
+                       "sample_div": div_of["tc_sq8"],
+                       "refine_r": rr_q, "candidate_cap": "none"},
         }
 
     # ---- the headline: the fastest form at recall@100 >= 0.95 (or the one asked for) ----
@@ -483,7 +496,7 @@ def run_ours(args, rank, world, local):
                for name, f in forms.items()}
     if "ivf" in sel:  # the IVF-SQ8 query of one query replayed as a CUDA graph
         from annvedi_b200 import graphs
-        gi = graphs.ivf_exact(ivf, 1, K_NN, npc, args.refine, local)
+        gi = graphs.ivf_exact(ivf, 1, K_NN, npc, rr_x, local)
         lat = []
         for i in range(args.latency_queries):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -514,42 +527,17 @@ def run_ours(args, rank, world, local):
                   "select": stt["tc_select_ms"], "rerank": stt["rerank_ms"]}
         stage_ms = {k2: round(v / args.steps, 4) for k2, v in stages.items()}
         extra = {"gemm_launches_per_batch": round(stt["tc_gemm_launches"] / args.steps, 2)}
-    elif head in ("ivf_tc", "ivf_tc_sq8"):
-        prof = ivf.get_profile_results()
-        stage = prof.get("stage_ms", {})
-        calls = max(1, prof.get("profiled_calls", 1))
-        rr_ms = stage.get("rerank", 0.0) / calls
-        r_eff = min(args.refine, int(cands_timed / max(1, args.steps) / q))
-        bytes_per_launch = q * r_eff * d * 4 + q * r_eff * 8  # the candidates' FP32 rows, their keys and ids
-        achieved = bytes_per_launch / (rr_ms / 1e3) / 1e9 if rr_ms > 0 else 0.0
-        default_size = (n, d, q, args.refine) == (1_000_000, 384, 10_000, 300)
-        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(achieved / hbm_peak, 4), "peak_kind": peak_kind,
-                "traffic": MEASURED_TRAFFIC_PER_QUERY["ivf_rerank"] * q if default_size else None,
-                "traffic_unit": "bytes per launch",
-                "kernel": "ivf_rerank_kernel (exact FP32 re-rank, the largest kernel of this form)",
-                "bytes_per_launch": int(bytes_per_launch), "kernel_ms": round(rr_ms, 4)}
-        if roof["traffic"]:
-            # queries run grouped by first probed list, so most gathered rows come from L2: the DRAM side
-            roof["dram_achieved"] = round(roof["traffic"] / (rr_ms / 1e3) / 1e9, 1) if rr_ms > 0 else None
-            roof["dram_frac"] = round(roof["dram_achieved"] / hbm_peak, 4) if roof["dram_achieved"] else None
-            roof["note"] = ("achieved counts the algorithmic bytes (every candidate row once); the measured DRAM "
-                            "traffic is lower because candidate rows shared by queries of the same lists hit L2")
-        stage_ms = {k2: round(v / calls, 4) for k2, v in stage.items()}
-        extra = {"candidates_per_query": round(cands_timed / max(1, args.steps) / q, 1)}
     else:
         prof = ivf.get_profile_results()
         stage = prof.get("stage_ms", {})
         calls = max(1, prof.get("profiled_calls", 1))
-        sq8_ms = stage.get("keys", 0.0) / calls
-        cands = cands_timed
-        bytes_per_launch = (cands / max(1, args.steps)) * d
-        achieved = bytes_per_launch / (sq8_ms / 1e3) / 1e9 if sq8_ms > 0 else 0.0
-        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(achieved / hbm_peak, 4), "traffic": None, "peak_kind": peak_kind,
-                "kernel": "ivf_batched_kernel", "bytes_per_launch": int(bytes_per_launch), "kernel_ms": round(sq8_ms, 4)}
         stage_ms = {k2: round(v / calls, 4) for k2, v in stage.items()}
-        extra = {"candidates_per_query": round(cands / max(1, args.steps) / q, 1)}
+        cands = cands_timed / max(1, args.steps)  # candidate rows scored per batch
+        extra = {"candidates_per_query": round(cands / q, 1)}
+        kern = ivf.get_kernel_times()
+        roof = ivf_roofline(head, kern, cands, q, d, hf["config"]["refine_r"], hbm_peak, bf16_peak, peak_kind,
+                            unique_rows=_unique_candidate_rows(ivf, queries, hf))
+        extra["kernel_ms_per_batch"] = {k2: round(v["ms"] / max(1, args.steps), 4) for k2, v in kern.items()}
 
     summary = {name: {"qps": round(f["qps"], 1), "recall_at_100": round(f["recall"], 4),
                       "speedup_vs_plain_fp32_scan": round(f["qps"] / flat_qps, 2) if flat_qps else None,
@@ -567,7 +555,7 @@ def run_ours(args, rank, world, local):
         "forms": summary,
         "plain_fp32_scan": flat_line,
         "nprobe_sweep": {"ivf_sq8": sweep, "ivf_tc": sweep_tc, "ivf_tc_sq8": sweep_sq8,
-                         "chosen_by": "annvedi_b200.autotune.tune_ivf (cheapest nprobe with recall@100 >= 0.95)"},
+                         "chosen_by": "annvedi_b200.autotune.tune_ivf (fastest nprobe x refine_r x sample_div with recall@100 >= 0.95)"},
         "latency_ms_batch1": latency,
         "ivf_build_s": round(build_s, 3) if build_s is not None else None,
         "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": q * d * 4,
@@ -579,7 +567,8 @@ def run_ours(args, rank, world, local):
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and ivf is not None:
-        line["cpu_baseline"] = cpu_baseline_ivf(ivf, queries, npc if npc is not None else npc_tc, args)
+        line["cpu_baseline"] = cpu_baseline_ivf(ivf, queries, hf["config"].get("nprobe", npc_tc),
+                                                 hf["config"].get("refine_r", args.refine), args)
     if rank == 0 and world == 1 and args.gf:
         try:
             line["gpu_filter_dropin"] = gf_dropin_c3(args, base, queries, kth)
@@ -589,9 +578,10 @@ def run_ours(args, rank, world, local):
         line["scaled_fp8_4m_256"] = scaled_fp8_c4(args, local)
     if rank == 0 and world == 1 and args.serve_seconds > 0 and (npc is not None or "ivf_tc" in forms):
         if "ivf_tc" in forms:
-            line["serving"] = serving_c5(args, local, ivf, forms["ivf_tc"]["config"]["nprobe"], w, "tc")
+            line["serving"] = serving_c5(args, local, ivf, forms["ivf_tc"]["config"]["nprobe"], w, "tc",
+                                         forms["ivf_tc"]["config"]["refine_r"])
         else:
-            line["serving"] = serving_c5(args, local, ivf, npc, w, "exact")
+            line["serving"] = serving_c5(args, local, ivf, npc, w, "exact", rr_x)
     if rank == 0 and world == 1 and args.lsh and ivf is not None:
         line["ivf_lsh_tables"] = lsh_tables_c3(args, ivf, w)
     if rank == 0 and world == 1 and args.dropin:
@@ -599,7 +589,68 @@ def run_ours(args, rank, world, local):
     return line
 
 
-def serving_c5(args, local, ivf, npc, w3, ivf_mode="tc"):
+def _unique_candidate_rows(ivf, queries, hf):
+    """Distinct base rows among the batch's best-R candidate sets: the search asked for k = R returns
+    exactly the R candidates it re-ranks (the re-rank only orders them)."""
+    import torch
+    cfg = hf["config"]
+    mode = {"ivf on tensor cores": "tc", "ivf-sq8 codes on tensor cores": "tc_sq8"}.get(cfg["form"], "exact")
+    if "sample_div" in cfg:
+        ivf.set_option("sample_div", cfg["sample_div"])
+    ids, _ = ivf.search(queries, cfg["refine_r"], 0, cfg["nprobe"], cfg["refine_r"], max_candidates=0, mode=mode,
+                        with_dists=False)
+    return int(torch.unique(ids[ids >= 0]).numel())
+
+
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant kernel, measured once
+# with ncu on this workload at its tuned configuration, keyed by (form, kernel slot); other configurations
+# report null.
+MEASURED_TRAFFIC = {}
+
+
+def ivf_roofline(head, kern, cands, q, d, R, hbm_peak, bf16_peak, peak_kind, unique_rows):
+    """Roofline of the dominant kernel of an IVF form: the kernel with the largest CUDA-event time among the
+    list-keys kernel, the sampled bars, the best-R selection and the exact re-rank, each timed live around
+    its own launches. Algorithmic work per launch counts each item once:
+      keys (tensor-core forms): 2 x candidate rows x dim multiply-adds against the dense tensor peak (BF16:
+        the measured cuBLAS burst figure; int8: twice it, the B200's int8-to-BF16 rate ratio);
+      keys (SQ8 batched kernel): the candidates' code bytes (dim per row) against HBM;
+      bars: the sampled keys (4 bytes each, a 1/sample_div share of the candidates; 1/8 is counted);
+      select: the survivors' (key, row) pairs (about 3 R per query, 8 bytes); rerank: the distinct candidate
+      rows' FP32 vectors plus the keys and ids in and the top-k out."""
+    name = max(kern, key=lambda s2: kern[s2]["ms"])
+    ms = kern[name]["ms"] / max(1, kern[name]["launches"])
+    kname = {"keys": "tc_gemm_kernel (grouped list GEMM)" if head != "ivf_sq8" else "ivf_batched_kernel",
+             "bars": "block_bars_kernel", "select": "warp_select_kernel / radix_select_kernel",
+             "rerank": "ivf_rerank_kernel"}[name]
+    if name == "keys" and head != "ivf_sq8":
+        flops = 2.0 * cands * d
+        i8 = head == "ivf_tc_sq8"
+        peak = bf16_peak * (2 if i8 else 1)
+        achieved = flops / (ms / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": round(achieved, 1), "peak": round(peak, 1), "unit": "TFLOP/s",
+                "frac": round(achieved / peak, 4), "flops_per_launch": flops,
+                "peak_kind": (f"2 x {peak_kind} bf16 burst (int8 dense rate)" if i8 else f"{peak_kind} bf16 burst")}
+    else:
+        if name == "keys":
+            nbytes = cands * d
+        elif name == "bars":
+            nbytes = 4.0 * cands / 8
+        elif name == "select":
+            nbytes = 8.0 * 3 * R * q
+        else:
+            nbytes = unique_rows * d * 4.0 + q * R * 8.0 + q * K_NN * 12.0
+        achieved = nbytes / (ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(achieved / hbm_peak, 4), "bytes_per_launch": int(nbytes), "peak_kind": peak_kind}
+    roof.update({"kernel": kname, "kernel_ms": round(ms, 4), "launches": kern[name]["launches"],
+                 "traffic": MEASURED_TRAFFIC.get((head, name)), "traffic_unit": "bytes per launch",
+                 "unique_candidate_rows": unique_rows,
+                 "timing": "CUDA events around each launch of the kernel on its stream, over the timed steps"})
+    return roof
+
+
+def serving_c5(args, local, ivf, npc, w3, ivf_mode="tc", refine_r=300):
     """The serving configuration: two device-resident indexes -- the IVF index over the 1M x 384
     zipf mixture (the headline data set; its lists scored on the tensor cores, ivf_mode "tc", or by SQ8
     keys, "exact"; exact FP32 re-rank either way) and an exact 1M x 768 inner-product index (1,024-centre
@@ -645,7 +696,7 @@ def serving_c5(args, local, ivf, npc, w3, ivf_mode="tc"):
           "recall_at_100": round(float(np.mean(hit)), 4)}
     ivf_name = "ivf_tc_384" if ivf_mode == "tc" else "ivf_sq8_384"
     pools = {ivf_name: w3.queries.cpu().numpy(), "exact_ip_768": w2.queries.cpu().numpy()}
-    routes = [serving.ivf_route(ivf_name, ivf, npc, args.refine, mode=ivf_mode),
+    routes = [serving.ivf_route(ivf_name, ivf, npc, refine_r, mode=ivf_mode),
               serving.tc_route("exact_ip_768", exact, refine_r=400)]
     srv = serving.Server(routes, device=local, workers=3, max_batch=4096).start()
     out = []
@@ -689,7 +740,7 @@ def serving_c5(args, local, ivf, npc, w3, ivf_mode="tc"):
         srv.stop()
     del exact
     torch.cuda.empty_cache()
-    return {"config": f"IVF 1M x 384 ({ivf_mode} keys, nprobe {npc}, R {args.refine}; 70%) + exact IP 1M x 768 "
+    return {"config": f"IVF 1M x 384 ({ivf_mode} keys, nprobe {npc}, R {refine_r}; 70%) + exact IP 1M x 768 "
                       "tensor-core form (30%); Poisson arrivals, "
                       "request sizes geometric(0.1) capped at 256, k=100, 3 workers, admission by free HBM",
             "runs": out, "exact_ip_768_batch": c2}
@@ -940,21 +991,21 @@ def gf_dropin_c3(args, base, queries, kth):
         lib.gf_free(h)
 
 
-def cpu_baseline_ivf(ivf, queries, npc, args):
-    """Reference IVF query on the host cores over a bounded sample. refine_r is raised until the
-    reference's candidate cap (max(2000, 4 * refine_r)) no longer truncates the probed lists, so it
-    does the same search (and reaches the same recall) as the GPU form."""
+def cpu_baseline_ivf(ivf, queries, npc, refine_r, args):
+    """The reference's IVF query (ivf_lsh_cpp, oracle/_ref) on the host cores over a bounded sample, at the
+    headline form's nprobe and refine_r; the reference keeps its own candidate cap (max(2000, 4 * refine_r)),
+    as its stock path does."""
     ix, st = _reference_ivf_from(ivf)
     qs = queries[: args.cpu_sample].cpu().numpy()
-    ix.query(qs[0], K_NN, 0, npc, args.refine)
+    ix.query(qs[0], K_NN, 0, npc, refine_r)
     t0 = time.perf_counter()
     for qq in qs:
-        ix.query(qq, K_NN, 0, npc, args.refine)
+        ix.query(qq, K_NN, 0, npc, refine_r)
     dt = time.perf_counter() - t0
     cores = os.cpu_count() or 1
     return {"value": round(len(qs) / dt, 2), "unit": "queries/s", "cores": cores, "kind": "reference",
             "sample": f"{len(qs)} queries one at a time (the harness's pattern), ivf_lsh_cpp LSHIndex over this "
-                      f"index's state, n_probe_clusters={npc}, refine_r={args.refine} (its own candidate cap), "
+                      f"index's state, n_probe_clusters={npc}, refine_r={refine_r} (its own candidate cap), "
                       f"ThreadPool of {cores}"}
 
 
@@ -1045,7 +1096,7 @@ def run_reference(args, rank, world):
     rr = np.maximum(args.refine, -(-_probed_sizes(st, qs, npc) // 4))
     kth = _kth_f64_np(w.base, qs, K_NN)
 
-    def timed(refines):
+    def timed(refines, npc=npc):
         for i in range(min(args.warmup, len(qs))):
             ix.query(qs[i], K_NN, 0, npc, int(refines[i]))
         ix.reset_distances_count()
@@ -1062,13 +1113,18 @@ def run_reference(args, rank, world):
                 "recall_at_100": _recall_np(w.base, qs, np.stack(out), kth),
                 "candidates_per_query": ix.total_distances_count() // (len(qs) * args.steps)}
 
-    variants = {
-        "stock_refine_r": {**timed(np.full(len(qs), args.refine)), "refine_r": args.refine,
-                           "note": "the reference's own cap max(2000, 4 * refine_r) stops the probe loop early"},
-        "cap_lifted": {**timed(rr), "refine_r": f"per query max({args.refine}, ceil(probed rows / 4)), "
-                                                f"mean {float(rr.mean()):.0f}",
-                       "note": "every probed list scanned, as the GPU forms do; a quarter of the candidates re-ranked"},
-    }
+    # the stock path at the probe counts and re-rank depths the other arm's autotuner sweeps (its cap stays
+    # max(2000, 4 R)), and the cap lifted at --ref-nprobe
+    variants = {}
+    for np0 in (sorted({2, 3, 4, 6, npc}) if args.refine_sweep else (npc,)):
+        for r0 in ((100, 150, 200, 300) if args.refine_sweep else (args.refine,)):
+            variants[f"stock_nprobe_{np0}_refine_r_{r0}"] = {
+                **timed(np.full(len(qs), r0), np0), "nprobe": np0, "refine_r": r0,
+                "note": "the reference's own cap max(2000, 4 * refine_r) stops the probe loop early"}
+    variants["cap_lifted"] = {
+        **timed(rr), "nprobe": npc,
+        "refine_r": f"per query max({args.refine}, ceil(probed rows / 4)), mean {float(rr.mean()):.0f}",
+        "note": "every probed list scanned, as the GPU forms do; a quarter of the candidates re-ranked"}
     ok = {k2: v for k2, v in variants.items() if v["recall_at_100"] >= 0.95} or variants
     head = max(ok, key=lambda k2: ok[k2]["qps"])
     qps, rec = variants[head]["qps"], variants[head]["recall_at_100"]
@@ -1089,14 +1145,15 @@ def run_reference(args, rank, world):
                 "recall_at_100": round(_recall_np(lw.base, lw.queries, lids, _kth_f64_np(lw.base, lw.queries, K_NN)), 4),
                 "workload": "100k x 384 unit rows (N(0,1), normalised), 1,000 queries, k=100 (linear_ann_cpp)"}
     sample = (f"{len(qs)} queries per step one at a time, ivf_lsh_cpp LSHIndex (oracle/_ref) over the same 2,048 lists "
-              f"(state built by the oracle), n_probe_clusters={npc}, {head} (the faster of the reference's variants "
+              f"(state built by the oracle), {head} (the fastest of the reference's variants "
               f"at recall@100 >= 0.95), ThreadPool of {cores}")
     line = {"metric": METRIC, "value": round(qps, 2), "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (sq8 codes, fp32 re-rank)",
             "data": DATA,
             "config": {"workload": WORKLOAD, "form": "reference cpu (ivf_lsh_cpp)",
-                       "n": args.n, "dim": args.dim, "batch": len(qs), "k": K_NN, "nprobe": npc, "variant": head},
+                       "n": args.n, "dim": args.dim, "batch": len(qs), "k": K_NN, "nprobe": variants[head]["nprobe"],
+                       "refine_r": variants[head]["refine_r"], "variant": head},
             "impl": "reference",
             "recall_at_100": round(rec, 4),
             "cpu_baseline": {"value": round(qps, 2), "unit": "queries/s", "cores": cores, "kind": "reference",
@@ -1129,7 +1186,13 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--refine", type=int, default=300)
+    ap.add_argument("--refine", type=int, default=300,
+                    help="re-rank depth of the reference arm's capped variants and, with --no-refine-sweep or "
+                         "--nprobe, of the IVF forms")
+    ap.add_argument("--no-refine-sweep", dest="refine_sweep", action="store_false",
+                    help="the autotuners of both arms keep refine_r at --refine instead of sweeping it")
+    ap.add_argument("--nprobe", type=int, default=0,
+                    help="IVF forms at this nprobe and --refine, without the autotuner's sweep (for profiling)")
     ap.add_argument("--tc-refine", type=int, default=400)
     ap.add_argument("--form", choices=["auto", "tc", "ivf", "ivf_tc", "ivf_tc_sq8"], default="auto")
     ap.add_argument("--forms", default="plain,tc,ivf,ivf_tc,ivf_tc_sq8",

@@ -261,6 +261,20 @@ int ann_ivf_reset_distances(ann_ivf* h);
  * re-rank + top-k ms, profiled calls, queries}. Totals, not averages. */
 int ann_ivf_set_profiling(ann_ivf* h, int32_t enable);
 int ann_ivf_profile(ann_ivf* h, double* out8);
+/* Query options of an index (no counterpart in the reference, whose query takes its settings as
+ * arguments); none of them changes results:
+ *   ANN_IVF_OPT_SAMPLE_DIV: the tensor-core forms' sampled bars score the first ceil(size / value) rows of
+ *     each probed list (2..64, default 8); the bars only prune.
+ *   ANN_IVF_OPT_SAMPLED_MIN: batches of at least this many queries take the sampled path (default 256). */
+#define ANN_IVF_OPT_SAMPLE_DIV 2
+#define ANN_IVF_OPT_SAMPLED_MIN 3
+int ann_ivf_set_option(ann_ivf* h, int32_t option, int64_t value);
+
+/* Single-kernel times of the same profiled calls (CUDA events around each launch, on the query stream):
+ * out8 = {list-keys kernel ms (the grouped tensor-core GEMM of the list rows, or the SQ8 batched
+ * kernel), sampled-bar kernel ms, best-R selection kernel ms, FP32 re-rank kernel ms, then the launch
+ * count of each}. Totals; cleared by ann_ivf_reset_profile. No counterpart in the reference. */
+int ann_ivf_kernel_profile(ann_ivf* h, double* out8);
 int ann_ivf_reset_profile(ann_ivf* h);
 
 #ifdef __cplusplus

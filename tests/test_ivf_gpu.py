@@ -419,3 +419,46 @@ def test_lsh_gpu_build_matches_reference_tables(cuda):
 
     same = np.mean(bucket_of_row(got) == bucket_of_row(want))
     assert same > 0.999, same
+
+
+@pytest.mark.parametrize("mode", ["tc", "tc_sq8"])
+def test_sample_divisor_does_not_change_results(cuda, mode):
+    """The sampled bars over 1/4, 1/8 or 1/16 of each probed list (ANN_IVF_OPT_SAMPLE_DIV) only prune: the
+    result is the same id for id and bit for bit; out-of-range values are refused."""
+    w = synth.zipf_mixture(60000, 128, 3000, c=128, lo=20, hi=5000, seed=31)
+    st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
+    ix = _ivf(mode=mode)
+    ix.import_state(st)
+    want_i, want_d = ix.search(w.queries, 100, 0, 6, 150)
+    for div in (4, 16, 2):
+        ix.set_option("sample_div", div)
+        got_i, got_d = ix.search(w.queries, 100, 0, 6, 150)
+        np.testing.assert_array_equal(got_i, want_i)
+        np.testing.assert_array_equal(got_d, want_d)
+    with pytest.raises(Exception):
+        ix.set_option("sample_div", 1)
+    with pytest.raises(Exception):
+        ix.set_option("sampled_min_queries", 0)
+
+
+def test_kernel_timers_count_the_profiled_launches(cuda):
+    """ann_ivf_kernel_profile: CUDA-event times of the list-keys, bars, selection and re-rank launches of
+    the profiled calls, cleared by reset_profile_results."""
+    import torch
+    w = synth.zipf_mixture(40000, 128, 600, c=96, lo=20, hi=4000, seed=8)
+    st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
+    ix = _ivf(mode="tc")
+    ix.import_state(st)
+    q = torch.from_numpy(w.queries).cuda()
+    ix.search(q, 100, 0, 8, 200)
+    ix.reset_profile_results()
+    ix.set_profiling(True)
+    for _ in range(3):
+        ix.search(q, 100, 0, 8, 200)
+    ix.set_profiling(False)
+    kt = ix.get_kernel_times()
+    assert kt["keys"]["launches"] == 3 and kt["select"]["launches"] == 3 and kt["rerank"]["launches"] == 3
+    assert kt["bars"]["launches"] == 3
+    assert all(v["ms"] > 0 for v in kt.values())
+    ix.reset_profile_results()
+    assert all(v["launches"] == 0 for v in ix.get_kernel_times().values())
