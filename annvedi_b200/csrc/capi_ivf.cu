@@ -1060,27 +1060,37 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     // n rows. The main pass sees them as empty streams; each is redone below on its own, split over the
     // whole GPU. (Small exact batches already split every query that widely and skip the host read.)
     std::vector<int> every_row;
-    if (c.fallback && (c.ref || c.nsplit < kEveryRowMinSplit)) {
+    auto take_every_row = [&]() -> int {
         std::vector<int32_t> ns(nq);
         ANN_CUDA_TRY(cudaMemcpyAsync(ns.data(), n_seg, sizeof(int32_t) * (size_t)nq, cudaMemcpyDeviceToHost, st));
         ANN_CUDA_TRY(cudaStreamSynchronize(st));
         for (int i = 0; i < nq; ++i)
             if (ns[i] < 0) every_row.push_back(i);
         if (!every_row.empty()) {
-            if ((rc = launch_clear_every_row(a.plan, st))) return rc;
+            int r = launch_clear_every_row(a.plan, st);
+            if (r) return r;
             const int64_t len = h->n;
             const int32_t seg = -1;
             ANN_CUDA_TRY(cudaMemcpyAsync(every_len, &len, sizeof(len), cudaMemcpyHostToDevice, st));
             ANN_CUDA_TRY(cudaMemcpyAsync(every_seg, &seg, sizeof(seg), cudaMemcpyHostToDevice, st));
             ANN_CUDA_TRY(cudaStreamSynchronize(st));  // the host values above live on this frame
         }
-    }
+        return ANN_OK;
+    };
+    const bool every_row_apart = c.fallback && (c.ref || c.nsplit < kEveryRowMinSplit);
+    // batched passes learn of every-row queries from the batch set-up's own host read (below), so the common
+    // case takes no extra round trip here
+    if (every_row_apart && !(c.batched && !c.ref) && (rc = take_every_row())) return rc;
     // 3. SQ8 pass -> best R per query
     bool done = false;
     if (!c.ref && c.batched) {
         IvfBatchArgs b{};
         int64_t tot[3] = {0, 0, 0};
         if ((rc = batched_prepare(a, bscratch, c.sort_tmp, c.scan_tmp, &b, tot, st))) return rc;
+        if (tot[2] != 0 && every_row_apart) {  // every-row queries: set apart, then the batch set up again
+            if ((rc = take_every_row())) return rc;
+            if ((rc = batched_prepare(a, bscratch, c.sort_tmp, c.scan_tmp, &b, tot, st))) return rc;
+        }
         bool sampled_done = false;
         if (tot[2] == 0 && c.tc && nq >= h->sampled_min_queries) {
             if ((rc = ivf_tc_sampled(h, ws, c, a, b, tc_operands(h, c, qb, q8, qfac, pfac), Apk, titem, titem_list,

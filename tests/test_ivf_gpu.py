@@ -462,3 +462,27 @@ def test_kernel_timers_count_the_profiled_launches(cuda):
     assert all(v["ms"] > 0 for v in kt.values())
     ix.reset_profile_results()
     assert all(v["launches"] == 0 for v in ix.get_kernel_times().values())
+
+
+@pytest.mark.parametrize("mode", ["exact", "tc"])
+def test_batch_with_every_row_queries_equals_alone(cuda, mode):
+    """A batch of 300 queries, some of whose probed lists hold fewer than k rows (those scan every row, as
+    the reference does): the batch sets them apart after its own set-up and redoes them over the whole GPU;
+    every query's ids and distances equal those of the query run alone."""
+    from tests.helpers import assert_ids_equal_up_to_ties
+    w = synth.zipf_mixture(30000, 64, 300, c=300, lo=5, hi=1500, seed=12)
+    st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
+    ix = _ivf(mode=mode)
+    ix.import_state(st)
+    k, npc, rr = 40, 1, 100
+    ids, d = ix.search(w.queries, k, 0, npc, rr)
+    alone_i, alone_d, every = [], [], 0
+    for i in range(len(w.queries)):
+        ix.reset_distances_count()
+        oi, od = ix.search(w.queries[i:i + 1], k, 0, npc, rr)
+        every += ix.total_distances_count() == w.base.shape[0]
+        alone_i.append(oi[0])
+        alone_d.append(od[0])
+    assert 0 < every < len(w.queries), every
+    assert_ids_equal_up_to_ties(w.base, w.queries, ids, np.stack(alone_i), rtol=1e-6)
+    np.testing.assert_allclose(d, np.stack(alone_d), rtol=1e-6, atol=1e-7)
