@@ -755,7 +755,7 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
         sz.take<float>((size_t)nq * c.npc);
         sz.take<int64_t>((size_t)nq * c.npc);
         sz.take<int64_t>((size_t)h->C + 1);
-        sz.take<int32_t>((size_t)tc_items_bound((int64_t)nq * c.npc, (int)h->C, h->sizes_desc[0]));
+        sz.take<int4>((size_t)tc_items_bound((int64_t)nq * c.npc, (int)h->C, h->sizes_desc[0]));
     }
     sz.take<int32_t>((size_t)nq);  // re-rank query order
     sz.take<int64_t>(1);           // an every-row stream: its length
@@ -797,7 +797,7 @@ constexpr int kRowCapFactor = 16;
 
 static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, const IvfQueryArgs& a,
                           const IvfBatchArgs& b, const TcOperands& op, unsigned char* Apk, int64_t* titem,
-                          int32_t* titem_list, int64_t items_cap, float* keyR, int* idR, int prec, bool* done,
+                          int4* titem_desc, int64_t items_cap, float* keyR, int* idR, int prec, bool* done,
                           cudaStream_t st) {
     *done = false;
     const int nq = a.plan.nq, npc = c.npc, C = (int)h->C, R = c.R;
@@ -818,7 +818,7 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     sz.take<int64_t>((size_t)nq + 1);            // soff
     sz.take<char>(scan_tmp);
     sz.take<int64_t>((size_t)C + 1);             // sample items
-    sz.take<int32_t>((size_t)scap);
+    sz.take<int4>((size_t)scap);
     sz.take<int64_t>((size_t)max_pairs);         // sdbase
     sz.take<int32_t>((size_t)max_pairs);         // row -> query
     sz.take<float>((size_t)s_bound);             // sample keys
@@ -836,7 +836,7 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     int64_t* soff = cv.take<int64_t>((size_t)nq + 1);
     void* stmp = cv.take<char>(scan_tmp);
     int64_t* sitem = cv.take<int64_t>((size_t)C + 1);
-    int32_t* sitem_list = cv.take<int32_t>((size_t)scap);
+    int4* sitem_desc = cv.take<int4>((size_t)scap);
     int64_t* sdbase = cv.take<int64_t>((size_t)max_pairs);
     int32_t* rowq = cv.take<int32_t>((size_t)max_pairs);
     float* SK = cv.take<float>((size_t)s_bound);
@@ -867,7 +867,7 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
         return rc;
     // 1. sample pass: keys of the list heads into the sample streams; the two bars per query
     if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, C, sitem, st, lcap))) return rc;
-    if ((rc = launch_tc_item_lists(sitem, C, sitem_list, scap, st))) return rc;
+    if ((rc = launch_tc_item_descs(sitem, C, b.lq_off, h->list_off, lcap, sitem_desc, scap, st))) return rc;
     TcGemmArgs gs{(int)max_pairs, (int)h->n, op.K, nullptr, SK, 0, h->d_err};
     gs.kind = op.kind;
     gs.col_fac = op.col_fac;
@@ -879,14 +879,14 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
     gs.g_dbase = sdbase;
     gs.g_total = sitem + C;
     gs.g_lists = C;
-    gs.g_item_list = sitem_list;
+    gs.g_item_desc = sitem_desc;
     if ((rc = launch_tc_gemm(Apk, op.B, gs, st))) return rc;
     int kt = h->prof.kbegin(st);
     if ((rc = launch_warp_bars(SK, soff, slen, nq, rF, R, tauF, tauS, st, (int64_t)npc * head_max))) return rc;
     h->prof.kend(kt, kKernBars, st);
     // 2. filter pass over every row of the probed lists into the queries' buffers
     if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, C, titem, st))) return rc;
-    if ((rc = launch_tc_item_lists(titem, C, titem_list, items_cap, st))) return rc;
+    if ((rc = launch_tc_item_descs(titem, C, b.lq_off, h->list_off, nullptr, titem_desc, items_cap, st))) return rc;
     auto filter = [&](const float* tau, const int* skip_if_zero) -> int {
         TcGemmArgs g{(int)max_pairs, (int)h->n, op.K, nullptr, nullptr, 0, h->d_err};
         g.skip_if_zero = skip_if_zero;
@@ -898,7 +898,7 @@ static int ivf_tc_sampled(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c, c
         g.g_b_off = h->list_off;
         g.g_total = titem + C;
         g.g_lists = C;
-        g.g_item_list = titem_list;
+        g.g_item_desc = titem_desc;
         g.g_row_query = rowq;
         g.tau = tau;
         g.fkey = skey;
@@ -973,7 +973,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     int64_t* dbase = c.tc ? cv.take<int64_t>((size_t)nq * c.npc) : nullptr;
     int64_t* titem = c.tc ? cv.take<int64_t>((size_t)h->C + 1) : nullptr;
     const int64_t items_cap = c.tc ? tc_items_bound((int64_t)nq * c.npc, (int)h->C, h->sizes_desc[0]) : 0;
-    int32_t* titem_list = c.tc ? cv.take<int32_t>((size_t)items_cap) : nullptr;
+    int4* titem_desc = c.tc ? cv.take<int4>((size_t)items_cap) : nullptr;
     int32_t* qorder = cv.take<int32_t>((size_t)nq);
     int64_t* every_len = cv.take<int64_t>(1);
     int32_t* every_seg = cv.take<int32_t>(1);
@@ -1093,7 +1093,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         }
         bool sampled_done = false;
         if (tot[2] == 0 && c.tc && nq >= h->sampled_min_queries) {
-            if ((rc = ivf_tc_sampled(h, ws, c, a, b, tc_operands(h, c, qb, q8, qfac, pfac), Apk, titem, titem_list,
+            if ((rc = ivf_tc_sampled(h, ws, c, a, b, tc_operands(h, c, qb, q8, qfac, pfac), Apk, titem, titem_desc,
                                      items_cap, keyR, idR, prec, &sampled_done, st)))
                 return rc;
             done = sampled_done;
@@ -1114,7 +1114,9 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                                               st, maps)))
                     return rc;
                 if ((rc = launch_tc_ivf_items(b.lq_off, h->list_off, h->C, titem, st))) return rc;
-                if ((rc = launch_tc_item_lists(titem, (int)h->C, titem_list, items_cap, st))) return rc;
+                if ((rc = launch_tc_item_descs(titem, (int)h->C, b.lq_off, h->list_off, nullptr, titem_desc, items_cap,
+                                               st)))
+                    return rc;
                 TcGemmArgs g{(int)max_pairs, (int)h->n, op.K, nullptr, D, 0, h->d_err};
                 g.kind = op.kind;
                 g.col_fac = op.col_fac;
@@ -1125,7 +1127,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
                 g.g_dbase = dbase;
                 g.g_total = titem + h->C;
                 g.g_lists = h->C;
-                g.g_item_list = titem_list;
+                g.g_item_desc = titem_desc;
                 const int kg = h->prof.kbegin(st);
                 if ((rc = launch_tc_gemm(Apk, op.B, g, st))) return rc;
                 h->prof.kend(kg, kKernKeys, st);

@@ -5,9 +5,9 @@
 // (:52-63), a CUB radix sort orders all N (key, row) pairs, the first R row ids come back to the host,
 // and the host re-ranks them in FP32 from the borrowed train array and partial-sorts (distance, id)
 // pairs (:135-176). Here, per query:
-//   gf_scan_kernel     the same key with the same FMA chain per row (4 rows per thread, one 32-bit load
-//                      of 4 codes per dimension, scale and q - offset staged in shared memory) -- HBM-
-//                      bound, N * dim code bytes per query;
+//   gf_scan_kernel     the same key with the same FMA chain per row (8 rows per thread, one 64-bit load
+//                      of 8 codes per dimension, 16 dimensions' loads in flight, scale and q - offset
+//                      staged in shared memory) -- HBM-bound, N * dim code bytes per query;
 //   selection          the R rows with the smallest (key, row) -- the rows the reference's stable
 //                      ascending sort puts first -- in two stages: radix selection (radix_select.cu)
 //                      of each of up to 64 row segments' R smallest as a set (ties to the lower row),
@@ -62,39 +62,50 @@ __global__ void gf_encode_kernel(const float* __restrict__ x, int64_t n, int dim
     codes[t] = (uint8_t)c;
 }
 
+// The code byte `sel` of w as a float, exactly: its bits placed in the mantissa of 2^23 (byte permute),
+// then 2^23 subtracted -- two full-rate instructions where an integer-to-float conversion runs at a quarter.
+__device__ __forceinline__ float gf_byte_f(uint32_t w, uint32_t sel) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | sel)) - 8388608.0f;
+}
+__device__ __forceinline__ void gf_acc8(uint2 c, float s, float nq, float (&a)[8]) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float v0 = fmaf(gf_byte_f(c.x, i), s, nq);
+        const float v1 = fmaf(gf_byte_f(c.y, i), s, nq);
+        a[i] = fmaf(v0, v0, a[i]);
+        a[4 + i] = fmaf(v1, v1, a[4 + i]);
+    }
+}
+
 // dist[i] = sum_d fma(code[d][i], scale[d], -(q[d] - offset[d]))^2, accumulated with fma in dimension
-// order; thread t takes rows 4t .. 4t + 3 (npad a multiple of 4; rows past n get keys nobody reads).
-__global__ void __launch_bounds__(256) gf_scan_kernel(const uint8_t* __restrict__ codes, int64_t npad, int dim,
+// order; thread t takes rows 8t .. 8t + 7 (npad a multiple of 16; rows past n get keys nobody reads): one
+// 8-byte load of their codes per dimension, sixteen dimensions' loads to a batch (eight 128-thread CTAs a
+// multiprocessor leave the registers for them; the small CTAs spread the rows evenly over the SMs).
+constexpr int kGfScanBatch = 16;
+__global__ void __launch_bounds__(128, 8) gf_scan_kernel(const uint8_t* __restrict__ codes, int64_t npad, int dim,
                                                       const float* __restrict__ scale,
                                                       const float* __restrict__ offset,
                                                       const float* __restrict__ q, float* __restrict__ dist) {
-    extern __shared__ float gf_sm[];
-    float* ssc = gf_sm;         // [dim]
-    float* snq = gf_sm + dim;   // [dim] -(q - offset)
-    for (int d = threadIdx.x; d < dim; d += blockDim.x) {
-        ssc[d] = scale[d];
-        snq[d] = -__fsub_rn(q[d], offset[d]);
-    }
+    extern __shared__ float2 gf_sn[];  // [dim] (scale, -(q - offset))
+    for (int d = threadIdx.x; d < dim; d += blockDim.x) gf_sn[d] = make_float2(scale[d], -__fsub_rn(q[d], offset[d]));
     __syncthreads();
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t quads = npad >> 2;
-    if (t >= quads) return;
-    const uchar4* col = reinterpret_cast<const uchar4*>(codes) + t;
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-#pragma unroll 16
-    for (int d = 0; d < dim; ++d) {
-        const uchar4 c = __ldcs(col + (int64_t)d * quads);
-        const float s = ssc[d], nq = snq[d];
-        const float v0 = fmaf((float)c.x, s, nq);
-        const float v1 = fmaf((float)c.y, s, nq);
-        const float v2 = fmaf((float)c.z, s, nq);
-        const float v3 = fmaf((float)c.w, s, nq);
-        a0 = fmaf(v0, v0, a0);
-        a1 = fmaf(v1, v1, a1);
-        a2 = fmaf(v2, v2, a2);
-        a3 = fmaf(v3, v3, a3);
+    const int64_t octs = npad >> 3;
+    if (t >= octs) return;
+    const uint2* col = reinterpret_cast<const uint2*>(codes) + t;
+    float a[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int d0 = 0;
+    for (; d0 + kGfScanBatch <= dim; d0 += kGfScanBatch) {
+        uint2 c[kGfScanBatch];
+#pragma unroll
+        for (int g = 0; g < kGfScanBatch; ++g) c[g] = __ldcs(col + (int64_t)(d0 + g) * octs);
+#pragma unroll
+        for (int g = 0; g < kGfScanBatch; ++g) gf_acc8(c[g], gf_sn[d0 + g].x, gf_sn[d0 + g].y, a);
     }
-    reinterpret_cast<float4*>(dist)[t] = make_float4(a0, a1, a2, a3);
+    for (; d0 < dim; ++d0) gf_acc8(col[(int64_t)d0 * octs], gf_sn[d0].x, gf_sn[d0].y, a);
+    float4* o = reinterpret_cast<float4*>(dist) + 2 * t;
+    o[0] = make_float4(a[0], a[1], a[2], a[3]);
+    o[1] = make_float4(a[4], a[5], a[6], a[7]);
 }
 
 // One warp per candidate (two per CTA): the warp brings the candidate's row into shared memory with
@@ -262,14 +273,27 @@ struct gf_handle {
     float* hq = nullptr;       // pinned staging: the query
     long long* hout = nullptr; // pinned staging: the ids
     int64_t rcap = 0;
+    // gf_query's launches and copies for a (k, r), captured once and replayed as one graph
+    struct Graph {
+        int k, r;
+        cudaGraphExec_t exec;  // null: capture failed for this (k, r); the launches run one by one
+    };
+    std::vector<Graph> graphs;
     std::atomic<long long> ndist{0};
     std::mutex mu;
 };
 
 namespace {
 
+void gf_drop_graphs(gf_handle* h) {
+    for (auto& gr : h->graphs)
+        if (gr.exec) cudaGraphExecDestroy(gr.exec);
+    h->graphs.clear();
+}
+
 void gf_release(gf_handle* h) {
     DeviceGuard g(h->device);
+    gf_drop_graphs(h);
     for (void* p : {(void*)h->codes, (void*)h->base, (void*)h->scale, (void*)h->offset, (void*)h->q, (void*)h->dist,
                     (void*)h->selk, (void*)h->seli, (void*)h->keys, (void*)h->out, (void*)h->segs, (void*)h->kth,
                     (void*)h->count, (void*)h->near})
@@ -340,6 +364,7 @@ int gf_build(gf_handle* h, const float* train) {
 
 int gf_reserve(gf_handle* h, int64_t r) {
     if (r <= h->rcap) return ANN_OK;
+    gf_drop_graphs(h);  // the graphs hold the old buffers' addresses
     if (h->selk) cudaFree(h->selk);
     if (h->seli) cudaFree(h->seli);
     if (h->keys) cudaFree(h->keys);
@@ -368,19 +393,14 @@ int launch_gf_topk(const unsigned long long* keys, int64_t r, const unsigned lon
     return ANN_OK;
 }
 
-int gf_search(gf_handle* h, const float* q, int k, int r, long long* out_ids) {
+// The launches and copies of one query on h->st (query from h->hq in, ids to h->hout out), no sync.
+int gf_enqueue(gf_handle* h, int k, int r, int nseg) {
     const int64_t n = h->n;
     const int dim = h->dim;
     cudaStream_t st = h->st;
-    // one segment when R exceeds the top-k kernel's bound (the second stage keeps R keys in front of each
-    // sorted round)
-    const int nseg = r <= kGfMaxK ? h->nseg : 1;
-    int rc = gf_reserve(h, (int64_t)nseg * r);
-    if (rc) return rc;
-    std::memcpy(h->hq, q, sizeof(float) * dim);
+    int rc;
     ANN_CUDA_TRY(cudaMemcpyAsync(h->q, h->hq, sizeof(float) * dim, cudaMemcpyHostToDevice, st));
-    const int64_t quads = h->npad >> 2;
-    gf_scan_kernel<<<(unsigned)ceil_div(quads, 256), 256, sizeof(float) * 2 * dim, st>>>(
+    gf_scan_kernel<<<(unsigned)ceil_div(h->npad >> 3, 128), 128, sizeof(float) * 2 * dim, st>>>(
         h->codes, h->npad, dim, h->scale, h->offset, h->q, h->dist);
     ANN_LAUNCH_CHECK();
     RadixSelectArgs sa{};
@@ -411,8 +431,45 @@ int gf_search(gf_handle* h, const float* q, int k, int r, long long* out_ids) {
     ANN_LAUNCH_CHECK();
     if ((rc = launch_gf_topk<long long>(h->keys, r, nullptr, nullptr, 0, k, h->out, st))) return rc;
     ANN_CUDA_TRY(cudaMemcpyAsync(h->hout, h->out, sizeof(long long) * k, cudaMemcpyDeviceToHost, st));
+    return ANN_OK;
+}
+
+// The first query of a (k, r) runs its launches one by one and then records them into a graph (no work
+// runs while recording); later queries of that (k, r) replay the graph: one launch instead of about ten
+// calls. The graphs read the query from, and write the ids to, the handle's pinned staging buffers.
+int gf_search(gf_handle* h, const float* q, int k, int r, long long* out_ids) {
+    cudaStream_t st = h->st;
+    // one segment when R exceeds the top-k kernel's bound (the second stage keeps R keys in front of each
+    // sorted round)
+    const int nseg = r <= kGfMaxK ? h->nseg : 1;
+    int rc = gf_reserve(h, (int64_t)nseg * r);
+    if (rc) return rc;
+    std::memcpy(h->hq, q, sizeof(float) * h->dim);
+    gf_handle::Graph* gr = nullptr;
+    for (auto& x : h->graphs)
+        if (x.k == k && x.r == r) gr = &x;
+    if (gr && gr->exec) {
+        ANN_CUDA_TRY(cudaGraphLaunch(gr->exec, st));
+    } else if ((rc = gf_enqueue(h, k, r, nseg))) {
+        return rc;
+    }
     ANN_CUDA_TRY(cudaStreamSynchronize(st));
     std::memcpy(out_ids, h->hout, sizeof(long long) * k);
+    if (!gr && h->graphs.size() < 16) {  // record this (k, r) once
+        gf_handle::Graph x{k, r, nullptr};
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const int erc = gf_enqueue(h, k, r, nseg);
+            const cudaError_t e = cudaStreamEndCapture(st, &graph);
+            if (erc == ANN_OK && e == cudaSuccess && graph &&
+                cudaGraphInstantiate(&x.exec, graph, 0) != cudaSuccess)
+                x.exec = nullptr;
+            if (graph) cudaGraphDestroy(graph);
+        }
+        cudaGetLastError();  // a failed recording leaves the launches one by one for this (k, r)
+        clear_error();
+        h->graphs.push_back(x);
+    }
     return ANN_OK;
 }
 

@@ -185,7 +185,9 @@ struct GroupTile {
     int64_t a0, b0;
     int am, bn;
 };
+__device__ __forceinline__ GroupTile tile_of_desc(int4 d) { return GroupTile{d.x, d.y, d.z, d.w}; }
 __device__ __forceinline__ GroupTile group_tile(const TcGemmArgs& a, int64_t t) {
+    if (a.g_item_desc) return tile_of_desc(a.g_item_desc[t]);
     int lo = 0, hi = a.g_lists - 1;
     if (a.g_item_list) {
         lo = a.g_item_list[t];  // one load, where a search would chain a dozen
@@ -279,9 +281,17 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
         if (lane == 0 && !a.test_no_loads) {
             int64_t it = 0;
             bool ok = true;
+            // with item descriptors, the next item's is loaded while this one's copies are issued
+            const bool pre = grouped && a.g_item_desc != nullptr;
+            int4 dnext = pre && (int64_t)blockIdx.x < tiles ? a.g_item_desc[blockIdx.x] : make_int4(0, 0, 0, 0);
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
                 int64_t arow, brow;
-                if (grouped) {
+                if (pre) {
+                    const int4 d = dnext;
+                    if (t + gridDim.x < tiles) dnext = a.g_item_desc[t + gridDim.x];
+                    arow = d.x;
+                    brow = d.y;
+                } else if (grouped) {
                     const GroupTile gt = group_tile(a, t);
                     arow = gt.a0;
                     brow = gt.b0;
@@ -339,15 +349,36 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
         int64_t acc = 0;
         for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x, ++acc) {
             const int b = (int)(acc & 1);
+            // the tile's rows and columns, and the per-row values the filter needs, read before the wait for
+            // the accumulator, so that their loads overlap the tile's MMAs: a dense tile, or a grouped one (a
+            // list's pairs and rows; rows and columns past them belong to the next list and are masked like
+            // rows past M)
+            const int m0 = (int)(t % mt) * kBM, n0 = (int)(t / mt) * kBN;
+            const int m = m0 + lane_base + lane;
+            const GroupTile gt = grouped ? group_tile(a, t) : GroupTile{0, 0, 0, 0};
+            int rq = m;                         // the row recorded for a survivor (grouped: its query)
+            int64_t arow = m;                   // the A row (per-row factors)
+            bool mvalid = m < a.M;
+            int64_t cbase = n0;                 // recorded column of the tile's first column
+            int ncols = a.N - n0;               // valid columns of the tile from its first
+            if (grouped) {
+                const int ml = lane_base + lane;
+                mvalid = ml < gt.am;
+                arow = gt.a0 + ml;
+                rq = mvalid ? (a.g_row_query ? a.g_row_query[gt.a0 + ml] : (int)(gt.a0 + ml)) : 0;
+                cbase = gt.b0;
+                ncols = gt.bn;
+            }
+            const float an = (a.normA && mvalid) ? a.normA[arow] : 0.f;
+            const float rfac = (a.row_fac && mvalid) ? a.row_fac[arow] : 1.f;
+            // rows past M (TMA zero fill) get a bar no key passes
+            const float tau = (a.tau && mvalid) ? a.tau[rq] : -kInf;
             // every lane waits; the warp leaves together if any lane gave up, so that no lane is left
             // behind at a warp-wide instruction
             const bool got = bar_wait(&tfull[b], (uint32_t)((acc >> 1) & 1), a.err, a.wait_ns);
             if (!__all_sync(0xffffffffu, got)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const int m0 = (int)(t % mt) * kBM, n0 = (int)(t / mt) * kBN;
-            const int m = m0 + lane_base + lane;
             if (!kFilterOnly && grouped) {  // keys of pair a0 + row, list rows b0 + column, to their stream positions
-                const GroupTile gt = group_tile(a, t);
                 const int ml = lane_base + lane;
                 // the stream position of list row b0 for each of the warp's 32 pairs (lane r holds row r's)
                 const int64_t dst_lane = (ml < gt.am ? a.g_dbase[gt.a0 + ml] : 0) + gt.b0;
@@ -391,26 +422,6 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                 bar_arrive(&tempty[b]);
                 continue;
             }
-            // the tile's rows and columns: a dense tile, or a grouped one (a list's pairs and rows; rows and
-            // columns past them belong to the next list and are masked like rows past M)
-            int rq = m;                         // the row recorded for a survivor (grouped: its query)
-            int64_t arow = m;                   // the A row (per-row factors)
-            bool mvalid = m < a.M;
-            int64_t cbase = n0;                 // recorded column of the tile's first column
-            int ncols = a.N - n0;               // valid columns of the tile from its first
-            if (grouped) {
-                const GroupTile gt = group_tile(a, t);
-                const int ml = lane_base + lane;
-                mvalid = ml < gt.am;
-                arow = gt.a0 + ml;
-                rq = mvalid ? (a.g_row_query ? a.g_row_query[gt.a0 + ml] : (int)(gt.a0 + ml)) : 0;
-                cbase = gt.b0;
-                ncols = gt.bn;
-            }
-            const float an = (a.normA && mvalid) ? a.normA[arow] : 0.f;
-            const float rfac = (a.row_fac && mvalid) ? a.row_fac[arow] : 1.f;
-            // rows past M (TMA zero fill) get a bar no key passes
-            const float tau = (a.tau && mvalid) ? a.tau[rq] : -kInf;
             const float tau_up = nextafterf(tau, kInf);
             const float2 ntau2 = make_float2(-tau_up, -tau_up);
             const uint32_t tbase = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kBN + col0);
@@ -676,6 +687,34 @@ int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream
         e = filter ? run_tc_gemm<kTcI8, kFilterEpi>(tmA, tmB, a, grid, st)
                    : run_tc_gemm<kTcI8, kKeyEpi>(tmA, tmB, a, grid, st);
     ANN_CUDA_TRY(e);
+    ANN_LAUNCH_CHECK();
+    return ANN_OK;
+}
+
+namespace {
+// desc[t] for the items of list l = blockIdx.x (strided): the tile group_tile would derive for item t.
+__global__ void tc_item_descs_kernel(const int64_t* __restrict__ item_off, int C, const int64_t* __restrict__ a_off,
+                                     const int64_t* __restrict__ b_off, const int64_t* __restrict__ b_len,
+                                     int4* __restrict__ desc, int64_t cap) {
+    for (int l = blockIdx.x; l < C; l += gridDim.x) {
+        const int64_t np = a_off[l + 1] - a_off[l];
+        const int64_t nr = b_len ? b_len[l] : b_off[l + 1] - b_off[l];
+        const int64_t npt = (np + kBM - 1) / kBM;
+        for (int64_t t = item_off[l] + threadIdx.x; t < item_off[l + 1] && t < cap; t += blockDim.x) {
+            const int64_t local = t - item_off[l];
+            const int64_t g = local % npt, rt = local / npt;
+            desc[t] = make_int4((int)(a_off[l] + g * kBM), (int)(b_off[l] + rt * kBN),
+                                (int)min((int64_t)kBM, np - g * kBM), (int)min((int64_t)kBN, nr - rt * kBN));
+        }
+    }
+}
+}  // namespace
+
+int launch_tc_item_descs(const int64_t* item_off, int C, const int64_t* a_off, const int64_t* b_off,
+                         const int64_t* b_len, int4* desc, int64_t cap, cudaStream_t st) {
+    ANN_CHECK_ARG(C >= 1, "tensor-core grouping: no lists");
+    tc_item_descs_kernel<<<(unsigned)std::min(C, 4 * kNumSMs), 128, 0, st>>>(item_off, C, a_off, b_off, b_len, desc,
+                                                                             cap);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

@@ -50,6 +50,9 @@ struct TcGemmArgs {
     const int64_t* g_total = nullptr;
     int g_lists = 0;
     const int32_t* g_item_list = nullptr;  // optional: the list of each item (else a search of g_item_off)
+    // optional, in place of the two above: item t's tile as (first A row, first B row, A rows, B rows), one
+    // 16-byte load (launch_tc_item_descs); the roles read the next item's ahead of its use
+    const int4* g_item_desc = nullptr;
     const int64_t* g_b_len = nullptr;      // optional: rows of list l taken (else g_b_off[l+1] - g_b_off[l])
     // Grouped filter mode (grouped, out == null): A row i belongs to query g_row_query[i]; its bar is
     // tau[g_row_query[i]], and a survivor is recorded as (key, list row g_b_off[l] + r, that query).
@@ -80,6 +83,11 @@ int tc_filter_warps(int M, int N);
 // ... and of a grouped filter launch (persistent over the work items).
 int tc_grouped_filter_warps();
 size_t tc_gemm_smem();
+// The grouped mode's item descriptors (TcGemmArgs::g_item_desc) for items [0, min(item_off[C], cap)): list l's
+// items from item_off[l] (launch_tc_ivf_items), its A rows [a_off[l], a_off[l+1]) and B rows from b_off[l]
+// (b_len[l] of them when given, else to b_off[l+1]).
+int launch_tc_item_descs(const int64_t* item_off, int C, const int64_t* a_off, const int64_t* b_off,
+                         const int64_t* b_len, int4* desc, int64_t cap, cudaStream_t st);
 int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream_t st);
 // Runs one small GEMM whose producer issues no copies, with every wait limited to wait_ns, and returns the
 // device flag it left (2: a bounded wait gave up, as it must); the flag is cleared afterwards.

@@ -159,3 +159,25 @@ def test_golden_outputs_of_the_reference(ours, golden_dir):
             assert ours.lib.gf_ndist(h) == int(g[f"{name}_ndist"]), name
         finally:
             ours.lib.gf_free(h)
+
+
+def test_replayed_queries_over_changing_k_and_r(ref, ours):
+    """Each (k, r) runs its first query launch by launch and later ones as a replayed graph; a larger r
+    reallocates the candidate buffers and drops the graphs. Interleaved (k, r) settings, with r growing
+    part-way, return the reference's ids every time."""
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal((50_000, 64)).astype(np.float32)
+    qs = rng.standard_normal((15, 64)).astype(np.float32)
+    hr, ho = ref.create(x), ours.create(x)
+    try:
+        settings = [(10, 50), (20, 400), (10, 50), (5, 2000), (20, 400)]
+        for i, q in enumerate(qs):
+            k, r = settings[i % len(settings)]
+            gr, ir = ref.query(hr, q, k, r)
+            go, io = ours.query(ho, q, k, r)
+            assert go == gr, (i, k, r)
+            np.testing.assert_array_equal(io, ir, err_msg=f"query {i} (k={k}, r={r})")
+        assert ours.lib.gf_ndist(ho) == ref.lib.gf_ndist(hr)
+    finally:
+        ref.lib.gf_free(hr)
+        ours.lib.gf_free(ho)
