@@ -11,9 +11,10 @@
 //   selection          the R rows with the smallest (key, row) -- the rows the reference's stable
 //                      ascending sort puts first -- in two stages: radix selection (radix_select.cu)
 //                      of each of up to 64 row segments' R smallest as a set (ties to the lower row),
-//                      in parallel, then the R smallest of their union as 64-bit keys (key bits << 32 |
-//                      row, exact for the non-negative keys) in gf_topk_kernel; one segment when the
-//                      base is small or R is above the top-k kernel's bound;
+//                      in parallel, then the R smallest (key, row) of their union by one block
+//                      (gf_union_select_kernel: an exact radix selection of the R-th key, then one of
+//                      the cut among the rows that share it); one segment when the base is small or R
+//                      is above the top-k kernel's bound;
 //   gf_rerank_kernel   each candidate's FP32 squared distance from a device copy of train, with the
 //                      reference's host arithmetic (v = p - q, acc = acc + v * v, no fused multiply-add);
 //   gf_topk_kernel     the best k (distance, id) pairs in ascending order, as 64-bit keys
@@ -142,85 +143,137 @@ __global__ void __launch_bounds__(32 * kGfRerankWarps) gf_rerank_kernel(const fl
     keys[j] = ((unsigned long long)__float_as_uint(acc) << 32) | (unsigned)id;
 }
 
-// kth[s] = segment s's R-th smallest key: the largest key of its selected set (the set is its R
-// smallest), or +inf when the set is padded (a segment shorter than R bounds nothing). One CTA per segment.
-__global__ void __launch_bounds__(256) gf_kth_kernel(const float* __restrict__ selk, const int* __restrict__ selp,
-                                                     int R, float* __restrict__ kth) {
-    __shared__ float sMax[8];
-    __shared__ int sPad[8];
-    const int64_t base = (int64_t)blockIdx.x * R;
-    float m = -kInf;
-    bool pad = false;
-    for (int j = threadIdx.x; j < R; j += blockDim.x) {
-        const int p = selp[base + j];
-        const float kv = selk[base + j];
-        if (p < 0 || p == kNoId || !(kv < kInf))
-            pad = true;
-        else
-            m = fmaxf(m, kv);
-    }
-    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    const bool wpad = __any_sync(0xffffffffu, pad);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) {
-        sMax[warp] = m;
-        sPad[warp] = wpad ? 1 : 0;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float mm = -kInf;
-        int pp = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-            mm = fmaxf(mm, sMax[w]);
-            pp |= sPad[w];
-        }
-        kth[blockIdx.x] = pp ? kInf : mm;
-    }
+// ---- the union's R smallest (key, row), by one block ----------------------------------------------------
+constexpr int kGfUnionThreads = 1024;
+__device__ __forceinline__ uint32_t gf_ord(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
-// Segment s's selected set (keys and in-segment positions, R per segment, +inf / kNoId padding) as
-// 64-bit keys: key bits << 32 | (segment start + position), padding as the largest key, all of them
-// into keys[j]; and those at or below the bar -- the smallest segment R-th key, which the union's R-th
-// smallest key cannot exceed (a segment alone holds R keys at or below its own) -- appended to near[]
-// at slots from an atomic counter (their order does not matter: the next step sorts them).
-__global__ void gf_pack_kernel(const float* __restrict__ selk, const int* __restrict__ selp,
-                               const int64_t* __restrict__ offs, const float* __restrict__ kth, int nseg, int R,
-                               unsigned long long* __restrict__ keys, unsigned long long* __restrict__ near,
-                               int cap, int* __restrict__ count) {
-    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= (int64_t)nseg * R) return;
-    float bar = kInf;
-    for (int s2 = 0; s2 < nseg; ++s2) bar = fminf(bar, kth[s2]);
-    const int p = selp[j];
-    const float kv = selk[j];
-    const bool real = p >= 0 && p != kNoId && kv < kInf;
-    const unsigned long long key =
-        real ? ((unsigned long long)__float_as_uint(kv) << 32) | (unsigned)(offs[j / R] + p) : ~0ull;
-    keys[j] = key;
-    if (real && kv <= bar) {
-        const int slot = atomicAdd(count, 1);
-        if (slot < cap) near[slot] = key;
+// Entry j of the segments' selected sets (segment j / R, its R entries in any order): its ordered key and
+// its row, or valid = false for padding.
+struct GfUnion {
+    const float* selk;
+    const int* selp;
+    const int64_t* offs;
+    int R, total;
+    __device__ __forceinline__ bool at(int j, uint32_t* key, uint32_t* row) const {
+        const int p = selp[j];
+        const float kv = selk[j];
+        if (p < 0 || p == kNoId || !(kv < kInf)) return false;
+        *key = gf_ord(kv);
+        *row = (uint32_t)(offs[j / R] + p);
+        return true;
     }
+};
+
+// The rank-th smallest (1 <= rank <= count) of the values v(j) of the entries j with sel(j), over four 8-bit
+// passes of a block histogram (warp-aggregated shared atomics). Every thread returns it.
+template <typename Val>
+__device__ uint32_t gf_block_select(const GfUnion& u, Val val, int64_t rank, int* hist, int* pick) {
+    uint32_t prefix = 0, pmask = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        for (int j0 = 0; j0 < u.total; j0 += blockDim.x) {  // uniform trip count: whole warps match
+            const int j = j0 + threadIdx.x;
+            uint32_t v = 0;
+            const bool ok = j < u.total && val(j, &v) && (v & pmask) == prefix;
+            const uint32_t dgt = (v >> shift) & 255u;
+            const unsigned peers = __match_any_sync(0xffffffffu, ok ? dgt : 0xffffffffu);
+            if (ok && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[dgt], __popc(peers));
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {  // the digit holding rank, and the count below it
+            const int lane = threadIdx.x;
+            int c[8], sum = 0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                c[i] = hist[lane * 8 + i];
+                sum += c[i];
+            }
+            int incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int excl = incl - sum;
+            if (excl < rank && rank <= incl) {
+                int acc = excl;
+                for (int i = 0; i < 8; ++i) {
+                    if (acc + c[i] >= rank) {
+                        pick[0] = lane * 8 + i;
+                        pick[1] = acc;
+                        break;
+                    }
+                    acc += c[i];
+                }
+            }
+        }
+        __syncthreads();
+        prefix |= (uint32_t)pick[0] << shift;
+        rank -= pick[1];
+        pmask |= 255u << shift;
+        __syncthreads();  // pick is rewritten by the next pass
+    }
+    return prefix;
+}
+
+// out[0 .. min(R, valid)) = the rows of the R smallest (key, row) of the union, in no particular order (the
+// re-rank reads them as a set): the keys below the R-th smallest key, then the rows with that key below the
+// cut among them, found by a second selection over the tie rows (rows are distinct, so the cut is exact).
+// Entries past the valid count are -1. One block.
+__global__ void __launch_bounds__(kGfUnionThreads) gf_union_select_kernel(GfUnion u, int* __restrict__ out) {
+    __shared__ int hist[256];
+    __shared__ int pick[2];
+    __shared__ int sCount[3];  // valid entries, written below, written ties
+    if (threadIdx.x == 0) sCount[0] = sCount[1] = sCount[2] = 0;
+    __syncthreads();
+    int nv = 0;
+    for (int j = threadIdx.x; j < u.total; j += blockDim.x) {
+        uint32_t k, r;
+        nv += u.at(j, &k, &r);
+    }
+    atomicAdd(&sCount[0], nv);
+    __syncthreads();
+    const int valid = sCount[0];
+    const int R = min(u.R, valid);
+    if (R == 0) {
+        for (int j = threadIdx.x; j < u.R; j += blockDim.x) out[j] = -1;
+        return;
+    }
+    const uint32_t T = gf_block_select(u, [&](int j, uint32_t* v) {
+        uint32_t r;
+        return u.at(j, v, &r);
+    }, R, hist, pick);
+    // keys below T all belong; count them while writing
+    for (int j = threadIdx.x; j < u.total; j += blockDim.x) {
+        uint32_t k, r;
+        if (u.at(j, &k, &r) && k < T) out[atomicAdd(&sCount[1], 1)] = (int)r;
+    }
+    __syncthreads();
+    const int below = sCount[1];
+    const int need = R - below;  // >= 1: T itself is the R-th key
+    const uint32_t Trow = gf_block_select(u, [&](int j, uint32_t* v) {
+        uint32_t k;
+        return u.at(j, &k, v) && k == T;
+    }, need, hist, pick);
+    for (int j = threadIdx.x; j < u.total; j += blockDim.x) {
+        uint32_t k, r;
+        if (u.at(j, &k, &r) && k == T && r <= Trow) out[below + atomicAdd(&sCount[2], 1)] = (int)r;
+    }
+    for (int j = R + threadIdx.x; j < u.R; j += blockDim.x) out[j] = -1;
 }
 
 // The k smallest of r 64-bit keys, ascending, into out (the low 32 bits: row ids). P (a power of two,
 // <= kGfSortCap) keys sit in shared memory: the running best k in front, then the next P - k keys;
-// each round bitonic-sorts all P.
-// With count set: when the near set fits (*count <= cap) it replaces keys (r = *count). P is the
-// smallest power of two >= min(r + k, Pmax), Pmax the keys the launch's shared memory holds.
+// each round bitonic-sorts all P. P is the smallest power of two >= min(r + k, Pmax), Pmax the keys the
+// launch's shared memory holds.
 template <typename OutT>
-__global__ void __launch_bounds__(512) gf_topk_kernel(const unsigned long long* __restrict__ keys, int r,
-                                                      const unsigned long long* __restrict__ near,
-                                                      const int* __restrict__ count, int cap, int k, int Pmax,
-                                                      OutT* __restrict__ out) {
+__global__ void __launch_bounds__(512) gf_topk_kernel(const unsigned long long* __restrict__ keys, int r, int k,
+                                                      int Pmax, OutT* __restrict__ out) {
     extern __shared__ unsigned long long gf_buf[];
-    if (count != nullptr) {
-        const int c = *count;
-        if (c <= cap) {
-            keys = near;
-            r = c;
-        }
-    }
     int P = 64;
     while (P < min(r + k, Pmax)) P <<= 1;
     const int C = P - k;
@@ -263,12 +316,10 @@ struct gf_handle {
     float* dist = nullptr;     // [npad]
     float* selk = nullptr;     // [rcap]
     int* seli = nullptr;       // [rcap]
+    int* uni = nullptr;        // [rcap] the union's R rows (several segments)
     unsigned long long* keys = nullptr;  // [rcap]
     long long* out = nullptr;  // [kGfMaxK]
     int64_t* segs = nullptr;   // [2][kGfMaxSeg] segment starts and lengths (fixed by n)
-    float* kth = nullptr;      // [kGfMaxSeg] each segment's R-th smallest key
-    int* count = nullptr;      // the near set's size
-    unsigned long long* near = nullptr;  // [kGfSortCap] keys at or below the bar
     int nseg = 1;              // first-stage segments when R <= kGfMaxK
     float* hq = nullptr;       // pinned staging: the query
     long long* hout = nullptr; // pinned staging: the ids
@@ -295,8 +346,8 @@ void gf_release(gf_handle* h) {
     DeviceGuard g(h->device);
     gf_drop_graphs(h);
     for (void* p : {(void*)h->codes, (void*)h->base, (void*)h->scale, (void*)h->offset, (void*)h->q, (void*)h->dist,
-                    (void*)h->selk, (void*)h->seli, (void*)h->keys, (void*)h->out, (void*)h->segs, (void*)h->kth,
-                    (void*)h->count, (void*)h->near})
+                    (void*)h->selk, (void*)h->seli, (void*)h->keys, (void*)h->out, (void*)h->segs,
+                    (void*)h->uni})
         if (p) cudaFree(p);
     if (h->hq) cudaFreeHost(h->hq);
     if (h->hout) cudaFreeHost(h->hout);
@@ -315,9 +366,6 @@ int gf_build(gf_handle* h, const float* train) {
     ANN_CUDA_TRY(cudaMalloc(&h->dist, sizeof(float) * (size_t)h->npad));
     ANN_CUDA_TRY(cudaMalloc(&h->out, sizeof(long long) * kGfMaxK));
     ANN_CUDA_TRY(cudaMalloc(&h->segs, sizeof(int64_t) * 2 * kGfMaxSeg));
-    ANN_CUDA_TRY(cudaMalloc(&h->kth, sizeof(float) * kGfMaxSeg));
-    ANN_CUDA_TRY(cudaMalloc(&h->count, sizeof(int)));
-    ANN_CUDA_TRY(cudaMalloc(&h->near, sizeof(unsigned long long) * kGfSortCap));
     ANN_CUDA_TRY(cudaHostAlloc(&h->hq, sizeof(float) * dim, cudaHostAllocDefault));
     ANN_CUDA_TRY(cudaHostAlloc(&h->hout, sizeof(long long) * kGfMaxK, cudaHostAllocDefault));
     // first-stage segments: about kGfSegRows rows each, at most kGfMaxSeg
@@ -368,6 +416,8 @@ int gf_reserve(gf_handle* h, int64_t r) {
     if (h->selk) cudaFree(h->selk);
     if (h->seli) cudaFree(h->seli);
     if (h->keys) cudaFree(h->keys);
+    if (h->uni) cudaFree(h->uni);
+    h->uni = nullptr;
     h->selk = nullptr;
     h->seli = nullptr;
     h->keys = nullptr;
@@ -375,6 +425,7 @@ int gf_reserve(gf_handle* h, int64_t r) {
     ANN_CUDA_TRY(cudaMalloc(&h->selk, sizeof(float) * (size_t)r));
     ANN_CUDA_TRY(cudaMalloc(&h->seli, sizeof(int) * (size_t)r));
     ANN_CUDA_TRY(cudaMalloc(&h->keys, sizeof(unsigned long long) * (size_t)r));
+    ANN_CUDA_TRY(cudaMalloc(&h->uni, sizeof(int) * (size_t)r));
     h->rcap = r;
     return ANN_OK;
 }
@@ -382,13 +433,11 @@ int gf_reserve(gf_handle* h, int64_t r) {
 // keys [r] (or the near set, see gf_topk_kernel) -> the k smallest, ascending; shared memory for
 // min(r + k, kGfSortCap) keys rounded up to a power of two.
 template <typename OutT>
-int launch_gf_topk(const unsigned long long* keys, int64_t r, const unsigned long long* near, const int* count,
-                   int cap, int k, OutT* out, cudaStream_t st) {
+int launch_gf_topk(const unsigned long long* keys, int64_t r, int k, OutT* out, cudaStream_t st) {
     int Pmax = 64;
     while (Pmax < std::min<int64_t>(r + k, kGfSortCap)) Pmax <<= 1;
     ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(gf_topk_kernel<OutT>)));
-    gf_topk_kernel<OutT><<<1, 512, sizeof(unsigned long long) * Pmax, st>>>(keys, (int)r, near, count, cap, k, Pmax,
-                                                                            out);
+    gf_topk_kernel<OutT><<<1, 512, sizeof(unsigned long long) * Pmax, st>>>(keys, (int)r, k, Pmax, out);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }
@@ -412,24 +461,19 @@ int gf_enqueue(gf_handle* h, int k, int r, int nseg) {
     if (nseg > 1) {
         sa.offs = h->segs;
         sa.lens = h->segs + kGfMaxSeg;
-        ANN_CUDA_TRY(cudaMemsetAsync(h->count, 0, sizeof(int), st));
     }
     if ((rc = launch_radix_select(sa, nseg, st))) return rc;
-    if (nseg > 1) {  // the union's R smallest (key, row), as row ids over the first R entries of seli
-        const int64_t tot = (int64_t)nseg * r;
-        const int cap = kGfSortCap - r;  // the near set sorts in one round
-        gf_kth_kernel<<<nseg, 256, 0, st>>>(h->selk, h->seli, r, h->kth);
+    if (nseg > 1) {  // the union's R smallest (key, row), as row ids in the first R entries of the union
+        GfUnion u{h->selk, h->seli, h->segs, r, nseg * r};
+        gf_union_select_kernel<<<1, kGfUnionThreads, 0, st>>>(u, h->uni);
         ANN_LAUNCH_CHECK();
-        gf_pack_kernel<<<(unsigned)ceil_div(tot, 256), 256, 0, st>>>(h->selk, h->seli, h->segs, h->kth, nseg, r,
-                                                                     h->keys, h->near, cap, h->count);
-        ANN_LAUNCH_CHECK();
-        if ((rc = launch_gf_topk<int>(h->keys, tot, h->near, h->count, cap, r, h->seli, st))) return rc;
     }
+    const int* cand = nseg > 1 ? h->uni : h->seli;
     ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(gf_rerank_kernel)));
     gf_rerank_kernel<<<(unsigned)ceil_div(r, kGfRerankWarps), 32 * kGfRerankWarps,
-                       sizeof(float) * dim * (1 + kGfRerankWarps), st>>>(h->base, n, dim, h->q, h->seli, r, h->keys);
+                       sizeof(float) * dim * (1 + kGfRerankWarps), st>>>(h->base, n, dim, h->q, cand, r, h->keys);
     ANN_LAUNCH_CHECK();
-    if ((rc = launch_gf_topk<long long>(h->keys, r, nullptr, nullptr, 0, k, h->out, st))) return rc;
+    if ((rc = launch_gf_topk<long long>(h->keys, r, k, h->out, st))) return rc;
     ANN_CUDA_TRY(cudaMemcpyAsync(h->hout, h->out, sizeof(long long) * k, cudaMemcpyDeviceToHost, st));
     return ANN_OK;
 }

@@ -28,6 +28,20 @@ import numpy as np
 from . import _lib
 
 
+def _host_out(out, shape, dtype, name):
+    """The host array a search writes: `out` (a C-contiguous numpy array, or a CPU torch tensor, of this
+    shape and type -- page-locked memory makes the device-to-host copy a direct one) or a new array."""
+    if out is None:
+        return np.empty(shape, dtype)
+    if _lib.is_torch(out):
+        if out.is_cuda:
+            raise RuntimeError(f"{name}: host queries need a host output")
+        out = out.numpy()
+    if out.shape != shape or out.dtype != dtype or not out.flags.c_contiguous:
+        raise RuntimeError(f"{name} must be a C-contiguous {np.dtype(dtype).name} array of shape {shape}")
+    return out
+
+
 class IVFIndex:
     def __init__(self, device: int = 0, mode: str = "reference", num_threads: int | None = None):
         self._lib = _lib.load()
@@ -230,7 +244,9 @@ class IVFIndex:
         """Top-k per query row: (ids int64 [nq, k], squared distances float32 [nq, k]).
         max_candidates: None = the mode's default (reference: the reference's cap; exact: none),
         -1 = the reference's cap, 0 = none, > 0 = that cap. shard: this index holds one rank's share of the
-        lists (ShardedIVFIndex); a query short of k candidates returns what it has (-1 padded)."""
+        lists (ShardedIVFIndex); a query short of k candidates returns what it has (-1 padded).
+        out_ids / out_dists: where the results go -- device tensors for device queries, or for host queries
+        host arrays (numpy or CPU torch, C-contiguous [nq, k]; page-locked ones take a direct copy)."""
         if self._n == 0:
             raise RuntimeError("index not fitted")
         k = int(k)
@@ -260,8 +276,8 @@ class IVFIndex:
         if x.shape[1] != self._dim:
             raise RuntimeError("Query dimension mismatch")
         nq = x.shape[0]
-        ids = np.empty((nq, k), np.int64)
-        dists = np.empty((nq, k), np.float32) if with_dists else None
+        ids = _host_out(out_ids, (nq, k), np.int64, "out_ids")
+        dists = _host_out(out_dists, (nq, k), np.float32, "out_dists") if with_dists else None
         _lib.check(self._lib.ann_ivf_query(self._h, ws, _lib.ptr(x), nq, x.shape[1], k, *args, _lib.MEM_HOST,
                                            _lib.ptr(ids), _lib.ptr(dists), None))
         return ids, dists

@@ -250,6 +250,9 @@ def run_ours(args, rank, world, local):
     qpin = torch.empty(q, d, dtype=torch.float32, pin_memory=True)
     qpin.copy_(queries)
     qh = qpin.numpy()
+    # the end-to-end calls' ids land in page-locked host memory, as a throughput-minded caller keeps them
+    ids_pin_t = torch.empty(q, K_NN, dtype=torch.int64, pin_memory=True)
+    ids_pin = ids_pin_t.numpy()
 
     sel = set(args.forms.split(","))
     tcx = ivf = None
@@ -385,7 +388,7 @@ def run_ours(args, rank, world, local):
 
         forms["ivf_sq8"] = {
             "qps": ivf_qps, "recall": ivf_rec, "step": ivf_step,
-            "host": lambda: ivf.search(qh, K_NN, 0, npc, rr_x, max_candidates=0, with_dists=False),
+            "host": lambda: ivf.search(qh, K_NN, 0, npc, rr_x, max_candidates=0, with_dists=False, out_ids=ids_pin),
             "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc, rr_x, max_candidates=0, out_ids=o_ids[:1],
                                             with_dists=False),
             "lat_host": lambda x: ivf.search(x, K_NN, 0, npc, rr_x, max_candidates=0, with_dists=False),
@@ -406,7 +409,8 @@ def run_ours(args, rank, world, local):
         forms["ivf_tc"] = {
             "qps": tc_qps, "recall": tc_rec, "step": ivf_tc_step,
             "host": lambda: (ivf.set_option("sample_div", div_of["tc"]),
-                             ivf.search(qh, K_NN, 0, npc_tc, rr_t, max_candidates=0, mode="tc", with_dists=False)),
+                             ivf.search(qh, K_NN, 0, npc_tc, rr_t, max_candidates=0, mode="tc", with_dists=False,
+                                        out_ids=ids_pin)),
             "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc_tc, rr_t, max_candidates=0, mode="tc",
                                             out_ids=o_ids[:1], with_dists=False),
             "lat_host": lambda x: ivf.search(x, K_NN, 0, npc_tc, rr_t, max_candidates=0, mode="tc",
@@ -431,7 +435,8 @@ def run_ours(args, rank, world, local):
         forms["ivf_tc_sq8"] = {
             "qps": q_qps, "recall": q_rec, "step": ivf_q_step,
             "host": lambda: (ivf.set_option("sample_div", div_of["tc_sq8"]),
-                             ivf.search(qh, K_NN, 0, npc_q, rr_q, max_candidates=0, mode="tc_sq8", with_dists=False)),
+                             ivf.search(qh, K_NN, 0, npc_q, rr_q, max_candidates=0, mode="tc_sq8", with_dists=False,
+                                        out_ids=ids_pin)),
             "lat_dev": lambda x: ivf.search(x, K_NN, 0, npc_q, rr_q, max_candidates=0, mode="tc_sq8",
                                             out_ids=o_ids[:1], with_dists=False),
             "lat_host": lambda x: ivf.search(x, K_NN, 0, npc_q, rr_q, max_candidates=0, mode="tc_sq8",

@@ -486,3 +486,25 @@ def test_batch_with_every_row_queries_equals_alone(cuda, mode):
     assert 0 < every < len(w.queries), every
     assert_ids_equal_up_to_ties(w.base, w.queries, ids, np.stack(alone_i), rtol=1e-6)
     np.testing.assert_allclose(d, np.stack(alone_d), rtol=1e-6, atol=1e-7)
+
+
+def test_host_search_into_callers_page_locked_arrays(cuda):
+    """Host queries may give their own output arrays (page-locked torch CPU tensors or numpy arrays): the
+    search writes them and returns them, equal to a search that allocates its own; wrong shapes or types
+    are refused."""
+    import torch
+    w = synth.zipf_mixture(30000, 64, 500, c=64, lo=20, hi=3000, seed=21)
+    st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
+    ix = _ivf(mode="tc")
+    ix.import_state(st)
+    want_i, want_d = ix.search(w.queries, 50, 0, 4, 100)
+    oi = torch.empty(500, 50, dtype=torch.int64, pin_memory=True)
+    od = torch.empty(500, 50, dtype=torch.float32, pin_memory=True)
+    got_i, got_d = ix.search(w.queries, 50, 0, 4, 100, out_ids=oi, out_dists=od)
+    np.testing.assert_array_equal(got_i, want_i)
+    np.testing.assert_array_equal(oi.numpy(), want_i)
+    np.testing.assert_array_equal(od.numpy(), want_d)
+    with pytest.raises(RuntimeError):
+        ix.search(w.queries, 50, 0, 4, 100, out_ids=np.empty((500, 49), np.int64))
+    with pytest.raises(RuntimeError):
+        ix.search(w.queries, 50, 0, 4, 100, out_ids=np.empty((500, 50), np.int32))
