@@ -55,6 +55,8 @@ def main(argv=None):
     ap.add_argument("--sample-div", type=int, default=16)
     ap.add_argument("--form", choices=["tc", "tc_sq8"], default="tc")
     ap.add_argument("--gf-r", type=int, default=300, help="gf_scan: the drop-in's re-rank depth r")
+    ap.add_argument("--sampled-min", type=int, default=0,
+                    help="ivf_tc: batch size from which the sampled path runs (0: the library's default)")
     args = ap.parse_args(argv)
     import torch
     nq = args.nq or {"flat_scan": 1000, "flat_stream": 1, "ivf_batched": 10000, "ivf_tc": 10000, "gf_scan": 16}[args.case]
@@ -77,11 +79,20 @@ def main(argv=None):
         mode = "exact" if args.case == "ivf_batched" else args.form
         if mode != "exact":
             ix.set_option("sample_div", args.sample_div)
+            if args.sampled_min:
+                ix.set_option("sampled_min_queries", args.sampled_min)
         ids = torch.empty(nq, k, dtype=torch.int64, device=base.device)
         d = torch.empty(nq, k, dtype=torch.float32, device=base.device)
         out.update({"mode": mode, "nprobe": args.nprobe, "refine_r": args.refine})
-        out["ms_per_call"] = _time(lambda: ix.search(queries[:nq], k, 0, args.nprobe, args.refine, max_candidates=0,
-                                                     mode=mode, out_ids=ids, out_dists=d), args.reps)
+        call = lambda: ix.search(queries[:nq], k, 0, args.nprobe, args.refine, max_candidates=0, mode=mode,
+                                 out_ids=ids, out_dists=d)
+        out["ms_per_call"] = _time(call, args.reps)
+        ix.reset_profile_results()  # the kernel timers over --reps more calls
+        ix.set_profiling(True)
+        for _ in range(args.reps):
+            call()
+        ix.set_profiling(False)
+        out["kernel_ms"] = {k2: round(v["ms"] / max(1, v["launches"]), 4) for k2, v in ix.get_kernel_times().items()}
     else:
         import numpy as np
         from .gpu_filter import Algorithm
