@@ -70,6 +70,22 @@ int ws_reserve_device(ann_workspace* ws, size_t bytes) {
     return ANN_OK;
 }
 
+int ws_pinned(ann_workspace* ws, int64_t** out) {
+    std::lock_guard<std::mutex> lk(ws->mu);
+    if (!ws->pinned) {
+        void* p = nullptr;
+        const cudaError_t e = cudaHostAlloc(&p, 8 * sizeof(int64_t), cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error("workspace: cannot allocate page-locked host words (%s)", cudaGetErrorString(e));
+            return ANN_ERR_NOMEM;
+        }
+        ws->pinned = static_cast<int64_t*>(p);
+    }
+    *out = ws->pinned;
+    return ANN_OK;
+}
+
 int ws_reserve_big(ann_workspace* ws, size_t bytes) {
     std::lock_guard<std::mutex> lk(ws->mu);
     if (ws->big_cap >= bytes) return ANN_OK;
@@ -159,6 +175,8 @@ static void ws_release(ann_workspace* ws) {
     DeviceGuard g(ws->device);
     if (ws->dev) cudaFree(ws->dev);
     if (ws->big) cudaFree(ws->big);
+    if (ws->pinned) cudaFreeHost(ws->pinned);
+    ws->pinned = nullptr;
     ws->dev = nullptr;
     ws->big = nullptr;
     ws->dev_cap = ws->big_cap = 0;

@@ -224,6 +224,8 @@ int ann_ivf_destroy(ann_ivf* h) {
         if (h->d_err) cudaFree(h->d_err);
         if (h->ws.dev) cudaFree(h->ws.dev);
         if (h->ws.big) cudaFree(h->ws.big);
+        if (h->ws.pinned) cudaFreeHost(h->ws.pinned);
+        h->ws.pinned = nullptr;
         h->ws.dev = nullptr;
         h->ws.big = nullptr;
     }
@@ -1085,19 +1087,27 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     bool done = false;
     if (!c.ref && c.batched) {
         IvfBatchArgs b{};
-        int64_t tot[3] = {0, 0, 0};
-        if ((rc = batched_prepare(a, bscratch, c.sort_tmp, c.scan_tmp, &b, tot, st))) return rc;
+        int64_t tot_local[3] = {0, 0, 0};
+        int64_t* tot = tot_local;
+        // The sampled path needs none of the set-up's totals to run: they land in page-locked words and are read
+        // after its own synchronisation (a batch with every-row queries, rare, is then set up again and redone).
+        const bool sampled = c.tc && nq >= h->sampled_min_queries;
+        if (sampled && (rc = ws_pinned(ws, &tot))) return rc;
+        tot[0] = tot[1] = tot[2] = 0;
+        auto run_sampled = [&](bool* ok) -> int {
+            return ivf_tc_sampled(h, ws, c, a, b, tc_operands(h, c, qb, q8, qfac, pfac), Apk, titem, titem_desc,
+                                  items_cap, keyR, idR, prec, ok, st);
+        };
+        bool sampled_done = false;
+        if ((rc = batched_prepare(a, bscratch, c.sort_tmp, c.scan_tmp, &b, tot, st, !sampled))) return rc;
+        if (sampled && (rc = run_sampled(&sampled_done))) return rc;  // synchronises st: tot is current
+        if (tot[2] != 0) sampled_done = false;
         if (tot[2] != 0 && every_row_apart) {  // every-row queries: set apart, then the batch set up again
             if ((rc = take_every_row())) return rc;
             if ((rc = batched_prepare(a, bscratch, c.sort_tmp, c.scan_tmp, &b, tot, st))) return rc;
+            if (tot[2] == 0 && sampled && (rc = run_sampled(&sampled_done))) return rc;
         }
-        bool sampled_done = false;
-        if (tot[2] == 0 && c.tc && nq >= h->sampled_min_queries) {
-            if ((rc = ivf_tc_sampled(h, ws, c, a, b, tc_operands(h, c, qb, q8, qfac, pfac), Apk, titem, titem_desc,
-                                     items_cap, keyR, idR, prec, &sampled_done, st)))
-                return rc;
-            done = sampled_done;
-        }
+        done = sampled_done;
         if (tot[2] == 0 && !sampled_done) {  // no query fell back to scanning every row
             if ((rc = ws_reserve_big(ws, sizeof(float) * (size_t)std::max<int64_t>(tot[1], 1)))) return rc;
             float* D = reinterpret_cast<float*>(ws->big);

@@ -261,7 +261,7 @@ size_t batched_scratch_bytes(int nq, int npc, int C, size_t* sort_tmp, size_t* s
 }
 
 int batched_prepare(const IvfQueryArgs& a, void* scratch, size_t sort_tmp, size_t scan_tmp, IvfBatchArgs* out,
-                    int64_t* host_totals, cudaStream_t st) {
+                    int64_t* host_totals, cudaStream_t st, bool sync) {
     const int nq = a.plan.nq, npc = a.plan.npc, C = a.ix.C;
     const int n = nq * npc;
     Carver cv(scratch);
@@ -299,7 +299,7 @@ int batched_prepare(const IvfQueryArgs& a, void* scratch, size_t sort_tmp, size_
     ANN_CUDA_TRY(cudaMemcpyAsync(host_totals, item_off + C, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     ANN_CUDA_TRY(cudaMemcpyAsync(host_totals + 1, cand_off + nq, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     ANN_CUDA_TRY(cudaMemcpyAsync(host_totals + 2, flags, sizeof(int), cudaMemcpyDeviceToHost, st));
-    ANN_CUDA_TRY(cudaStreamSynchronize(st));
+    if (sync) ANN_CUDA_TRY(cudaStreamSynchronize(st));
     IvfBatchArgs b{};
     b.ix = a.ix;
     b.plan = a.plan;

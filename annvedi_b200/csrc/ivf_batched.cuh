@@ -27,8 +27,10 @@ struct IvfBatchArgs {
 size_t batched_scratch_bytes(int nq, int npc, int C, size_t* sort_tmp, size_t* scan_tmp);
 // Groups the plan's probes by list, counts work items and candidate offsets; host_totals[0..2] =
 // {work items, total candidates, fallback flag}. Synchronises the stream.
+// With sync = false the totals are copied to host_totals (which must then be page-locked) without waiting: they
+// are valid after the caller's next synchronisation of st.
 int batched_prepare(const IvfQueryArgs& a, void* scratch, size_t sort_tmp, size_t scan_tmp, IvfBatchArgs* out,
-                    int64_t* host_totals, cudaStream_t st);
+                    int64_t* host_totals, cudaStream_t st, bool sync = true);
 int launch_batched(const IvfBatchArgs& b, const float* qdev, float* qs, float* D, cudaStream_t st);
 
 }  // namespace annb

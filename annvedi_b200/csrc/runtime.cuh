@@ -15,6 +15,7 @@ struct ann_workspace {
     size_t dev_cap = 0;
     char* big = nullptr;   // second device arena for large per-batch buffers sized after planning
     size_t big_cap = 0;
+    int64_t* pinned = nullptr;  // page-locked host words for totals read after a later synchronisation
     std::mutex mu;         // serialises growth; concurrent calls must still use separate workspaces
 };
 
@@ -38,6 +39,8 @@ struct DeviceGuard {
 // block may be in use by earlier asynchronous work).
 int ws_reserve_device(ann_workspace* ws, size_t bytes);
 int ws_reserve_big(ann_workspace* ws, size_t bytes);
+// The workspace's page-locked host words (at least 8), allocated on first use.
+int ws_pinned(ann_workspace* ws, int64_t** out);
 
 // Stage timer: records CUDA events around consecutive stages of a call on its stream; totals are
 // accumulated lazily (collect() synchronises on the recorded events). A call's first stage index is
