@@ -57,6 +57,7 @@ struct ann_ivf {
     __nv_bfloat16* cent_bf16 = nullptr;  // [C, kpad] BF16 operand form of the centroids
     float2* sq8_fac = nullptr;           // [n] (1, reconstructed |x|^2) of the SQ8 rows (codes on the tensor cores)
     int kpad = 0;
+    float cent_norm_max = 0.f;           // the largest centroid norm (the coarse ranking's key error bound)
     std::mutex tc_mu;
     int64_t query_count = 0;
     // query options (ann_ivf_set_option)
@@ -88,6 +89,7 @@ static void ivf_free_state(ann_ivf* h) {
         if (p) cudaFree(p);
     h->base_bf16 = nullptr;
     h->cent_bf16 = nullptr;
+    h->cent_norm_max = 0.f;
     h->sq8_fac = nullptr;
     h->proj = h->projT = h->lsh_mean = nullptr;
     h->tab_off = nullptr;
@@ -677,6 +679,21 @@ static int ivf_ensure_tc(ann_ivf* h, bool i8, cudaStream_t st) {
             return rc;
         }
         ANN_CUDA_TRY(cudaStreamSynchronize(st));
+        // the largest centroid norm, from a host copy of the (small) centroid table
+        std::vector<float> hc((size_t)h->C * h->dpad);
+        const cudaError_t ce = cudaMemcpy(hc.data(), h->centroids, sizeof(float) * hc.size(), cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) {
+            cudaFree(cb);
+            set_error("tensor-core IVF: %s", cudaGetErrorString(ce));
+            return ANN_ERR_CUDA;
+        }
+        double mx = 0.0;
+        for (int c = 0; c < h->C; ++c) {
+            double s2 = 0.0;
+            for (int d = 0; d < h->dim; ++d) s2 += (double)hc[(size_t)c * h->dpad + d] * hc[(size_t)c * h->dpad + d];
+            mx = std::max(mx, s2);
+        }
+        h->cent_norm_max = (float)(std::sqrt(mx) * (1.0 + 1e-6));
         h->cent_bf16 = cb;
         h->kpad = kpad;
     }
@@ -1010,7 +1027,8 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         if ((rc = launch_tc_operand(qdev, nq, h->dim, h->dpad, qb, h->kpad, kTcQuery, ANN_METRIC_L2, 0, st))) return rc;
         TcGemmArgs ca{nq, h->C, h->kpad, nullptr, ckeys, h->C, h->d_err};
         if ((rc = launch_tc_gemm(qb, h->cent_bf16, ca, st))) return rc;
-        if ((rc = launch_tc_coarse(ckeys, h->C, nq, h->C, c.npc, 16, qdev, h->centroids, h->dpad, probes, st)))
+        if ((rc = launch_tc_coarse(ckeys, h->C, nq, h->C, c.npc, 16, qdev, h->centroids, h->dpad, probes, st,
+                                   h->cent_norm_max, h->dim)))
             return rc;
         if (c.i8 && (rc = launch_tc_sq8_query(qdev, nq, h->dim, h->dpad, h->scale, h->offset, q8, h->dpad8, qfac, st)))
             return rc;

@@ -492,7 +492,8 @@ constexpr int kCoarseChunks = 16;  // dims up to 512 take the register path of t
 // one warp per query
 __global__ void __launch_bounds__(128) tc_coarse_kernel(const float* __restrict__ keys, int64_t ldk, int nq, int C,
                                                        int npc, int m, const float* __restrict__ q,
-                                                       const float* __restrict__ cent, int dpad, int32_t* probes) {
+                                                       const float* __restrict__ cent, int dpad, int32_t* probes,
+                                                       float cmax, int dim) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cap = topk_cap(m);
@@ -542,17 +543,42 @@ __global__ void __launch_bounds__(128) tc_coarse_kernel(const float* __restrict_
         }
     }
     top.compact();
-    const int cnt = top.count;
-    // exact FP32 squared distances of the m candidates
+    const int cnt = top.count;  // sK / sI [0, cnt): the best m by (key, id), ascending
     const float* qv = q + (int64_t)qi * dpad;
+    // The certified window. A BF16 key differs from the real key |c|^2 - 2 q.c by at most
+    //   eps = |q| |c| (2^-7 * 1.05 + (dim + 3) 2^-21 * 2.1) + |c|^2 (dim + 3) 2^-21
+    // (both operands rounded to 8 significant bits, relative 2^-9 each; FP32 accumulation of dim + 3 products,
+    // bounded with a factor 2 to allow truncating adds). With T the npc-th smallest key, a candidate whose key
+    // exceeds T + 2 eps + delta -- delta bounding the FP32 rounding of the exact distances below -- is farther
+    // than the best npc candidates in FP32 as in real arithmetic, so it is never among them: only the
+    // candidates inside the window get exact distances, and the result is the one over all m.
+    int ncert = cnt;
+    if (cmax > 0.f && cnt > npc) {
+        float s2 = 0.f;
+        for (int d = lane; d < dpad; d += 32) s2 = fmaf(qv[d], qv[d], s2);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        const float qn = sqrtf(s2) * 1.0001f;
+        const float acc = (float)(dim + 3) * 4.76837158e-7f;  // (dim + 3) 2^-21
+        const float eps = qn * cmax * (7.8125e-3f * 1.05f + 2.1f * acc) + cmax * cmax * acc;
+        const float delta = acc * (qn + cmax) * (qn + cmax);
+        const float lim = sK[npc - 1] + 2.f * eps + delta;
+        int inside = 0;
+        for (int e = lane; e < cnt; e += 32) inside += sK[e] <= lim;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) inside += __shfl_xor_sync(0xffffffffu, inside, o);
+        ncert = max(npc, inside);  // sK is sorted: the window is a prefix
+        __syncwarp();
+    }
+    // exact FP32 squared distances of the candidates in the window
     if (dpad <= 32 * kCoarseChunks) {
         // the query's pieces in registers; two centroids at a time with all their pieces loaded before
         // use; per lane the sum runs over d = lane, lane + 32, ... as in the loop below
         float qr[kCoarseChunks];
 #pragma unroll
         for (int i = 0; i < kCoarseChunks; ++i) qr[i] = lane + 32 * i < dpad ? qv[lane + 32 * i] : 0.f;
-        for (int e = 0; e < cnt; e += 2) {
-            const bool two = e + 1 < cnt;
+        for (int e = 0; e < ncert; e += 2) {
+            const bool two = e + 1 < ncert;
             const float* xa = cent + (int64_t)sI[e] * dpad;
             const float* xb = cent + (int64_t)(two ? sI[e + 1] : sI[e]) * dpad;
             float va[kCoarseChunks], vb[kCoarseChunks];
@@ -583,7 +609,7 @@ __global__ void __launch_bounds__(128) tc_coarse_kernel(const float* __restrict_
             __syncwarp();
         }
     }
-    for (int e = 0; e < cnt && dpad > 32 * kCoarseChunks; ++e) {
+    for (int e = 0; e < ncert && dpad > 32 * kCoarseChunks; ++e) {
         const int c = sI[e];
         const float* x = cent + (int64_t)c * dpad;
         float acc = 0.f;
@@ -596,9 +622,9 @@ __global__ void __launch_bounds__(128) tc_coarse_kernel(const float* __restrict_
         if (lane == 0) sK[e] = acc;
         __syncwarp();
     }
-    for (int e = cnt + lane; e < cap; e += 32) {
+    for (int e = ncert + lane; e < cap; e += 32) {  // outside the window (or empty): sorted last
         sK[e] = kInf;
-        sI[e] = kNoId;
+        if (e >= cnt) sI[e] = kNoId;
     }
     __syncwarp();
     warp_sort_smem(sK, sI, cap);
@@ -608,13 +634,14 @@ __global__ void __launch_bounds__(128) tc_coarse_kernel(const float* __restrict_
 }  // namespace
 
 int launch_tc_coarse(const float* keys, int64_t ldk, int nq, int C, int npc, int margin, const float* q,
-                     const float* centroids, int dpad, int32_t* probes, cudaStream_t st) {
+                     const float* centroids, int dpad, int32_t* probes, cudaStream_t st, float cmax, int dim) {
     if (nq == 0) return ANN_OK;
     const int m = std::min(C, npc + margin);
     ANN_CHECK_ARG(npc >= 1 && npc <= m && m <= 1024, "tensor-core coarse ranking: npc=%d, m=%d", npc, m);
     const size_t smem = (size_t)4 * 2 * topk_cap(m) * 4;
     ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(tc_coarse_kernel)));
-    tc_coarse_kernel<<<(unsigned)ceil_div(nq, 4), 128, smem, st>>>(keys, ldk, nq, C, npc, m, q, centroids, dpad, probes);
+    tc_coarse_kernel<<<(unsigned)ceil_div(nq, 4), 128, smem, st>>>(keys, ldk, nq, C, npc, m, q, centroids, dpad, probes,
+                                                                    cmax, dim > 0 ? dim : dpad);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

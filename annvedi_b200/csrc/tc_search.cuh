@@ -109,8 +109,11 @@ int launch_tc_compact_rows(const int* list, const int* count, int max_count, con
 // Coarse ranking of the tensor-core IVF form from BF16 keys [nq, C] (ldk per row): per query, the best
 // m = min(C, npc + margin) centroids by key, their exact FP32 squared distances (FP32 queries and
 // centroids, row stride dpad), and the best npc of those by (distance, id) into probes [nq, npc],
-// best first.
+// best first. With cmax > 0 (the largest centroid norm; dim the vectors' dimension) only the candidates whose
+// key lies within the keys' certified error window of the npc-th key get exact distances: the others cannot
+// be among the best npc, so the result is the same.
 int launch_tc_coarse(const float* keys, int64_t ldk, int nq, int C, int npc, int margin, const float* q,
-                     const float* centroids, int dpad, int32_t* probes, cudaStream_t st);
+                     const float* centroids, int dpad, int32_t* probes, cudaStream_t st, float cmax = 0.f,
+                     int dim = 0);
 
 }  // namespace annb
