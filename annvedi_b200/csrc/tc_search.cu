@@ -356,6 +356,40 @@ __device__ __forceinline__ void warp_hist_add(int* hist, bool valid, uint32_t di
 // `staged` keys is read once into shared memory (as ordered keys) and the passes run there; a longer one is read
 // from global memory by every pass.
 constexpr int kBarThreads = 128;
+constexpr int kBarBins = 1024;   // linear bins of the staged form
+constexpr int kBarBinCap = 256;  // keys of a rank's bin picked by counting; more fall back to radix passes
+
+// The bin of rank `rank` (1-based) in hist[0..kBarBins) and the count of keys in lower bins, by one warp (each
+// lane sums 32 consecutive bins, a warp scan, then the holding lane walks its bins). Every lane returns them.
+__device__ __forceinline__ void warp_bin_pick(const int* hist, int rank, int* bin, int* before) {
+    const int lane = threadIdx.x & 31;
+    int sum = 0;
+    for (int j = 0; j < kBarBins / 32; ++j) sum += hist[lane * (kBarBins / 32) + j];
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int excl = incl - sum;
+    const unsigned hit = __ballot_sync(0xffffffffu, excl < rank && rank <= incl);
+    const int src = hit ? __ffs(hit) - 1 : 31;
+    int b = kBarBins - 1, bf = 0;
+    if (lane == src && hit) {
+        int acc = excl;
+        for (int j = 0; j < kBarBins / 32; ++j) {
+            const int c = hist[lane * (kBarBins / 32) + j];
+            if (acc + c >= rank) {
+                b = lane * (kBarBins / 32) + j;
+                bf = acc;
+                break;
+            }
+            acc += c;
+        }
+    }
+    *bin = __shfl_sync(0xffffffffu, b, src);
+    *before = __shfl_sync(0xffffffffu, bf, src);
+}
 __global__ void __launch_bounds__(kBarThreads) block_bars_kernel(const float* __restrict__ keys,
                                                                  const int64_t* __restrict__ offs,
                                                                  const int64_t* __restrict__ lens, int nq, int r1,
@@ -373,6 +407,94 @@ __global__ void __launch_bounds__(kBarThreads) block_bars_kernel(const float* __
     if (in_smem)
         for (int64_t p = threadIdx.x; p < n; p += kBarThreads) smem_bars[p] = ord_key(kq[p]);
     const bool want1 = r1 <= n, want2 = r2 <= n;  // uniform across the block
+    if (in_smem && n > 0 && (want1 || want2)) {
+        // Linear bins over [min, max] of the staged keys. The bin of a key is monotone in the key, so a rank's key
+        // lies in the bin where the running count reaches the rank; it is picked among that bin's keys by
+        // counting, exactly. A bin holding more than kBarBinCap keys leaves the rank to the radix passes below.
+        __shared__ int sBin[kBarBins];
+        __shared__ uint32_t sList[2][kBarBinCap];
+        __shared__ int sAux[8];  // [2..5] bin and count below per rank, [6,7] list sizes
+        __shared__ float sRes[2];
+        if (threadIdx.x == 0) sAux[6] = sAux[7] = 0;
+        for (int i = threadIdx.x; i < kBarBins; i += kBarThreads) sBin[i] = 0;
+        __syncthreads();  // also orders the staging above
+        uint32_t omin = 0xffffffffu, omax = 0u;
+        for (int64_t p = threadIdx.x; p < n; p += kBarThreads) {
+            omin = min(omin, smem_bars[p]);
+            omax = max(omax, smem_bars[p]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            omin = min(omin, __shfl_xor_sync(0xffffffffu, omin, o));
+            omax = max(omax, __shfl_xor_sync(0xffffffffu, omax, o));
+        }
+        __shared__ uint32_t sMinMax[2];
+        if (threadIdx.x == 0) {
+            sMinMax[0] = 0xffffffffu;
+            sMinMax[1] = 0u;
+        }
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&sMinMax[0], omin);
+            atomicMax(&sMinMax[1], omax);
+        }
+        __syncthreads();
+        const float lo = from_ord(sMinMax[0]), hi = from_ord(sMinMax[1]);
+        const float scale = (float)kBarBins / (hi - lo);
+        if (!(hi > lo) || !isfinite(scale)) {  // every key the same (or not finite): each rank's key is lo
+            if (threadIdx.x == 0 && hi == lo) {
+                bar1[q] = want1 ? lo : kInf;
+                bar2[q] = want2 ? lo : kInf;
+            }
+            if (hi == lo) return;
+        } else {
+            auto bin_of = [&](uint32_t o) { return min(kBarBins - 1, (int)((from_ord(o) - lo) * scale)); };
+            for (int64_t p = threadIdx.x; p < n; p += kBarThreads) atomicAdd(&sBin[bin_of(smem_bars[p])], 1);
+            __syncthreads();
+            if (warp < 2 && (warp == 0 ? want1 : want2)) {
+                int b, bf;
+                warp_bin_pick(sBin, warp == 0 ? r1 : r2, &b, &bf);
+                if ((threadIdx.x & 31) == 0) {
+                    sAux[2 + 2 * warp] = b;
+                    sAux[3 + 2 * warp] = bf;
+                }
+            }
+            __syncthreads();
+            const bool fit1 = want1 && sBin[sAux[2]] <= kBarBinCap;
+            const bool fit2 = want2 && sBin[sAux[4]] <= kBarBinCap;
+            if ((!want1 || fit1) && (!want2 || fit2)) {  // uniform: both ranks settle here
+                for (int64_t p = threadIdx.x; p < n; p += kBarThreads) {
+                    const uint32_t o = smem_bars[p];
+                    const int b = bin_of(o);
+                    if (want1 && b == sAux[2]) sList[0][atomicAdd(&sAux[6], 1)] = o;
+                    if (want2 && b == sAux[4]) sList[1][atomicAdd(&sAux[7], 1)] = o;
+                }
+                __syncthreads();
+                for (int r = 0; r < 2; ++r) {
+                    if (r == 0 ? !want1 : !want2) continue;
+                    const int cnt = sAux[6 + r];
+                    const int want = (r == 0 ? r1 : r2) - sAux[3 + 2 * r] - 1;  // 0-based rank inside the bin
+                    for (int t = threadIdx.x; t < cnt; t += kBarThreads) {
+                        const uint32_t v = sList[r][t];
+                        int below = 0, equal_before = 0;
+                        for (int u = 0; u < cnt; ++u) {
+                            const uint32_t w = sList[r][u];
+                            below += w < v;
+                            equal_before += (w == v) && (u < t);
+                        }
+                        if (below + equal_before == want) sRes[r] = from_ord(v);
+                    }
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    bar1[q] = want1 ? sRes[0] : kInf;
+                    bar2[q] = want2 ? sRes[1] : kInf;
+                }
+                return;
+            }
+        }
+        __syncthreads();  // the radix passes below reuse nothing of the above but the staged keys
+    }
     uint32_t p1 = 0, p2 = 0, pmask = 0;
     int64_t rem1 = r1, rem2 = r2;
     for (int shift = 24; shift >= 0 && (want1 || want2); shift -= 8) {
