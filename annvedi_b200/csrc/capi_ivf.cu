@@ -1395,15 +1395,18 @@ int ann_ivf_query(ann_ivf* h, ann_workspace* ws, const float* queries, int32_t n
         dists_dev = cv.take<float>((size_t)nq * k);
     }
     char* scratch = ws->dev + head_bytes;
+    const float* qrows = qdev;  // the queries in the padded layout the kernels read (read only)
     if (host) {
         if ((rc = queries_in(qdev, dpad, queries, ldq, nq, h->dim, st))) return rc;
+    } else if (h->dim == dpad && ldq == dpad && (reinterpret_cast<uintptr_t>(queries) & 15) == 0) {
+        qrows = queries;  // already in that layout: no copy
     } else {
         rc = launch_pad_rows(queries, nq, h->dim, ldq, qdev, dpad, st);
         if (rc) return rc;
     }
     for (int q0 = 0; q0 < nq; q0 += qc) {
         const int nc = std::min(qc, nq - q0);
-        rc = ivf_query_device(h, ws, c, scratch, qdev + (size_t)q0 * dpad, nc, ids_dev + (size_t)q0 * k,
+        rc = ivf_query_device(h, ws, c, scratch, qrows + (size_t)q0 * dpad, nc, ids_dev + (size_t)q0 * k,
                               dists_dev ? dists_dev + (size_t)q0 * k : nullptr, st);
         if (rc) return rc;
     }
