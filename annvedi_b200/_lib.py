@@ -80,6 +80,7 @@ SIGNATURES = [
     ("ann_flat_query_tc", ctypes.c_int, [_vp, _vp, _vp, _i32, _i64, _i32, _i32, _i32, _vp, _vp, _vp]),
     ("ann_flat_scores_tc", ctypes.c_int, [_vp, _vp, _i32, _i64, _vp, _vp]),
     ("ann_flat_set_tc_precision", ctypes.c_int, [_vp, _i32]),
+    ("ann_flat_set_option", ctypes.c_int, [_vp, _i32, ctypes.c_int64]),
     ("ann_flat_device_status", ctypes.c_int, [_vp]),
     ("ann_merge_topk", ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp, _vp]),
     ("ann_select_smallest", ctypes.c_int, [_vp, _i64, _vp, _i32, _i32, _vp, _vp, _vp]),

@@ -115,3 +115,22 @@ def tune_flat_tc(index, base, queries, kth, k: int = 100, target: float = 0.95, 
         if rec >= target and (best is None or row["qps"] > best["qps"]):
             best = row
     return {"best": best, "table": table, "target": target}
+
+
+def tune_flat_tile(index, queries, k: int = 100, tiles=(8, 16, 32), reps: int = 2) -> dict:
+    """Fastest query tile (queries per CTA) of a LinearIndex's exact scan for this batch, timed over `reps`
+    calls after a warm-up call; the tile is left set on the index. Results do not depend on the tile, so no
+    recall is needed. Returns {"best": {...}, "table": [...]} with tile, ms_per_batch and qps."""
+    import torch
+    stream = torch.cuda.current_stream()
+    nq = queries.shape[0]
+    ids = torch.empty(nq, k, dtype=torch.int64, device=queries.device)
+    dists = torch.empty(nq, k, dtype=torch.float32, device=queries.device)
+    table = []
+    for tile in tiles:
+        index.set_query_tile(tile)
+        ms = _time(lambda: index.search(queries, k, mode="exact", out_ids=ids, out_dists=dists), reps, stream)
+        table.append({"tile": tile, "ms_per_batch": round(ms, 3), "qps": round(nq / (ms / 1e3), 1)})
+    best = min(table, key=lambda r: r["ms_per_batch"])
+    index.set_query_tile(best["tile"])
+    return {"best": best, "table": table}

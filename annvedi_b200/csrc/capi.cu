@@ -343,7 +343,7 @@ int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t
     }
     bool radix_merge = false;
     if (mode == ANN_MODE_EXACT) {
-        bq = std::min(flat_scan_bq(nq), flat_scan_max_bq(kk));
+        bq = std::min(h->query_tile > 0 ? h->query_tile : flat_scan_bq(nq), flat_scan_max_bq(kk));
         nsplit = flat_choose_nsplit(h->n, nq, bq, &rps, flat_scan_ctas_per_sm(bq, kk, dpad, h->metric));
         sz.take<float>((size_t)nq * nsplit * kk);
         sz.take<int>((size_t)nq * nsplit * kk);
@@ -612,6 +612,21 @@ int ann_flat_scores_tc(ann_flat* h, const float* queries, int32_t nq, int64_t ld
     if ((rc = launch_tc_unpermute(tmp, nq, h->n, h->row_mult, out_keys, st))) return rc;
     ANN_CUDA_TRY(cudaStreamSynchronize(st));
     return flat_check_err(h);
+}
+
+int ann_flat_set_option(ann_flat* h, int32_t option, int64_t value) {
+    clear_error();
+    ANN_CHECK_ARG(h != nullptr, "ann_flat_set_option: null index");
+    switch (option) {
+        case ANN_FLAT_OPT_QUERY_TILE:
+            ANN_CHECK_ARG(value == 0 || value == 8 || value == 16 || value == 32,
+                          "ann_flat_set_option: query tile %lld (0, 8, 16 or 32)", (long long)value);
+            h->query_tile = (int)value;
+            return ANN_OK;
+        default:
+            set_error("ann_flat_set_option: unknown option %d", option);
+            return ANN_ERR_INVALID;
+    }
 }
 
 int ann_flat_set_tc_precision(ann_flat* h, int32_t precision) {

@@ -20,6 +20,7 @@ struct ann_flat {
     __nv_bfloat16* base_bf16 = nullptr;  // [n, kpad] BF16 operand form for the tensor-core scan (built on first use)
     int64_t row_mult = 1;                // position p of base_bf16 holds row (p * row_mult) mod n
     int kpad = 0;                        // operand columns: dim plus the key columns, rounded up to 64
+    int query_tile = 0;                  // the exact scan's queries per CTA (0: chosen by the batch size)
     int* d_err = nullptr;                // device flag of bounded waits
     int tc_kind = 0;                     // element kind of the tensor-core search (0 BF16, 1 E4M3)
     uint8_t* base_e4m3 = nullptr;        // [n, kpad8] E4M3 operand form, Weyl order, built on first use

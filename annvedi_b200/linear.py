@@ -172,6 +172,11 @@ class LinearIndex:
                                                _lib.MEM_HOST, _lib.ptr(ids), _lib.ptr(dists), None))
         return ids, dists
 
+    def set_query_tile(self, tile: int = 0) -> None:
+        """Queries per CTA of the exact scan's staged form (ANN_FLAT_OPT_QUERY_TILE): 8, 16 or 32, or 0 to pick
+        by the batch size. Results are the same for 8, 16 and 32; the tile changes speed only."""
+        _lib.check(self._lib.ann_flat_set_option(self._h, 1, int(tile)))
+
     def set_tc_precision(self, precision: str = "bf16") -> None:
         """Element kind of search_tc / scores_tc: "bf16" (default) or "e4m3" (scaled FP8: twice the tensor
         rate, a coarser key; pair it with a deeper refine_r)."""

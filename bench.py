@@ -268,6 +268,11 @@ def run_ours(args, rank, world, local):
         def flat_step():
             flat.search(queries, K_NN, mode="exact", out_ids=f_ids, out_dists=f_d)
 
+        # the scan's query tile (a tile shape: queries sharing each staged row chunk) chosen by timing, so the
+        # denominator is the plain scan at its best tile
+        from annvedi_b200 import autotune
+        flat_tiles = autotune.tune_flat_tile(flat, queries, K_NN, tiles=(8, 16, 32), reps=1)
+
         flat_step()
         torch.cuda.synchronize()
         flat_recall = recall_evaluator(base, queries[:1000], f_ids[:1000], kth[:1000])
@@ -281,7 +286,9 @@ def run_ours(args, rank, world, local):
         fscan_ms = fprof["scan_ms"] / max(1, fprof["scan_launches"])
         fp32_instr = 2.0 * n * d * q  # one sub + one fma per element pair
         flat_line = {"qps": round(flat_qps, 1), "ms_per_batch": round(flat_ms, 3), "recall_at_100": round(flat_recall, 4),
-                     "kernel": "flat_scan_kernel", "fp32_instr_per_s": round(fp32_instr / (fscan_ms / 1e3), 1)}
+                     "kernel": "flat_scan_kernel", "fp32_instr_per_s": round(fp32_instr / (fscan_ms / 1e3), 1),
+                     "query_tile": flat_tiles["best"]["tile"], "query_tile_sweep": flat_tiles["table"]}
+        flat.set_query_tile(0)  # small batches below pick their own tiles
         # HBM-bound regime: a query per call streams the whole base once (flat_stream_kernel)
         dpad = -(-d // 32) * 32
         small = {}

@@ -138,6 +138,15 @@ int ann_flat_query_tc(ann_flat* h, ann_workspace* ws, const float* queries, int3
 #define ANN_TC_E4M3 1
 int ann_flat_set_tc_precision(ann_flat* h, int32_t precision);
 
+/* Options of the exact scan (no counterpart in the reference):
+ *   ANN_FLAT_OPT_QUERY_TILE: queries per CTA of the exact scan's staged form -- 8, 16 or 32 queries share
+ *     each staged row chunk; 0 (the default) picks by the batch size (batches of up to 4 queries then stream
+ *     the rows instead, whose sums run in another order). Among 8, 16 and 32 the results are identical (every
+ *     tile sums a pair's terms in the same order and the splits merge by (distance, id)); the tile changes
+ *     speed only, and autotune.tune_flat_tile picks it by timing. */
+#define ANN_FLAT_OPT_QUERY_TILE 1
+int ann_flat_set_option(ann_flat* h, int32_t option, int64_t value);
+
 /* Diagnostic: the tensor-core key matrix out_keys[nq][n] (device pointers; synchronous). */
 int ann_flat_scores_tc(ann_flat* h, const float* queries, int32_t nq, int64_t ldq, float* out_keys, void* stream);
 

@@ -161,3 +161,27 @@ def test_full_size_c1_exact_and_reference(cuda):
     oids, ovals = refmod.linear_query(w.base, w.queries[:32], 100, lanes=16)
     np.testing.assert_array_equal(rids, oids)
     assert ix.total_distances_count() == 100_000 * 1032
+
+
+@pytest.mark.parametrize("k", [10, 100])
+def test_query_tile_does_not_change_results(cuda, k):
+    """The exact scan's query tile (ANN_FLAT_OPT_QUERY_TILE) changes speed only: tiles of 8, 16 and 32 queries
+    return the same ids and distances as the automatic choice for this batch, bit for bit; other tiles are
+    refused."""
+    import torch
+    from annvedi_b200.linear import LinearIndex
+    rng = np.random.default_rng(40)
+    base = rng.standard_normal((60000, 96)).astype(np.float32)
+    q = torch.from_numpy(rng.standard_normal((300, 96)).astype(np.float32)).cuda()
+    ix = LinearIndex(device=0, mode="exact")
+    ix.fit(torch.from_numpy(base).cuda())
+    want_i, want_d = ix.search(q, k, mode="exact")
+    want_i, want_d = want_i.cpu().numpy(), want_d.cpu().numpy()
+    for tile in (8, 16, 32):
+        ix.set_query_tile(tile)
+        got_i, got_d = ix.search(q, k, mode="exact")
+        np.testing.assert_array_equal(got_i.cpu().numpy(), want_i, err_msg=f"tile {tile}")
+        np.testing.assert_array_equal(got_d.cpu().numpy(), want_d, err_msg=f"tile {tile}")
+    for bad in (1, 4, 3):
+        with pytest.raises(Exception):
+            ix.set_query_tile(bad)
