@@ -767,6 +767,7 @@ static size_t ivf_scratch(const ann_ivf* h, const IvfQueryCfg& c, int nq) {
     if (c.lsh_keys) sz.take<float>((size_t)nq * c.ub_cand);
     if (c.tc) {
         sz.take<float>((size_t)nq * h->C);  // BF16 coarse keys
+        sz.take<float>((size_t)nq * ceil_div(h->C, 32));  // their 32-centroid chunk minima
         sz.take<__nv_bfloat16>((size_t)nq * h->kpad);
         sz.take<unsigned char>((size_t)nq * c.npc * tc_pair_row_bytes(h));
         sz.take<int8_t>((size_t)nq * h->dpad8);  // int8 query weights and factors (ANN_MODE_TC_SQ8)
@@ -984,6 +985,7 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
     int* lpert = c.lsh ? cv.take<int>((size_t)nq * h->T * std::max(1, lsh_p)) : nullptr;
     float* lkeys = c.lsh_keys ? cv.take<float>((size_t)nq * c.ub_cand) : nullptr;
     float* ckeys = c.tc ? cv.take<float>((size_t)nq * h->C) : nullptr;
+    float* ckmin = c.tc ? cv.take<float>((size_t)nq * ceil_div(h->C, 32)) : nullptr;
     __nv_bfloat16* qb = c.tc ? cv.take<__nv_bfloat16>((size_t)nq * h->kpad) : nullptr;
     unsigned char* Apk = c.tc ? cv.take<unsigned char>((size_t)nq * c.npc * tc_pair_row_bytes(h)) : nullptr;
     int8_t* q8 = c.tc ? cv.take<int8_t>((size_t)nq * h->dpad8) : nullptr;
@@ -1026,9 +1028,10 @@ static int ivf_query_device(ann_ivf* h, ann_workspace* ws, const IvfQueryCfg& c,
         // BF16 keys to every centroid, then the exact FP32 order of the best npc + 16
         if ((rc = launch_tc_operand(qdev, nq, h->dim, h->dpad, qb, h->kpad, kTcQuery, ANN_METRIC_L2, 0, st))) return rc;
         TcGemmArgs ca{nq, h->C, h->kpad, nullptr, ckeys, h->C, h->d_err};
+        ca.out_cmin = ckmin;  // and each query's 32-centroid chunk minima, which let the ranking skip chunks
         if ((rc = launch_tc_gemm(qb, h->cent_bf16, ca, st))) return rc;
         if ((rc = launch_tc_coarse(ckeys, h->C, nq, h->C, c.npc, 16, qdev, h->centroids, h->dpad, probes, st,
-                                   h->cent_norm_max, h->dim)))
+                                   h->cent_norm_max, h->dim, ckmin)))
             return rc;
         if (c.i8 && (rc = launch_tc_sq8_query(qdev, nq, h->dim, h->dpad, h->scale, h->offset, q8, h->dpad8, qfac, st)))
             return rc;

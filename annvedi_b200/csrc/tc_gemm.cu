@@ -45,6 +45,11 @@ struct KindOf {
 constexpr int kTmemCols = 512;
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// 4 bytes from global src to shared dst, asynchronously (zeros when !valid: no bytes are read)
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(su32(dst)), "l"(src), "r"(valid ? 4 : 0)
+                 : "memory");
+}
 __device__ __forceinline__ uint64_t gtimer() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -371,8 +376,29 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
             }
             const float an = (a.normA && mvalid) ? a.normA[arow] : 0.f;
             const float rfac = (a.row_fac && mvalid) ? a.row_fac[arow] : 1.f;
-            // rows past M (TMA zero fill) get a bar no key passes
-            const float tau = (a.tau && mvalid) ? a.tau[rq] : -kInf;
+            // rows past M or past a grouped item's pairs get a NaN bar, which no key passes (not even a -inf
+            // key, which a -inf bar would let through)
+            const float tau = (a.tau && mvalid) ? a.tau[rq] : __int_as_float(0x7fffffff);
+            // filter mode with scaled operands: the warp's kCols column factors, copied here (asynchronously,
+            // so that they land while the MMAs run) into its (otherwise unused) transpose buffer as two arrays
+            // (x then y), so that the factors of two adjacent columns load as one float2 broadcast; zeros past
+            // the valid columns
+            const bool staged = a.col_fac != nullptr && (kFilterOnly || a.out == nullptr);
+            float* sfx = tw;
+            float* sfy = tw + kCols;
+            if (staged) {
+                __syncwarp();  // every lane is done with the last tile's factors
+#pragma unroll
+                for (int i = 0; i < kCols / 32; ++i) {
+                    const int lcol = col0 + 32 * i + lane;  // column within the tile
+                    const int col = n0 + lcol;
+                    const int64_t nrow = grouped ? cbase + lcol : (int64_t)(col / kBN) * kBN * a.b_tile_stride + col % kBN;
+                    const bool in = lcol < ncols;
+                    const float* src = reinterpret_cast<const float*>(a.col_fac + (in ? nrow : 0));
+                    cp_async4(sfx + 32 * i + lane, src, in);
+                    cp_async4(sfy + 32 * i + lane, src + 1, in);
+                }
+            }
             // every lane waits; the warp leaves together if any lane gave up, so that no lane is left
             // behind at a warp-wide instruction
             const bool got = bar_wait(&tfull[b], (uint32_t)((acc >> 1) & 1), a.err, a.wait_ns);
@@ -425,28 +451,108 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
             const float tau_up = nextafterf(tau, kInf);
             const float2 ntau2 = make_float2(-tau_up, -tau_up);
             const uint32_t tbase = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(b * kBN + col0);
-            // filter mode with scaled operands: the warp's kCols column factors staged once per tile in
-            // its (otherwise unused) transpose buffer as two arrays (x then y), so that the factors of
-            // two adjacent columns load as one float2 broadcast
-            const bool staged = a.col_fac != nullptr && (kFilterOnly || a.out == nullptr);
-            float* sfx = tw;
-            float* sfy = tw + kCols;
             if (staged) {
-                __syncwarp();
-#pragma unroll
-                for (int i = 0; i < kCols / 32; ++i) {
-                    const int lcol = col0 + 32 * i + lane;  // column within the tile
-                    const int col = n0 + lcol;
-                    const int64_t nrow = grouped ? cbase + lcol : (int64_t)(col / kBN) * kBN * a.b_tile_stride + col % kBN;
-                    const float2 f = lcol < ncols ? a.col_fac[nrow] : make_float2(0.f, 0.f);
-                    sfx[32 * i + lane] = f.x;
-                    sfy[32 * i + lane] = f.y;
-                }
+                asm volatile("cp.async.wait_all;" ::: "memory");
                 __syncwarp();
             }
             const bool has_an = a.normA != nullptr;  // uniform
+            const bool rowbuf = a.row_cap > 0 && (kFilterOnly || a.out == nullptr);
+            // filter keys of the 32 columns from col0 + c + 32 h (raw accumulators r): the row norm, the
+            // scale factors, NaN past the tile's valid columns
+            auto half_keys = [&](const uint32_t (&r)[32], int h, int c, float (&v)[32]) {
+#pragma unroll
+                for (int u = 0; u < 32; ++u) v[u] = acc_value<KIND>(r[u]) + (has_an ? an : 0.f);
+                if (staged) {
+                    const float2 r2 = make_float2(rfac, rfac);
+#pragma unroll
+                    for (int u = 0; u < 32; u += 4) {
+                        const float4 fx = *reinterpret_cast<const float4*>(sfx + c + 32 * h + u);
+                        const float4 fy = *reinterpret_cast<const float4*>(sfy + c + 32 * h + u);
+                        const float2 t0 = __fmul2_rn(r2, make_float2(v[u], v[u + 1]));
+                        const float2 t1 = __fmul2_rn(r2, make_float2(v[u + 2], v[u + 3]));
+                        const float2 k0 = __ffma2_rn(make_float2(fx.x, fx.y), t0, make_float2(fy.x, fy.y));
+                        const float2 k1 = __ffma2_rn(make_float2(fx.z, fx.w), t1, make_float2(fy.z, fy.w));
+                        v[u] = k0.x;
+                        v[u + 1] = k0.y;
+                        v[u + 2] = k1.x;
+                        v[u + 3] = k1.y;
+                    }
+                }
+                const int lb = col0 + c + 32 * h;
+                if (lb + 32 > ncols) {
+#pragma unroll
+                    for (int u = 0; u < 32; ++u)
+                        if (lb + u >= ncols) v[u] = __int_as_float(0x7fffffff);
+                }
+            };
+            // bit u set when v[u] passes the bar: v[u] <= tau exactly when v[u] - tau_up < 0 (tau_up the next
+            // float above tau: a difference of two distinct floats is never +0, equal ones give +0, a NaN key
+            // gives the positive default NaN), so the sign bits of packed differences, shifted in by funnel
+            // shifts in four independent 8-key chains, form the mask
+            auto half_mask = [&](const float (&v)[32]) -> uint32_t {
+                uint32_t mq[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+#pragma unroll
+                    for (int u = 7; u >= 1; u -= 2) {
+                        const float2 d = __fadd2_rn(make_float2(v[8 * j + u - 1], v[8 * j + u]), ntau2);
+                        mq[j] = __funnelshift_l(__float_as_uint(d.y), mq[j], 1);
+                        mq[j] = __funnelshift_l(__float_as_uint(d.x), mq[j], 1);
+                    }
+                }
+                return (mq[0] | (mq[1] << 8)) | ((mq[2] << 16) | (mq[3] << 24));
+            };
+            // the survivors (mask mm) of keys v, columns col + u, into the row's buffer from slot sl
+            auto put_row = [&](const float (&v)[32], uint32_t mm, int sl, int64_t rbase, int64_t col) {
+                while (mm) {
+                    const int u = __ffs(mm) - 1;
+                    mm &= mm - 1;
+                    if (sl < a.row_cap) {
+                        // v[u] for a run-time u: a five-level select tree on u's bits
+                        float s16[16], s8[8], s4[4], s2[2];
+#pragma unroll
+                        for (int z = 0; z < 16; ++z) s16[z] = (u & 16) ? v[z + 16] : v[z];
+#pragma unroll
+                        for (int z = 0; z < 8; ++z) s8[z] = (u & 8) ? s16[z + 8] : s16[z];
+#pragma unroll
+                        for (int z = 0; z < 4; ++z) s4[z] = (u & 4) ? s8[z + 4] : s8[z];
+#pragma unroll
+                        for (int z = 0; z < 2; ++z) s2[z] = (u & 2) ? s4[z + 2] : s4[z];
+                        a.fkey[rbase + sl] = (u & 1) ? s2[1] : s2[0];
+                        a.fcol[rbase + sl] = (int)(col + u);
+                    }
+                    ++sl;
+                }
+            };
 #pragma unroll 1
             for (int c = 0; c < kCols; c += 64) {
+                // per-row buffers: the survivors of the 64 columns under one atomic, so that the lane waits
+                // for one round trip per 64 columns; one 32-column half in registers at a time (the first
+                // half's keys are loaded and made again for their stores)
+                if (rowbuf) {
+                    uint32_t r[32];
+                    float v[32];
+                    __syncwarp();  // .sync.aligned loads after the divergent survivor stores of the last step
+                    tmem_ld32(tbase + (uint32_t)c, r);
+                    tmem_wait(r);
+                    half_keys(r, 0, c, v);
+                    const uint32_t ma = half_mask(v);
+                    tmem_ld32(tbase + (uint32_t)(c + 32), r);
+                    tmem_wait(r);
+                    half_keys(r, 1, c, v);
+                    const uint32_t mb = half_mask(v);
+                    const int na = __popc(ma);
+                    const int slot = (ma | mb) ? atomicAdd(&a.rcount[rq], na + __popc(mb)) : 0;
+                    const int64_t rbase = (int64_t)rq * a.row_cap;
+                    put_row(v, mb, slot + na, rbase, cbase + col0 + c + 32);
+                    if (__any_sync(0xffffffffu, ma != 0u)) {  // uniform: the warp reloads the first half
+                        tmem_ld32(tbase + (uint32_t)c, r);
+                        tmem_wait(r);
+                        half_keys(r, 0, c, v);
+                        put_row(v, ma, slot, rbase, cbase + col0 + c);
+                    }
+                    continue;
+                }
                 uint32_t r0[32], r1[32];
                 __syncwarp();  // .sync.aligned loads after the divergent survivor stores of the last chunk
                 tmem_ld32(tbase + (uint32_t)c, r0);
@@ -494,6 +600,12 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                             if (lb + u >= ncols) v[u] = __int_as_float(0x7fffffff);
                     }
                     if (!kFilterOnly && a.out) {
+                        if (a.out_cmin && m < a.M && nb < a.N) {  // the chunk's minimum (NaN columns past N ignored)
+                            float mn = v[0];
+#pragma unroll
+                            for (int u = 1; u < 32; ++u) mn = fminf(mn, v[u]);
+                            a.out_cmin[(int64_t)m * ((a.N + 31) / 32) + nb / 32] = mn;
+                        }
                         // transpose through shared memory so each store covers 32 consecutive columns
 #pragma unroll
                         for (int u = 0; u < 32; ++u) tw[lane * 33 + u] = v[u];
@@ -504,45 +616,8 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                         }
                         __syncwarp();
                     } else {
-                        // v[u] <= tau exactly when v[u] - tau_up < 0 (tau_up the next float above tau: a
-                        // difference of two distinct floats is never +0, equal ones give +0, a NaN key
-                        // gives the positive default NaN), so the sign bits of packed differences, shifted
-                        // in by funnel shifts in four independent 8-key chains, form the mask
-                        uint32_t mq[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-#pragma unroll
-                            for (int u = 7; u >= 1; u -= 2) {
-                                const float2 d = __fadd2_rn(make_float2(v[8 * j + u - 1], v[8 * j + u]), ntau2);
-                                mq[j] = __funnelshift_l(__float_as_uint(d.y), mq[j], 1);
-                                mq[j] = __funnelshift_l(__float_as_uint(d.x), mq[j], 1);
-                            }
-                        }
-                        uint32_t msk = (mq[0] | (mq[1] << 8)) | ((mq[2] << 16) | (mq[3] << 24));
-                        if (a.row_cap > 0) {  // per-row buffers: this lane's survivors, one atomic
-                            if (msk) {
-                                int slot = atomicAdd(&a.rcount[rq], __popc(msk));
-                                const int64_t rbase = (int64_t)rq * a.row_cap;
-                                while (msk) {
-                                    const int u = __ffs(msk) - 1;
-                                    msk &= msk - 1;
-                                    if (slot < a.row_cap) {
-                                        float s16[16], s8[8], s4[4], s2[2];
-#pragma unroll
-                                        for (int z = 0; z < 16; ++z) s16[z] = (u & 16) ? v[z + 16] : v[z];
-#pragma unroll
-                                        for (int z = 0; z < 8; ++z) s8[z] = (u & 8) ? s16[z + 8] : s16[z];
-#pragma unroll
-                                        for (int z = 0; z < 4; ++z) s4[z] = (u & 4) ? s8[z + 4] : s8[z];
-#pragma unroll
-                                        for (int z = 0; z < 2; ++z) s2[z] = (u & 2) ? s4[z + 2] : s4[z];
-                                        a.fkey[rbase + slot] = (u & 1) ? s2[1] : s2[0];
-                                        a.fcol[rbase + slot] = (int)(cbase + lb + u);
-                                    }
-                                    ++slot;
-                                }
-                            }
-                        } else if (__any_sync(0xffffffffu, msk != 0)) {
+                        uint32_t msk = half_mask(v);
+                        if (__any_sync(0xffffffffu, msk != 0)) {
                             const int cnt = __popc(msk);
                             int incl = cnt;
 #pragma unroll
@@ -664,6 +739,8 @@ int launch_tc_gemm(const void* A, const void* B, const TcGemmArgs& a, cudaStream
                        ((a.out && a.g_dbase && a.tau == nullptr) || (a.out == nullptr && a.tau && a.g_row_query))),
                   "tensor-core scan: incomplete grouping");
     ANN_CHECK_ARG(a.b_tile_stride >= 1, "tensor-core scan: bad sample stride");
+    ANN_CHECK_ARG(a.out_cmin == nullptr || (a.out && a.g_item_off == nullptr && a.b_tile_stride == 1),
+                  "tensor-core scan: chunk minima need the dense key-matrix mode");
     if (a.M == 0 || a.N == 0) return ANN_OK;
     const int64_t b_rows = a.b_rows > 0 ? a.b_rows : a.N;
     // the last sampled tile must start inside B

@@ -68,6 +68,9 @@ struct TcGemmArgs {
     // the producer issues no copies, so the waits run out with nothing in flight.
     uint64_t wait_ns = 0;
     int test_no_loads = 0;
+    // Key-matrix mode (dense, out given): if out_cmin is given, it also receives the minimum key of each row's
+    // 32-column chunks, out_cmin[m * ceil(N / 32) + n / 32], so that a reader can skip chunks.
+    float* out_cmin = nullptr;
     // If given and *skip_if_zero == 0 (read on the device), the launch does nothing: a pass whose need is
     // known only on the device, without a host round trip.
     const int* skip_if_zero = nullptr;

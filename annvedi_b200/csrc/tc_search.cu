@@ -611,11 +611,136 @@ __global__ void tc_compact_rows_kernel(const int* __restrict__ list, const int* 
 
 constexpr int kCoarseChunks = 16;  // dims up to 512 take the register path of the exact distances
 
-// one warp per query
+// The coarse ranking of one query (one warp) from its keys kr [C] and their 32-key chunk minima cq [nch],
+// nch = ceil(C / 32) <= 64, for npc <= 32 and dpad <= 32 kCoarseChunks (cmax > 0).
+//  1. bar = the npc-th smallest chunk minimum (total order by (minimum, chunk); +inf when npc > nch): each
+//     of those npc chunks holds a key <= bar, so the npc-th smallest key T is <= bar.
+//  2. The window lim = bar + 2 eps + delta (the keys' certified error, as below): a centroid whose key
+//     exceeds lim exceeds T + 2 eps + delta, so its exact distance exceeds those of the npc centroids of
+//     smallest key, and it is not among the best npc.
+//  3. Every key <= lim (found in the chunks whose minimum is <= lim) gets its exact FP32 distance, and the
+//     best npc by (distance, id) are kept, lane j holding the j-th: no candidate buffer and no sort.
+__device__ __forceinline__ void coarse_by_chunks(const float* __restrict__ kr, const float* __restrict__ cq, int C,
+                                                 int npc, const float* __restrict__ qv,
+                                                 const float* __restrict__ cent, int dpad, int dim, float cmax,
+                                                 int32_t* __restrict__ pout) {
+    const int lane = threadIdx.x & 31;
+    const int nch = (C + 31) >> 5;
+    const float a0 = lane < nch ? cq[lane] : kInf, a1 = lane + 32 < nch ? cq[lane + 32] : kInf;
+    float qr[kCoarseChunks];
+    float s2 = 0.f;
+#pragma unroll
+    for (int i = 0; i < kCoarseChunks; ++i) {
+        qr[i] = lane + 32 * i < dpad ? qv[lane + 32 * i] : 0.f;
+        s2 = fmaf(qr[i], qr[i], s2);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    float bar = kInf;
+    if (npc <= nch) {  // lane l holds chunks l and l + 32; ranks among the 64 (padding +inf, sorted last)
+        int r0 = 0, r1 = 0;
+#pragma unroll 8
+        for (int j = 0; j < 32; ++j) {
+            const float o0 = __shfl_sync(0xffffffffu, a0, j), o1 = __shfl_sync(0xffffffffu, a1, j);
+            r0 += (o0 < a0 || (o0 == a0 && j < lane)) + (o1 < a0);
+            r1 += (o0 <= a1) + (o1 < a1 || (o1 == a1 && j < lane));
+        }
+        const unsigned s0 = __ballot_sync(0xffffffffu, r0 == npc - 1);
+        const unsigned s1 = __ballot_sync(0xffffffffu, r1 == npc - 1);
+        const float b0 = __shfl_sync(0xffffffffu, a0, s0 ? __ffs(s0) - 1 : 0);
+        const float b1 = __shfl_sync(0xffffffffu, a1, s1 ? __ffs(s1) - 1 : 0);
+        bar = s0 ? b0 : (s1 ? b1 : kInf);  // no rank npc - 1 only with NaN minima: every chunk
+    }
+    const float qn = sqrtf(s2) * 1.0001f;
+    const float acc = (float)(dim + 3) * 4.76837158e-7f;  // (dim + 3) 2^-21
+    const float eps = qn * cmax * (7.8125e-3f * 1.05f + 2.1f * acc) + cmax * cmax * acc;
+    const float delta = acc * (qn + cmax) * (qn + cmax);
+    const float lim = bar + 2.f * eps + delta;
+    float bd = kInf;  // lane j < npc: the j-th best (distance, id) so far
+    int bi = kNoId;
+    auto insert = [&](float d, int id) {  // warp-uniform (d, id)
+        const int pos = __popc(__ballot_sync(0xffffffffu, lane < npc && pair_less(bd, bi, d, id)));
+        const float ud = __shfl_up_sync(0xffffffffu, bd, 1);
+        const int ui = __shfl_up_sync(0xffffffffu, bi, 1);
+        if (pos < npc) {
+            if (lane == pos) {
+                bd = d;
+                bi = id;
+            } else if (lane > pos) {
+                bd = ud;
+                bi = ui;
+            }
+        }
+    };
+    unsigned c0m = __ballot_sync(0xffffffffu, lane < nch && !(a0 > lim));
+    unsigned c1m = __ballot_sync(0xffffffffu, lane + 32 < nch && !(a1 > lim));
+    while (c0m | c1m) {  // four chunks' loads in flight
+        int ch[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (c0m) {
+                ch[u] = __ffs(c0m) - 1;
+                c0m &= c0m - 1;
+            } else if (c1m) {
+                ch[u] = 32 + __ffs(c1m) - 1;
+                c1m &= c1m - 1;
+            } else {
+                ch[u] = -1;
+            }
+        }
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int c = ch[u] * 32 + lane;
+            v[u] = ch[u] >= 0 && c < C ? kr[c] : kInf;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            unsigned hit = __ballot_sync(0xffffffffu, ch[u] >= 0 && ch[u] * 32 + lane < C && v[u] <= lim);
+            while (hit) {  // two centroids at a time, all their pieces loaded before use; per lane the sum
+                           // runs over d = lane, lane + 32, ... as in the kernel below
+                const int ca = ch[u] * 32 + __ffs(hit) - 1;
+                hit &= hit - 1;
+                const bool two = hit != 0;
+                const int cb = two ? ch[u] * 32 + __ffs(hit) - 1 : ca;
+                hit &= hit - 1;
+                const float* xa = cent + (int64_t)ca * dpad;
+                const float* xb = cent + (int64_t)cb * dpad;
+                float va[kCoarseChunks], vb[kCoarseChunks];
+#pragma unroll
+                for (int i = 0; i < kCoarseChunks; ++i) {
+                    const int d = lane + 32 * i;
+                    va[i] = d < dpad ? xa[d] : 0.f;
+                    vb[i] = d < dpad ? xb[d] : 0.f;
+                }
+                float accA = 0.f, accB = 0.f;
+#pragma unroll
+                for (int i = 0; i < kCoarseChunks; ++i) {
+                    if (lane + 32 * i < dpad) {
+                        const float ta = va[i] - qr[i], tb = vb[i] - qr[i];
+                        accA = fmaf(ta, ta, accA);
+                        accB = fmaf(tb, tb, accB);
+                    }
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    accA += __shfl_xor_sync(0xffffffffu, accA, o);
+                    accB += __shfl_xor_sync(0xffffffffu, accB, o);
+                }
+                insert(accA, ca);
+                if (two) insert(accB, cb);
+            }
+        }
+    }
+    if (lane < npc) pout[lane] = bi != kNoId ? bi : 0;
+}
+
+// one warp per query; CMIN: the keys' 32-column chunk minima are given, and coarse_by_chunks ranks the query
+template <bool CMIN>
 __global__ void __launch_bounds__(128) tc_coarse_kernel(const float* __restrict__ keys, int64_t ldk, int nq, int C,
                                                        int npc, int m, const float* __restrict__ q,
                                                        const float* __restrict__ cent, int dpad, int32_t* probes,
-                                                       float cmax, int dim) {
+                                                       float cmax, int dim, const float* __restrict__ cmin) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cap = topk_cap(m);
@@ -623,6 +748,11 @@ __global__ void __launch_bounds__(128) tc_coarse_kernel(const float* __restrict_
     int* sI = reinterpret_cast<int*>(sK + cap);
     const int qi = blockIdx.x * 4 + warp;
     if (qi >= nq) return;
+    if (CMIN) {
+        coarse_by_chunks(keys + (int64_t)qi * ldk, cmin + (int64_t)qi * ((C + 31) >> 5), C, npc, q + (int64_t)qi * dpad,
+                         cent, dpad, dim, cmax, probes + (int64_t)qi * npc);
+        return;
+    }
     WarpTopK top;
     top.init(sK, sI, m);
     const float* kr = keys + (int64_t)qi * ldk;
@@ -756,14 +886,17 @@ __global__ void __launch_bounds__(128) tc_coarse_kernel(const float* __restrict_
 }  // namespace
 
 int launch_tc_coarse(const float* keys, int64_t ldk, int nq, int C, int npc, int margin, const float* q,
-                     const float* centroids, int dpad, int32_t* probes, cudaStream_t st, float cmax, int dim) {
+                     const float* centroids, int dpad, int32_t* probes, cudaStream_t st, float cmax, int dim,
+                     const float* cmin) {
     if (nq == 0) return ANN_OK;
     const int m = std::min(C, npc + margin);
     ANN_CHECK_ARG(npc >= 1 && npc <= m && m <= 1024, "tensor-core coarse ranking: npc=%d, m=%d", npc, m);
     const size_t smem = (size_t)4 * 2 * topk_cap(m) * 4;
-    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(tc_coarse_kernel)));
-    tc_coarse_kernel<<<(unsigned)ceil_div(nq, 4), 128, smem, st>>>(keys, ldk, nq, C, npc, m, q, centroids, dpad, probes,
-                                                                    cmax, dim > 0 ? dim : dpad);
+    const bool chunks = cmin != nullptr && C <= 64 * 32 && npc <= 32 && cmax > 0.f && dpad <= 32 * kCoarseChunks;
+    auto kern = chunks ? tc_coarse_kernel<true> : tc_coarse_kernel<false>;
+    ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(kern)));
+    kern<<<(unsigned)ceil_div(nq, 4), 128, smem, st>>>(keys, ldk, nq, C, npc, m, q, centroids, dpad, probes, cmax,
+                                                       dim > 0 ? dim : dpad, cmin);
     ANN_LAUNCH_CHECK();
     return ANN_OK;
 }

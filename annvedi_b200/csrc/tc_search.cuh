@@ -111,9 +111,11 @@ int launch_tc_compact_rows(const int* list, const int* count, int max_count, con
 // centroids, row stride dpad), and the best npc of those by (distance, id) into probes [nq, npc],
 // best first. With cmax > 0 (the largest centroid norm; dim the vectors' dimension) only the candidates whose
 // key lies within the keys' certified error window of the npc-th key get exact distances: the others cannot
-// be among the best npc, so the result is the same.
+// be among the best npc, so the result is the same. cmin (optional): the keys' 32-column chunk minima
+// [nq, ceil(C / 32)] (TcGemmArgs::out_cmin); with C <= 2,048 and m <= 32, only the chunks at or below a bar
+// taken from them are read, with the same result.
 int launch_tc_coarse(const float* keys, int64_t ldk, int nq, int C, int npc, int margin, const float* q,
                      const float* centroids, int dpad, int32_t* probes, cudaStream_t st, float cmax = 0.f,
-                     int dim = 0);
+                     int dim = 0, const float* cmin = nullptr);
 
 }  // namespace annb

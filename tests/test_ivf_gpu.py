@@ -238,6 +238,32 @@ def test_tc_mode_ranks_the_same_streams(cuda, nq, mode):
     assert ix.total_distances_count() == ex.total_distances_count()
 
 
+@pytest.mark.parametrize("c", [40, 96, 700, 2048, 2050])
+def test_tc_coarse_probes_the_exact_lists(cuda, c):
+    """The tensor-core coarse ranking (BF16 keys to every centroid, then exact FP32 distances inside the
+    keys' certified error window) probes the lists the exact FP32 ranking probes: from the keys' 32-list
+    chunk minima (up to 2,048 lists; with 40 or 96 lists there are fewer chunks than probes and every
+    chunk is read) and without them (2,050 lists): the same candidates are counted per query and over a
+    300-query batch."""
+    w = synth.zipf_mixture(20000, 64, 300, c=c, lo=5, hi=2000, seed=c)
+    st = ivf_state.build_state(w.base, w.centres, w.assign, 1, 0)
+    k, R = 20, 60
+    for npc in (2, 5):
+        counts = {}
+        for mode in ("exact", "tc"):
+            ix = _ivf(mode=mode)
+            ix.import_state(st)
+            per = []
+            for i in range(24):
+                ix.reset_distances_count()
+                ix.search(w.queries[i:i + 1], k, 0, npc, R)
+                per.append(ix.total_distances_count())
+            ix.reset_distances_count()
+            ix.search(w.queries, k, 0, npc, R)
+            counts[mode] = (per, ix.total_distances_count())
+        assert counts["tc"] == counts["exact"], npc
+
+
 @pytest.mark.parametrize("nq,npc,R,mode", [(1200, 12, 300, "tc"), (600, 40, 100, "tc"), (256, 3, 500, "tc"),
                                            (1200, 12, 300, "tc_sq8"), (300, 20, 200, "tc_sq8")])
 def test_tc_sampled_bars_select_what_the_key_stream_selects(cuda, nq, npc, R, mode):
