@@ -65,16 +65,20 @@ __global__ void gf_encode_kernel(const float* __restrict__ x, int64_t n, int dim
 
 // The code byte `sel` of w as a float, exactly: its bits placed in the mantissa of 2^23 (byte permute),
 // then 2^23 subtracted -- two full-rate instructions where an integer-to-float conversion runs at a quarter.
-__device__ __forceinline__ float gf_byte_f(uint32_t w, uint32_t sel) {
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | sel)) - 8388608.0f;
+// byte sel of w as a float: its bits under the exponent of 2^23, then 2^23 taken off (exact)
+__device__ __forceinline__ float gf_byte_bits(uint32_t w, uint32_t sel) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | sel));
 }
-__device__ __forceinline__ void gf_acc8(uint2 c, float s, float nq, float (&a)[8]) {
+// rows i (byte i of c.x) and 4 + i (byte i of c.y) as the pair a[i], with packed FP32 instructions: each
+// half rounds as its scalar form (x - 2^23, fma(x, s, nq), fma(v, v, a)), so the keys are those of the
+// scalar chain, at 2.5 instructions a code byte instead of 4
+__device__ __forceinline__ void gf_acc8(uint2 c, float s, float nq, float2 (&a)[4]) {
+    const float2 s2 = make_float2(s, s), n2 = make_float2(nq, nq), m2 = make_float2(-8388608.0f, -8388608.0f);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const float v0 = fmaf(gf_byte_f(c.x, i), s, nq);
-        const float v1 = fmaf(gf_byte_f(c.y, i), s, nq);
-        a[i] = fmaf(v0, v0, a[i]);
-        a[4 + i] = fmaf(v1, v1, a[4 + i]);
+        const float2 x = __fadd2_rn(make_float2(gf_byte_bits(c.x, i), gf_byte_bits(c.y, i)), m2);
+        const float2 v = __ffma2_rn(x, s2, n2);
+        a[i] = __ffma2_rn(v, v, a[i]);
     }
 }
 
@@ -94,7 +98,7 @@ __global__ void __launch_bounds__(128, 8) gf_scan_kernel(const uint8_t* __restri
     const int64_t octs = npad >> 3;
     if (t >= octs) return;
     const uint2* col = reinterpret_cast<const uint2*>(codes) + t;
-    float a[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float2 a[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
     int d0 = 0;
     for (; d0 + kGfScanBatch <= dim; d0 += kGfScanBatch) {
         uint2 c[kGfScanBatch];
@@ -105,8 +109,8 @@ __global__ void __launch_bounds__(128, 8) gf_scan_kernel(const uint8_t* __restri
     }
     for (; d0 < dim; ++d0) gf_acc8(col[(int64_t)d0 * octs], gf_sn[d0].x, gf_sn[d0].y, a);
     float4* o = reinterpret_cast<float4*>(dist) + 2 * t;
-    o[0] = make_float4(a[0], a[1], a[2], a[3]);
-    o[1] = make_float4(a[4], a[5], a[6], a[7]);
+    o[0] = make_float4(a[0].x, a[1].x, a[2].x, a[3].x);
+    o[1] = make_float4(a[0].y, a[1].y, a[2].y, a[3].y);
 }
 
 // One warp per candidate (two per CTA): the warp brings the candidate's row into shared memory with
