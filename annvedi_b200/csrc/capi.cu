@@ -347,6 +347,7 @@ int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t
         nsplit = flat_choose_nsplit(h->n, nq, bq, &rps, flat_scan_ctas_per_sm(bq, kk, dpad, h->metric));
         sz.take<float>((size_t)nq * nsplit * kk);
         sz.take<int>((size_t)nq * nsplit * kk);
+        sz.take<float>((size_t)(nq + 1) / 2 * 2 * dpad);  // the paired query tile
         // many splits per query: select the k best with the radix selection, then sort them
         radix_merge = nsplit >= 16;
         if (radix_merge) {
@@ -393,7 +394,9 @@ int ann_flat_query(ann_flat* h, ann_workspace* ws, const float* queries, int32_t
     if (mode == ANN_MODE_EXACT) {
         float* skey = cv.take<float>((size_t)nq * nsplit * kk);
         int* sid = cv.take<int>((size_t)nq * nsplit * kk);
+        float* qpair = cv.take<float>((size_t)(nq + 1) / 2 * 2 * dpad);
         FlatScanArgs a{h->base, h->n, dpad, qdev, nq, h->metric, kk, rps, nsplit, skey, sid};
+        a.qpair = qpair;
         rc = launch_flat_scan(a, bq, st);
         if (rc) return rc;
         h->prof.mark(prec, st);

@@ -61,9 +61,16 @@ struct ScanCfg {
     static_assert(BQ % TQ == 0 && THREADS % WQ == 0, "bad tile");
 };
 
-template <int BQ, int TQ, int TR, int STAGES, int METRIC>
+// PQ: the query tile comes from FlatScanArgs::qpair (query pairs interleaved element by element, negated for
+// L2), staged per chunk as BQ / 2 rows of 2 KC floats; thread query pairs (2 jj, 2 jj + 1) share each x element
+// through packed FP32 instructions (x - q as x + (-q), then fma, per half exactly the scalar steps)
+template <int BQ, int TQ, int TR, int STAGES, int METRIC, bool PQ>
 __global__ void __launch_bounds__(256) flat_scan_kernel(FlatScanArgs a) {
     using C = ScanCfg<BQ, TQ, TR, STAGES, METRIC>;
+    static_assert(!PQ || TQ % 2 == 0, "query pairs");
+    constexpr int PITCHQ = 2 * C::KC + 4;  // paired query tile: floats per pair row
+    constexpr int TQ2 = TQ / 2 > 0 ? TQ / 2 : 1;
+    static_assert(!PQ || (BQ / 2) * PITCHQ <= (int)C::SQ, "paired query tile fits the query stage");
     const int cap = a.cap;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* sX = reinterpret_cast<float*>(smem_raw);
@@ -112,11 +119,21 @@ __global__ void __launch_bounds__(256) flat_scan_kernel(FlatScanArgs a) {
                 cp_async16(dx + r * C::PITCH + piece * 4, src, ok);
             }
             float* dq = sQ + buf * C::SQ;
-            for (int c = tid; c < BQ * 8; c += C::THREADS) {
-                const int qq = c >> 3, piece = c & 7;
-                const bool ok = (q0 + qq) < a.nq;
-                const float* src = a.q + (int64_t)(ok ? q0 + qq : 0) * a.dpad + kc * C::KC + piece * 4;
-                cp_async16(dq + qq * C::PITCH + piece * 4, src, ok);
+            if constexpr (PQ) {
+                for (int c = tid; c < (BQ / 2) * 16; c += C::THREADS) {  // pair rows x 16 16-byte pieces
+                    const int pp = c >> 4, piece = c & 15;
+                    const int64_t pr = q0 / 2 + pp;
+                    const bool ok = 2 * pr < a.nq;
+                    const float* src = a.qpair + ((ok ? pr : 0) * a.dpad + kc * C::KC) * 2 + piece * 4;
+                    cp_async16(dq + pp * PITCHQ + piece * 4, src, ok);
+                }
+            } else {
+                for (int c = tid; c < BQ * 8; c += C::THREADS) {
+                    const int qq = c >> 3, piece = c & 7;
+                    const bool ok = (q0 + qq) < a.nq;
+                    const float* src = a.q + (int64_t)(ok ? q0 + qq : 0) * a.dpad + kc * C::KC + piece * 4;
+                    cp_async16(dq + qq * C::PITCH + piece * 4, src, ok);
+                }
             }
         }
         cp_async_commit();
@@ -130,6 +147,11 @@ __global__ void __launch_bounds__(256) flat_scan_kernel(FlatScanArgs a) {
     for (int j = 0; j < TQ; ++j)
 #pragma unroll
         for (int i = 0; i < TR; ++i) acc[j][i] = 0.f;
+    float2 acc2[TQ2][TR];  // PQ: queries (2 jj, 2 jj + 1) of row i
+#pragma unroll
+    for (int jj = 0; jj < TQ2; ++jj)
+#pragma unroll
+        for (int i = 0; i < TR; ++i) acc2[jj][i] = make_float2(0.f, 0.f);
 
     for (int64_t step = 0; step < nsteps; ++step) {
         cp_async_wait<STAGES - 2>();
@@ -139,7 +161,41 @@ __global__ void __launch_bounds__(256) flat_scan_kernel(FlatScanArgs a) {
         const float* xs = sX + buf * C::SX;
         const float* qs = sQ + buf * C::SQ;
 #pragma unroll
-        for (int kk = 0; kk < C::KC; kk += 4) {
+        for (int kk = 0; kk < C::KC && PQ; kk += 4) {
+            float4 xv[TR], qa[TQ2], qb[TQ2];
+#pragma unroll
+            for (int i = 0; i < TR; ++i) xv[i] = *reinterpret_cast<const float4*>(xs + (tr + i * C::WR) * C::PITCH + kk);
+#pragma unroll
+            for (int jj = 0; jj < TQ2; ++jj) {  // (A kk, B kk, A kk+1, B kk+1), (A kk+2, B kk+2, A kk+3, B kk+3)
+                const float* qp = qs + (tq * (TQ / 2) + jj) * PITCHQ + 2 * kk;
+                qa[jj] = *reinterpret_cast<const float4*>(qp);
+                qb[jj] = *reinterpret_cast<const float4*>(qp + 4);
+            }
+#pragma unroll
+            for (int jj = 0; jj < TQ2; ++jj)
+#pragma unroll
+                for (int i = 0; i < TR; ++i) {
+                    const float2 q0v = make_float2(qa[jj].x, qa[jj].y), q1v = make_float2(qa[jj].z, qa[jj].w);
+                    const float2 q2v = make_float2(qb[jj].x, qb[jj].y), q3v = make_float2(qb[jj].z, qb[jj].w);
+                    if (METRIC == ANN_METRIC_L2) {  // the pairs hold -q: x + (-q) is x - q
+                        const float2 d0 = __fadd2_rn(make_float2(xv[i].x, xv[i].x), q0v);
+                        const float2 d1 = __fadd2_rn(make_float2(xv[i].y, xv[i].y), q1v);
+                        const float2 d2 = __fadd2_rn(make_float2(xv[i].z, xv[i].z), q2v);
+                        const float2 d3 = __fadd2_rn(make_float2(xv[i].w, xv[i].w), q3v);
+                        acc2[jj][i] = __ffma2_rn(d0, d0, acc2[jj][i]);
+                        acc2[jj][i] = __ffma2_rn(d1, d1, acc2[jj][i]);
+                        acc2[jj][i] = __ffma2_rn(d2, d2, acc2[jj][i]);
+                        acc2[jj][i] = __ffma2_rn(d3, d3, acc2[jj][i]);
+                    } else {
+                        acc2[jj][i] = __ffma2_rn(make_float2(xv[i].x, xv[i].x), q0v, acc2[jj][i]);
+                        acc2[jj][i] = __ffma2_rn(make_float2(xv[i].y, xv[i].y), q1v, acc2[jj][i]);
+                        acc2[jj][i] = __ffma2_rn(make_float2(xv[i].z, xv[i].z), q2v, acc2[jj][i]);
+                        acc2[jj][i] = __ffma2_rn(make_float2(xv[i].w, xv[i].w), q3v, acc2[jj][i]);
+                    }
+                }
+        }
+#pragma unroll
+        for (int kk = 0; kk < C::KC && !PQ; kk += 4) {
             float4 xv[TR], qv[TQ];
 #pragma unroll
             for (int i = 0; i < TR; ++i) xv[i] = *reinterpret_cast<const float4*>(xs + (tr + i * C::WR) * C::PITCH + kk);
@@ -185,7 +241,8 @@ __global__ void __launch_bounds__(256) flat_scan_kernel(FlatScanArgs a) {
                         const uint32_t bit = 1u << (j * TR + i);
                         if (pend & bit) {
                             const int row = (int)(r0 + tr + i * C::WR);
-                            const float key = METRIC == ANN_METRIC_L2 ? acc[j][i] : -acc[j][i];
+                            const float av = PQ ? ((j & 1) ? acc2[j >> 1][i].y : acc2[j >> 1][i].x) : acc[j][i];
+                            const float key = METRIC == ANN_METRIC_L2 ? av : -av;
                             if (pair_less(key, row, sTau[ql], sTauId[ql])) {
                                 const int slot = atomicAdd(&sCnt[ql], 1);
                                 if (slot < cap) {
@@ -211,6 +268,10 @@ __global__ void __launch_bounds__(256) flat_scan_kernel(FlatScanArgs a) {
             for (int j = 0; j < TQ; ++j)
 #pragma unroll
                 for (int i = 0; i < TR; ++i) acc[j][i] = 0.f;
+#pragma unroll
+            for (int jj = 0; jj < TQ2; ++jj)
+#pragma unroll
+                for (int i = 0; i < TR; ++i) acc2[jj][i] = make_float2(0.f, 0.f);
         }
     }
     cp_async_wait<0>();
@@ -511,10 +572,10 @@ static int dispatch_stream(const FlatScanArgs& a, int bq, int n_qtiles, cudaStre
 // ---------------------------------------------------------------------------------------------
 // Host-side launch selection.
 // ---------------------------------------------------------------------------------------------
-template <int BQ, int TQ, int TR, int STAGES, int METRIC>
+template <int BQ, int TQ, int TR, int STAGES, int METRIC, bool PQ = false>
 static int launch_scan_t(FlatScanArgs a, int n_qtiles, cudaStream_t st) {
     using C = ScanCfg<BQ, TQ, TR, STAGES, METRIC>;
-    auto kern = flat_scan_kernel<BQ, TQ, TR, STAGES, METRIC>;
+    auto kern = flat_scan_kernel<BQ, TQ, TR, STAGES, METRIC, PQ>;
     const size_t smem = C::smem(a.cap);
     ANN_CHECK_ARG(smem <= 227 * 1024, "flat scan: %zu bytes of shared memory for k=%d", smem, a.k);
     ANN_CUDA_TRY(smem_optin(reinterpret_cast<const void*>(kern)));
@@ -544,7 +605,26 @@ static int dispatch_bq(const FlatScanArgs& a, int bq, int n_qtiles, cudaStream_t
     case 4: return launch_scan_t<4, 4, 1, kSmallTileStages, METRIC>(a, n_qtiles, st);
     case 8: return launch_scan_t<8, 8, 1, kSmallTileStages, METRIC>(a, n_qtiles, st);
     case 16: return launch_scan_t<16, 8, 2, 3, METRIC>(a, n_qtiles, st);
-    default: return launch_scan_t<32, 8, 4, 3, METRIC>(a, n_qtiles, st);
+    default:
+        // the paired query tile where ptxas keeps it spill-free: 32-query tiles of squared L2
+        if constexpr (METRIC == ANN_METRIC_L2) {
+            if (a.qpair) return launch_scan_t<32, 8, 4, 3, METRIC, true>(a, n_qtiles, st);
+        }
+        return launch_scan_t<32, 8, 4, 3, METRIC>(a, n_qtiles, st);
+    }
+}
+
+// qpair[(p dpad + d) 2 + h] = s q[2 p + h][d] (s = -1 for L2, +1 for inner products; 0 past nq)
+__global__ void flat_pair_queries_kernel(const float* __restrict__ q, int nq, int dpad, float s,
+                                         float* __restrict__ qpair) {
+    const int64_t total = (int64_t)((nq + 1) / 2) * dpad * 2;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int h = (int)(e & 1);
+        const int64_t pd = e >> 1;
+        const int64_t p = pd / dpad;
+        const int d = (int)(pd % dpad);
+        const int64_t qi = 2 * p + h;
+        qpair[e] = qi < nq ? s * q[qi * dpad + d] : 0.f;
     }
 }
 
@@ -558,6 +638,14 @@ int launch_flat_scan(const FlatScanArgs& a0, int bq, cudaStream_t st) {
     if (flat_stream_eligible(bq, a.k, a.dpad)) {
         if (a.metric == ANN_METRIC_L2) return dispatch_stream<ANN_METRIC_L2>(a, bq, n_qtiles, st);
         return dispatch_stream<ANN_METRIC_IP>(a, bq, n_qtiles, st);
+    }
+    if (a.qpair && bq >= 32 && a.metric == ANN_METRIC_L2 && a.nq > 0) {  // the paired query tile
+        const int64_t total = (int64_t)((a.nq + 1) / 2) * a.dpad * 2;
+        flat_pair_queries_kernel<<<(unsigned)std::min<int64_t>(ceil_div(total, 256), 8 * kNumSMs), 256, 0, st>>>(
+            a.q, a.nq, a.dpad, a.metric == ANN_METRIC_L2 ? -1.f : 1.f, a.qpair);
+        ANN_LAUNCH_CHECK();
+    } else {
+        a.qpair = nullptr;
     }
     if (a.metric == ANN_METRIC_L2) return dispatch_bq<ANN_METRIC_L2>(a, bq, n_qtiles, st);
     return dispatch_bq<ANN_METRIC_IP>(a, bq, n_qtiles, st);

@@ -18,6 +18,10 @@ struct FlatScanArgs {
     float* out_key;          // [nq, nsplit, k] scratch
     int* out_id;             // [nq, nsplit, k] scratch
     int cap;                 // per-query buffer capacity (set by launch_flat_scan)
+    // optional scratch of 2 ceil(nq / 2) dpad floats: with 32-query tiles of squared L2, launch_flat_scan writes
+    // the queries there as interleaved negated pairs and the scan takes two queries a packed FP32
+    // instruction, each half rounding as the scalar form (the same distances)
+    float* qpair = nullptr;
 };
 
 struct MergeArgs {

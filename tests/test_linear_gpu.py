@@ -166,13 +166,13 @@ def test_full_size_c1_exact_and_reference(cuda):
 @pytest.mark.parametrize("k", [10, 100])
 def test_query_tile_does_not_change_results(cuda, k):
     """The exact scan's query tile (ANN_FLAT_OPT_QUERY_TILE) changes speed only: tiles of 8, 16 and 32 queries
-    return the same ids and distances as the automatic choice for this batch, bit for bit; other tiles are
-    refused."""
+    (the last with its queries in packed pairs) return the same ids and distances as the automatic choice for
+    this batch, bit for bit; other tiles are refused."""
     import torch
     from annvedi_b200.linear import LinearIndex
     rng = np.random.default_rng(40)
     base = rng.standard_normal((60000, 96)).astype(np.float32)
-    q = torch.from_numpy(rng.standard_normal((300, 96)).astype(np.float32)).cuda()
+    q = torch.from_numpy(rng.standard_normal((301, 96)).astype(np.float32)).cuda()  # odd: a half-empty pair
     ix = LinearIndex(device=0, mode="exact")
     ix.fit(torch.from_numpy(base).cuda())
     want_i, want_d = ix.search(q, k, mode="exact")
