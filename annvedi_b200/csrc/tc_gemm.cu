@@ -546,6 +546,7 @@ __global__ void __launch_bounds__(epi_threads(EPI), 1) tc_gemm_kernel(const __gr
                     const int64_t rbase = (int64_t)rq * a.row_cap;
                     put_row(v, mb, slot + na, rbase, cbase + col0 + c + 32);
                     if (__any_sync(0xffffffffu, ma != 0u)) {  // uniform: the warp reloads the first half
+                        __syncwarp();  // converged for the .sync.aligned load after the divergent stores
                         tmem_ld32(tbase + (uint32_t)c, r);
                         tmem_wait(r);
                         half_keys(r, 0, c, v);
