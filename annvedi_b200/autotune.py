@@ -37,21 +37,31 @@ def _time(fn, reps, stream):
     return e0.elapsed_time(e1) / reps
 
 
+def _timer(timer):
+    """timer(fn, reps) -> ms per call: the given one, else CUDA events on the current stream."""
+    if timer is not None:
+        return timer
+    import torch
+    stream = torch.cuda.current_stream()
+    return lambda fn, reps: _time(fn, reps, stream)
+
+
 IVF_NPROBES = (2, 3, 4, 5, 6, 8, 10, 12, 16, 24, 32, 64, 128)
 IVF_REFINES = (100, 150, 200, 300)
 
 
 def tune_ivf(index, base, queries, kth, k: int = 100, target: float = 0.95, modes=("tc", "exact"),
-             nprobes=IVF_NPROBES, refines=IVF_REFINES, reps: int = 3, sample_divs=(4, 8, 16)) -> dict:
+             nprobes=IVF_NPROBES, refines=IVF_REFINES, reps: int = 3, sample_divs=(4, 8, 16), timer=None) -> dict:
     """Fastest (mode, nprobe, refine_r) of an IVFIndex whose recall@k on `queries` is >= target.
 
     For every mode and re-rank depth the probe counts run in increasing order up to the first that meets
     the target. At each tensor-core mode's best point the sampled bars' list share (sample_divs) is then
     swept and the fastest kept on the index. Returns {"best": {...} or None, "best_by_mode": {mode: {...}},
     "table": [...]}; each entry has mode, nprobe, refine_r, recall, ms_per_batch and qps (queries per second at
-    this batch size), and sample_div where swept. The index keeps the last mode's best sample_div."""
+    this batch size), and sample_div where swept. The index keeps the last mode's best sample_div. timer(fn,
+    reps) -> ms per call replaces the CUDA-event timing (the host-logic tests)."""
     import torch
-    stream = torch.cuda.current_stream()
+    time_fn = _timer(timer)
     nq = queries.shape[0]
     ids = torch.empty(nq, k, dtype=torch.int64, device=queries.device)
     dists = torch.empty(nq, k, dtype=torch.float32, device=queries.device)
@@ -61,7 +71,7 @@ def tune_ivf(index, base, queries, kth, k: int = 100, target: float = 0.95, mode
             for npc in nprobes:
                 fn = lambda: index.search(queries, k, 0, npc, rr, max_candidates=0, mode=mode, out_ids=ids,
                                           out_dists=dists)
-                ms = _time(fn, reps, stream)
+                ms = time_fn(fn, reps)
                 rec = recall_at_k(base, queries, ids, kth)
                 row = {"mode": mode, "nprobe": npc, "refine_r": rr, "recall": round(rec, 4),
                        "ms_per_batch": round(ms, 4), "qps": round(nq / (ms / 1e3), 1)}
@@ -87,7 +97,7 @@ def tune_ivf(index, base, queries, kth, k: int = 100, target: float = 0.95, mode
             index.set_option("sample_div", div)
             fn = lambda: index.search(queries, k, 0, row["nprobe"], row["refine_r"], max_candidates=0, mode=mode,
                                       out_ids=ids, out_dists=dists)
-            ms = _time(fn, reps, stream)
+            ms = time_fn(fn, reps)
             alt = {**row, "sample_div": div, "ms_per_batch": round(ms, 4), "qps": round(nq / (ms / 1e3), 1)}
             table.append(alt)
             if alt["qps"] > by_mode[mode]["qps"]:
@@ -98,17 +108,17 @@ def tune_ivf(index, base, queries, kth, k: int = 100, target: float = 0.95, mode
 
 
 def tune_flat_tc(index, base, queries, kth, k: int = 100, target: float = 0.95, refines=(100, 200, 400),
-                 reps: int = 3) -> dict:
+                 reps: int = 3, timer=None) -> dict:
     """Fastest re-rank depth of a LinearIndex's tensor-core search whose recall@k is >= target."""
     import torch
-    stream = torch.cuda.current_stream()
+    time_fn = _timer(timer)
     nq = queries.shape[0]
     ids = torch.empty(nq, k, dtype=torch.int64, device=queries.device)
     dists = torch.empty(nq, k, dtype=torch.float32, device=queries.device)
     table, best = [], None
     for rr in refines:
         fn = lambda: index.search_tc(queries, k, refine_r=rr, out_ids=ids, out_dists=dists)
-        ms = _time(fn, reps, stream)
+        ms = time_fn(fn, reps)
         rec = recall_at_k(base, queries, ids, kth)
         row = {"refine_r": rr, "recall": round(rec, 4), "ms_per_batch": round(ms, 4), "qps": round(nq / (ms / 1e3), 1)}
         table.append(row)
@@ -117,19 +127,19 @@ def tune_flat_tc(index, base, queries, kth, k: int = 100, target: float = 0.95, 
     return {"best": best, "table": table, "target": target}
 
 
-def tune_flat_tile(index, queries, k: int = 100, tiles=(8, 16, 32), reps: int = 2) -> dict:
+def tune_flat_tile(index, queries, k: int = 100, tiles=(8, 16, 32), reps: int = 2, timer=None) -> dict:
     """Fastest query tile (queries per CTA) of a LinearIndex's exact scan for this batch, timed over `reps`
     calls after a warm-up call; the tile is left set on the index. Results do not depend on the tile, so no
     recall is needed. Returns {"best": {...}, "table": [...]} with tile, ms_per_batch and qps."""
     import torch
-    stream = torch.cuda.current_stream()
+    time_fn = _timer(timer)
     nq = queries.shape[0]
     ids = torch.empty(nq, k, dtype=torch.int64, device=queries.device)
     dists = torch.empty(nq, k, dtype=torch.float32, device=queries.device)
     table = []
     for tile in tiles:
         index.set_query_tile(tile)
-        ms = _time(lambda: index.search(queries, k, mode="exact", out_ids=ids, out_dists=dists), reps, stream)
+        ms = time_fn(lambda: index.search(queries, k, mode="exact", out_ids=ids, out_dists=dists), reps)
         table.append({"tile": tile, "ms_per_batch": round(ms, 3), "qps": round(nq / (ms / 1e3), 1)})
     best = min(table, key=lambda r: r["ms_per_batch"])
     index.set_query_tile(best["tile"])
